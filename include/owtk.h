@@ -1,0 +1,235 @@
+/*
+ * owtk.h — C ABI of the B200 (sm_100a) single-rank OWT-Krylov solve path.
+ *
+ * Plain pointers, sizes and opaque handles; no C++ or CUDA types in any
+ * signature.  Every call returns an owtk_status; owtk_last_error() gives the
+ * message of the last failure on the calling thread.  The status codes map
+ * one-to-one onto the exceptions of the reference's header-only API:
+ *   std::invalid_argument -> OWTK_ERR_INVALID_ARGUMENT
+ *   std::runtime_error("zero pivot in ILU(0)") -> OWTK_ERR_ZERO_PIVOT
+ *   std::out_of_range     -> OWTK_ERR_OUT_OF_RANGE
+ * Solver failures are not errors: they are reported in owtk_solver_result,
+ * exactly like the reference's SolverResult (core.hpp:118-146).
+ *
+ * Reference anchors (file:line) are into include/owt/krylov/ of OWT-Krylov.
+ * Vectors, matrices and preconditioners live in device memory (HBM) and
+ * every operation is enqueued on the context's CUDA stream; *_host entry
+ * points take host buffers and include the host<->device copies.
+ */
+#ifndef OWTK_H
+#define OWTK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum owtk_status {
+    OWTK_OK = 0,
+    OWTK_ERR_INVALID_ARGUMENT = 1,
+    OWTK_ERR_ZERO_PIVOT = 2,
+    OWTK_ERR_OUT_OF_RANGE = 3,
+    OWTK_ERR_CUDA = 4,
+    OWTK_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    OWTK_ERR_NO_DEVICE = 6,
+    OWTK_ERR_RUNTIME = 7
+} owtk_status;
+
+typedef enum owtk_dtype { OWTK_F64 = 0, OWTK_F32 = 1 } owtk_dtype;
+
+typedef struct owtk_context owtk_context;
+typedef struct owtk_vector owtk_vector;
+typedef struct owtk_matrix owtk_matrix;
+typedef struct owtk_preconditioner owtk_preconditioner;
+typedef struct owtk_workspace owtk_workspace;
+
+const char* owtk_last_error(void);
+int owtk_abi_version(void);
+
+/* ---- context: one device, one stream ------------------------------------ */
+owtk_status owtk_context_create(int device, owtk_context** out);
+owtk_status owtk_context_destroy(owtk_context* ctx);
+owtk_status owtk_context_synchronize(owtk_context* ctx);
+/* The cudaStream_t every call of this context is enqueued on. */
+void* owtk_context_stream(owtk_context* ctx);
+/* Kernels this library has launched on the context so far. */
+uint64_t owtk_context_kernel_launches(owtk_context* ctx);
+
+/* ---- BlockVector<T> (core.hpp:197-395): owned nodes then ghost nodes,
+ *      bs contiguous values per node.  *_view wraps caller device memory
+ *      without copying (core.hpp:223-230).  Invalid layouts are rejected as
+ *      in core.hpp:371-377. -------------------------------------------------- */
+owtk_status owtk_vector_create(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes,
+                               size_t ghost_nodes, size_t block_size, owtk_vector** out);
+owtk_status owtk_vector_view(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes,
+                             size_t ghost_nodes, size_t block_size, void* device_values,
+                             size_t value_count, owtk_vector** out);
+owtk_status owtk_vector_destroy(owtk_vector* v);
+void* owtk_vector_data(owtk_vector* v);
+/* Copy `count` values from/to the start of the vector (host memory). */
+owtk_status owtk_vector_upload(owtk_vector* v, const void* host, size_t count);
+owtk_status owtk_vector_download(owtk_vector* v, void* host, size_t count);
+/* fill_owned / fill (core.hpp:339-340). */
+owtk_status owtk_vector_fill(owtk_vector* v, double value, int owned_only);
+
+/* ---- owned-only BLAS-1 (core.hpp:562-601, simd.hpp:15-202) --------------- */
+owtk_status owtk_copy_owned(owtk_vector* source, owtk_vector* destination);
+owtk_status owtk_axpy(double alpha, owtk_vector* x, owtk_vector* y);
+owtk_status owtk_scale(double alpha, owtk_vector* x);
+owtk_status owtk_assign_linear_combination(owtk_vector* out, double alpha, owtk_vector* x,
+                                           double beta, owtk_vector* y);
+/* SerialReduction::dot / norm (reduction.hpp:114-150). */
+owtk_status owtk_dot(owtk_vector* lhs, owtk_vector* rhs, double* result);
+owtk_status owtk_norm(owtk_vector* v, double* result);
+/* k dots of w against basis[0..k) and w.w in one pass (krylov_solvers.hpp:273-281). */
+owtk_status owtk_dot_batch(owtk_vector* w, owtk_vector* const* basis, size_t k, double* results);
+
+/* ---- matrices ------------------------------------------------------------
+ * Index arrays are host size_t-compatible (uint64), values host arrays in
+ * the matrix dtype; they are validated (block_csr.hpp:281-300), narrowed to
+ * int32 and uploaded once. */
+/* BlockCsrMatrix<T> (block_csr.hpp:22-360): values [entry][component]. */
+owtk_status owtk_bsr_create(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes,
+                            size_t ghost_nodes, size_t block_size, const uint64_t* row_offsets,
+                            const uint64_t* column_indices, const void* values,
+                            owtk_matrix** out);
+/* New numeric values for the same pattern (host array). */
+owtk_status owtk_bsr_update_values(owtk_matrix* m, const void* values);
+/* SplitBlockCsrMatrixView<T> (split_block_csr.hpp:29-196): diagonal[node][c]
+ * and off_diagonal[edge][c].  The coefficient arrays are BORROWED device
+ * memory: writes to them are seen by the next apply without any update call
+ * (split_block_csr.hpp:25-27); only the structure is copied. */
+owtk_status owtk_split_view_create(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes,
+                                   size_t ghost_nodes, size_t block_size,
+                                   const uint64_t* off_diagonal_row_offsets,
+                                   const uint64_t* off_diagonal_columns,
+                                   const void* device_diagonal, const void* device_off_diagonal,
+                                   owtk_matrix** out);
+/* DenseBlockCsrMatrix<T> (dense_block_csr.hpp:15-330): row-major bs x bs blocks. */
+owtk_status owtk_dense_bsr_create(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes,
+                                  size_t ghost_nodes, size_t block_size,
+                                  const uint64_t* row_offsets, const uint64_t* column_indices,
+                                  const void* values, owtk_matrix** out);
+owtk_status owtk_matrix_destroy(owtk_matrix* m);
+/* kind: 0 component-diagonal BSR, 1 split view, 2 dense BSR. */
+owtk_status owtk_matrix_info(owtk_matrix* m, int* kind, size_t* owned_nodes,
+                             size_t* ghost_nodes, size_t* block_size, size_t* entries);
+/* Matrix::apply (block_csr.hpp:192-215, split_block_csr.hpp:89-119,
+ * dense_block_csr.hpp:173-205): owned rows of out are overwritten. */
+owtk_status owtk_spmv(owtk_matrix* m, owtk_vector* in, owtk_vector* out);
+/* BlockCsrMatrix::diagonal (block_csr.hpp:217-236), host output. */
+owtk_status owtk_matrix_diagonal(owtk_matrix* m, void* host_out);
+
+/* ---- preconditioners (preconditioner.hpp, split_block_csr.hpp:205-332) ---- */
+typedef enum owtk_pc_kind {
+    OWTK_PC_IDENTITY = 0,    /* IdentityPreconditioner (preconditioner.hpp:17-23) */
+    OWTK_PC_JACOBI = 1,      /* JacobiPreconditioner (:25-113); parameter = minimum diagonal (<= 0: 64 eps) */
+    OWTK_PC_SSOR = 2,        /* LocalSsorPreconditioner (:124-247); parameter = omega */
+    OWTK_PC_SPLIT_SSOR = 3,  /* SplitLocalSsorPreconditioner (split_block_csr.hpp:205-332); parameter = omega */
+    OWTK_PC_ILU = 4          /* IluLevelPreconditioner / Ilu0Preconditioner (:253-508); parameter = fill level */
+} owtk_pc_kind;
+
+owtk_status owtk_pc_create(owtk_matrix* m, owtk_pc_kind kind, double parameter,
+                           owtk_preconditioner** out);
+owtk_status owtk_pc_destroy(owtk_preconditioner* pc);
+/* apply(const in, out); in == out is allowed for ILU and split SSOR. */
+owtk_status owtk_pc_apply(owtk_preconditioner* pc, owtk_vector* in, owtk_vector* out);
+/* update_values(matrix) — re-validates the pattern and refactors; SSOR
+ * refreshes its diagonal cache from the same matrix (preconditioner.hpp:142). */
+owtk_status owtk_pc_update_values(owtk_preconditioner* pc, owtk_matrix* m);
+uint64_t owtk_pc_numeric_updates(owtk_preconditioner* pc);
+/* ILU factor storage (preconditioner.hpp:367-370); pass NULL arrays to query
+ * the entry count first.  Values and inverse diagonal in the PC's dtype. */
+owtk_status owtk_ilu_factors(owtk_preconditioner* pc, uint64_t* entries, uint64_t* row_offsets,
+                             uint64_t* columns, void* values, void* inverse_diagonal);
+/* Level sets the sweeps were scheduled with (no reference counterpart): per
+ * owned row its lower (forward-sweep) and upper (backward-sweep) level. */
+owtk_status owtk_pc_levels(owtk_preconditioner* pc, int32_t* lower_level, int32_t* upper_level,
+                           uint64_t* lower_depth, uint64_t* upper_depth);
+
+/* ---- host setup (ordering.hpp) -------------------------------------------- */
+/* reverse_cuthill_mckee_order (ordering.hpp:138-180); new_to_old[owned]. */
+owtk_status owtk_rcm_order(size_t owned_nodes, size_t ghost_nodes, const uint64_t* row_offsets,
+                           const uint64_t* column_indices, uint64_t* new_to_old);
+/* hilbert_order (ordering.hpp:231-261); xy holds n (x, y) pairs. */
+owtk_status owtk_hilbert_order(size_t n, const double* xy, uint64_t* new_to_old);
+/* inverse_permutation (ordering.hpp:263-277). */
+owtk_status owtk_inverse_permutation(size_t n, const uint64_t* new_to_old, uint64_t* old_to_new);
+/* Level sets of a pattern (no reference counterpart); depths are max level + 1. */
+owtk_status owtk_level_sets(size_t owned_nodes, const uint64_t* row_offsets,
+                            const uint64_t* column_indices, int32_t* lower_level,
+                            int32_t* upper_level, uint64_t* lower_depth, uint64_t* upper_depth);
+
+/* ---- solvers (krylov_solvers.hpp, pipelined_bicgstab.hpp, idrs.hpp) ------- */
+typedef enum owtk_solver_kind {
+    OWTK_SOLVER_FGMRES = 0,                   /* fgmres / gmres (krylov_solvers.hpp:159-540) */
+    OWTK_SOLVER_BICGSTAB = 1,                 /* bicgstab (:542-809) */
+    OWTK_SOLVER_PIPELINED_BICGSTAB = 2,       /* pipelined_bicgstab (pipelined_bicgstab.hpp:20-313) */
+    OWTK_SOLVER_COMM_HIDING_BICGSTAB = 3,     /* communication_hiding_bicgstab (:321-661) */
+    OWTK_SOLVER_IDRS = 4                      /* idrs (idrs.hpp:128-506) */
+} owtk_solver_kind;
+
+/* SolverOptions<T> (core.hpp:88-111) without the callback. */
+typedef struct owtk_solver_options {
+    double relative_tolerance;
+    double absolute_tolerance;
+    double breakdown_tolerance;
+    uint64_t maximum_iterations;
+    uint64_t convergence_check_interval;
+    uint64_t restart;
+    uint64_t residual_replacement_interval;
+    uint64_t idr_shadow_space;
+    double relaxation;
+    int32_t verify_true_residual;
+    int32_t gmres_orthogonalization;  /* 0 iterated CGS, 1 adaptive CGS, 2 one-sync CGS */
+} owtk_solver_options;
+
+/* SolverResult<T> (core.hpp:118-146); status / breakdown_reason carry the
+ * numeric values of SolverStatus (:24-30) and BreakdownReason (:41-52). */
+typedef struct owtk_solver_result {
+    int32_t status;
+    int32_t breakdown_reason;
+    uint64_t iterations;
+    uint64_t operator_applications;
+    uint64_t preconditioner_applications;
+    uint64_t global_reductions;
+    uint64_t reorthogonalizations;
+    uint64_t arnoldi_norm_verifications;
+    double initial_residual_norm;
+    double recursive_residual_norm;
+    double true_residual_norm;
+    double relative_residual_norm;
+    int32_t converged_by_application;
+    int32_t reserved;
+    double solve_seconds;
+} owtk_solver_result;
+
+void owtk_default_options(owtk_solver_options* options);
+
+/* SolverWorkspace<T> (core.hpp:402-459): device vectors reused across solves
+ * of the same layout; allocation_epochs() counts (re)allocations. */
+owtk_status owtk_workspace_create(owtk_context* ctx, owtk_workspace** out);
+owtk_status owtk_workspace_destroy(owtk_workspace* ws);
+uint64_t owtk_workspace_allocation_epochs(owtk_workspace* ws);
+/* Workspace vector `index` (same slot order as the reference solver), or NULL. */
+owtk_vector* owtk_workspace_vector(owtk_workspace* ws, size_t index);
+
+/* Device-resident solve: rhs and x are device vectors with the matrix layout.
+ * pc may be NULL (identity); workspace may be NULL (a temporary is used). */
+owtk_status owtk_solve(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,
+                       owtk_vector* rhs, owtk_vector* x, const owtk_solver_options* options,
+                       owtk_workspace* workspace, owtk_solver_result* result);
+/* The reference-facing call on HOST buffers ((owned+ghost)*bs values each):
+ * copies rhs and x in, solves on the device, copies x back. */
+owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,
+                            const void* host_rhs, void* host_x,
+                            const owtk_solver_options* options, owtk_workspace* workspace,
+                            owtk_solver_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OWTK_H */

@@ -1,0 +1,710 @@
+// Vector updates and reductions of the Krylov solvers (sm_100a).
+//
+// Element-wise kernels: each thread owns kIlp elements spaced one CTA apart,
+// loads them all before computing (independent 8-byte loads, fully coalesced
+// per warp), and evaluates the reference expression with the same rounding
+// sequence (device_common.cuh).
+//
+// Reductions: fixed-size first stage (one partial per CTA and dot), then the
+// last CTA to finish (atomic ticket) combines the partials in a fixed order.
+// Results are deterministic run to run and land both in device memory (for
+// kernels that consume them) and in mapped pinned memory (for the host).
+
+#include <cmath>
+
+#include "device_common.cuh"
+#include "owtk_internal.h"
+
+namespace owtk {
+namespace {
+
+using namespace dev;
+constexpr int kIlp = 4;
+constexpr int kPerBlock = kThreads * kIlp;
+
+inline unsigned ew_blocks(std::size_t n)
+{
+    return static_cast<unsigned>((n + kPerBlock - 1) / kPerBlock);
+}
+
+#define EW_PROLOGUE                                                            \
+    const std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * kPerBlock   \
+        + threadIdx.x;
+
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_fill(std::size_t n, T v, T* __restrict__ x)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) x[i] = v;
+    }
+}
+
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_copy(std::size_t n, const T* __restrict__ x, T* __restrict__ y)
+{
+    EW_PROLOGUE
+    T a[kIlp];
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) a[k] = x[i];
+    }
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) y[i] = a[k];
+    }
+}
+
+// y[i] += alpha * x[i]   (simd.hpp:533-535 scalar form)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_axpy(std::size_t n, T alpha, const T* __restrict__ x, T* __restrict__ y)
+{
+    EW_PROLOGUE
+    T a[kIlp], b[kIlp];
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) { a[k] = x[i]; b[k] = y[i]; }
+    }
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) y[i] = add_rn(b[k], mul_rn(alpha, a[k]));
+    }
+}
+
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_scale(std::size_t n, T alpha, T* __restrict__ x)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) x[i] = mul_rn(x[i], alpha);
+    }
+}
+
+// out = a*x + b*y   (core.hpp:598-600)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_lincomb(std::size_t n, T a, const T* __restrict__ x, T b,
+                                                      const T* __restrict__ y, T* __restrict__ out)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) out[i] = add_rn(mul_rn(a, x[i]), mul_rn(b, y[i]));
+    }
+}
+
+// out = b - a   (krylov_solvers.hpp:71-73)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_sub(std::size_t n, const T* __restrict__ b, const T* __restrict__ a,
+                                                  T* __restrict__ out)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) out[i] = sub_rn(b[i], a[i]);
+    }
+}
+
+// out = x / s   (krylov_solvers.hpp:256-258)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_divide(std::size_t n, const T* __restrict__ x, T s, T* __restrict__ out)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) out[i] = div_rn(x[i], s);
+    }
+}
+
+// p = r + beta*(p - omega*v)   (krylov_solvers.hpp:629-632)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_bicg_p(std::size_t n, const T* __restrict__ r, T beta, T omega,
+                                                     const T* __restrict__ v, T* __restrict__ p)
+{
+    EW_PROLOGUE
+    T rr[kIlp], pp[kIlp], vv[kIlp];
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) { rr[k] = r[i]; pp[k] = p[i]; vv[k] = v[i]; }
+    }
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) p[i] = add_rn(rr[k], mul_rn(beta, sub_rn(pp[k], mul_rn(omega, vv[k]))));
+    }
+}
+
+// x += alpha*ph; x += omega*sh; r = s - omega*t   (krylov_solvers.hpp:703-708)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_bicg_xr(std::size_t n, T alpha, const T* __restrict__ ph, T omega,
+                                                      const T* __restrict__ sh, const T* __restrict__ s,
+                                                      const T* __restrict__ t, T* __restrict__ x,
+                                                      T* __restrict__ r)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) {
+            const T xv = add_rn(add_rn(x[i], mul_rn(alpha, ph[i])), mul_rn(omega, sh[i]));
+            const T rv = sub_rn(s[i], mul_rn(omega, t[i]));
+            x[i] = xv;
+            r[i] = rv;
+        }
+    }
+}
+
+// pipelined_bicgstab.hpp:436-445
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_ch_psz(std::size_t n, T beta, T omega, const T* __restrict__ r2,
+                                                     const T* __restrict__ w, const T* __restrict__ w2,
+                                                     const T* __restrict__ t, const T* __restrict__ z2,
+                                                     const T* __restrict__ v, T* __restrict__ p2,
+                                                     T* __restrict__ s, T* __restrict__ s2, T* __restrict__ z)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) {
+            p2[i] = add_rn(r2[i], mul_rn(beta, sub_rn(p2[i], mul_rn(omega, s2[i]))));
+            s[i] = add_rn(w[i], mul_rn(beta, sub_rn(s[i], mul_rn(omega, z[i]))));
+            s2[i] = add_rn(w2[i], mul_rn(beta, sub_rn(s2[i], mul_rn(omega, z2[i]))));
+            z[i] = add_rn(t[i], mul_rn(beta, sub_rn(z[i], mul_rn(omega, v[i]))));
+        }
+    }
+}
+
+// pipelined_bicgstab.hpp:447-451
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_ch_qy(std::size_t n, T alpha, const T* __restrict__ r,
+                                                    const T* __restrict__ s, const T* __restrict__ r2,
+                                                    const T* __restrict__ s2, const T* __restrict__ w,
+                                                    const T* __restrict__ z, T* __restrict__ q,
+                                                    T* __restrict__ q2, T* __restrict__ y)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) {
+            q[i] = sub_rn(r[i], mul_rn(alpha, s[i]));
+            q2[i] = sub_rn(r2[i], mul_rn(alpha, s2[i]));
+            y[i] = sub_rn(w[i], mul_rn(alpha, z[i]));
+        }
+    }
+}
+
+// pipelined_bicgstab.hpp:506-512
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_ch_rw(std::size_t n, T alpha, T omega, const T* __restrict__ q,
+                                                    const T* __restrict__ y, const T* __restrict__ q2,
+                                                    const T* __restrict__ w2, const T* __restrict__ z2,
+                                                    const T* __restrict__ t, const T* __restrict__ v,
+                                                    T* __restrict__ r, T* __restrict__ r2, T* __restrict__ w)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) {
+            r[i] = sub_rn(q[i], mul_rn(omega, y[i]));
+            r2[i] = sub_rn(q2[i], mul_rn(omega, sub_rn(w2[i], mul_rn(alpha, z2[i]))));
+            w[i] = sub_rn(y[i], mul_rn(omega, sub_rn(t[i], mul_rn(alpha, v[i]))));
+        }
+    }
+}
+
+// out = x * s   (copy_owned + scale, krylov_solvers.hpp:355-356)
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_scaled_copy(std::size_t n, const T* __restrict__ x, T s,
+                                                          T* __restrict__ out)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) out[i] = mul_rn(x[i], s);
+    }
+}
+
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_jacobi(std::size_t n, const T* __restrict__ inv,
+                                                     const T* __restrict__ in, T* __restrict__ out)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) out[i] = mul_rn(inv[i], in[i]);
+    }
+}
+
+// inv = 1/d with the singular-diagonal check (preconditioner.hpp:62-69).
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_reciprocal(std::size_t n, const T* __restrict__ d, T minimum,
+                                                         T* __restrict__ inv, unsigned* status)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) {
+            const T v = d[i];
+            if (!isfinite(v) || fabs(v) <= minimum) atomicOr(status, kErrSingularDiagonal);
+            inv[i] = div_rn(T(1), v);
+        }
+    }
+}
+
+// --------------------------------------------------------------- pointer packs
+struct PtrPack {
+    const void* p[kMaxBatch];
+};
+
+// w -= sum_j h_j V_j in the reference's axpy order (krylov_solvers.hpp:286-290).
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_cgs_update(std::size_t n, int k, PtrPack basis,
+                                                         const double* __restrict__ h, T* __restrict__ w)
+{
+    __shared__ const T* sp[kMaxBatch];
+    __shared__ T sh[kMaxBatch];
+    for (int j = threadIdx.x; j < k; j += kThreads) {
+        sp[j] = static_cast<const T*>(basis.p[j]);
+        sh[j] = -static_cast<T>(h[j]);
+    }
+    __syncthreads();
+    EW_PROLOGUE
+#pragma unroll
+    for (int u = 0; u < kIlp; ++u) {
+        const std::size_t i = i0 + static_cast<std::size_t>(u) * kThreads;
+        if (i >= n) continue;
+        T wv = w[i];
+        for (int j = 0; j < k; ++j) wv = add_rn(wv, mul_rn(sh[j], sp[j][i]));
+        w[i] = wv;
+    }
+}
+
+// Neumaier-compensated correction sum (krylov_solvers.hpp:24-40).
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_gmres_update(std::size_t n, int k, PtrPack dirs,
+                                                           const double* __restrict__ coef,
+                                                           const T* base, T* out)
+{
+    __shared__ const T* sp[kMaxBatch];
+    __shared__ T sc[kMaxBatch];
+    for (int j = threadIdx.x; j < k; j += kThreads) {
+        sp[j] = static_cast<const T*>(dirs.p[j]);
+        sc[j] = static_cast<T>(coef[j]);
+    }
+    __syncthreads();
+    EW_PROLOGUE
+#pragma unroll
+    for (int u = 0; u < kIlp; ++u) {
+        const std::size_t i = i0 + static_cast<std::size_t>(u) * kThreads;
+        if (i >= n) continue;
+        T sum = 0, comp = 0;
+        for (int j = 0; j < k; ++j) {
+            const T term = mul_rn(sc[j], sp[j][i]);
+            const T upd = add_rn(sum, term);
+            comp = add_rn(comp, fabs(sum) >= fabs(term) ? add_rn(sub_rn(sum, upd), term)
+                                                        : add_rn(sub_rn(term, upd), sum));
+            sum = upd;
+        }
+        out[i] = add_rn(base[i], add_rn(sum, comp));
+    }
+}
+
+// --------------------------------------------------------------- reductions
+unsigned reduce_blocks(const Context& c, std::size_t n)
+{
+    const std::size_t want = (n + kThreads * 8 - 1) / (kThreads * 8);
+    const std::size_t cap = static_cast<std::size_t>(c.sm_count) * 4;
+    return static_cast<unsigned>(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
+// Reduce G per-thread accumulators across the CTA; thread j < G writes the
+// CTA's partial for accumulator j.
+template<int G>
+__device__ __forceinline__ void block_partials(const double (&acc)[G], int count, double* partials,
+                                               int slot0)
+{
+    __shared__ double red[G][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        const double v = warp_sum(acc[j]);
+        if (lane == 0) red[j][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < count) {
+        double s = 0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) s += red[threadIdx.x][w];
+        partials[static_cast<std::size_t>(slot0 + threadIdx.x) * gridDim.x + blockIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// Last CTA: sum each accumulator's partials over CTAs in a fixed order.
+__device__ __forceinline__ bool last_block(unsigned* ticket)
+{
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    return is_last;
+}
+
+__device__ __forceinline__ void combine(int count, const double* partials, double* out_dev,
+                                        double* out_host)
+{
+    __threadfence();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = warp; j < count; j += kThreads / 32) {
+        double s = 0;
+        for (unsigned b = lane; b < gridDim.x; b += 32)
+            s += __ldcg(partials + static_cast<std::size_t>(j) * gridDim.x + b);
+        s = warp_sum(s);
+        if (lane == 0) {
+            out_dev[j] = s;
+            out_host[j] = s;
+        }
+    }
+}
+
+// k dots a_j . b_j, FP64 accumulation (float inputs are widened as the
+// reference's SerialReduction<float> does, reduction.hpp:123-133).
+template<class T, int G>
+__global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, PtrPack a, PtrPack b,
+                                                       double* partials, unsigned* ticket,
+                                                       double* out_dev, double* out_host)
+{
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    __shared__ const T* sa[kMaxBatch];
+    __shared__ const T* sb[kMaxBatch];
+    for (int j = threadIdx.x; j < k; j += kThreads) {
+        sa[j] = static_cast<const T*>(a.p[j]);
+        sb[j] = static_cast<const T*>(b.p[j]);
+    }
+    __syncthreads();
+    for (int g0 = 0; g0 < k; g0 += G) {
+        double acc[G];
+        const T* pa[G];
+        const T* pb[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            acc[j] = 0;
+            pa[j] = g0 + j < k ? sa[g0 + j] : nullptr;
+            pb[j] = g0 + j < k ? sb[g0 + j] : nullptr;
+        }
+        for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                if (g0 + j < k)
+                    acc[j] += static_cast<double>(pa[j][i]) * static_cast<double>(pb[j][i]);
+            }
+        }
+        block_partials<G>(acc, k - g0 < G ? k - g0 : G, partials, g0);
+    }
+    if (last_block(ticket)) {
+        combine(k, partials, out_dev, out_host);
+        if (threadIdx.x == 0) *ticket = 0;
+    }
+}
+
+// w -= V h (reference axpy order), then dots of the updated w with every V_j
+// and w.w, in one pass over V (second Gram-Schmidt pass, krylov_solvers.hpp:310-322).
+template<class T, int G>
+__global__ void __launch_bounds__(kThreads) k_cgs_update_dot(std::size_t n, int k, PtrPack basis,
+                                                             const double* __restrict__ h, T* __restrict__ w,
+                                                             double* partials, unsigned* ticket,
+                                                             double* out_dev, double* out_host)
+{
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    double acc[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) acc[j] = 0;
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+        T wv = w[i];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            if (j < k) {
+                const T coef = -static_cast<T>(h[j]);
+                wv = add_rn(wv, mul_rn(coef, static_cast<const T*>(basis.p[j])[i]));
+            }
+        }
+        w[i] = wv;
+        const double wd = static_cast<double>(wv);
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            if (j < k) acc[j] += wd * static_cast<double>(static_cast<const T*>(basis.p[j])[i]);
+            else if (j == k) acc[j] += wd * wd;
+        }
+    }
+    block_partials<G>(acc, k + 1, partials, 0);
+    if (last_block(ticket)) {
+        combine(k + 1, partials, out_dev, out_host);
+        if (threadIdx.x == 0) *ticket = 0;
+    }
+}
+
+// One-pass scaled 2-norm: each thread keeps (scale, sum of squares relative
+// to scale) and rescales when a larger magnitude arrives; pairs combine the
+// same way.  NaN anywhere gives NaN and an infinite entry gives infinity,
+// as the reference's two-pass scaled norm does (reduction.hpp:64-89).
+struct ScaledSum {
+    double scale, ssq;
+    int nan;
+};
+
+__device__ __forceinline__ void norm_push(ScaledSum& a, double x)
+{
+    const double m = fabs(x);
+    if (isnan(m)) { a.nan = 1; return; }
+    if (m == 0.0 || isinf(a.scale)) return;
+    if (m > a.scale) {
+        if (isinf(m)) { a.scale = m; a.ssq = 1.0; return; }
+        const double r = a.scale / m;
+        a.ssq = 1.0 + a.ssq * r * r;
+        a.scale = m;
+    } else {
+        const double r = m / a.scale;
+        a.ssq += r * r;
+    }
+}
+
+__device__ __forceinline__ ScaledSum norm_merge(ScaledSum a, ScaledSum b)
+{
+    ScaledSum r;
+    r.nan = a.nan | b.nan;
+    if (a.scale < b.scale) { const ScaledSum t = a; a = b; b = t; }
+    r.scale = a.scale;
+    if (a.scale == 0.0) { r.ssq = 0.0; return r; }
+    if (isinf(a.scale)) { r.ssq = 1.0; return r; }
+    const double q = b.scale / a.scale;
+    r.ssq = a.ssq + b.ssq * q * q;
+    return r;
+}
+
+__device__ __forceinline__ ScaledSum norm_warp(ScaledSum a)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ScaledSum b;
+        b.scale = __shfl_xor_sync(0xffffffffu, a.scale, o);
+        b.ssq = __shfl_xor_sync(0xffffffffu, a.ssq, o);
+        b.nan = __shfl_xor_sync(0xffffffffu, a.nan, o);
+        a = norm_merge(a, b);
+    }
+    return a;
+}
+
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __restrict__ x, double* partials,
+                                                   unsigned* ticket, double* out_dev, double* out_host)
+{
+    ScaledSum a{0.0, 0.0, 0};
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride)
+        norm_push(a, static_cast<double>(x[i]));
+    a = norm_warp(a);
+    __shared__ ScaledSum red[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ScaledSum s = red[0];
+        for (int w = 1; w < kThreads / 32; ++w) s = norm_merge(s, red[w]);
+        partials[3 * blockIdx.x + 0] = s.scale;
+        partials[3 * blockIdx.x + 1] = s.ssq;
+        partials[3 * blockIdx.x + 2] = s.nan;
+    }
+    if (last_block(ticket)) {
+        __threadfence();
+        if (threadIdx.x == 0) {
+            ScaledSum s{0.0, 0.0, 0};
+            for (unsigned b = 0; b < gridDim.x; ++b) {
+                ScaledSum t{__ldcg(partials + 3 * b), __ldcg(partials + 3 * b + 1),
+                            __ldcg(partials + 3 * b + 2) != 0.0};
+                s = norm_merge(s, t);
+            }
+            double r;
+            if (s.nan) r = __longlong_as_double(0x7ff8000000000000LL);
+            else if (s.scale == 0.0 || isinf(s.scale)) r = s.scale;
+            else r = s.scale * sqrt(s.ssq);
+            *out_dev = r;
+            *out_host = r;
+            *ticket = 0;
+        }
+    }
+}
+
+inline PtrPack pack(const void* const* p, int k)
+{
+    PtrPack pk{};
+    for (int i = 0; i < k; ++i) pk.p[i] = p[i];
+    return pk;
+}
+
+double* partials_of(Context& c) { return c.partials.as<double>(); }
+unsigned* ticket_of(Context& c) { return c.tickets.as<unsigned>(); }
+
+}  // namespace
+
+namespace kern {
+
+#define LAUNCH_EW(kernel, n, ...)                                                  \
+    do {                                                                           \
+        if ((n) == 0) break;                                                       \
+        kernel<<<ew_blocks(n), kThreads, 0, c.stream>>>((n), __VA_ARGS__);         \
+        OWTK_CUDA(cudaGetLastError());                                             \
+        c.launched();                                                              \
+    } while (0)
+
+template<class T> void fill(Context& c, std::size_t n, T value, T* x) { LAUNCH_EW(k_fill<T>, n, value, x); }
+template<class T> void copy(Context& c, std::size_t n, const T* x, T* y)
+{
+    if (x == y) return;
+    LAUNCH_EW(k_copy<T>, n, x, y);
+}
+template<class T> void axpy(Context& c, std::size_t n, T alpha, const T* x, T* y) { LAUNCH_EW(k_axpy<T>, n, alpha, x, y); }
+template<class T> void scale(Context& c, std::size_t n, T alpha, T* x) { LAUNCH_EW(k_scale<T>, n, alpha, x); }
+template<class T> void lincomb(Context& c, std::size_t n, T a, const T* x, T b, const T* y, T* out)
+{
+    LAUNCH_EW(k_lincomb<T>, n, a, x, b, y, out);
+}
+template<class T> void sub(Context& c, std::size_t n, const T* b, const T* a, T* out) { LAUNCH_EW(k_sub<T>, n, b, a, out); }
+template<class T> void divide(Context& c, std::size_t n, const T* x, T s, T* out) { LAUNCH_EW(k_divide<T>, n, x, s, out); }
+template<class T> void bicg_p(Context& c, std::size_t n, const T* r, T beta, T omega, const T* v, T* p)
+{
+    LAUNCH_EW(k_bicg_p<T>, n, r, beta, omega, v, p);
+}
+template<class T> void bicg_xr(Context& c, std::size_t n, T alpha, const T* ph, T omega, const T* sh,
+                               const T* s, const T* t, T* x, T* r)
+{
+    LAUNCH_EW(k_bicg_xr<T>, n, alpha, ph, omega, sh, s, t, x, r);
+}
+template<class T> void ch_pszupdate(Context& c, std::size_t n, T beta, T omega, const T* r2, const T* w,
+                                    const T* w2, const T* t, const T* z2, const T* v,
+                                    T* p2, T* s, T* s2, T* z)
+{
+    LAUNCH_EW(k_ch_psz<T>, n, beta, omega, r2, w, w2, t, z2, v, p2, s, s2, z);
+}
+template<class T> void ch_qy(Context& c, std::size_t n, T alpha, const T* r, const T* s, const T* r2,
+                             const T* s2, const T* w, const T* z, T* q, T* q2, T* y)
+{
+    LAUNCH_EW(k_ch_qy<T>, n, alpha, r, s, r2, s2, w, z, q, q2, y);
+}
+template<class T> void ch_rw(Context& c, std::size_t n, T alpha, T omega, const T* q, const T* y,
+                             const T* q2, const T* w2, const T* z2, const T* t, const T* v,
+                             T* r, T* r2, T* w)
+{
+    LAUNCH_EW(k_ch_rw<T>, n, alpha, omega, q, y, q2, w2, z2, t, v, r, r2, w);
+}
+template<class T> void scaled_copy(Context& c, std::size_t n, const T* x, T s, T* out)
+{
+    LAUNCH_EW(k_scaled_copy<T>, n, x, s, out);
+}
+template<class T> void jacobi(Context& c, std::size_t n, const T* inv, const T* in, T* out)
+{
+    LAUNCH_EW(k_jacobi<T>, n, inv, in, out);
+}
+template<class T> void reciprocal_checked(Context& c, std::size_t n, const T* d, T minimum, T* inv)
+{
+    LAUNCH_EW(k_reciprocal<T>, n, d, minimum, inv, c.status.as<unsigned>());
+}
+template<class T> void cgs_update(Context& c, std::size_t n, int k, const T* const* basis, const double* h, T* w)
+{
+    LAUNCH_EW(k_cgs_update<T>, n, k, pack(reinterpret_cast<const void* const*>(basis), k), h, w);
+}
+template<class T> void gmres_update(Context& c, std::size_t n, int k, const T* const* dirs,
+                                    const double* coef, const T* base, T* out)
+{
+    LAUNCH_EW(k_gmres_update<T>, n, k, pack(reinterpret_cast<const void* const*>(dirs), k), coef, base, out);
+}
+
+template<class T> void multidot(Context& c, std::size_t n, int k, const T* const* a,
+                                const T* const* b, double* out_dev, double* out_host)
+{
+    if (k <= 0) return;
+    if (k > kMaxBatch) fail(OWTK_ERR_INVALID_ARGUMENT, "dot batch too large");
+    const unsigned blocks = reduce_blocks(c, n);
+    const PtrPack pa = pack(reinterpret_cast<const void* const*>(a), k);
+    const PtrPack pb = pack(reinterpret_cast<const void* const*>(b), k);
+    if (k <= 4)
+        k_multidot<T, 4><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, partials_of(c), ticket_of(c), out_dev, out_host);
+    else
+        k_multidot<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, partials_of(c), ticket_of(c), out_dev, out_host);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T* const* basis,
+                                      const double* h, T* w, double* out_dev, double* out_host)
+{
+    if (k + 1 > kMaxBatch) fail(OWTK_ERR_INVALID_ARGUMENT, "Gram-Schmidt batch too large");
+    const unsigned blocks = reduce_blocks(c, n);
+    const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
+    if (k + 1 <= 8)
+        k_cgs_update_dot<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 16)
+        k_cgs_update_dot<T, 16><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 32)
+        k_cgs_update_dot<T, 32><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    else
+        k_cgs_update_dot<T, kMaxBatch><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_dev, double* out_host)
+{
+    const unsigned blocks = reduce_blocks(c, n);
+    k_norm<T><<<blocks, kThreads, 0, c.stream>>>(n, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+#define INSTANTIATE(T)                                                                              \
+    template void fill<T>(Context&, std::size_t, T, T*);                                           \
+    template void copy<T>(Context&, std::size_t, const T*, T*);                                    \
+    template void axpy<T>(Context&, std::size_t, T, const T*, T*);                                 \
+    template void scale<T>(Context&, std::size_t, T, T*);                                          \
+    template void lincomb<T>(Context&, std::size_t, T, const T*, T, const T*, T*);                 \
+    template void sub<T>(Context&, std::size_t, const T*, const T*, T*);                           \
+    template void divide<T>(Context&, std::size_t, const T*, T, T*);                               \
+    template void bicg_p<T>(Context&, std::size_t, const T*, T, T, const T*, T*);                  \
+    template void bicg_xr<T>(Context&, std::size_t, T, const T*, T, const T*, const T*, const T*, T*, T*); \
+    template void ch_pszupdate<T>(Context&, std::size_t, T, T, const T*, const T*, const T*, const T*,    \
+                                  const T*, const T*, T*, T*, T*, T*);                             \
+    template void ch_qy<T>(Context&, std::size_t, T, const T*, const T*, const T*, const T*, const T*,    \
+                           const T*, T*, T*, T*);                                                  \
+    template void ch_rw<T>(Context&, std::size_t, T, T, const T*, const T*, const T*, const T*, const T*, \
+                           const T*, const T*, T*, T*, T*);                                        \
+    template void jacobi<T>(Context&, std::size_t, const T*, const T*, T*);                        \
+    template void scaled_copy<T>(Context&, std::size_t, const T*, T, T*);                          \
+    template void reciprocal_checked<T>(Context&, std::size_t, const T*, T, T*);                   \
+    template void cgs_update<T>(Context&, std::size_t, int, const T* const*, const double*, T*);   \
+    template void gmres_update<T>(Context&, std::size_t, int, const T* const*, const double*, const T*, T*); \
+    template void multidot<T>(Context&, std::size_t, int, const T* const*, const T* const*, double*, double*); \
+    template void cgs_update_dot<T>(Context&, std::size_t, int, const T* const*, const double*, T*, double*, double*); \
+    template void norm<T>(Context&, std::size_t, const T*, double*, double*);
+
+INSTANTIATE(double)
+INSTANTIATE(float)
+
+}  // namespace kern
+}  // namespace owtk

@@ -1,0 +1,246 @@
+// Internal declarations shared by the kernels (*.cu) and the host runtime
+// (capi.cu, setup.cpp, solvers.cpp).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/owtk.h"
+
+namespace owtk {
+
+// ---------------------------------------------------------------- errors
+struct Error {
+    owtk_status code;
+    std::string message;
+};
+[[noreturn]] void fail(owtk_status code, const std::string& message);
+void cuda_check(cudaError_t e, const char* what);
+#define OWTK_CUDA(call) ::owtk::cuda_check((call), #call)
+
+// ---------------------------------------------------------------- device buffers
+// Owning device allocation (cudaMalloc) released on destruction.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    std::size_t bytes = 0;
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(std::size_t n) { allocate(n); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept;
+    ~DeviceBuffer();
+    void allocate(std::size_t n);
+    template<class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Upload a host vector into a fresh device buffer (synchronous on the stream).
+template<class T>
+DeviceBuffer upload(cudaStream_t s, const std::vector<T>& host)
+{
+    DeviceBuffer b(host.size() * sizeof(T) + 16);
+    if (!host.empty())
+        OWTK_CUDA(cudaMemcpyAsync(b.ptr, host.data(), host.size() * sizeof(T),
+                                  cudaMemcpyHostToDevice, s));
+    return b;
+}
+
+// ---------------------------------------------------------------- context
+// Scalar results of reductions land in a mapped pinned block the host reads
+// after one stream synchronisation.
+constexpr int kScalarSlots = 256;
+constexpr int kMaxBatch = 40;            // largest dot batch (restart + 2)
+constexpr int kReduceBlocks = 4 * 148;   // two-stage reductions: max first-stage blocks
+
+struct Context {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    double* host_scalars = nullptr;      // mapped pinned, kScalarSlots
+    double* dev_scalars = nullptr;       // device alias of host_scalars
+    DeviceBuffer dev_scalar_copy;        // device-resident copies for kernels
+    DeviceBuffer partials;               // kReduceBlocks * kMaxBatch * 2 doubles
+    DeviceBuffer tickets;                // reduction tickets (self-resetting)
+    DeviceBuffer status;                 // device error word(s)
+    std::uint64_t launches = 0;
+    ~Context();
+    void sync();
+    void launched(int n = 1) { launches += static_cast<std::uint64_t>(n); }
+    // Device error word: set by bounded waits (timeout) and the device factorisation.
+    void check_device_status();
+};
+
+// ---------------------------------------------------------------- objects
+struct Vector {
+    Context* ctx = nullptr;
+    owtk_dtype dtype = OWTK_F64;
+    std::size_t owned = 0, ghost = 0, bs = 0;
+    void* data = nullptr;
+    DeviceBuffer storage;      // empty for views
+    bool is_view = false;
+    std::size_t owned_size() const { return owned * bs; }
+    std::size_t local_size() const { return (owned + ghost) * bs; }
+    std::size_t elem() const { return dtype == OWTK_F64 ? 8 : 4; }
+    bool same_layout(const Vector& o) const
+    {
+        return owned == o.owned && ghost == o.ghost && bs == o.bs;
+    }
+};
+
+// Row tiles for the SpMV kernels: a tile is a run of consecutive rows whose
+// work fits one CTA's shared-memory stage; a row that does not fit alone is a
+// "long" tile handled component-parallel.
+struct TilePlan {
+    DeviceBuffer tile_rows;    // int32, tiles + 1
+    int tiles = 0;
+    int tile_values = 0;       // stage capacity used to build the plan
+};
+
+struct Matrix {
+    Context* ctx = nullptr;
+    int kind = 0;              // 0 component-diagonal BSR, 1 split view, 2 dense BSR
+    owtk_dtype dtype = OWTK_F64;
+    std::size_t owned = 0, ghost = 0, bs = 0, entries = 0;
+    // Host copies of the structure (needed for setup and pattern checks).
+    std::vector<std::int32_t> h_rowptr, h_cols;
+    DeviceBuffer rowptr, cols;       // int32
+    DeviceBuffer values;             // owning kinds: nnz*bs (BSR) / nnz*bs*bs (dense)
+    const void* diag = nullptr;      // split view: borrowed device diagonal
+    const void* off = nullptr;       // split view: borrowed device off-diagonal
+    TilePlan plan;
+    const void* value_ptr() const { return kind == 1 ? off : values.ptr; }
+    std::size_t local_size() const { return (owned + ghost) * bs; }
+};
+
+// A scheduled triangular sweep: rows ordered by (level, row), cut into warp
+// tasks that never straddle a level; dependencies are the row's entries whose
+// column lies on the solved side.
+struct Sweep {
+    DeviceBuffer order;        // int32 rows
+    DeviceBuffer task_start;   // int32, tasks + 1 (positions in order)
+    int tasks = 0;
+    int depth = 0;             // number of levels
+    int rows_per_task = 1;
+    std::vector<std::int32_t> h_level;
+};
+
+struct Preconditioner {
+    Context* ctx = nullptr;
+    owtk_pc_kind kind = OWTK_PC_IDENTITY;
+    owtk_dtype dtype = OWTK_F64;
+    Matrix* matrix = nullptr;
+    std::size_t owned = 0, ghost = 0, bs = 0;
+    double parameter = 0;
+    std::uint64_t numeric_updates = 0;
+    DeviceBuffer inv_diag;     // Jacobi, ILU
+    DeviceBuffer diag_cache;   // BSR SSOR diagonal cache
+    DeviceBuffer work;         // SSOR forward-sweep scratch
+    // ILU factor pattern (host copies + device).
+    std::vector<std::int32_t> f_rowptr, f_cols, f_diagpos;
+    std::vector<std::int64_t> f_source;     // matrix entry or -1 (fill)
+    std::vector<std::int32_t> row_counts;   // local entries per matrix row
+    DeviceBuffer d_frowptr, d_fcols, d_fdiagpos, d_fsource, d_fvalues;
+    // IKJ update list of the numeric factorisation: for every lower entry l,
+    // the (target, upper) entry pairs it updates, in reference order.
+    DeviceBuffer d_upd_start, d_upd_target, d_upd_upper;
+    // SSOR dependency patterns reuse the matrix structure.
+    Sweep lower, upper;
+    DeviceBuffer flags;        // uint32 per row, epoch-stamped
+    DeviceBuffer ticket;       // uint64 monotone task counter
+    std::uint32_t epoch = 0;
+    std::uint64_t ticket_base = 0;
+};
+
+struct Workspace {
+    Context* ctx = nullptr;
+    std::vector<std::unique_ptr<Vector>> vectors;
+    std::vector<std::unique_ptr<Vector>> stage;   // host-buffer solve staging (rhs, x)
+    std::uint64_t epochs = 0;
+    void prepare(const Vector& layout, std::size_t count);
+};
+
+// ---------------------------------------------------------------- setup (setup.cpp)
+void build_tile_plan(Matrix& m);
+void levels_of(std::size_t owned, const std::int32_t* rowptr, const std::int32_t* cols,
+               std::vector<std::int32_t>& lower, std::vector<std::int32_t>& upper);
+void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
+                 const std::vector<std::int32_t>& level, bool descending_rows);
+void rcm_order(std::size_t owned, const std::int32_t* rowptr, const std::int32_t* cols,
+               std::uint64_t* out);
+void hilbert_order(std::size_t n, const double* xy, std::uint64_t* out);
+
+// ---------------------------------------------------------------- kernels
+namespace kern {
+
+template<class T> void fill(Context& c, std::size_t n, T value, T* x);
+template<class T> void copy(Context& c, std::size_t n, const T* x, T* y);
+template<class T> void axpy(Context& c, std::size_t n, T alpha, const T* x, T* y);
+template<class T> void scale(Context& c, std::size_t n, T alpha, T* x);
+template<class T> void lincomb(Context& c, std::size_t n, T a, const T* x, T b, const T* y, T* out);
+// out = b - a (true residual)
+template<class T> void sub(Context& c, std::size_t n, const T* b, const T* a, T* out);
+// out = x / s (GMRES first basis vector)
+template<class T> void divide(Context& c, std::size_t n, const T* x, T s, T* out);
+// BiCGSTAB search update: p = r + beta*(p - omega*v)
+template<class T> void bicg_p(Context& c, std::size_t n, const T* r, T beta, T omega, const T* v, T* p);
+// x += alpha*ph; x += omega*sh; r = s - omega*t
+template<class T> void bicg_xr(Context& c, std::size_t n, T alpha, const T* ph, T omega, const T* sh,
+                               const T* s, const T* t, T* x, T* r);
+// Communication-hiding recurrences (pipelined_bicgstab.hpp:436-451, :506-512).
+template<class T> void ch_pszupdate(Context& c, std::size_t n, T beta, T omega, const T* r2, const T* w,
+                                    const T* w2, const T* t, const T* z2, const T* v,
+                                    T* p2, T* s, T* s2, T* z);
+template<class T> void ch_qy(Context& c, std::size_t n, T alpha, const T* r, const T* s, const T* r2,
+                             const T* s2, const T* w, const T* z, T* q, T* q2, T* y);
+template<class T> void ch_rw(Context& c, std::size_t n, T alpha, T omega, const T* q, const T* y,
+                             const T* q2, const T* w2, const T* z2, const T* t, const T* v,
+                             T* r, T* r2, T* w);
+// GMRES: w -= sum_i h_i V_i in reference order (h on device, negated inside).
+template<class T> void cgs_update(Context& c, std::size_t n, int k, const T* const* basis,
+                                  const double* h, T* w);
+// GMRES fused: w -= sum_i h_i V_i, then dots of the new w with V_i and w.w.
+template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T* const* basis,
+                                      const double* h, T* w, double* out_dev, double* out_host);
+// Compensated GMRES update (krylov_solvers.hpp:24-40).
+template<class T> void gmres_update(Context& c, std::size_t n, int k, const T* const* dirs,
+                                    const double* coef, const T* base, T* out);
+// k dot products a_i . b_i (FP64 accumulation); results to out_dev and out_host.
+template<class T> void multidot(Context& c, std::size_t n, int k, const T* const* a,
+                                const T* const* b, double* out_dev, double* out_host);
+template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_dev, double* out_host);
+template<class T> void jacobi(Context& c, std::size_t n, const T* inv, const T* in, T* out);
+template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y);
+template<class T> void gather_values(Context& c, std::size_t entries, std::size_t bs,
+                                     const std::int64_t* source, const T* values, T* out);
+// ILU(0)/SSOR sweeps.
+template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* matrix_values);
+template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
+template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T* out);
+template<class T> void reciprocal_checked(Context& c, std::size_t n, const T* d, T minimum, T* inv);
+template<class T> void bsr_diagonal(Context& c, const Matrix& m, T* out);
+
+template<class T> void scaled_copy(Context& c, std::size_t n, const T* x, T s, T* out);
+
+}  // namespace kern
+
+// Operator / preconditioner application on device vectors (capi.cu).
+void apply_operator(Matrix& m, Vector& in, Vector& out);
+void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out);
+
+// Solver recurrences (solvers.cpp).
+void solve(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& rhs, Vector& x,
+           const owtk_solver_options& options, Workspace& ws, owtk_solver_result& result);
+
+}  // namespace owtk
+
+// The opaque handles of the C ABI are the runtime objects themselves.
+struct owtk_context : owtk::Context {};
+struct owtk_vector : owtk::Vector {};
+struct owtk_matrix : owtk::Matrix {};
+struct owtk_preconditioner : owtk::Preconditioner {};
+struct owtk_workspace : owtk::Workspace {};

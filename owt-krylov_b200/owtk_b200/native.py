@@ -1,0 +1,450 @@
+"""ctypes binding of the C ABI in include/owtk.h (lib/libowtk_b200.so).
+
+The library is the product: this module only marshals arguments.  Loading
+fails loudly when the shared object is missing — there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_size_t, c_uint64, c_void_p
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libowtk_b200.so")
+
+F64, F32 = 0, 1
+PC_IDENTITY, PC_JACOBI, PC_SSOR, PC_SPLIT_SSOR, PC_ILU = 0, 1, 2, 3, 4
+FGMRES, BICGSTAB, PIPELINED_BICGSTAB, COMM_HIDING_BICGSTAB, IDRS = 0, 1, 2, 3, 4
+
+STATUS = {0: "ok", 1: "invalid_argument", 2: "zero_pivot", 3: "out_of_range", 4: "cuda_error",
+          5: "timeout", 6: "no_device", 7: "runtime_error"}
+SOLVER_STATUS = ["converged", "maximum_iterations", "breakdown", "diverged", "invalid_input"]
+BREAKDOWN = ["none", "arnoldi_invariant_subspace", "singular_projected_system",
+             "biorthogonality_loss", "alpha_denominator", "omega_denominator", "omega_zero",
+             "idr_shadow_space", "idr_small_system", "non_finite_scalar"]
+
+
+class OwtkError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS.get(code, code)}: {message}")
+        self.code = code
+        self.kind = STATUS.get(code, str(code))
+        self.message = message
+
+
+class SolverOptions(ctypes.Structure):
+    _fields_ = [("relative_tolerance", c_double), ("absolute_tolerance", c_double),
+                ("breakdown_tolerance", c_double), ("maximum_iterations", c_uint64),
+                ("convergence_check_interval", c_uint64), ("restart", c_uint64),
+                ("residual_replacement_interval", c_uint64), ("idr_shadow_space", c_uint64),
+                ("relaxation", c_double), ("verify_true_residual", c_int32),
+                ("gmres_orthogonalization", c_int32)]
+
+
+class SolverResult(ctypes.Structure):
+    _fields_ = [("status", c_int32), ("breakdown_reason", c_int32), ("iterations", c_uint64),
+                ("operator_applications", c_uint64), ("preconditioner_applications", c_uint64),
+                ("global_reductions", c_uint64), ("reorthogonalizations", c_uint64),
+                ("arnoldi_norm_verifications", c_uint64), ("initial_residual_norm", c_double),
+                ("recursive_residual_norm", c_double), ("true_residual_norm", c_double),
+                ("relative_residual_norm", c_double), ("converged_by_application", c_int32),
+                ("reserved", c_int32), ("solve_seconds", c_double)]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        d["status_name"] = SOLVER_STATUS[self.status] if 0 <= self.status < 5 else str(self.status)
+        d["breakdown_name"] = BREAKDOWN[self.breakdown_reason] if 0 <= self.breakdown_reason < 10 else "?"
+        return d
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"owtk CUDA library not built: {LIB_PATH} (run `make -C owt-krylov_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, sz, u64p = c_void_p, c_size_t, POINTER(c_uint64)
+        sig = {
+            "owtk_last_error": (c_char_p, []),
+            "owtk_abi_version": (c_int, []),
+            "owtk_context_create": (c_int, [c_int, POINTER(vp)]),
+            "owtk_context_destroy": (c_int, [vp]),
+            "owtk_context_synchronize": (c_int, [vp]),
+            "owtk_context_stream": (vp, [vp]),
+            "owtk_context_kernel_launches": (c_uint64, [vp]),
+            "owtk_vector_create": (c_int, [vp, c_int, sz, sz, sz, POINTER(vp)]),
+            "owtk_vector_view": (c_int, [vp, c_int, sz, sz, sz, vp, sz, POINTER(vp)]),
+            "owtk_vector_destroy": (c_int, [vp]),
+            "owtk_vector_data": (vp, [vp]),
+            "owtk_vector_upload": (c_int, [vp, vp, sz]),
+            "owtk_vector_download": (c_int, [vp, vp, sz]),
+            "owtk_vector_fill": (c_int, [vp, c_double, c_int]),
+            "owtk_copy_owned": (c_int, [vp, vp]),
+            "owtk_axpy": (c_int, [c_double, vp, vp]),
+            "owtk_scale": (c_int, [c_double, vp]),
+            "owtk_assign_linear_combination": (c_int, [vp, c_double, vp, c_double, vp]),
+            "owtk_dot": (c_int, [vp, vp, POINTER(c_double)]),
+            "owtk_norm": (c_int, [vp, POINTER(c_double)]),
+            "owtk_dot_batch": (c_int, [vp, POINTER(vp), sz, POINTER(c_double)]),
+            "owtk_bsr_create": (c_int, [vp, c_int, sz, sz, sz, vp, vp, vp, POINTER(vp)]),
+            "owtk_bsr_update_values": (c_int, [vp, vp]),
+            "owtk_split_view_create": (c_int, [vp, c_int, sz, sz, sz, vp, vp, vp, vp, POINTER(vp)]),
+            "owtk_dense_bsr_create": (c_int, [vp, c_int, sz, sz, sz, vp, vp, vp, POINTER(vp)]),
+            "owtk_matrix_destroy": (c_int, [vp]),
+            "owtk_matrix_info": (c_int, [vp, POINTER(c_int), POINTER(sz), POINTER(sz), POINTER(sz), POINTER(sz)]),
+            "owtk_spmv": (c_int, [vp, vp, vp]),
+            "owtk_matrix_diagonal": (c_int, [vp, vp]),
+            "owtk_pc_create": (c_int, [vp, c_int, c_double, POINTER(vp)]),
+            "owtk_pc_destroy": (c_int, [vp]),
+            "owtk_pc_apply": (c_int, [vp, vp, vp]),
+            "owtk_pc_update_values": (c_int, [vp, vp]),
+            "owtk_pc_numeric_updates": (c_uint64, [vp]),
+            "owtk_ilu_factors": (c_int, [vp, u64p, vp, vp, vp, vp]),
+            "owtk_pc_levels": (c_int, [vp, vp, vp, u64p, u64p]),
+            "owtk_rcm_order": (c_int, [sz, sz, vp, vp, vp]),
+            "owtk_hilbert_order": (c_int, [sz, vp, vp]),
+            "owtk_inverse_permutation": (c_int, [sz, vp, vp]),
+            "owtk_level_sets": (c_int, [sz, vp, vp, vp, vp, u64p, u64p]),
+            "owtk_default_options": (None, [POINTER(SolverOptions)]),
+            "owtk_workspace_create": (c_int, [vp, POINTER(vp)]),
+            "owtk_workspace_destroy": (c_int, [vp]),
+            "owtk_workspace_allocation_epochs": (c_uint64, [vp]),
+            "owtk_workspace_vector": (vp, [vp, sz]),
+            "owtk_solve": (c_int, [c_int, vp, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
+            "owtk_solve_host": (c_int, [c_int, vp, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int):
+    if code != 0:
+        raise OwtkError(code, lib().owtk_last_error().decode())
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(c_void_p)
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+
+
+def default_options(**kw) -> SolverOptions:
+    o = SolverOptions()
+    lib().owtk_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = c_void_p()
+        check(lib().owtk_context_create(device, ctypes.byref(h)))
+        self.h = h
+
+    def synchronize(self):
+        check(lib().owtk_context_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return lib().owtk_context_stream(self.h) or 0
+
+    @property
+    def kernel_launches(self) -> int:
+        return lib().owtk_context_kernel_launches(self.h)
+
+    def close(self):
+        if self.h:
+            lib().owtk_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _dtype_code(dt) -> int:
+    return F64 if np.dtype(dt) == np.float64 else F32
+
+
+def _np_dtype(code: int):
+    return np.float64 if code == F64 else np.float32
+
+
+class Vector:
+    def __init__(self, ctx: Context, owned: int, ghost: int, bs: int, dtype=np.float64, handle=None,
+                 owner=True):
+        self.ctx, self.owned, self.ghost, self.bs = ctx, owned, ghost, bs
+        self.dtype = np.dtype(dtype)
+        self.owner = owner
+        if handle is None:
+            h = c_void_p()
+            check(lib().owtk_vector_create(ctx.h, _dtype_code(dtype), owned, ghost, bs, ctypes.byref(h)))
+            handle = h
+        self.h = handle
+
+    @classmethod
+    def view(cls, ctx, owned, ghost, bs, device_ptr: int, count: int, dtype=np.float64):
+        h = c_void_p()
+        check(lib().owtk_vector_view(ctx.h, _dtype_code(dtype), owned, ghost, bs, c_void_p(device_ptr),
+                                     count, ctypes.byref(h)))
+        return cls(ctx, owned, ghost, bs, dtype, handle=h)
+
+    @property
+    def size(self) -> int:
+        return (self.owned + self.ghost) * self.bs
+
+    @property
+    def data_ptr(self) -> int:
+        return lib().owtk_vector_data(self.h) or 0
+
+    def upload(self, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        check(lib().owtk_vector_upload(self.h, _ptr(a), a.size))
+        return self
+
+    def download(self, count: int | None = None) -> np.ndarray:
+        count = self.size if count is None else count
+        out = np.empty(count, dtype=self.dtype)
+        check(lib().owtk_vector_download(self.h, _ptr(out), count))
+        return out
+
+    def fill(self, value: float, owned_only: bool = False):
+        check(lib().owtk_vector_fill(self.h, value, 1 if owned_only else 0))
+
+    def close(self):
+        if self.h is not None and self.owner:
+            lib().owtk_vector_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dot(a: Vector, b: Vector) -> float:
+    r = c_double()
+    check(lib().owtk_dot(a.h, b.h, ctypes.byref(r)))
+    return r.value
+
+
+def norm(a: Vector) -> float:
+    r = c_double()
+    check(lib().owtk_norm(a.h, ctypes.byref(r)))
+    return r.value
+
+
+def dot_batch(w: Vector, basis: list[Vector]) -> np.ndarray:
+    arr = (c_void_p * max(1, len(basis)))(*[v.h for v in basis])
+    out = (c_double * (len(basis) + 1))()
+    check(lib().owtk_dot_batch(w.h, arr, len(basis), out))
+    return np.array(out[:])
+
+
+def axpy(alpha: float, x: Vector, y: Vector):
+    check(lib().owtk_axpy(alpha, x.h, y.h))
+
+
+def scale(alpha: float, x: Vector):
+    check(lib().owtk_scale(alpha, x.h))
+
+
+def copy_owned(src: Vector, dst: Vector):
+    check(lib().owtk_copy_owned(src.h, dst.h))
+
+
+def assign_linear_combination(out: Vector, a: float, x: Vector, b: float, y: Vector):
+    check(lib().owtk_assign_linear_combination(out.h, a, x.h, b, y.h))
+
+
+class Matrix:
+    """Device matrix: kind 'bsr', 'split' (borrowed device coefficients) or 'dense'."""
+
+    def __init__(self, ctx: Context, kind: str, owned: int, ghost: int, bs: int, rowptr, cols,
+                 values=None, diag_ptr: int = 0, off_ptr: int = 0, dtype=np.float64):
+        self.ctx, self.kind, self.owned, self.ghost, self.bs = ctx, kind, owned, ghost, bs
+        self.dtype = np.dtype(dtype)
+        rp, ci = _u64(rowptr), _u64(cols)
+        if ci.size == 0:
+            ci = np.zeros(1, dtype=np.uint64)
+        h = c_void_p()
+        code = _dtype_code(dtype)
+        if kind == "bsr":
+            v = np.ascontiguousarray(values, dtype=self.dtype)
+            check(lib().owtk_bsr_create(ctx.h, code, owned, ghost, bs, _ptr(rp), _ptr(ci), _ptr(v), ctypes.byref(h)))
+        elif kind == "dense":
+            v = np.ascontiguousarray(values, dtype=self.dtype)
+            check(lib().owtk_dense_bsr_create(ctx.h, code, owned, ghost, bs, _ptr(rp), _ptr(ci), _ptr(v),
+                                              ctypes.byref(h)))
+        elif kind == "split":
+            check(lib().owtk_split_view_create(ctx.h, code, owned, ghost, bs, _ptr(rp), _ptr(ci),
+                                               c_void_p(diag_ptr), c_void_p(off_ptr), ctypes.byref(h)))
+        else:
+            raise ValueError(kind)
+        self.h = h
+
+    def update_values(self, values):
+        v = np.ascontiguousarray(values, dtype=self.dtype)
+        check(lib().owtk_bsr_update_values(self.h, _ptr(v)))
+
+    def diagonal(self) -> np.ndarray:
+        out = np.empty(self.owned * self.bs, dtype=self.dtype)
+        check(lib().owtk_matrix_diagonal(self.h, _ptr(out)))
+        return out
+
+    def apply(self, x: Vector, y: Vector):
+        check(lib().owtk_spmv(self.h, x.h, y.h))
+
+    def close(self):
+        if self.h is not None:
+            lib().owtk_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Preconditioner:
+    def __init__(self, matrix: Matrix, kind: int, parameter: float = 0.0):
+        h = c_void_p()
+        check(lib().owtk_pc_create(matrix.h, kind, parameter, ctypes.byref(h)))
+        self.h, self.matrix, self.kind = h, matrix, kind
+
+    def apply(self, x: Vector, y: Vector):
+        check(lib().owtk_pc_apply(self.h, x.h, y.h))
+
+    def update_values(self, matrix: Matrix | None = None):
+        check(lib().owtk_pc_update_values(self.h, (matrix or self.matrix).h))
+
+    @property
+    def numeric_updates(self) -> int:
+        return lib().owtk_pc_numeric_updates(self.h)
+
+    def ilu_factors(self):
+        n = c_uint64()
+        check(lib().owtk_ilu_factors(self.h, ctypes.byref(n), None, None, None, None))
+        m = self.matrix
+        rp = np.empty(m.owned + 1, dtype=np.uint64)
+        ci = np.empty(max(1, n.value), dtype=np.uint64)
+        vals = np.empty(n.value * m.bs, dtype=m.dtype)
+        inv = np.empty(m.owned * m.bs, dtype=m.dtype)
+        check(lib().owtk_ilu_factors(self.h, ctypes.byref(n), _ptr(rp), _ptr(ci), _ptr(vals), _ptr(inv)))
+        return rp, ci[:n.value], vals, inv
+
+    def levels(self):
+        m = self.matrix
+        lo = np.empty(m.owned, dtype=np.int32)
+        up = np.empty(m.owned, dtype=np.int32)
+        dl, du = c_uint64(), c_uint64()
+        check(lib().owtk_pc_levels(self.h, _ptr(lo), _ptr(up), ctypes.byref(dl), ctypes.byref(du)))
+        return lo, up, dl.value, du.value
+
+    def close(self):
+        if self.h is not None:
+            lib().owtk_pc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Workspace:
+    def __init__(self, ctx: Context):
+        h = c_void_p()
+        check(lib().owtk_workspace_create(ctx.h, ctypes.byref(h)))
+        self.h, self.ctx = h, ctx
+
+    @property
+    def allocation_epochs(self) -> int:
+        return lib().owtk_workspace_allocation_epochs(self.h)
+
+    def vector_data(self, index: int, count: int, dtype=np.float64) -> np.ndarray:
+        vh = lib().owtk_workspace_vector(self.h, index)
+        if not vh:
+            raise IndexError(index)
+        out = np.empty(count, dtype=dtype)
+        check(lib().owtk_vector_download(c_void_p(vh), _ptr(out), count))
+        return out
+
+    def close(self):
+        if self.h is not None:
+            lib().owtk_workspace_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve(kind: int, matrix: Matrix, pc: Preconditioner | None, rhs: Vector, x: Vector,
+          options: SolverOptions | None = None, workspace: Workspace | None = None) -> SolverResult:
+    o = options or default_options()
+    r = SolverResult()
+    check(lib().owtk_solve(kind, matrix.h, pc.h if pc else None, rhs.h, x.h, ctypes.byref(o),
+                           workspace.h if workspace else None, ctypes.byref(r)))
+    return r
+
+
+def solve_host(kind: int, matrix: Matrix, pc: Preconditioner | None, rhs_ptr: int, x_ptr: int,
+               options: SolverOptions | None = None, workspace: Workspace | None = None) -> SolverResult:
+    o = options or default_options()
+    r = SolverResult()
+    check(lib().owtk_solve_host(kind, matrix.h, pc.h if pc else None, c_void_p(rhs_ptr), c_void_p(x_ptr),
+                                ctypes.byref(o), workspace.h if workspace else None, ctypes.byref(r)))
+    return r
+
+
+# ---------------------------------------------------------------- host setup
+def rcm_order(owned: int, rowptr, cols, ghost: int = 0) -> np.ndarray:
+    rp, ci = _u64(rowptr), _u64(cols)
+    out = np.empty(owned, dtype=np.uint64)
+    check(lib().owtk_rcm_order(owned, ghost, _ptr(rp), _ptr(ci), _ptr(out)))
+    return out.astype(np.int64)
+
+
+def hilbert_order(xy: np.ndarray) -> np.ndarray:
+    xy = np.ascontiguousarray(xy, dtype=np.float64)
+    out = np.empty(xy.shape[0], dtype=np.uint64)
+    check(lib().owtk_hilbert_order(xy.shape[0], _ptr(xy), _ptr(out)))
+    return out.astype(np.int64)
+
+
+def inverse_permutation(p) -> np.ndarray:
+    p = _u64(p)
+    out = np.empty(p.size, dtype=np.uint64)
+    check(lib().owtk_inverse_permutation(p.size, _ptr(p), _ptr(out)))
+    return out.astype(np.int64)
+
+
+def level_sets(owned: int, rowptr, cols):
+    rp, ci = _u64(rowptr), _u64(cols)
+    lo = np.empty(owned, dtype=np.int32)
+    up = np.empty(owned, dtype=np.int32)
+    dl, du = c_uint64(), c_uint64()
+    check(lib().owtk_level_sets(owned, _ptr(rp), _ptr(ci), _ptr(lo), _ptr(up), ctypes.byref(dl), ctypes.byref(du)))
+    return lo, up, dl.value, du.value

@@ -1,0 +1,197 @@
+"""Seeded synthetic linear systems with the shapes of the benchmark configurations.
+
+Every system is a vertex graph of a triangle mesh with a ``bs``-component
+block per vertex.  The component-diagonal block-CSR matrix is built per
+component ``c`` and undirected edge ``(i, j)`` as
+
+    a_ij = -w_ij (1 + s_ij),   a_ji = -w_ij (1 - s_ij),
+    w ~ U(0.5, 1.5),  s ~ U(-0.3, 0.3),
+    a_ii = 1.05 * sum_j |a_ij| + U(0, 0.1),
+
+with rows stored in ascending column order, the diagonal included.  RNG
+streams are numpy PCG64 generators drawn in a fixed order (points, w, s,
+diagonal noise, right-hand side), so a seed pins the system on any machine.
+Point sets: jittered triangulated lattices, or Poisson-disk samples triangulated
+with Delaunay (scipy's Qhull).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_DIR = os.path.join(os.path.dirname(_HERE), "lib")
+
+
+@dataclass
+class BlockSystem:
+    """Host arrays of one system: CSR pattern (int64), values, rhs, coordinates."""
+
+    owned: int
+    bs: int
+    rowptr: np.ndarray
+    cols: np.ndarray
+    vals: np.ndarray            # component-diagonal: nnz*bs ; dense: nnz*bs*bs
+    rhs: np.ndarray
+    xy: np.ndarray | None = None
+    ghost: int = 0
+    kind: str = "bsr"           # "bsr" or "dense"
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowptr[-1])
+
+    def split(self):
+        """Split diagonal/edge view arrays: (off_rowptr, off_cols, diag, off)."""
+        bs = self.bs
+        rows = np.repeat(np.arange(self.owned), np.diff(self.rowptr))
+        is_diag = self.cols == rows
+        diag = self.vals.reshape(-1, bs)[is_diag].reshape(-1).copy()
+        off_mask = ~is_diag
+        off_cols = self.cols[off_mask].copy()
+        off = self.vals.reshape(-1, bs)[off_mask].reshape(-1).copy()
+        counts = np.bincount(rows[off_mask], minlength=self.owned)
+        off_rowptr = np.zeros(self.owned + 1, dtype=np.int64)
+        np.cumsum(counts, out=off_rowptr[1:])
+        return off_rowptr, off_cols, diag, off
+
+
+def _meshgen():
+    lib = ctypes.CDLL(os.path.join(_LIB_DIR, "libowtk_meshgen.so"))
+    lib.owtk_poisson_disk.restype = ctypes.c_longlong
+    lib.owtk_poisson_disk.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
+                                      ctypes.c_longlong, ctypes.c_void_p]
+    return lib
+
+
+def poisson_disk(target: int, domain: str, seed: int) -> np.ndarray:
+    """About ``target`` Poisson-disk points in the unit disk or the unit square."""
+    area = math.pi if domain == "disk" else 1.0
+    radius = math.sqrt(0.616 * area / target)
+    cap = int(target * 1.5) + 1024
+    buf = np.empty((cap, 2), dtype=np.float64)
+    count = _meshgen().owtk_poisson_disk(radius, 1 if domain == "disk" else 0, seed, cap,
+                                         buf.ctypes.data)
+    if count < 0:
+        raise RuntimeError("Poisson-disk buffer overflow")
+    return buf[:count].copy()
+
+
+def delaunay_edges(xy: np.ndarray) -> np.ndarray:
+    from scipy.spatial import Delaunay
+
+    tri = Delaunay(xy).simplices.astype(np.int64)
+    e = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]])
+    e.sort(axis=1)
+    key = np.unique(e[:, 0] * xy.shape[0] + e[:, 1])
+    return np.stack([key // xy.shape[0], key % xy.shape[0]], axis=1)
+
+
+def lattice(nx: int, ny: int, jitter: float, rng, aspect: float = 1.0):
+    """Jittered nx*ny lattice, every cell split along the same diagonal."""
+    hx, hy = aspect / max(nx - 1, 1), 1.0 / max(ny - 1, 1)
+    gx, gy = np.meshgrid(np.arange(nx) * hx, np.arange(ny) * hy)
+    xy = np.stack([gx.ravel(), gy.ravel()], axis=1)
+    xy += rng.uniform(-jitter, jitter, size=xy.shape) * np.array([hx, hy])
+    idx = np.arange(nx * ny).reshape(ny, nx)
+    horiz = np.stack([idx[:, :-1].ravel(), idx[:, 1:].ravel()], axis=1)
+    vert = np.stack([idx[:-1, :].ravel(), idx[1:, :].ravel()], axis=1)
+    diag = np.stack([idx[:-1, :-1].ravel(), idx[1:, 1:].ravel()], axis=1)
+    edges = np.concatenate([horiz, vert, diag]).astype(np.int64)
+    return xy, edges
+
+
+def _assemble(n: int, edges: np.ndarray, bs: int, a_fwd, a_bwd, diag):
+    """CSR (rows sorted by column) from edge coefficients and the diagonal."""
+    i, j = edges[:, 0], edges[:, 1]
+    rows = np.concatenate([np.arange(n), i, j])
+    cols = np.concatenate([np.arange(n), j, i])
+    order = np.lexsort((cols, rows))
+    rows, cols = rows[order], cols[order]
+    if bs is None:
+        vals = None
+    else:
+        vals = np.concatenate([diag, a_fwd, a_bwd])[order]
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n), out=rowptr[1:])
+    return rowptr, cols.astype(np.int64), vals
+
+
+def pattern(n: int, edges: np.ndarray):
+    rowptr, cols, _ = _assemble(n, edges, None, None, None, None)
+    return rowptr, cols
+
+
+def _coefficients(n: int, edges: np.ndarray, bs: int, rng):
+    e = edges.shape[0]
+    w = rng.uniform(0.5, 1.5, size=(e, bs))
+    s = rng.uniform(-0.3, 0.3, size=(e, bs))
+    a_fwd = -w * (1.0 + s)
+    a_bwd = -w * (1.0 - s)
+    absum = np.zeros((n, bs))
+    np.add.at(absum, edges[:, 0], np.abs(a_fwd))
+    np.add.at(absum, edges[:, 1], np.abs(a_bwd))
+    diag = 1.05 * absum + rng.uniform(0.0, 0.1, size=(n, bs))
+    return a_fwd, a_bwd, diag
+
+
+def _relabel(edges: np.ndarray, new_to_old: np.ndarray):
+    old_to_new = np.empty_like(new_to_old)
+    old_to_new[new_to_old] = np.arange(new_to_old.shape[0])
+    e = old_to_new[edges]
+    return e
+
+
+def component_diagonal_system(xy, edges, bs, rng, order: str = "natural") -> BlockSystem:
+    """Coefficients as documented above; optional RCM or Hilbert relabelling."""
+    n = xy.shape[0]
+    a_fwd, a_bwd, diag = _coefficients(n, edges, bs, rng)
+    rhs = rng.uniform(-1.0, 1.0, size=n * bs)
+    meta = {"order": order}
+    if order != "natural":
+        from . import native
+        if order == "rcm":
+            rp, cp = pattern(n, edges)
+            new_to_old = native.rcm_order(n, rp, cp)
+        elif order == "hilbert":
+            new_to_old = native.hilbert_order(xy)
+        else:
+            raise ValueError(order)
+        edges = _relabel(edges, new_to_old)
+        flip = edges[:, 0] > edges[:, 1]
+        a_fwd, a_bwd = np.where(flip[:, None], a_bwd, a_fwd), np.where(flip[:, None], a_fwd, a_bwd)
+        edges = np.sort(edges, axis=1)
+        diag = diag[new_to_old]
+        rhs = rhs.reshape(n, bs)[new_to_old].reshape(-1)
+        xy = xy[new_to_old]
+    rowptr, cols, vals = _assemble(n, edges, bs, a_fwd, a_bwd, diag)
+    return BlockSystem(n, bs, rowptr, cols, np.ascontiguousarray(vals).reshape(-1), rhs, xy,
+                       meta=meta)
+
+
+def config0(seed: int = 0, side: int = 64, bs: int = 3) -> BlockSystem:
+    """64x64 jittered triangulated lattice (4096 vertices), bs 3."""
+    rng = np.random.default_rng(seed)
+    xy, edges = lattice(side, side, 0.2, rng)
+    sysm = component_diagonal_system(xy, edges, bs, rng)
+    sysm.meta.update(config="lattice-64x64-bs3", seed=seed)
+    return sysm
+
+
+def disk_mesh(n_target: int, seed: int, domain: str = "disk"):
+    xy = poisson_disk(n_target, domain, seed)
+    return xy, delaunay_edges(xy)
+
+
+def config1(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm") -> BlockSystem:
+    """Poisson-disk points in the unit disk, Delaunay, RCM-ordered, bs 3."""
+    xy, edges = disk_mesh(n_target, seed)
+    rng = np.random.default_rng(seed)
+    sysm = component_diagonal_system(xy, edges, bs, rng, order=order)
+    sysm.meta.update(config=f"poisson-disk-{xy.shape[0]}-delaunay-{order}-bs{bs}", seed=seed)
+    return sysm
