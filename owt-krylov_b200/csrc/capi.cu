@@ -76,7 +76,7 @@ void Context::check_device_status()
     if (word & dev::kErrSingularDiagonal) fail(OWTK_ERR_INVALID_ARGUMENT, "singular diagonal");
 }
 
-void Workspace::prepare(const Vector& layout, std::size_t count)
+void Workspace::prepare(const Vector& layout, std::size_t count, std::size_t scalars)
 {
     const bool changed = vectors.empty() || !vectors.front()->same_layout(layout)
         || vectors.front()->dtype != layout.dtype;
@@ -94,6 +94,10 @@ void Workspace::prepare(const Vector& layout, std::size_t count)
             v->data = v->storage.ptr;
             vectors.push_back(std::move(v));
         }
+        ++epochs;
+    }
+    if (scalar_capacity < scalars) {
+        scalar_capacity = scalars;
         ++epochs;
     }
 }
@@ -239,6 +243,7 @@ void ilu_symbolic(Preconditioner& p, const Matrix& m, std::size_t fill)
     p.d_upd_upper = upload(s, upper);
     p.d_fvalues.allocate(nnz * p.bs * dsize(p.dtype) + 16);
     p.inv_diag.allocate(n * p.bs * dsize(p.dtype) + 16);
+    p.work.allocate(n * p.bs * dsize(p.dtype) + 16);   // forward-sweep result of an apply
     std::vector<std::int32_t> lower_level, upper_level;
     levels_of(n, p.f_rowptr.data(), p.f_cols.data(), lower_level, upper_level);
     build_sweep(*p.ctx, p.lower, n, p.bs, lower_level, false);

@@ -330,7 +330,8 @@ __global__ void __launch_bounds__(kThreads) k_gmres_update(std::size_t n, int k,
 unsigned reduce_blocks(const Context& c, std::size_t n)
 {
     const std::size_t want = (n + kThreads * 8 - 1) / (kThreads * 8);
-    const std::size_t cap = static_cast<std::size_t>(c.sm_count) * 4;
+    std::size_t cap = static_cast<std::size_t>(c.sm_count) * 4;
+    if (cap > static_cast<std::size_t>(kReduceBlocks)) cap = kReduceBlocks;
     return static_cast<unsigned>(want < 1 ? 1 : (want > cap ? cap : want));
 }
 
@@ -655,17 +656,15 @@ template<class T> void multidot(Context& c, std::size_t n, int k, const T* const
 template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T* const* basis,
                                       const double* h, T* w, double* out_dev, double* out_host)
 {
-    if (k + 1 > kMaxBatch) fail(OWTK_ERR_INVALID_ARGUMENT, "Gram-Schmidt batch too large");
+    if (k + 1 > 32) fail(OWTK_ERR_INVALID_ARGUMENT, "fused Gram-Schmidt pass takes at most 31 basis vectors");
     const unsigned blocks = reduce_blocks(c, n);
     const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
     if (k + 1 <= 8)
         k_cgs_update_dot<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     else if (k + 1 <= 16)
         k_cgs_update_dot<T, 16><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
-    else if (k + 1 <= 32)
-        k_cgs_update_dot<T, 32><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     else
-        k_cgs_update_dot<T, kMaxBatch><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_cgs_update_dot<T, 32><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }

@@ -3,14 +3,13 @@
 //
 // Work unit: a row tile (consecutive rows whose value stream fits kStage
 // elements; built once per matrix on the host).  One CTA per tile:
-//   1. stage the tile's column indices and row offsets in shared memory
-//      (coalesced loads);
-//   2. product phase: thread k of the tile's value stream loads value k
-//      (consecutive threads, consecutive addresses: the whole value stream is
-//      read exactly once, fully coalesced), gathers x[col][c] (L2-resident for
+//   1. product phase: thread k of the tile's value stream loads value k and
+//      its column (consecutive threads, consecutive addresses: the value
+//      stream is read exactly once, fully coalesced, with every thread's
+//      loads issued together), then gathers x[col][c] (L2-resident for
 //      RCM/Hilbert-ordered meshes) and stores the rounded product in shared
 //      memory;
-//   3. output phase: thread o owns output (row, c) and adds that row's
+//   2. output phase: thread o owns output (row, c) and adds that row's
 //      products in entry order, writing y coalesced.
 // The sum starts from +0 (or diag*x for the split view) and adds rounded
 // products in entry order, which is the reference's sequence
@@ -27,8 +26,8 @@ namespace {
 
 using namespace dev;
 
-constexpr int kStage = 2048;      // staged values (products) per tile
-constexpr int kRowCap = 512;      // rows per tile
+constexpr int kStage = 1024;      // staged values (products) per tile: 4 per thread
+constexpr int kRowCap = 1024;     // rows per tile (outputs are bounded by kStage too)
 
 template<class T>
 struct SpmvArgs {
@@ -50,18 +49,17 @@ __device__ __forceinline__ int div_bs(int k, unsigned long long magic)
 
 // KIND 0: component-diagonal BSR, 1: split view, 2: dense BSR.
 template<class T, int KIND>
-__global__ void __launch_bounds__(kThreads) k_spmv_tiles(SpmvArgs<T> a)
+__global__ void __launch_bounds__(kThreads, 8) k_spmv_tiles(SpmvArgs<T> a)
 {
+    constexpr int kPer = kStage / kThreads;   // staged units per thread
     __shared__ T prod[kStage];
-    __shared__ int scol[kStage];
-    __shared__ int srp[kRowCap + 1];
     const int tile = blockIdx.x;
     const int r0 = a.tile_rows[tile], r1 = a.tile_rows[tile + 1];
     const int e0 = a.rowptr[r0], e1 = a.rowptr[r1];
     const int bs = a.bs;
     const int units = (e1 - e0) * bs;   // products (KIND 0/1) or block-row contributions (KIND 2)
 
-    if (units > kStage || r1 - r0 > kRowCap) {
+    if (units > kStage || (r1 - r0) * bs > kStage) {
         // Long tile: one row; threads over components.
         for (int r = r0; r < r1; ++r) {
             const int b0 = a.rowptr[r], b1 = a.rowptr[r + 1];
@@ -86,40 +84,62 @@ __global__ void __launch_bounds__(kThreads) k_spmv_tiles(SpmvArgs<T> a)
         return;
     }
 
-    for (int k = threadIdx.x; k < e1 - e0; k += kThreads) scol[k] = a.cols[e0 + k];
-    for (int k = threadIdx.x; k <= r1 - r0; k += kThreads) srp[k] = a.rowptr[r0 + k] - e0;
-    __syncthreads();
+    // Row bounds of this thread's outputs, loaded early (independent of the products).
+    const int outs = (r1 - r0) * bs;
+    int ob[kPer], oe[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int o = threadIdx.x + j * kThreads;
+        if (o < outs) {
+            const int rl = div_bs(o, a.magic);
+            ob[j] = a.rowptr[r0 + rl] - e0;
+            oe[j] = a.rowptr[r0 + rl + 1] - e0;
+        }
+    }
 
     if (KIND == 2) {
         // Contribution of entry e to block row br: sum_bc B[e][br][bc] x[col][bc].
         for (int k = threadIdx.x; k < units; k += kThreads) {
             const int e = div_bs(k, a.magic);
-            const int br = k - e * bs;
             const T* blk = a.vals + (static_cast<std::size_t>(e0) * bs + k) * bs;
-            const T* xs = a.x + static_cast<std::size_t>(scol[e]) * bs;
+            const T* xs = a.x + static_cast<std::size_t>(a.cols[e0 + e]) * bs;
             T contribution = 0;
             for (int bc = 0; bc < bs; ++bc) contribution = add_rn(contribution, mul_rn(blk[bc], xs[bc]));
             prod[k] = contribution;
-            (void)br;
         }
     } else {
+        // All value and column loads first, then all x gathers: kPer
+        // independent requests in flight per thread at each step.
         const T* v = a.vals + static_cast<std::size_t>(e0) * bs;
-        for (int k = threadIdx.x; k < units; k += kThreads) {
-            const int e = div_bs(k, a.magic);
-            const int c = k - e * bs;
-            prod[k] = mul_rn(v[k], a.x[static_cast<std::size_t>(scol[e]) * bs + c]);
+        T pv[kPer];
+        int px[kPer];   // element index col*bs + c (the plan checks it fits in 31 bits)
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            if (k < units) {
+                const int e = div_bs(k, a.magic);
+                pv[j] = __ldcs(v + k);
+                px[j] = __ldg(a.cols + e0 + e) * bs + (k - e * bs);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            if (k < units) prod[k] = mul_rn(pv[j], __ldg(a.x + px[j]));
         }
     }
     __syncthreads();
 
-    const int outs = (r1 - r0) * bs;
     const std::size_t ybase = static_cast<std::size_t>(r0) * bs;
-    for (int o = threadIdx.x; o < outs; o += kThreads) {
-        const int rl = div_bs(o, a.magic);
-        const int c = o - rl * bs;
-        T acc = KIND == 1 ? mul_rn(a.diag[ybase + o], a.x[ybase + o]) : T(0);
-        for (int e = srp[rl]; e < srp[rl + 1]; ++e) acc = add_rn(acc, prod[e * bs + c]);
-        a.y[ybase + o] = acc;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int o = threadIdx.x + j * kThreads;
+        if (o < outs) {
+            const int c = o - div_bs(o, a.magic) * bs;
+            T acc = KIND == 1 ? mul_rn(a.diag[ybase + o], a.x[ybase + o]) : T(0);
+            for (int e = ob[j]; e < oe[j]; ++e) acc = add_rn(acc, prod[e * bs + c]);
+            a.y[ybase + o] = acc;
+        }
     }
 }
 
@@ -210,6 +230,8 @@ template void gather_values<float>(Context&, std::size_t, std::size_t, const std
 void build_tile_plan(Matrix& m)
 {
     const int bs = static_cast<int>(m.bs);
+    if ((m.owned + m.ghost) * m.bs >= (1ull << 31))
+        fail(OWTK_ERR_INVALID_ARGUMENT, "vector too large for 32-bit element indices");
     std::vector<std::int32_t> tiles{0};
     int units = 0, rows = 0;
     for (std::size_t r = 0; r < m.owned; ++r) {

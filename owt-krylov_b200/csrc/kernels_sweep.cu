@@ -5,19 +5,27 @@
 // apply): rows are ordered by (level, row) and cut into warp tasks of up to
 // 32/bs rows from a single level, so rows inside a task never depend on each
 // other.  Warps take tasks in order from a monotone 64-bit ticket; a task's
-// lanes are (row, component) pairs.  Before reading a dependency a lane waits
-// for that row's epoch flag (acquire); after a task's rows are written the
-// warp publishes their flags (fence + release).  Every dependency lies in an
-// earlier task, held by a warp that is already running, so the sweep always
-// makes progress; each wait is still bounded (kSpinLimit polls) and a wait
-// that gives up sets the timeout bit of the device status word and carries
-// on, so a kernel can never hang the GPU.
+// lanes are (row, component) pairs.  Every dependency lies in an earlier task,
+// held by a warp that is already running, so a sweep always makes progress.
+//
+// Applies (ILU and SSOR sweeps) synchronise on the data itself: the sweep's
+// output is first filled with a signalling-NaN sentinel that no arithmetic
+// result can equal (NaN results are stored as the canonical quiet NaN), and a
+// lane reads a dependency with a relaxed 8-byte load until it is no longer
+// the sentinel.  One load both waits and fetches, so a level costs about one
+// L2 round trip.  The numeric factorisation, which updates factor entries in
+// place, publishes per-row epoch flags instead (fence + release / relaxed
+// loads + fence).  Every wait is bounded (kSpinLimit polls): a wait that gives
+// up sets the timeout bit of the device status word and carries on, and later
+// waits of the launch then return at once, so a kernel can never hang the GPU.
 //
 // Per (row, component) the arithmetic is the reference's, term by term and
 // in entry order, with explicit rounding (device_common.cuh), so results equal
 // the CPU path bit for bit whatever order the rows complete in.
 
 #include <cfloat>
+#include <cmath>
+#include <cstdlib>
 
 #include "device_common.cuh"
 #include "owtk_internal.h"
@@ -58,80 +66,196 @@ struct SweepArgs {
     const int* upd_upper;
 };
 
-__device__ __forceinline__ void wait_row(const unsigned* flags, int row, unsigned epoch, unsigned* status)
+constexpr int kChunk = 8;   // dependency entries handled per unrolled step
+
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p)
 {
-    if (ld_acquire(flags + row) == epoch) return;
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template<class T> struct Bits;
+template<> struct Bits<double> {
+    using U = unsigned long long;
+    static constexpr U kSentinel = 0x7ff0dead5eed0badull;   // signalling NaN
+    static constexpr U kQuietNan = 0x7ff8000000000000ull;
+};
+template<> struct Bits<float> {
+    using U = unsigned;
+    static constexpr U kSentinel = 0x7f80deadu;              // signalling NaN
+    static constexpr U kQuietNan = 0x7fc00000u;
+};
+
+__device__ __forceinline__ unsigned long long ld_relaxed_bits(const double* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_relaxed_bits(const float* p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v)
+{
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(float* p, float v)
+{
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ double from_bits(unsigned long long u) { return __longlong_as_double(static_cast<long long>(u)); }
+__device__ __forceinline__ float from_bits(unsigned u) { return __uint_as_float(u); }
+
+// Publish a sweep result: NaN is stored canonically so it can never equal the sentinel.
+template<class T>
+__device__ __forceinline__ void publish(T* p, T v)
+{
+    if (v != v) v = from_bits(Bits<T>::kQuietNan);
+    st_relaxed(p, v);
+}
+
+// Bounded wait for a dependency value that is still the sentinel.
+template<class T>
+__device__ __noinline__ T spin_value(const T* p, unsigned* status)
+{
+    using U = typename Bits<T>::U;
     for (int it = 0; it < kSpinLimit; ++it) {
-        __nanosleep(32);
-        if (ld_acquire(flags + row) == epoch) return;
+        const U v = ld_relaxed_bits(p);
+        if (v != Bits<T>::kSentinel) return from_bits(v);
+        if (it >= 256) __nanosleep(32);
+        if ((it & 1023) == 1023 && (*reinterpret_cast<volatile unsigned*>(status) & kErrTimeout))
+            return from_bits(v);
     }
     atomicOr(status, kErrTimeout);
+    return from_bits(Bits<T>::kQuietNan);
+}
+
+template<class T>
+__global__ void k_fill_sentinel(std::size_t n, T* x)
+{
+    const std::size_t i = static_cast<std::size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) reinterpret_cast<typename Bits<T>::U*>(x)[i] = Bits<T>::kSentinel;
+}
+
+// Bounded spin on one dependency flag.  Once any wait of the launch has given
+// up (status timeout bit), later waits return at once, so a sweep with a
+// broken schedule ends after one timeout instead of one per dependency.
+__device__ __noinline__ void spin_until(const unsigned* flag, unsigned epoch, unsigned* status)
+{
+    for (int it = 0; it < kSpinLimit; ++it) {
+        if (ld_relaxed(flag) == epoch) return;
+        if (it >= 256) __nanosleep(64);
+        if ((it & 1023) == 1023 && (*reinterpret_cast<volatile unsigned*>(status) & kErrTimeout)) return;
+    }
+    atomicOr(status, kErrTimeout);
+}
+
+// Wait until every dependency of a row is published.  `filter`: 0 all
+// entries of [b, e) are dependencies (ILU factor rows), 1 columns < row
+// (SSOR forward), 2 row < column < owned (SSOR backward).  Flags are loaded
+// kChunk at a time with relaxed loads; one fence afterwards gives acquire
+// ordering for the dependency values read next.
+template<int FILTER>
+__device__ __forceinline__ void wait_deps(const unsigned* flags, const int* cols, int b, int e, int row,
+                                          int owned, unsigned epoch, unsigned* status)
+{
+    for (int k0 = b; k0 < e; k0 += kChunk) {
+        int cc[kChunk];
+        unsigned f[kChunk];
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) {
+            int c = k0 + j < e ? cols[k0 + j] : -1;
+            if (FILTER == 1 && c >= row) c = -1;
+            if (FILTER == 2 && (c <= row || c >= owned)) c = -1;
+            cc[j] = c;
+        }
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) f[j] = cc[j] >= 0 ? ld_relaxed(flags + cc[j]) : epoch;
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j)
+            if (f[j] != epoch) spin_until(flags + cc[j], epoch, status);
+    }
+    __threadfence();
 }
 
 template<class T> __device__ __forceinline__ T pivot_tolerance();
 template<> __device__ __forceinline__ double pivot_tolerance<double>() { return 64.0 * DBL_EPSILON; }
 template<> __device__ __forceinline__ float pivot_tolerance<float>() { return 64.0f * FLT_EPSILON; }
 
+// y -= sum_e vals[e][c] * dep[col_e][c] over e in [b, e) in entry order;
+// FILTER as in wait_deps, OMEGA multiplies each coefficient first (SSOR).
+// POLL: dependency values are read with relaxed loads and waited on until
+// they differ from the sentinel (applies); otherwise they are already final
+// (the caller waited on flags) and read through L2.
+template<class T, int FILTER, bool OMEGA, bool POLL>
+__device__ __forceinline__ T eliminate(T y, const SweepArgs<T>& a, const T* dep, int b, int e, int row, int c)
+{
+    using U = typename Bits<T>::U;
+    const int bs = a.bs;
+    for (int k0 = b; k0 < e; k0 += kChunk) {
+        T fv[kChunk], xv[kChunk];
+        bool on[kChunk];
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) {
+            const int k = k0 + j;
+            int col = k < e ? a.cols[k] : -1;
+            if (FILTER == 1 && col >= row) col = -1;
+            if (FILTER == 2 && (col <= row || col >= a.owned)) col = -1;
+            on[j] = col >= 0;
+            if (on[j]) {
+                fv[j] = a.vals[static_cast<std::size_t>(k) * bs + c];
+                const T* src = dep + static_cast<std::size_t>(col) * bs + c;
+                if (POLL) {
+                    const U bits = ld_relaxed_bits(src);
+                    xv[j] = bits != Bits<T>::kSentinel ? from_bits(bits) : spin_value(src, a.status);
+                } else {
+                    xv[j] = __ldcg(src);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) {
+            if (on[j]) {
+                const T coef = OMEGA ? mul_rn(a.omega, fv[j]) : fv[j];
+                y = sub_rn(y, mul_rn(coef, xv[j]));
+            }
+        }
+    }
+    return y;
+}
+
 template<class T, int MODE>
 __device__ __forceinline__ void row_body(const SweepArgs<T>& a, int row, int c0, int cstep)
 {
     const int bs = a.bs;
     const std::size_t rb = static_cast<std::size_t>(row) * bs;
-    if (MODE == kIluForward) {
+    if (MODE == kIluForward) {          // in -> work (unit lower solve)
         const int b = a.rowptr[row], d = a.diagpos[row];
-        for (int e = b; e < d; ++e) wait_row(a.flags, a.cols[e], a.epoch, a.status);
-        for (int c = c0; c < bs; c += cstep) {
-            T y = a.in[rb + c];
-            for (int e = b; e < d; ++e)
-                y = sub_rn(y, mul_rn(a.vals[static_cast<std::size_t>(e) * bs + c],
-                                     __ldcg(a.out + static_cast<std::size_t>(a.cols[e]) * bs + c)));
-            a.out[rb + c] = y;
-        }
-    } else if (MODE == kIluBackward) {
+        for (int c = c0; c < bs; c += cstep)
+            publish(a.work + rb + c, eliminate<T, 0, false, true>(a.in[rb + c], a, a.work, b, d, row, c));
+    } else if (MODE == kIluBackward) {  // work -> out (upper solve, times the inverse diagonal)
         const int d = a.diagpos[row], end = a.rowptr[row + 1];
-        for (int e = d + 1; e < end; ++e) wait_row(a.flags, a.cols[e], a.epoch, a.status);
-        for (int c = c0; c < bs; c += cstep) {
-            T x = a.out[rb + c];
-            for (int e = d + 1; e < end; ++e)
-                x = sub_rn(x, mul_rn(a.vals[static_cast<std::size_t>(e) * bs + c],
-                                     __ldcg(a.out + static_cast<std::size_t>(a.cols[e]) * bs + c)));
-            a.out[rb + c] = mul_rn(x, a.inv[rb + c]);
-        }
-    } else if (MODE == kSsorForward) {
+        for (int c = c0; c < bs; c += cstep)
+            publish(a.out + rb + c,
+                    mul_rn(eliminate<T, 0, false, true>(a.work[rb + c], a, a.out, d + 1, end, row, c), a.inv[rb + c]));
+    } else if (MODE == kSsorForward) {  // in -> work
         const int b = a.rowptr[row], end = a.rowptr[row + 1];
-        for (int e = b; e < end; ++e) {
-            const int col = a.cols[e];
-            if (col < row) wait_row(a.flags, col, a.epoch, a.status);
-        }
-        for (int c = c0; c < bs; c += cstep) {
-            T y = a.in[rb + c];
-            for (int e = b; e < end; ++e) {
-                const int col = a.cols[e];
-                if (col >= row || col >= a.owned) continue;
-                y = sub_rn(y, mul_rn(mul_rn(a.omega, a.vals[static_cast<std::size_t>(e) * bs + c]),
-                                     __ldcg(a.work + static_cast<std::size_t>(col) * bs + c)));
-            }
-            a.work[rb + c] = div_rn(y, a.diag[rb + c]);
-        }
-    } else if (MODE == kSsorBackward) {
+        for (int c = c0; c < bs; c += cstep)
+            publish(a.work + rb + c,
+                    div_rn(eliminate<T, 1, true, true>(a.in[rb + c], a, a.work, b, end, row, c), a.diag[rb + c]));
+    } else if (MODE == kSsorBackward) { // work -> out
         const int b = a.rowptr[row], end = a.rowptr[row + 1];
-        for (int e = b; e < end; ++e) {
-            const int col = a.cols[e];
-            if (col > row && col < a.owned) wait_row(a.flags, col, a.epoch, a.status);
-        }
         for (int c = c0; c < bs; c += cstep) {
-            T z = mul_rn(a.diag[rb + c], a.work[rb + c]);
-            for (int e = b; e < end; ++e) {
-                const int col = a.cols[e];
-                if (col <= row || col >= a.owned) continue;
-                z = sub_rn(z, mul_rn(mul_rn(a.omega, a.vals[static_cast<std::size_t>(e) * bs + c]),
-                                     __ldcg(a.out + static_cast<std::size_t>(col) * bs + c)));
-            }
-            a.out[rb + c] = div_rn(z, a.diag[rb + c]);
+            const T z0 = mul_rn(a.diag[rb + c], a.work[rb + c]);
+            publish(a.out + rb + c, div_rn(eliminate<T, 2, true, true>(z0, a, a.out, b, end, row, c), a.diag[rb + c]));
         }
     } else {  // kIluFactor: IKJ elimination of one row (preconditioner.hpp:442-469)
         const int b = a.rowptr[row], d = a.diagpos[row];
-        for (int l = b; l < d; ++l) wait_row(a.flags, a.cols[l], a.epoch, a.status);
+        wait_deps<0>(a.flags, a.cols, b, d, row, a.owned, a.epoch, a.status);
         const T tol = pivot_tolerance<T>();
         for (int c = c0; c < bs; c += cstep) {
             for (int l = b; l < d; ++l) {
@@ -158,43 +282,64 @@ __global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T> a)
 {
     const int lane = threadIdx.x & 31;
     const int bs = a.bs;
+    int rl, c0, cstep;
+    if (bs <= 32) {
+        rl = lane / bs;
+        c0 = lane - rl * bs;
+        cstep = bs;
+    } else {
+        rl = 0;
+        c0 = lane;
+        cstep = 32;
+    }
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(a.ticket, 1ull) - a.base;
     for (;;) {
-        unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(a.ticket, 1ull) - a.base;
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= static_cast<unsigned long long>(a.tasks)) break;
+        // Reserve the next task now; the atomic's latency overlaps this task.
+        unsigned long long next = 0;
+        if (lane == 0) next = atomicAdd(a.ticket, 1ull) - a.base;
         const int s = a.task_start[t], nrows = a.task_start[t + 1] - s;
-        int rl, c0, cstep;
-        if (bs <= 32) {
-            rl = lane / bs;
-            c0 = lane - rl * bs;
-            cstep = bs;
-        } else {
-            rl = 0;
-            c0 = lane;
-            cstep = 32;
+        const int row = rl < nrows ? a.order[s + rl] : -1;
+        if (row >= 0) row_body<T, MODE>(a, row, c0, cstep);
+        if (MODE == kIluFactor) {
+            __syncwarp();
+            if (lane < nrows) {
+                __threadfence();
+                st_release(a.flags + a.order[s + lane], a.epoch);
+            }
         }
-        if (rl < nrows) row_body<T, MODE>(a, a.order[s + rl], c0, cstep);
-        __syncwarp();
-        if (lane < nrows) {
-            __threadfence();
-            st_release(a.flags + a.order[s + lane], a.epoch);
-        }
+        t = next;
     }
+}
+
+// Warps per sweep launch: enough to hold a few levels' worth of tasks in
+// flight.  More warps only add polling traffic on the dependency flags while
+// the sweep is bound by its level-to-level latency.
+int sweep_warps(const Context& c, const Sweep& s)
+{
+    const char* env = std::getenv("OWTK_SWEEP_WARPS_PER_LEVEL");
+    const double factor = env ? std::atof(env) : 4.0;
+    const double per_level = s.depth > 0 ? static_cast<double>(s.tasks) / s.depth : s.tasks;
+    long long warps = factor > 0 ? static_cast<long long>(std::ceil(factor * per_level)) : s.tasks;
+    const long long cap = static_cast<long long>(c.sm_count) * 64;
+    if (warps < 32) warps = 32;
+    if (warps > cap) warps = cap;
+    if (warps > s.tasks) warps = s.tasks;
+    return static_cast<int>(warps);
 }
 
 template<class T, int MODE>
 void launch(Context& c, Preconditioner& p, Sweep& s, SweepArgs<T>& a)
 {
     if (s.tasks == 0) return;
-    if (++p.epoch == 0xffffffffu) {
+    if (MODE == kIluFactor && ++p.epoch == 0xffffffffu) {
         OWTK_CUDA(cudaMemsetAsync(p.flags.ptr, 0, p.owned * sizeof(unsigned), c.stream));
         p.epoch = 1;
     }
     const int warps_per_block = kThreads / 32;
-    int blocks = (s.tasks + warps_per_block - 1) / warps_per_block;
-    const int cap = c.sm_count * 8;
-    if (blocks > cap) blocks = cap;
+    const int blocks = (sweep_warps(c, s) + warps_per_block - 1) / warps_per_block;
     a.order = s.order.as<int>();
     a.task_start = s.task_start.as<int>();
     a.tasks = s.tasks;
@@ -232,6 +377,16 @@ template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* mat
     launch<T, kIluFactor>(c, p, p.lower, a);
 }
 
+template<class T> void fill_sentinel(Context& c, std::size_t n, T* x)
+{
+    if (n == 0) return;
+    k_fill_sentinel<T><<<static_cast<unsigned>((n + 255) / 256), 256, 0, c.stream>>>(n, x);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+// preconditioner.hpp:320-363.  The forward result goes to the PC's work
+// vector, so in == out is allowed: `in` is fully read before `out` is reset.
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out)
 {
     SweepArgs<T> a{};
@@ -242,7 +397,11 @@ template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* 
     a.inv = p.inv_diag.as<T>();
     a.in = in;
     a.out = out;
+    a.work = p.work.as<T>();
+    const std::size_t n = p.owned * p.bs;
+    fill_sentinel<T>(c, n, a.work);
     launch<T, kIluForward>(c, p, p.lower, a);
+    fill_sentinel<T>(c, n, out);
     launch<T, kIluBackward>(c, p, p.upper, a);
 }
 
@@ -258,7 +417,10 @@ template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T*
     a.out = out;
     a.work = p.work.as<T>();
     a.omega = static_cast<T>(p.parameter);
+    const std::size_t n = p.owned * p.bs;
+    fill_sentinel<T>(c, n, a.work);
     launch<T, kSsorForward>(c, p, p.lower, a);
+    fill_sentinel<T>(c, n, out);
     launch<T, kSsorBackward>(c, p, p.upper, a);
     const T omega = static_cast<T>(p.parameter);
     if (omega != T(1)) scale<T>(c, p.owned * p.bs, omega * (T(2) - omega), out);

@@ -53,8 +53,8 @@ DeviceBuffer upload(cudaStream_t s, const std::vector<T>& host)
 // ---------------------------------------------------------------- context
 // Scalar results of reductions land in a mapped pinned block the host reads
 // after one stream synchronisation.
-constexpr int kScalarSlots = 256;
-constexpr int kMaxBatch = 40;            // largest dot batch (restart + 2)
+constexpr int kScalarSlots = 512;
+constexpr int kMaxBatch = 128;           // largest dot batch (GMRES restart + 2)
 constexpr int kReduceBlocks = 4 * 148;   // two-stage reductions: max first-stage blocks
 
 struct Context {
@@ -160,8 +160,11 @@ struct Workspace {
     Context* ctx = nullptr;
     std::vector<std::unique_ptr<Vector>> vectors;
     std::vector<std::unique_ptr<Vector>> stage;   // host-buffer solve staging (rhs, x)
+    std::size_t scalar_capacity = 0;              // host scalar arrays (Hessenberg etc.)
     std::uint64_t epochs = 0;
-    void prepare(const Vector& layout, std::size_t count);
+    // core.hpp:405-423: (re)allocate when the layout changes or more vectors /
+    // scalars are needed; each growth counts one allocation epoch.
+    void prepare(const Vector& layout, std::size_t count, std::size_t scalars = 0);
 };
 
 // ---------------------------------------------------------------- setup (setup.cpp)

@@ -29,8 +29,8 @@ enum Reason {
 
 // Scalar slots in the context's mapped block.
 constexpr int kSlotA = 0;      // first reduction batch
-constexpr int kSlotB = 64;     // second Gram-Schmidt batch
-constexpr int kSlotCoef = 128; // coefficients uploaded for update kernels
+constexpr int kSlotB = 128;    // second Gram-Schmidt batch
+constexpr int kSlotCoef = 256; // coefficients uploaded for update kernels
 
 template<class T>
 struct Engine {
@@ -511,7 +511,8 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
     const auto& o = e.o;
     const std::size_t R = o.restart;
     if (R + 2 > static_cast<std::size_t>(kMaxBatch)) fail(OWTK_ERR_INVALID_ARGUMENT, "restart too large");
-    ws.prepare(b, 2 + (R + 1) + R);
+    // krylov_solvers.hpp:183-201: vectors and the scalar block it sizes.
+    ws.prepare(b, 2 + (R + 1) + R, (R + 1) * R + R + R + (R + 1) + (R + 2) + (R + 2));
     Vector& r = *ws.vectors[0];
     Vector& w = *ws.vectors[1];
     std::vector<Vector*> V(R + 1), Z(R);
@@ -558,9 +559,20 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
                 kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(kSlotA), e.hslot(kSlotA));
             }
             if (iterated) {
-                // w -= V h1, fused with the second batch; then w -= V h2.
-                kern::cgs_update_dot<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w),
-                                        e.dslot(kSlotB), e.hslot(kSlotB));
+                // w -= V h1, fused with the second batch (one pass over V while
+                // the batch fits the fused kernel); then w -= V h2.
+                if (k + 1 <= 32) {
+                    kern::cgs_update_dot<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w),
+                                            e.dslot(kSlotB), e.hslot(kSlotB));
+                } else {
+                    kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w));
+                    const T* pa[kMaxBatch];
+                    const T* pb[kMaxBatch];
+                    for (std::size_t j = 0; j < k; ++j) { pa[j] = e.p(w); pb[j] = vptr[j]; }
+                    pa[k] = e.p(w);
+                    pb[k] = e.p(w);
+                    kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(kSlotB), e.hslot(kSlotB));
+                }
                 kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotB), e.p(w));
             } else {
                 kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w));

@@ -111,7 +111,7 @@ def _assemble(n: int, edges: np.ndarray, bs: int, a_fwd, a_bwd, diag):
     i, j = edges[:, 0], edges[:, 1]
     rows = np.concatenate([np.arange(n), i, j])
     cols = np.concatenate([np.arange(n), j, i])
-    order = np.lexsort((cols, rows))
+    order = np.argsort(rows * np.int64(n) + cols, kind="stable")
     rows, cols = rows[order], cols[order]
     if bs is None:
         vals = None
@@ -133,9 +133,10 @@ def _coefficients(n: int, edges: np.ndarray, bs: int, rng):
     s = rng.uniform(-0.3, 0.3, size=(e, bs))
     a_fwd = -w * (1.0 + s)
     a_bwd = -w * (1.0 - s)
-    absum = np.zeros((n, bs))
-    np.add.at(absum, edges[:, 0], np.abs(a_fwd))
-    np.add.at(absum, edges[:, 1], np.abs(a_bwd))
+    absum = np.empty((n, bs))
+    for c in range(bs):
+        absum[:, c] = (np.bincount(edges[:, 0], weights=np.abs(a_fwd[:, c]), minlength=n)
+                       + np.bincount(edges[:, 1], weights=np.abs(a_bwd[:, c]), minlength=n))
     diag = 1.05 * absum + rng.uniform(0.0, 0.1, size=(n, bs))
     return a_fwd, a_bwd, diag
 
@@ -188,10 +189,63 @@ def disk_mesh(n_target: int, seed: int, domain: str = "disk"):
     return xy, delaunay_edges(xy)
 
 
+def _cached(key: str, build):
+    """Optional on-disk cache (directory in OWTK_CACHE_DIR) for large systems."""
+    root = os.environ.get("OWTK_CACHE_DIR")
+    if not root:
+        return build()
+    path = os.path.join(root, key + ".npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        return BlockSystem(int(d["owned"]), int(d["bs"]), d["rowptr"], d["cols"], d["vals"], d["rhs"], d["xy"],
+                           meta={"cached": path})
+    s = build()
+    os.makedirs(root, exist_ok=True)
+    np.savez(path, owned=s.owned, bs=s.bs, rowptr=s.rowptr, cols=s.cols, vals=s.vals, rhs=s.rhs, xy=s.xy)
+    return s
+
+
 def config1(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm") -> BlockSystem:
     """Poisson-disk points in the unit disk, Delaunay, RCM-ordered, bs 3."""
-    xy, edges = disk_mesh(n_target, seed)
-    rng = np.random.default_rng(seed)
-    sysm = component_diagonal_system(xy, edges, bs, rng, order=order)
-    sysm.meta.update(config=f"poisson-disk-{xy.shape[0]}-delaunay-{order}-bs{bs}", seed=seed)
+    def build():
+        xy, edges = disk_mesh(n_target, seed)
+        rng = np.random.default_rng(seed)
+        return component_diagonal_system(xy, edges, bs, rng, order=order)
+
+    sysm = _cached(f"disk-{n_target}-{seed}-{bs}-{order}", build)
+    sysm.meta.update(config=f"poisson-disk-{sysm.owned}-delaunay-{order}-bs{bs}", seed=seed)
     return sysm
+
+
+def dense_block_system(xy, edges, bs: int, rng, order: str = "natural") -> BlockSystem:
+    """Dense bs x bs blocks: off-diagonal -w_ij (I + 0.3 R_ij), R ~ N(0,1)/3 drawn
+    per direction; diagonal 1.1 * sum ||off||_1 * I + 0.05 N(0,1)."""
+    n = xy.shape[0]
+    if order == "rcm":
+        from . import native
+        rp, cp = pattern(n, edges)
+        new_to_old = native.rcm_order(n, rp, cp)
+        edges = np.sort(_relabel(edges, new_to_old), axis=1)
+        xy = xy[new_to_old]
+    e = edges.shape[0]
+    eye = np.eye(bs)
+    w = rng.uniform(0.5, 1.5, size=e)
+    r_fwd = rng.normal(0.0, 1.0, size=(e, bs, bs)) / 3.0
+    r_bwd = rng.normal(0.0, 1.0, size=(e, bs, bs)) / 3.0
+    b_fwd = -w[:, None, None] * (eye + 0.3 * r_fwd)
+    b_bwd = -w[:, None, None] * (eye + 0.3 * r_bwd)
+    norm1 = lambda b: np.abs(b).sum(axis=1).max(axis=1)   # induced 1-norm: max column sum
+    acc = np.zeros(n)
+    np.add.at(acc, edges[:, 0], norm1(b_fwd))
+    np.add.at(acc, edges[:, 1], norm1(b_bwd))
+    diag = 1.1 * acc[:, None, None] * eye + 0.05 * rng.normal(0.0, 1.0, size=(n, bs, bs))
+    rhs = rng.uniform(-1.0, 1.0, size=n * bs)
+    i, j = edges[:, 0], edges[:, 1]
+    rows = np.concatenate([np.arange(n), i, j])
+    cols = np.concatenate([np.arange(n), j, i])
+    blocks = np.concatenate([diag, b_fwd, b_bwd])
+    o = np.lexsort((cols, rows))
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n), out=rowptr[1:])
+    return BlockSystem(n, bs, rowptr, cols[o].astype(np.int64), blocks[o].reshape(-1), rhs, xy,
+                       kind="dense", meta={"order": order})
