@@ -228,6 +228,22 @@ owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_precondi
                             const owtk_solver_options* options, owtk_workspace* workspace,
                             owtk_solver_result* result);
 
+/* ---- allocation-free variant (no counterpart in the reference) ----------
+ * The batched dot product of owtk_dot_batch for callers that cannot allocate
+ * device memory (a host framework that owns the device allocator, code where
+ * a cudaMalloc would be forbidden or would synchronise the device).  It needs
+ * no context and allocates nothing: w, the k basis vectors (a host array of
+ * device pointers, n doubles each) and results (k + 1 doubles: w.basis_j, then
+ * w.w) are caller-owned device memory; stream is a cudaStream_t (NULL: the
+ * legacy default stream).  Its reduction scratch is one static device array
+ * of about 148 KiB that every GPU loading the library holds until exit, so:
+ * k <= 31 (larger batches return OWTK_ERR_INVALID_ARGUMENT); calls that
+ * overlap on the GPU race on that array and must be serialised; and the
+ * first call on a device looks up the array's address with that device
+ * current, so make it before any stream capture. */
+owtk_status owtk_dot_batch_f64_noalloc(const double* w, const double* const* basis, size_t k,
+                                       size_t n, double* results, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,6 +22,8 @@ thread_local std::string g_last_error;
 
 void fail(owtk_status code, const std::string& message) { throw Error{code, message}; }
 
+void record_error(const std::string& message) { g_last_error = message; }
+
 void cuda_check(cudaError_t e, const char* what)
 {
     if (e != cudaSuccess) fail(OWTK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
