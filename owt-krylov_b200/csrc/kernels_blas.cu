@@ -387,8 +387,10 @@ __device__ __forceinline__ void combine(int count, const double* partials, doubl
 }
 
 // k dots a_j . b_j, FP64 accumulation (float inputs are widened as the
-// reference's SerialReduction<float> does, reduction.hpp:123-133).
-template<class T, int G>
+// reference's SerialReduction<float> does, reduction.hpp:123-133).  G dots are
+// accumulated per pass; U elements per thread are loaded before use, so each
+// thread keeps 2*G*U independent loads in flight.
+template<class T, int G, int U>
 __global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, PtrPack a, PtrPack b,
                                                        double* partials, unsigned* ticket,
                                                        double* out_dev, double* out_host)
@@ -411,12 +413,23 @@ __global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, Ptr
             pa[j] = g0 + j < k ? sa[g0 + j] : nullptr;
             pb[j] = g0 + j < k ? sb[g0 + j] : nullptr;
         }
-        for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+        for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += U * stride) {
+            T va[U][G], vb[U][G];
 #pragma unroll
-            for (int j = 0; j < G; ++j) {
-                if (g0 + j < k)
-                    acc[j] += static_cast<double>(pa[j][i]) * static_cast<double>(pb[j][i]);
+            for (int u = 0; u < U; ++u) {
+                const std::size_t idx = i + u * stride;
+#pragma unroll
+                for (int j = 0; j < G; ++j) {
+                    const bool on = g0 + j < k && idx < n;
+                    va[u][j] = on ? pa[j][idx] : T(0);
+                    vb[u][j] = on ? pb[j][idx] : T(0);
+                }
             }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int j = 0; j < G; ++j)
+                    acc[j] += static_cast<double>(va[u][j]) * static_cast<double>(vb[u][j]);
         }
         block_partials<G>(acc, k - g0 < G ? k - g0 : G, partials, g0);
     }
@@ -519,8 +532,17 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
 {
     ScaledSum a{0.0, 0.0, 0};
     const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
-    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride)
-        norm_push(a, static_cast<double>(x[i]));
+    constexpr int kU = 8;   // loads in flight per thread
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += kU * stride) {
+        double v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const std::size_t idx = i + u * stride;
+            v[u] = idx < n ? static_cast<double>(x[idx]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) norm_push(a, v[u]);
+    }
     a = norm_warp(a);
     __shared__ ScaledSum red[kThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -535,13 +557,21 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
     }
     if (last_block(ticket)) {
         __threadfence();
+        // Every thread merges a strided share of the CTA partials, then the
+        // CTA merges the threads' results (fixed order: deterministic).
+        ScaledSum t{0.0, 0.0, 0};
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += kThreads) {
+            const ScaledSum p{__ldcg(partials + 3 * b), __ldcg(partials + 3 * b + 1),
+                              __ldcg(partials + 3 * b + 2) != 0.0};
+            t = norm_merge(t, p);
+        }
+        t = norm_warp(t);
+        __syncthreads();
+        if (lane == 0) red[warp] = t;
+        __syncthreads();
         if (threadIdx.x == 0) {
-            ScaledSum s{0.0, 0.0, 0};
-            for (unsigned b = 0; b < gridDim.x; ++b) {
-                ScaledSum t{__ldcg(partials + 3 * b), __ldcg(partials + 3 * b + 1),
-                            __ldcg(partials + 3 * b + 2) != 0.0};
-                s = norm_merge(s, t);
-            }
+            ScaledSum s = red[0];
+            for (int w = 1; w < kThreads / 32; ++w) s = norm_merge(s, red[w]);
             double r;
             if (s.nan) r = __longlong_as_double(0x7ff8000000000000LL);
             else if (s.scale == 0.0 || isinf(s.scale)) r = s.scale;
@@ -645,10 +675,16 @@ template<class T> void multidot(Context& c, std::size_t n, int k, const T* const
     const unsigned blocks = reduce_blocks(c, n);
     const PtrPack pa = pack(reinterpret_cast<const void* const*>(a), k);
     const PtrPack pb = pack(reinterpret_cast<const void* const*>(b), k);
-    if (k <= 4)
-        k_multidot<T, 4><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, partials_of(c), ticket_of(c), out_dev, out_host);
+    double* pp = partials_of(c);
+    unsigned* tk = ticket_of(c);
+    if (k == 1)
+        k_multidot<T, 1, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, pp, tk, out_dev, out_host);
+    else if (k == 2)
+        k_multidot<T, 2, 4><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, pp, tk, out_dev, out_host);
+    else if (k <= 4)
+        k_multidot<T, 4, 2><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, pp, tk, out_dev, out_host);
     else
-        k_multidot<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_multidot<T, 8, 1><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, pp, tk, out_dev, out_host);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }

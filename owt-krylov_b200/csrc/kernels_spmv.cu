@@ -18,6 +18,8 @@
 // "long" tile, processed with threads over components (coalesced for wide
 // blocks such as bs = 1296).
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "owtk_internal.h"
 
@@ -143,6 +145,102 @@ __global__ void __launch_bounds__(kThreads, 8) k_spmv_tiles(SpmvArgs<T> a)
     }
 }
 
+// Persistent variant for the component-diagonal and split forms: each CTA
+// walks tiles blockIdx.x, +gridDim.x, ... and issues the next tile's value and
+// column loads before the current tile's gather/sum/store phases, so the HBM
+// stream never waits for the shared-memory phases.  Same arithmetic as
+// k_spmv_tiles (bit-identical results).
+template<class T, int KIND>
+__global__ void __launch_bounds__(kThreads, 4) k_spmv_stream(SpmvArgs<T> a, const int4* __restrict__ meta,
+                                                              int ntiles)
+{
+    constexpr int kPer = kStage / kThreads;
+    __shared__ T prod[kStage];
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    const int bs = a.bs;
+    int4 m = meta[tile];   // r0, r1, e0, e1
+    T pv[kPer];
+    int pc[kPer];          // column of value k (times bs plus component below)
+
+#define OWTK_SPMV_ISSUE(t)                                                         \
+    do {                                                                           \
+        const int iu = ((t).w - (t).z) * bs;                                       \
+        if (iu <= kStage && ((t).y - (t).x) * bs <= kStage) {                      \
+            const T* iv = a.vals + static_cast<std::size_t>((t).z) * bs;           \
+            _Pragma("unroll") for (int j = 0; j < kPer; ++j) {                     \
+                const int k = threadIdx.x + j * kThreads;                          \
+                if (k < iu) {                                                      \
+                    const int e = div_bs(k, a.magic);                              \
+                    pv[j] = __ldcs(iv + k);                                        \
+                    pc[j] = __ldg(a.cols + (t).z + e) * bs + (k - e * bs);         \
+                }                                                                  \
+            }                                                                      \
+        }                                                                          \
+    } while (0)
+    OWTK_SPMV_ISSUE(m);
+    for (;;) {
+        const int next = tile + static_cast<int>(gridDim.x);
+        int4 mn = make_int4(0, 0, 0, 0);
+        if (next < ntiles) mn = meta[next];
+        const int r0 = m.x, r1 = m.y, e0 = m.z;
+        const int units = (m.w - e0) * bs;
+        const int outs = (r1 - r0) * bs;
+        const bool longtile = units > kStage || outs > kStage;
+        if (longtile) {
+            for (int r = r0; r < r1; ++r) {
+                const int b0 = a.rowptr[r], b1 = a.rowptr[r + 1];
+                for (int c = threadIdx.x; c < bs; c += kThreads) {
+                    const std::size_t o = static_cast<std::size_t>(r) * bs + c;
+                    T acc = KIND == 1 ? mul_rn(a.diag[o], a.x[o]) : T(0);
+                    for (int e = b0; e < b1; ++e)
+                        acc = add_rn(acc, mul_rn(a.vals[static_cast<std::size_t>(e) * bs + c],
+                                                 a.x[static_cast<std::size_t>(a.cols[e]) * bs + c]));
+                    a.y[o] = acc;
+                }
+            }
+            if (next >= ntiles) break;
+            tile = next;
+            m = mn;
+            OWTK_SPMV_ISSUE(m);
+            continue;
+        }
+        int ob[kPer], oe[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int o = threadIdx.x + j * kThreads;
+            if (o < outs) {
+                const int rl = div_bs(o, a.magic);
+                ob[j] = a.rowptr[r0 + rl] - e0;
+                oe[j] = a.rowptr[r0 + rl + 1] - e0;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            if (k < units) prod[k] = mul_rn(pv[j], __ldg(a.x + pc[j]));
+        }
+        if (next < ntiles) OWTK_SPMV_ISSUE(mn);   // next tile's stream flies during the phases below
+        __syncthreads();
+        const std::size_t ybase = static_cast<std::size_t>(r0) * bs;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int o = threadIdx.x + j * kThreads;
+            if (o < outs) {
+                const int c = o - div_bs(o, a.magic) * bs;
+                T acc = KIND == 1 ? mul_rn(a.diag[ybase + o], a.x[ybase + o]) : T(0);
+                for (int e = ob[j]; e < oe[j]; ++e) acc = add_rn(acc, prod[e * bs + c]);
+                a.y[ybase + o] = acc;
+            }
+        }
+        __syncthreads();
+        if (next >= ntiles) break;
+        tile = next;
+        m = mn;
+    }
+#undef OWTK_SPMV_ISSUE
+}
+
 // First diagonal entry of every row (block_csr.hpp:217-236).
 template<class T>
 __global__ void k_bsr_diagonal(int owned, int bs, const int* rowptr, const int* cols, const T* vals,
@@ -189,8 +287,10 @@ template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
     a.bs = static_cast<int>(m.bs);
     a.magic = ((1ull << 32) + m.bs - 1) / m.bs;
     const unsigned grid = static_cast<unsigned>(m.plan.tiles);
-    if (m.kind == 0) k_spmv_tiles<T, 0><<<grid, kThreads, 0, c.stream>>>(a);
-    else if (m.kind == 1) k_spmv_tiles<T, 1><<<grid, kThreads, 0, c.stream>>>(a);
+    const unsigned persistent = std::min<unsigned>(grid, static_cast<unsigned>(c.sm_count) * 4);
+    const int4* meta = m.plan.tile_meta.as<int4>();
+    if (m.kind == 0) k_spmv_stream<T, 0><<<persistent, kThreads, 0, c.stream>>>(a, meta, m.plan.tiles);
+    else if (m.kind == 1) k_spmv_stream<T, 1><<<persistent, kThreads, 0, c.stream>>>(a, meta, m.plan.tiles);
     else k_spmv_tiles<T, 2><<<grid, kThreads, 0, c.stream>>>(a);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
@@ -257,6 +357,14 @@ void build_tile_plan(Matrix& m)
     m.plan.tiles = static_cast<int>(tiles.size()) - 1;
     m.plan.tile_values = kStage;
     m.plan.tile_rows = upload(m.ctx->stream, tiles);
+    std::vector<std::int32_t> meta(4 * static_cast<std::size_t>(m.plan.tiles));
+    for (int t = 0; t < m.plan.tiles; ++t) {
+        meta[4 * t + 0] = tiles[t];
+        meta[4 * t + 1] = tiles[t + 1];
+        meta[4 * t + 2] = m.h_rowptr[tiles[t]];
+        meta[4 * t + 3] = m.h_rowptr[tiles[t + 1]];
+    }
+    m.plan.tile_meta = upload(m.ctx->stream, meta);
 }
 
 }  // namespace owtk

@@ -118,22 +118,6 @@ __device__ __forceinline__ void publish(T* p, T v)
     st_relaxed(p, v);
 }
 
-// Bounded wait for a dependency value that is still the sentinel.
-template<class T>
-__device__ __noinline__ T spin_value(const T* p, unsigned* status)
-{
-    using U = typename Bits<T>::U;
-    for (int it = 0; it < kSpinLimit; ++it) {
-        const U v = ld_relaxed_bits(p);
-        if (v != Bits<T>::kSentinel) return from_bits(v);
-        if (it >= 256) __nanosleep(32);
-        if ((it & 1023) == 1023 && (*reinterpret_cast<volatile unsigned*>(status) & kErrTimeout))
-            return from_bits(v);
-    }
-    atomicOr(status, kErrTimeout);
-    return from_bits(Bits<T>::kQuietNan);
-}
-
 template<class T>
 __global__ void k_fill_sentinel(std::size_t n, T* x)
 {
@@ -198,6 +182,8 @@ __device__ __forceinline__ T eliminate(T y, const SweepArgs<T>& a, const T* dep,
     const int bs = a.bs;
     for (int k0 = b; k0 < e; k0 += kChunk) {
         T fv[kChunk], xv[kChunk];
+        U xb[kChunk];
+        const T* src[kChunk];
         bool on[kChunk];
 #pragma unroll
         for (int j = 0; j < kChunk; ++j) {
@@ -206,16 +192,33 @@ __device__ __forceinline__ T eliminate(T y, const SweepArgs<T>& a, const T* dep,
             if (FILTER == 1 && col >= row) col = -1;
             if (FILTER == 2 && (col <= row || col >= a.owned)) col = -1;
             on[j] = col >= 0;
+            src[j] = dep + static_cast<std::size_t>(on[j] ? col : 0) * bs + c;
             if (on[j]) {
                 fv[j] = a.vals[static_cast<std::size_t>(k) * bs + c];
-                const T* src = dep + static_cast<std::size_t>(col) * bs + c;
-                if (POLL) {
-                    const U bits = ld_relaxed_bits(src);
-                    xv[j] = bits != Bits<T>::kSentinel ? from_bits(bits) : spin_value(src, a.status);
-                } else {
-                    xv[j] = __ldcg(src);
-                }
+                if (POLL) xb[j] = ld_relaxed_bits(src[j]);
+                else xv[j] = __ldcg(src[j]);
             }
+        }
+        if (POLL) {
+            // Re-poll every still-pending dependency together: one L2 round
+            // trip per round however many are pending.
+            for (int it = 0;; ++it) {
+                bool pending = false;
+#pragma unroll
+                for (int j = 0; j < kChunk; ++j) pending |= on[j] && xb[j] == Bits<T>::kSentinel;
+                if (!pending) break;
+                if (it >= kSpinLimit) {
+                    atomicOr(a.status, kErrTimeout);
+                    break;
+                }
+                if ((it & 1023) == 1023 && (*reinterpret_cast<volatile unsigned*>(a.status) & kErrTimeout)) break;
+                if (it >= 256) __nanosleep(32);
+#pragma unroll
+                for (int j = 0; j < kChunk; ++j)
+                    if (on[j] && xb[j] == Bits<T>::kSentinel) xb[j] = ld_relaxed_bits(src[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < kChunk; ++j) xv[j] = from_bits(xb[j]);
         }
 #pragma unroll
         for (int j = 0; j < kChunk; ++j) {
@@ -233,25 +236,32 @@ __device__ __forceinline__ void row_body(const SweepArgs<T>& a, int row, int c0,
 {
     const int bs = a.bs;
     const std::size_t rb = static_cast<std::size_t>(row) * bs;
+    // Row-local operands are loaded before the dependency wait so their
+    // latency is not added to the level-to-level critical path.
     if (MODE == kIluForward) {          // in -> work (unit lower solve)
         const int b = a.rowptr[row], d = a.diagpos[row];
-        for (int c = c0; c < bs; c += cstep)
-            publish(a.work + rb + c, eliminate<T, 0, false, true>(a.in[rb + c], a, a.work, b, d, row, c));
+        for (int c = c0; c < bs; c += cstep) {
+            const T own = a.in[rb + c];
+            publish(a.work + rb + c, eliminate<T, 0, false, true>(own, a, a.work, b, d, row, c));
+        }
     } else if (MODE == kIluBackward) {  // work -> out (upper solve, times the inverse diagonal)
         const int d = a.diagpos[row], end = a.rowptr[row + 1];
-        for (int c = c0; c < bs; c += cstep)
-            publish(a.out + rb + c,
-                    mul_rn(eliminate<T, 0, false, true>(a.work[rb + c], a, a.out, d + 1, end, row, c), a.inv[rb + c]));
+        for (int c = c0; c < bs; c += cstep) {
+            const T own = a.work[rb + c], inv = a.inv[rb + c];
+            publish(a.out + rb + c, mul_rn(eliminate<T, 0, false, true>(own, a, a.out, d + 1, end, row, c), inv));
+        }
     } else if (MODE == kSsorForward) {  // in -> work
         const int b = a.rowptr[row], end = a.rowptr[row + 1];
-        for (int c = c0; c < bs; c += cstep)
-            publish(a.work + rb + c,
-                    div_rn(eliminate<T, 1, true, true>(a.in[rb + c], a, a.work, b, end, row, c), a.diag[rb + c]));
+        for (int c = c0; c < bs; c += cstep) {
+            const T own = a.in[rb + c], dg = a.diag[rb + c];
+            publish(a.work + rb + c, div_rn(eliminate<T, 1, true, true>(own, a, a.work, b, end, row, c), dg));
+        }
     } else if (MODE == kSsorBackward) { // work -> out
         const int b = a.rowptr[row], end = a.rowptr[row + 1];
         for (int c = c0; c < bs; c += cstep) {
-            const T z0 = mul_rn(a.diag[rb + c], a.work[rb + c]);
-            publish(a.out + rb + c, div_rn(eliminate<T, 2, true, true>(z0, a, a.out, b, end, row, c), a.diag[rb + c]));
+            const T dg = a.diag[rb + c];
+            const T z0 = mul_rn(dg, a.work[rb + c]);
+            publish(a.out + rb + c, div_rn(eliminate<T, 2, true, true>(z0, a, a.out, b, end, row, c), dg));
         }
     } else {  // kIluFactor: IKJ elimination of one row (preconditioner.hpp:442-469)
         const int b = a.rowptr[row], d = a.diagpos[row];
@@ -320,7 +330,7 @@ __global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T> a)
 int sweep_warps(const Context& c, const Sweep& s)
 {
     const char* env = std::getenv("OWTK_SWEEP_WARPS_PER_LEVEL");
-    const double factor = env ? std::atof(env) : 4.0;
+    const double factor = env ? std::atof(env) : 16.0;
     const double per_level = s.depth > 0 ? static_cast<double>(s.tasks) / s.depth : s.tasks;
     long long warps = factor > 0 ? static_cast<long long>(std::ceil(factor * per_level)) : s.tasks;
     const long long cap = static_cast<long long>(c.sm_count) * 64;

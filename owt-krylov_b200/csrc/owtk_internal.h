@@ -97,6 +97,7 @@ struct Vector {
 // "long" tile handled component-parallel.
 struct TilePlan {
     DeviceBuffer tile_rows;    // int32, tiles + 1
+    DeviceBuffer tile_meta;    // int4 per tile: first row, end row, first entry, end entry
     int tiles = 0;
     int tile_values = 0;       // stage capacity used to build the plan
 };
