@@ -1,0 +1,122 @@
+// A reference-style consumer of the header-only API: the same calls an
+// OWT-Krylov application makes (BlockCsrMatrix, PolicyBlockOperator, Ilu0 /
+// Jacobi / split SSOR preconditioners, gmres / bicgstab / idrs, RCM), with
+// the device execution policy.  Reads a system written by the test, writes the
+// results back for comparison with the CPU oracle.
+//
+//   consumer <dir>   (dir holds meta.txt, rowptr.u64, cols.u64, vals.f64, rhs.f64)
+#include <owtk/krylov.hpp>
+
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+using namespace owt::krylov;
+
+template<class V>
+V read(const std::string& path, std::size_t n)
+{
+    V v(n);
+    std::ifstream f(path, std::ios::binary);
+    f.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(n * sizeof(typename V::value_type)));
+    if (!f) throw std::runtime_error("cannot read " + path);
+    return v;
+}
+
+template<class V>
+void write(const std::string& path, const V& v)
+{
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(v[0])));
+}
+
+template<class R>
+void report(std::ostream& out, const char* name, const R& r)
+{
+    out << name << ' ' << static_cast<int>(r.status) << ' ' << static_cast<int>(r.breakdown_reason) << ' '
+        << r.iterations << ' ' << r.operator_applications << ' ' << r.preconditioner_applications << ' '
+        << r.global_reductions << ' ' << r.true_residual_norm << '\n';
+}
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) return 2;
+    const std::string dir = argv[1];
+    std::size_t n = 0, bs = 0, nnz = 0;
+    {
+        std::ifstream meta(dir + "/meta.txt");
+        meta >> n >> bs >> nnz;
+    }
+    BlockCsrMatrix<double> A(n, 0, bs, read<std::vector<std::size_t>>(dir + "/rowptr.u64", n + 1),
+                             read<std::vector<std::size_t>>(dir + "/cols.u64", nnz),
+                             read<std::vector<double>>(dir + "/vals.f64", nnz * bs));
+    BlockVector<double> rhs(n, 0, bs);
+    const auto b = read<std::vector<double>>(dir + "/rhs.f64", n * bs);
+    std::copy(b.begin(), b.end(), rhs.data());
+
+    // The only change from a host consumer: the execution policy.
+    PolicyBlockOperator op(A, CudaExecutionPolicy{});
+
+    std::ofstream results(dir + "/results.txt");
+    BlockVector<double> y = rhs.clone_layout();
+    op.apply(rhs, y);
+    write(dir + "/spmv.f64", std::vector<double>(y.owned().begin(), y.owned().end()));
+
+    Ilu0Preconditioner ilu(A);
+    SolverOptions<double> options;
+    SolverWorkspace<double> workspace;
+    BlockVector<double> x1 = rhs.clone_layout();
+    const auto r1 = gmres(op, rhs, x1, options, ilu, SerialReduction<double>{}, &workspace);
+    report(results, "gmres_ilu0", r1);
+    write(dir + "/x_gmres.f64", std::vector<double>(x1.owned().begin(), x1.owned().end()));
+
+    JacobiPreconditioner jacobi(A);
+    SolverOptions<double> bench = options;
+    bench.convergence_check_interval = 1;
+    BlockVector<double> x2 = rhs.clone_layout();
+    const auto r2 = bicgstab_with_workspace(op, rhs, x2, workspace, bench, jacobi);
+    report(results, "bicgstab_jacobi", r2);
+    write(dir + "/x_bicgstab.f64", std::vector<double>(x2.owned().begin(), x2.owned().end()));
+
+    BlockVector<double> x3 = rhs.clone_layout();
+    const auto r3 = idrs(op, rhs, x3, bench, jacobi);
+    report(results, "idrs_jacobi", r3);
+
+    // Split diagonal/edge view and split SSOR over borrowed host arrays.
+    std::vector<std::size_t> off_rp{0}, off_ci;
+    std::vector<double> diag(n * bs), off;
+    for (std::size_t r = 0; r < n; ++r) {
+        for (std::size_t e = A.row_offsets()[r]; e < A.row_offsets()[r + 1]; ++e) {
+            const std::size_t c = A.column_indices()[e];
+            const double* v = A.values().data() + e * bs;
+            if (c == r) std::copy(v, v + bs, diag.data() + r * bs);
+            else {
+                off_ci.push_back(c);
+                off.insert(off.end(), v, v + bs);
+            }
+        }
+        off_rp.push_back(off_ci.size());
+    }
+    SplitBlockCsrMatrixView<double> split(n, 0, bs, std::span<const std::size_t>(off_rp),
+                                          std::span<const std::size_t>(off_ci), std::span<const double>(diag),
+                                          std::span<const double>(off));
+    SplitLocalSsorPreconditioner<double> ssor(split, 1.2);
+    BlockVector<double> z = rhs.clone_layout();
+    ssor.apply(rhs, z);
+    write(dir + "/split_ssor.f64", std::vector<double>(z.owned().begin(), z.owned().end()));
+
+    const auto order = reverse_cuthill_mckee_order(A);
+    write(dir + "/rcm.u64", order);
+    results << "epochs " << workspace.allocation_epochs() << '\n';
+    results << "ilu_updates " << ilu.numeric_updates() << '\n';
+    try {
+        BlockVector<double> wrong(n + 1, 0, bs);
+        ilu.apply(rhs, wrong);
+        results << "layout_error none\n";
+    } catch (const std::invalid_argument&) {
+        results << "layout_error invalid_argument\n";
+    }
+    return 0;
+}
