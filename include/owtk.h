@@ -37,7 +37,8 @@ typedef enum owtk_status {
     OWTK_ERR_RUNTIME = 7
 } owtk_status;
 
-typedef enum owtk_dtype { OWTK_F64 = 0, OWTK_F32 = 1 } owtk_dtype;
+/* OWTK_BF16 is a factor-storage type only (owtk_pc_create_stored/_mixed). */
+typedef enum owtk_dtype { OWTK_F64 = 0, OWTK_F32 = 1, OWTK_BF16 = 2 } owtk_dtype;
 
 typedef struct owtk_context owtk_context;
 typedef struct owtk_vector owtk_vector;
@@ -128,11 +129,28 @@ typedef enum owtk_pc_kind {
     OWTK_PC_JACOBI = 1,      /* JacobiPreconditioner (:25-113); parameter = minimum diagonal (<= 0: 64 eps) */
     OWTK_PC_SSOR = 2,        /* LocalSsorPreconditioner (:124-247); parameter = omega */
     OWTK_PC_SPLIT_SSOR = 3,  /* SplitLocalSsorPreconditioner (split_block_csr.hpp:205-332); parameter = omega */
-    OWTK_PC_ILU = 4          /* IluLevelPreconditioner / Ilu0Preconditioner (:253-508); parameter = fill level */
+    OWTK_PC_ILU = 4,         /* IluLevelPreconditioner / Ilu0Preconditioner (:253-508); parameter = fill level */
+    /* No reference counterpart: ILU(0) of a dense-block BSR (bs <= 4), block
+     * IKJ factorisation with inverted diagonal blocks; parameter unused. */
+    OWTK_PC_BLOCK_ILU = 5,
+    /* Created only by owtk_pc_create_mixed. */
+    OWTK_PC_MIXED = 6
 } owtk_pc_kind;
 
 owtk_status owtk_pc_create(owtk_matrix* m, owtk_pc_kind kind, double parameter,
                            owtk_preconditioner** out);
+/* Mixed precision (no reference counterpart).  owtk_pc_create_stored: an
+ * ILU / block ILU of an FP64 matrix, factorised in FP64 on the device, whose
+ * factors are kept in `storage` (OWTK_F32 or OWTK_BF16); its applies take
+ * FP32 vectors and compute in FP32.  owtk_pc_create_mixed: a preconditioner
+ * for FP64 (flexible) solves that hands its FP64 input to an FP32 inner
+ * solve — `inner_iterations` GMRES steps with an FP32 copy of the matrix and
+ * the stored-precision factors (0: one factor apply) — and returns the FP64
+ * result.  owtk_pc_update_values refreshes both from the FP64 matrix. */
+owtk_status owtk_pc_create_stored(owtk_matrix* m, owtk_pc_kind kind, double parameter, owtk_dtype storage,
+                                  owtk_preconditioner** out);
+owtk_status owtk_pc_create_mixed(owtk_matrix* m, owtk_pc_kind inner_kind, double parameter, owtk_dtype storage,
+                                 uint32_t inner_iterations, owtk_preconditioner** out);
 owtk_status owtk_pc_destroy(owtk_preconditioner* pc);
 /* apply(const in, out); in == out is allowed for ILU and split SSOR. */
 owtk_status owtk_pc_apply(owtk_preconditioner* pc, owtk_vector* in, owtk_vector* out);
@@ -141,7 +159,9 @@ owtk_status owtk_pc_apply(owtk_preconditioner* pc, owtk_vector* in, owtk_vector*
 owtk_status owtk_pc_update_values(owtk_preconditioner* pc, owtk_matrix* m);
 uint64_t owtk_pc_numeric_updates(owtk_preconditioner* pc);
 /* ILU factor storage (preconditioner.hpp:367-370); pass NULL arrays to query
- * the entry count first.  Values and inverse diagonal in the PC's dtype. */
+ * the entry count first.  Values and inverse diagonal in the PC's dtype (the
+ * FP64 factors for stored-precision PCs); for a block ILU the values hold
+ * bs*bs per entry and the inverse diagonal bs*bs per row. */
 owtk_status owtk_ilu_factors(owtk_preconditioner* pc, uint64_t* entries, uint64_t* row_offsets,
                              uint64_t* columns, void* values, void* inverse_diagonal);
 /* Level sets the sweeps were scheduled with (no reference counterpart): per

@@ -102,6 +102,11 @@ class Restatement:
             ("orc_levels", None, [c_int64, vp, vp, vp, vp]),
             ("orc_rcm", c_int, [c_int64, vp, vp, vp]),
             ("orc_hilbert", c_int, [c_int64, vp, vp]),
+            ("orc_block_ilu_create", vp, [c_int64, c_int64, vp, vp, vp, POINTER(c_int)]),
+            ("orc_block_ilu_apply", None, [vp, vp, vp]),
+            ("orc_block_ilu_copy", None, [vp, vp, vp]),
+            ("orc_block_ilu_entries", c_int64, [vp]),
+            ("orc_block_ilu_destroy", None, [vp]),
             ("orc_bicgstab", None, [vp, vp, POINTER(Options), vp, vp, POINTER(Result)]),
             ("orc_gmres", None, [vp, vp, POINTER(Options), vp, vp, POINTER(Result)]),
         ]:
@@ -166,6 +171,9 @@ class Restatement:
 
     def ilu(self, owned, bs, rp, ci, v, fill=0):
         return RestatedIlu(self, owned, bs, rp, ci, v, fill)
+
+    def block_ilu(self, owned, bs, rp, ci, v):
+        return RestatedBlockIlu(self, owned, bs, rp, ci, v)
 
     def levels(self, owned, rp, ci):
         rp, ci = _i64(rp), _i64(ci)
@@ -270,6 +278,38 @@ class RestatedIlu:
     def __del__(self):
         try:
             self.o.L.orc_ilu_destroy(self.h)
+        except Exception:
+            pass
+
+
+class RestatedBlockIlu:
+    """Dense-block ILU(0) (no reference counterpart; see owtk_oracle.c)."""
+
+    def __init__(self, o: Restatement, owned, bs, rp, ci, v):
+        self.o, self.owned, self.bs = o, owned, bs
+        rp, ci = _i64(rp), _i64(ci)
+        v = np.ascontiguousarray(v, np.float64)
+        st = c_int(0)
+        self.h = o.L.orc_block_ilu_create(owned, bs, _p(rp), _p(ci), _p(v), ctypes.byref(st))
+        self.status = st.value
+
+    def factors(self):
+        n = self.o.L.orc_block_ilu_entries(self.h)
+        b2 = self.bs * self.bs
+        val = np.zeros(max(n * b2, 1))
+        dinv = np.zeros(self.owned * b2)
+        self.o.L.orc_block_ilu_copy(self.h, _p(val), _p(dinv))
+        return val[: n * b2], dinv
+
+    def apply(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        out = np.zeros(self.owned * self.bs)
+        self.o.L.orc_block_ilu_apply(self.h, _p(x), _p(out))
+        return out
+
+    def __del__(self):
+        try:
+            self.o.L.orc_block_ilu_destroy(self.h)
         except Exception:
             pass
 

@@ -915,3 +915,158 @@ done:
 #undef HH
     free(mem); free(V); free(Z); free(H); free(cs); free(sn); free(g); free(proj); free(coef);
 }
+
+/* ------------------------------------------------------- dense-block ILU(0)
+ * No counterpart in the reference (its ILU exists for component-diagonal
+ * BlockCsrMatrix only, preconditioner.hpp:257).  Restated here as the checker
+ * of the device's block factorisation, with the device's operation order:
+ *   pattern   : ILU(0) of the block graph (sorted local columns, as
+ *               preconditioner.hpp:373-427 with k = 0);
+ *   factorise : per row, for each lower block l (pivot p, ascending column):
+ *               L_l = A_l * Dinv_p, then A_t -= L_l * U_pu for every upper
+ *               block u of row p whose column is present in the row;
+ *               Dinv_r = inverse of the final diagonal block (Gauss-Jordan,
+ *               partial pivoting, |pivot| <= 64 eps is a zero pivot);
+ *   apply     : y_r = b_r - sum_l L_l y_col, x_r = Dinv_r (y_r - sum_u U_u x_col),
+ *               each block product accumulated from +0 over j ascending. */
+typedef struct {
+    i64 owned, bs, entries;
+    i64 *rp, *ci, *diagpos, *src;
+    double *val, *dinv;   /* entries*bs*bs, owned*bs*bs */
+} orc_block_ilu;
+
+/* out = a (bs x bs) * b (bs x bs), row-major, sums from +0 in j order. */
+static void block_mul(i64 bs, const double* a, const double* b, double* out)
+{
+    for (i64 i = 0; i < bs; ++i)
+        for (i64 k = 0; k < bs; ++k) {
+            double s = 0.0;
+            for (i64 j = 0; j < bs; ++j) s += a[i * bs + j] * b[j * bs + k];
+            out[i * bs + k] = s;
+        }
+}
+
+/* Gauss-Jordan inverse with partial pivoting; returns 0 on a zero pivot. */
+static int block_inverse(i64 bs, const double* a, double* inv)
+{
+    double m[64], r[64];
+    for (i64 i = 0; i < bs * bs; ++i) { m[i] = a[i]; r[i] = 0.0; }
+    for (i64 i = 0; i < bs; ++i) r[i * bs + i] = 1.0;
+    for (i64 c = 0; c < bs; ++c) {
+        i64 p = c;
+        for (i64 i = c + 1; i < bs; ++i) if (fabs(m[i * bs + c]) > fabs(m[p * bs + c])) p = i;
+        if (!isfinite(m[p * bs + c]) || fabs(m[p * bs + c]) <= 64.0 * DBL_EPSILON) return 0;
+        if (p != c)
+            for (i64 j = 0; j < bs; ++j) {
+                double t = m[c * bs + j]; m[c * bs + j] = m[p * bs + j]; m[p * bs + j] = t;
+                t = r[c * bs + j]; r[c * bs + j] = r[p * bs + j]; r[p * bs + j] = t;
+            }
+        const double piv = m[c * bs + c];
+        for (i64 j = 0; j < bs; ++j) { m[c * bs + j] /= piv; r[c * bs + j] /= piv; }
+        for (i64 i = 0; i < bs; ++i) {
+            if (i == c) continue;
+            const double f = m[i * bs + c];
+            for (i64 j = 0; j < bs; ++j) { m[i * bs + j] -= f * m[c * bs + j]; r[i * bs + j] -= f * r[c * bs + j]; }
+        }
+    }
+    for (i64 i = 0; i < bs * bs; ++i) inv[i] = r[i];
+    return 1;
+}
+
+static i64 ilu_find_block(const orc_block_ilu* h, i64 r, i64 col)
+{
+    for (i64 e = h->rp[r]; e < h->rp[r + 1]; ++e)
+        if (h->ci[e] == col) return e;
+    return -1;
+}
+
+orc_block_ilu* orc_block_ilu_create(i64 owned, i64 bs, const i64* rp, const i64* ci, const double* v, int* status)
+{
+    int st = 0;
+    orc_ilu* pat = orc_ilu_create(owned, 1, rp, ci, v /* unused values */, 0, &st);
+    orc_block_ilu* h = (orc_block_ilu*)calloc(1, sizeof(orc_block_ilu));
+    h->owned = owned; h->bs = bs;
+    /* orc_ilu_create factorises bs=1 values too; only a pattern failure counts here. */
+    if (st == ORC_INVALID) { *status = st; orc_ilu_destroy(pat); return h; }
+    h->entries = pat->entries;
+    h->rp = pat->rp; h->ci = pat->ci; h->diagpos = pat->diagpos; h->src = pat->src;
+    pat->rp = pat->ci = pat->diagpos = pat->src = NULL;
+    orc_ilu_destroy(pat);
+    const i64 b2 = bs * bs;
+    h->val = (double*)calloc((size_t)(h->entries * b2) + 1, sizeof(double));
+    h->dinv = (double*)calloc((size_t)(owned * b2) + 1, sizeof(double));
+    for (i64 e = 0; e < h->entries; ++e)
+        if (h->src[e] >= 0) memcpy(h->val + e * b2, v + h->src[e] * b2, (size_t)b2 * sizeof(double));
+    double tmp[64], lu[64];
+    *status = ORC_OK;
+    for (i64 r = 0; r < owned; ++r) {
+        for (i64 l = h->rp[r]; l < h->diagpos[r]; ++l) {
+            const i64 p = h->ci[l];
+            block_mul(bs, h->val + l * b2, h->dinv + p * b2, tmp);
+            memcpy(h->val + l * b2, tmp, (size_t)b2 * sizeof(double));
+            for (i64 u = h->diagpos[p] + 1; u < h->rp[p + 1]; ++u) {
+                const i64 t = ilu_find_block(h, r, h->ci[u]);
+                if (t < 0) continue;
+                block_mul(bs, h->val + l * b2, h->val + u * b2, lu);
+                for (i64 k = 0; k < b2; ++k) h->val[t * b2 + k] -= lu[k];
+            }
+        }
+        if (!block_inverse(bs, h->val + h->diagpos[r] * b2, h->dinv + r * b2)) { *status = ORC_ZERO_PIVOT; return h; }
+    }
+    return h;
+}
+
+void orc_block_ilu_apply(const orc_block_ilu* h, const double* in, double* out)
+{
+    const i64 bs = h->bs, b2 = bs * bs;
+    double* y = (double*)malloc((size_t)(h->owned * bs) * sizeof(double));
+    for (i64 r = 0; r < h->owned; ++r) {
+        for (i64 i = 0; i < bs; ++i) {
+            double acc = in[r * bs + i];
+            for (i64 l = h->rp[r]; l < h->diagpos[r]; ++l) {
+                const double* L = h->val + l * b2;
+                const double* yc = y + h->ci[l] * bs;
+                double s = 0.0;
+                for (i64 j = 0; j < bs; ++j) s += L[i * bs + j] * yc[j];
+                acc -= s;
+            }
+            y[r * bs + i] = acc;
+        }
+    }
+    for (i64 r = h->owned - 1; r >= 0; --r) {
+        double w[8];
+        for (i64 i = 0; i < bs; ++i) {
+            double acc = y[r * bs + i];
+            for (i64 u = h->diagpos[r] + 1; u < h->rp[r + 1]; ++u) {
+                const double* U = h->val + u * b2;
+                const double* xc = out + h->ci[u] * bs;
+                double s = 0.0;
+                for (i64 j = 0; j < bs; ++j) s += U[i * bs + j] * xc[j];
+                acc -= s;
+            }
+            w[i] = acc;
+        }
+        const double* D = h->dinv + r * b2;
+        for (i64 i = 0; i < bs; ++i) {
+            double s = 0.0;
+            for (i64 j = 0; j < bs; ++j) s += D[i * bs + j] * w[j];
+            out[r * bs + i] = s;
+        }
+    }
+    free(y);
+}
+
+void orc_block_ilu_copy(const orc_block_ilu* h, double* val, double* dinv)
+{
+    const i64 b2 = h->bs * h->bs;
+    if (val) memcpy(val, h->val, (size_t)(h->entries * b2) * sizeof(double));
+    if (dinv) memcpy(dinv, h->dinv, (size_t)(h->owned * b2) * sizeof(double));
+}
+
+i64 orc_block_ilu_entries(const orc_block_ilu* h) { return h->entries; }
+
+void orc_block_ilu_destroy(orc_block_ilu* h)
+{
+    if (!h) return;
+    free(h->rp); free(h->ci); free(h->diagpos); free(h->src); free(h->val); free(h->dinv); free(h);
+}

@@ -11,6 +11,8 @@
 #include <string>
 #include <utility>
 
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
 #include "owtk_internal.h"
 
@@ -107,7 +109,7 @@ void Workspace::prepare(const Vector& layout, std::size_t count, std::size_t sca
 // ------------------------------------------------------------ helpers
 namespace {
 
-std::size_t dsize(owtk_dtype d) { return d == OWTK_F64 ? 8 : 4; }
+std::size_t dsize(owtk_dtype d) { return d == OWTK_F64 ? 8 : (d == OWTK_F32 ? 4 : 2); }
 
 void require(bool ok, const char* message)
 {
@@ -243,8 +245,9 @@ void ilu_symbolic(Preconditioner& p, const Matrix& m, std::size_t fill)
     p.d_upd_start = upload(s, start);
     p.d_upd_target = upload(s, target);
     p.d_upd_upper = upload(s, upper);
-    p.d_fvalues.allocate(nnz * p.bs * dsize(p.dtype) + 16);
-    p.inv_diag.allocate(n * p.bs * dsize(p.dtype) + 16);
+    const std::size_t per = p.block ? p.bs * p.bs : p.bs;   // values per factor entry
+    p.d_fvalues.allocate(nnz * per * dsize(p.dtype) + 16);
+    p.inv_diag.allocate(n * per * dsize(p.dtype) + 16);
     p.work.allocate(n * p.bs * dsize(p.dtype) + 16);   // forward-sweep result of an apply
     std::vector<std::int32_t> lower_level, upper_level;
     levels_of(n, p.f_rowptr.data(), p.f_cols.data(), lower_level, upper_level);
@@ -331,12 +334,44 @@ template<class T> void ssor_setup(Preconditioner& p, const Matrix& m)
     }
 }
 
+// Low-precision factor copies of an FP64 factorisation.
+void store_factors(Preconditioner& p)
+{
+    if (p.storage == OWTK_F64) return;
+    Context& c = *p.ctx;
+    const std::size_t per = p.block ? p.bs * p.bs : p.bs;
+    const std::size_t nv = p.f_cols.size() * per, ni = p.owned * per;
+    if (p.storage == OWTK_F32) {
+        kern::convert<float, double>(c, nv, p.d_fvalues.as<double>(), p.lp_vals.as<float>());
+        kern::convert<float, double>(c, ni, p.inv_diag.as<double>(), p.lp_inv.as<float>());
+    } else {
+        kern::convert<__nv_bfloat16, double>(c, nv, p.d_fvalues.as<double>(), p.lp_vals.as<__nv_bfloat16>());
+        kern::convert<__nv_bfloat16, double>(c, ni, p.inv_diag.as<double>(), p.lp_inv.as<__nv_bfloat16>());
+    }
+}
+
+void numeric_update(Preconditioner& p, Matrix& m);
+
+void mixed_update(Preconditioner& p, Matrix& m)
+{
+    const std::size_t per = m.kind == 2 ? m.bs * m.bs : m.bs;
+    kern::convert<float, double>(*p.ctx, m.entries * per, m.values.as<double>(), p.m32->values.as<float>());
+    numeric_update(*p.inner, m);
+}
+
 void numeric_update(Preconditioner& p, Matrix& m)
 {
-    if (p.dtype == OWTK_F64) {
+    if (p.kind == OWTK_PC_MIXED) {
+        mixed_update(p, m);
+    } else if (p.dtype == OWTK_F64) {
         if (p.kind == OWTK_PC_JACOBI) jacobi_setup<double>(p, m);
         else if (p.kind == OWTK_PC_SSOR || p.kind == OWTK_PC_SPLIT_SSOR) ssor_setup<double>(p, m);
         else if (p.kind == OWTK_PC_ILU) ilu_numeric<double>(p, m);
+        else if (p.kind == OWTK_PC_BLOCK_ILU) {
+            kern::block_ilu_factorize(*p.ctx, p, m.values.as<double>());
+            p.ctx->check_device_status();
+        }
+        store_factors(p);
     } else {
         if (p.kind == OWTK_PC_JACOBI) jacobi_setup<float>(p, m);
         else if (p.kind == OWTK_PC_SSOR || p.kind == OWTK_PC_SPLIT_SSOR) ssor_setup<float>(p, m);
@@ -377,11 +412,29 @@ void apply_operator(Matrix& m, Vector& in, Vector& out)
     }
 }
 
+void mixed_apply(Preconditioner& p, Vector& in, Vector& out);
+
 void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out)
 {
     if (!in.same_layout(out)) fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
     Context& c = *in.ctx;
     const std::size_t n = in.owned_size();
+    if (p != nullptr && (p->kind == OWTK_PC_MIXED || p->storage != OWTK_F64 || p->block)) {
+        if (in.owned != p->owned || in.ghost != p->ghost || in.bs != p->bs)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
+        const owtk_dtype want = (p->kind == OWTK_PC_MIXED || p->storage == OWTK_F64) ? OWTK_F64 : OWTK_F32;
+        if (in.dtype != want || out.dtype != want)
+            fail(OWTK_ERR_INVALID_ARGUMENT, want == OWTK_F32 ? "stored-precision factors apply to FP32 vectors"
+                                                             : "this preconditioner applies to FP64 vectors");
+        if (p->kind == OWTK_PC_MIXED) mixed_apply(*p, in, out);
+        else if (p->storage == OWTK_F32)
+            kern::ilu_apply_lp<float>(c, *p, static_cast<const float*>(in.data), static_cast<float*>(out.data));
+        else if (p->storage == OWTK_BF16)
+            kern::ilu_apply_lp<__nv_bfloat16>(c, *p, static_cast<const float*>(in.data), static_cast<float*>(out.data));
+        else
+            kern::block_ilu_apply(c, *p, static_cast<const double*>(in.data), static_cast<double*>(out.data));
+        return;
+    }
     if (p == nullptr || p->kind == OWTK_PC_IDENTITY) {
         if (in.dtype == OWTK_F64) kern::copy<double>(c, n, static_cast<const double*>(in.data), static_cast<double*>(out.data));
         else kern::copy<float>(c, n, static_cast<const float*>(in.data), static_cast<float*>(out.data));
@@ -772,64 +825,200 @@ owtk_status owtk_matrix_diagonal(owtk_matrix* m, void* host_out)
 }
 
 // ------------------------------------------------------------ preconditioners
+}  // extern "C"
+
+namespace owtk {
+namespace {
+
+std::unique_ptr<owtk_preconditioner> make_pc(owtk_matrix* m, owtk_pc_kind kind, double parameter,
+                                             owtk_dtype storage)
+{
+    require(m != nullptr, "null handle");
+    auto p = std::make_unique<owtk_preconditioner>();
+    p->ctx = m->ctx;
+    p->kind = kind;
+    p->dtype = m->dtype;
+    p->matrix = m;
+    p->owned = m->owned;
+    p->ghost = m->ghost;
+    p->bs = m->bs;
+    p->parameter = parameter;
+    const std::size_t n = m->owned * m->bs;
+    const std::size_t es = dsize(m->dtype);
+    switch (kind) {
+    case OWTK_PC_IDENTITY: break;
+    case OWTK_PC_JACOBI:
+        if (m->kind == 2) fail(OWTK_ERR_INVALID_ARGUMENT, "Jacobi needs a matrix with diagonal()");
+        p->inv_diag.allocate(n * es + 16);
+        break;
+    case OWTK_PC_SSOR:
+    case OWTK_PC_SPLIT_SSOR: {
+        if (kind == OWTK_PC_SSOR && m->kind != 0)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "SSOR needs a component-diagonal BSR matrix");
+        if (kind == OWTK_PC_SPLIT_SSOR && m->kind != 1)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "split SSOR needs a split view");
+        if (!(parameter > 0 && parameter < 2))
+            fail(OWTK_ERR_INVALID_ARGUMENT, kind == OWTK_PC_SSOR ? "SSOR omega must be in (0,2)"
+                                                                 : "split SSOR omega must be in (0,2)");
+        p->work.allocate(m->local_size() * es + 16);
+        if (kind == OWTK_PC_SSOR) p->diag_cache.allocate(n * es + 16);
+        std::vector<std::int32_t> lower, upper;
+        // The matrix pattern itself is the dependency pattern (ghosts excluded).
+        std::vector<std::int32_t> cols = m->h_cols;
+        for (auto& c : cols)
+            if (static_cast<std::size_t>(c) >= m->owned) c = static_cast<std::int32_t>(m->owned);
+        levels_of(m->owned, m->h_rowptr.data(), cols.data(), lower, upper);
+        build_sweep(*p->ctx, p->lower, m->owned, m->bs, lower, false);
+        build_sweep(*p->ctx, p->upper, m->owned, m->bs, upper, true);
+        break;
+    }
+    case OWTK_PC_ILU: {
+        if (m->kind != 0) fail(OWTK_ERR_INVALID_ARGUMENT, "ILU needs a component-diagonal BSR matrix");
+        if (!(parameter >= 0)) fail(OWTK_ERR_INVALID_ARGUMENT, "ILU fill level must be >= 0");
+        ilu_symbolic(*p, *m, static_cast<std::size_t>(parameter));
+        break;
+    }
+    case OWTK_PC_BLOCK_ILU: {
+        if (m->kind != 2) fail(OWTK_ERR_INVALID_ARGUMENT, "block ILU needs a dense-block BSR matrix");
+        if (m->dtype != OWTK_F64) fail(OWTK_ERR_INVALID_ARGUMENT, "block ILU factorises an FP64 matrix");
+        if (m->bs > 4) fail(OWTK_ERR_INVALID_ARGUMENT, "block ILU supports block sizes up to 4");
+        p->block = true;
+        ilu_symbolic(*p, *m, 0);
+        break;
+    }
+    default: fail(OWTK_ERR_INVALID_ARGUMENT, "unknown preconditioner kind");
+    }
+    if (storage != OWTK_F64) {
+        if (kind != OWTK_PC_ILU && kind != OWTK_PC_BLOCK_ILU)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "stored-precision factors exist for ILU and block ILU only");
+        if (m->dtype != OWTK_F64) fail(OWTK_ERR_INVALID_ARGUMENT, "stored-precision factors come from an FP64 matrix");
+        if (storage != OWTK_F32 && storage != OWTK_BF16) fail(OWTK_ERR_INVALID_ARGUMENT, "storage must be F32 or BF16");
+        p->storage = storage;
+        const std::size_t per = p->block ? m->bs * m->bs : m->bs;
+        p->lp_vals.allocate(p->f_cols.size() * per * dsize(storage) + 16);
+        p->lp_inv.allocate(m->owned * per * dsize(storage) + 16);
+        p->work32.allocate(n * sizeof(float) + 16);
+    }
+    if (kind == OWTK_PC_SSOR || kind == OWTK_PC_SPLIT_SSOR || kind == OWTK_PC_ILU || kind == OWTK_PC_BLOCK_ILU) {
+        p->flags.allocate(m->owned * sizeof(unsigned) + 16);
+        OWTK_CUDA(cudaMemsetAsync(p->flags.ptr, 0, m->owned * sizeof(unsigned), p->ctx->stream));
+        p->ticket.allocate(sizeof(unsigned long long));
+        OWTK_CUDA(cudaMemsetAsync(p->ticket.ptr, 0, sizeof(unsigned long long), p->ctx->stream));
+    }
+    if (kind != OWTK_PC_IDENTITY) numeric_update(*p, *m);
+    p->ctx->sync();
+    return p;
+}
+
+// FP32 copy of an FP64 owning matrix (structure shared by value, values
+// converted on the device by the mixed preconditioner's numeric update).
+std::unique_ptr<Matrix> f32_copy(const Matrix& m)
+{
+    if (m.kind == 1) fail(OWTK_ERR_INVALID_ARGUMENT, "mixed precision needs an owning matrix, not a split view");
+    auto c = std::make_unique<owtk_matrix>();
+    c->ctx = m.ctx;
+    c->kind = m.kind;
+    c->dtype = OWTK_F32;
+    c->owned = m.owned;
+    c->ghost = m.ghost;
+    c->bs = m.bs;
+    c->entries = m.entries;
+    c->h_rowptr = m.h_rowptr;
+    c->h_cols = m.h_cols;
+    c->rowptr = upload(m.ctx->stream, c->h_rowptr);
+    c->cols = upload(m.ctx->stream, c->h_cols);
+    build_tile_plan(*c);
+    const std::size_t per = m.kind == 2 ? m.bs * m.bs : m.bs;
+    c->values.allocate(m.entries * per * sizeof(float) + 16);
+    return c;
+}
+
+}  // namespace
+
+// FP64 in/out through an FP32 inner solve (owtk_pc_create_mixed).
+void mixed_apply(Preconditioner& p, Vector& in, Vector& out)
+{
+    Context& c = *p.ctx;
+    const std::size_t n = p.owned * p.bs;
+    owtk_vector vin, vout;
+    for (owtk_vector* v : {&vin, &vout}) {
+        v->ctx = p.ctx;
+        v->dtype = OWTK_F32;
+        v->owned = p.owned;
+        v->ghost = p.ghost;
+        v->bs = p.bs;
+        v->is_view = true;
+    }
+    vin.data = p.v32.ptr;
+    vout.data = p.z32.ptr;
+    kern::convert<float, double>(c, n, static_cast<const double*>(in.data), p.v32.as<float>());
+    if (p.inner_iterations == 0) {
+        apply_preconditioner(p.inner.get(), vin, vout);
+    } else {
+        kern::fill<float>(c, vout.local_size(), 0.0f, p.z32.as<float>());
+        owtk_solver_options o;
+        owtk_default_options(&o);
+        o.restart = p.inner_iterations;
+        o.maximum_iterations = p.inner_iterations;
+        o.relative_tolerance = 0;
+        o.absolute_tolerance = 0;
+        owtk_solver_result r;
+        solve(OWTK_SOLVER_FGMRES, *p.m32, p.inner.get(), vin, vout, o, *p.inner_ws, r);
+    }
+    kern::convert<double, float>(c, n, p.z32.as<float>(), static_cast<double*>(out.data));
+}
+
+}  // namespace owtk
+
+extern "C" {
+
 owtk_status owtk_pc_create(owtk_matrix* m, owtk_pc_kind kind, double parameter, owtk_preconditioner** out)
 {
     return guarded([&] {
         require(m != nullptr && out != nullptr, "null handle");
+        if (kind == OWTK_PC_MIXED) fail(OWTK_ERR_INVALID_ARGUMENT, "use owtk_pc_create_mixed");
+        *out = make_pc(m, kind, parameter, OWTK_F64).release();
+    });
+}
+
+owtk_status owtk_pc_create_stored(owtk_matrix* m, owtk_pc_kind kind, double parameter, owtk_dtype storage,
+                                  owtk_preconditioner** out)
+{
+    return guarded([&] {
+        require(m != nullptr && out != nullptr, "null handle");
+        *out = make_pc(m, kind, parameter, storage).release();
+    });
+}
+
+owtk_status owtk_pc_create_mixed(owtk_matrix* m, owtk_pc_kind inner_kind, double parameter, owtk_dtype storage,
+                                 uint32_t inner_iterations, owtk_preconditioner** out)
+{
+    return guarded([&] {
+        require(m != nullptr && out != nullptr, "null handle");
+        if (m->dtype != OWTK_F64) fail(OWTK_ERR_INVALID_ARGUMENT, "the mixed preconditioner serves FP64 solves");
+        if (storage == OWTK_F64) fail(OWTK_ERR_INVALID_ARGUMENT, "mixed precision stores factors in F32 or BF16");
         auto p = std::make_unique<owtk_preconditioner>();
         p->ctx = m->ctx;
-        p->kind = kind;
-        p->dtype = m->dtype;
+        p->kind = OWTK_PC_MIXED;
+        p->dtype = OWTK_F64;
         p->matrix = m;
         p->owned = m->owned;
         p->ghost = m->ghost;
         p->bs = m->bs;
         p->parameter = parameter;
-        const std::size_t n = m->owned * m->bs;
-        const std::size_t es = dsize(m->dtype);
-        switch (kind) {
-        case OWTK_PC_IDENTITY: break;
-        case OWTK_PC_JACOBI:
-            if (m->kind == 2) fail(OWTK_ERR_INVALID_ARGUMENT, "Jacobi needs a matrix with diagonal()");
-            p->inv_diag.allocate(n * es + 16);
-            break;
-        case OWTK_PC_SSOR:
-        case OWTK_PC_SPLIT_SSOR: {
-            if (kind == OWTK_PC_SSOR && m->kind != 0)
-                fail(OWTK_ERR_INVALID_ARGUMENT, "SSOR needs a component-diagonal BSR matrix");
-            if (kind == OWTK_PC_SPLIT_SSOR && m->kind != 1)
-                fail(OWTK_ERR_INVALID_ARGUMENT, "split SSOR needs a split view");
-            if (!(parameter > 0 && parameter < 2))
-                fail(OWTK_ERR_INVALID_ARGUMENT, kind == OWTK_PC_SSOR ? "SSOR omega must be in (0,2)"
-                                                                     : "split SSOR omega must be in (0,2)");
-            p->work.allocate(m->local_size() * es + 16);
-            if (kind == OWTK_PC_SSOR) p->diag_cache.allocate(n * es + 16);
-            std::vector<std::int32_t> lower, upper;
-            // The matrix pattern itself is the dependency pattern (ghosts excluded).
-            std::vector<std::int32_t> cols = m->h_cols;
-            for (auto& c : cols)
-                if (static_cast<std::size_t>(c) >= m->owned) c = static_cast<std::int32_t>(m->owned);
-            levels_of(m->owned, m->h_rowptr.data(), cols.data(), lower, upper);
-            build_sweep(*p->ctx, p->lower, m->owned, m->bs, lower, false);
-            build_sweep(*p->ctx, p->upper, m->owned, m->bs, upper, true);
-            break;
-        }
-        case OWTK_PC_ILU: {
-            if (m->kind != 0) fail(OWTK_ERR_INVALID_ARGUMENT, "ILU needs a component-diagonal BSR matrix");
-            if (!(parameter >= 0)) fail(OWTK_ERR_INVALID_ARGUMENT, "ILU fill level must be >= 0");
-            ilu_symbolic(*p, *m, static_cast<std::size_t>(parameter));
-            break;
-        }
-        default: fail(OWTK_ERR_INVALID_ARGUMENT, "unknown preconditioner kind");
-        }
-        if (kind == OWTK_PC_SSOR || kind == OWTK_PC_SPLIT_SSOR || kind == OWTK_PC_ILU) {
-            p->flags.allocate(m->owned * sizeof(unsigned) + 16);
-            OWTK_CUDA(cudaMemsetAsync(p->flags.ptr, 0, m->owned * sizeof(unsigned), p->ctx->stream));
-            p->ticket.allocate(sizeof(unsigned long long));
-            OWTK_CUDA(cudaMemsetAsync(p->ticket.ptr, 0, sizeof(unsigned long long), p->ctx->stream));
-        }
-        if (kind != OWTK_PC_IDENTITY) numeric_update(*p, *m);
-        p->ctx->sync();
+        p->storage = storage;
+        p->inner_iterations = inner_iterations;
+        p->m32 = f32_copy(*m);
+        p->inner = make_pc(m, inner_kind, parameter, storage);
+        p->inner_ws = std::make_unique<Workspace>();
+        p->inner_ws->ctx = m->ctx;
+        p->v32.allocate(m->local_size() * sizeof(float) + 16);
+        p->z32.allocate(m->local_size() * sizeof(float) + 16);
+        OWTK_CUDA(cudaMemsetAsync(p->v32.ptr, 0, m->local_size() * sizeof(float), m->ctx->stream));
+        const std::size_t per = m->kind == 2 ? m->bs * m->bs : m->bs;
+        kern::convert<float, double>(*m->ctx, m->entries * per, m->values.as<double>(), p->m32->values.as<float>());
+        p->numeric_updates = 1;
+        m->ctx->sync();
         *out = p.release();
     });
 }
@@ -853,7 +1042,12 @@ owtk_status owtk_pc_update_values(owtk_preconditioner* pc, owtk_matrix* m)
         require(pc != nullptr && m != nullptr, "null handle");
         if (m->owned != pc->owned || m->ghost != pc->ghost || m->bs != pc->bs || m->dtype != pc->dtype)
             fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner matrix layout mismatch");
-        if (pc->kind == OWTK_PC_ILU) ilu_pattern_check(*pc, *m);
+        if (pc->kind == OWTK_PC_ILU || pc->kind == OWTK_PC_BLOCK_ILU) ilu_pattern_check(*pc, *m);
+        if (pc->kind == OWTK_PC_MIXED) {
+            if (m->kind != pc->m32->kind) fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner matrix kind mismatch");
+            ilu_pattern_check(*pc->inner, *m);
+            pc->inner->matrix = m;
+        }
         if ((pc->kind == OWTK_PC_SSOR || pc->kind == OWTK_PC_SPLIT_SSOR) && m != pc->matrix)
             fail(OWTK_ERR_INVALID_ARGUMENT, "SSOR refreshes from the matrix it was built on");
         pc->matrix = m;
@@ -868,15 +1062,17 @@ owtk_status owtk_ilu_factors(owtk_preconditioner* pc, uint64_t* entries, uint64_
 {
     return guarded([&] {
         require(pc != nullptr && entries != nullptr, "null handle");
-        if (pc->kind != OWTK_PC_ILU) fail(OWTK_ERR_INVALID_ARGUMENT, "not an ILU preconditioner");
+        if (pc->kind != OWTK_PC_ILU && pc->kind != OWTK_PC_BLOCK_ILU)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "not an ILU preconditioner");
         *entries = pc->f_cols.size();
+        const std::size_t per = pc->block ? pc->bs * pc->bs : pc->bs;
         if (rowptr) for (std::size_t i = 0; i < pc->f_rowptr.size(); ++i) rowptr[i] = static_cast<std::uint64_t>(pc->f_rowptr[i]);
         if (cols) for (std::size_t i = 0; i < pc->f_cols.size(); ++i) cols[i] = static_cast<std::uint64_t>(pc->f_cols[i]);
         const std::size_t es = dsize(pc->dtype);
         if (values)
-            OWTK_CUDA(cudaMemcpyAsync(values, pc->d_fvalues.ptr, pc->f_cols.size() * pc->bs * es, cudaMemcpyDeviceToHost, pc->ctx->stream));
+            OWTK_CUDA(cudaMemcpyAsync(values, pc->d_fvalues.ptr, pc->f_cols.size() * per * es, cudaMemcpyDeviceToHost, pc->ctx->stream));
         if (inverse_diagonal)
-            OWTK_CUDA(cudaMemcpyAsync(inverse_diagonal, pc->inv_diag.ptr, pc->owned * pc->bs * es, cudaMemcpyDeviceToHost, pc->ctx->stream));
+            OWTK_CUDA(cudaMemcpyAsync(inverse_diagonal, pc->inv_diag.ptr, pc->owned * per * es, cudaMemcpyDeviceToHost, pc->ctx->stream));
         pc->ctx->sync();
     });
 }
@@ -886,7 +1082,8 @@ owtk_status owtk_pc_levels(owtk_preconditioner* pc, int32_t* lower, int32_t* upp
 {
     return guarded([&] {
         require(pc != nullptr, "null handle");
-        if (pc->kind != OWTK_PC_ILU && pc->kind != OWTK_PC_SSOR && pc->kind != OWTK_PC_SPLIT_SSOR)
+        if (pc->kind != OWTK_PC_ILU && pc->kind != OWTK_PC_SSOR && pc->kind != OWTK_PC_SPLIT_SSOR
+            && pc->kind != OWTK_PC_BLOCK_ILU)
             fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner has no sweep schedule");
         if (lower) std::copy(pc->lower.h_level.begin(), pc->lower.h_level.end(), lower);
         if (upper) std::copy(pc->upper.h_level.begin(), pc->upper.h_level.end(), upper);

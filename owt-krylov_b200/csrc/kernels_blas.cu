@@ -12,6 +12,8 @@
 
 #include <cmath>
 
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
 #include "owtk_internal.h"
 
@@ -265,6 +267,24 @@ __global__ void __launch_bounds__(kThreads) k_reciprocal(std::size_t n, const T*
             if (!isfinite(v) || fabs(v) <= minimum) atomicOr(status, kErrSingularDiagonal);
             inv[i] = div_rn(T(1), v);
         }
+    }
+}
+
+// Element-wise precision conversion (factor storage and mixed-precision
+// vector hand-off).
+__device__ __forceinline__ void cvt_store(float* d, double v) { *d = __double2float_rn(v); }
+__device__ __forceinline__ void cvt_store(double* d, float v) { *d = static_cast<double>(v); }
+__device__ __forceinline__ void cvt_store(__nv_bfloat16* d, double v) { *d = __double2bfloat16(v); }
+
+template<class To, class From>
+__global__ void __launch_bounds__(kThreads) k_convert(std::size_t n, const From* __restrict__ src,
+                                                      To* __restrict__ dst)
+{
+    EW_PROLOGUE
+#pragma unroll
+    for (int k = 0; k < kIlp; ++k) {
+        const std::size_t i = i0 + static_cast<std::size_t>(k) * kThreads;
+        if (i < n) cvt_store(dst + i, src[i]);
     }
 }
 
@@ -712,6 +732,14 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }
+
+template<class To, class From> void convert(Context& c, std::size_t n, const From* src, To* dst)
+{
+    LAUNCH_EW((k_convert<To, From>), n, src, dst);
+}
+template void convert<float, double>(Context&, std::size_t, const double*, float*);
+template void convert<double, float>(Context&, std::size_t, const float*, double*);
+template void convert<__nv_bfloat16, double>(Context&, std::size_t, const double*, __nv_bfloat16*);
 
 #define INSTANTIATE(T)                                                                              \
     template void fill<T>(Context&, std::size_t, T, T*);                                           \

@@ -27,6 +27,8 @@
 #include <cmath>
 #include <cstdlib>
 
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
 #include "owtk_internal.h"
 
@@ -37,9 +39,17 @@ using namespace dev;
 
 constexpr int kSpinLimit = 1 << 22;
 
-enum Mode { kIluForward, kIluBackward, kSsorForward, kSsorBackward, kIluFactor };
+enum Mode {
+    kIluForward, kIluBackward, kSsorForward, kSsorBackward, kIluFactor,
+    kBlockForward, kBlockBackward, kBlockFactor
+};
 
-template<class T>
+constexpr bool is_factor(int mode) { return mode == kIluFactor || mode == kBlockFactor; }
+constexpr int kMaxBlock = 4;   // dense-block ILU handles bs <= 4
+
+// T: vector / arithmetic type.  F: factor storage type (T, or float / bf16
+// storage under FP32 arithmetic).
+template<class T, class F = T>
 struct SweepArgs {
     const int* order;
     const int* task_start;
@@ -47,9 +57,9 @@ struct SweepArgs {
     const int* rowptr;      // dependency pattern (ILU factor pattern or matrix pattern)
     const int* cols;
     const int* diagpos;     // ILU only
-    T* vals;                // ILU factor values (written by the factorisation) or matrix/edge values
+    F* vals;                // ILU factor values (written by the factorisation) or matrix/edge values
     const T* diag;          // SSOR diagonal
-    T* inv;                 // ILU inverse diagonal (written by the factorisation)
+    F* inv;                 // ILU inverse diagonal (blocks for the dense-block ILU)
     const T* in;
     T* out;
     T* work;                // SSOR forward result
@@ -170,13 +180,17 @@ template<class T> __device__ __forceinline__ T pivot_tolerance();
 template<> __device__ __forceinline__ double pivot_tolerance<double>() { return 64.0 * DBL_EPSILON; }
 template<> __device__ __forceinline__ float pivot_tolerance<float>() { return 64.0f * FLT_EPSILON; }
 
+template<class T> __device__ __forceinline__ T cvt(double v) { return static_cast<T>(v); }
+template<class T> __device__ __forceinline__ T cvt(float v) { return static_cast<T>(v); }
+template<class T> __device__ __forceinline__ T cvt(__nv_bfloat16 v) { return static_cast<T>(__bfloat162float(v)); }
+
 // y -= sum_e vals[e][c] * dep[col_e][c] over e in [b, e) in entry order;
 // FILTER as in wait_deps, OMEGA multiplies each coefficient first (SSOR).
 // POLL: dependency values are read with relaxed loads and waited on until
 // they differ from the sentinel (applies); otherwise they are already final
 // (the caller waited on flags) and read through L2.
-template<class T, int FILTER, bool OMEGA, bool POLL>
-__device__ __forceinline__ T eliminate(T y, const SweepArgs<T>& a, const T* dep, int b, int e, int row, int c)
+template<class T, class F, int FILTER, bool OMEGA, bool POLL>
+__device__ __forceinline__ T eliminate(T y, const SweepArgs<T, F>& a, const T* dep, int b, int e, int row, int c)
 {
     using U = typename Bits<T>::U;
     const int bs = a.bs;
@@ -194,7 +208,7 @@ __device__ __forceinline__ T eliminate(T y, const SweepArgs<T>& a, const T* dep,
             on[j] = col >= 0;
             src[j] = dep + static_cast<std::size_t>(on[j] ? col : 0) * bs + c;
             if (on[j]) {
-                fv[j] = a.vals[static_cast<std::size_t>(k) * bs + c];
+                fv[j] = cvt<T>(a.vals[static_cast<std::size_t>(k) * bs + c]);
                 if (POLL) xb[j] = ld_relaxed_bits(src[j]);
                 else xv[j] = __ldcg(src[j]);
             }
@@ -231,39 +245,173 @@ __device__ __forceinline__ T eliminate(T y, const SweepArgs<T>& a, const T* dep,
     return y;
 }
 
-template<class T, int MODE>
-__device__ __forceinline__ void row_body(const SweepArgs<T>& a, int row, int c0, int cstep)
+// Dense-block rows: acc -= sum_k (sum_j B_k[i][j] dep[col_k][j]) over k in
+// [b, e), each block-row product summed from +0 over j (the dense SpMV's
+// order); dependency values are polled until published.
+template<class T, class F>
+__device__ __forceinline__ T block_eliminate(T acc, const SweepArgs<T, F>& a, const T* dep, int b, int e, int i)
+{
+    using U = typename Bits<T>::U;
+    const int bs = a.bs;
+    constexpr int kQ = 4;   // block entries per round
+    for (int k0 = b; k0 < e; k0 += kQ) {
+        T co[kQ][kMaxBlock], xv[kQ][kMaxBlock];
+        U xb[kQ][kMaxBlock];
+        const T* src[kQ];
+        bool on[kQ];
+#pragma unroll
+        for (int q = 0; q < kQ; ++q) {
+            const int k = k0 + q;
+            on[q] = k < e;
+            src[q] = dep + static_cast<std::size_t>(on[q] ? a.cols[k] : 0) * bs;
+#pragma unroll
+            for (int j = 0; j < kMaxBlock; ++j) {
+                if (on[q] && j < bs) {
+                    co[q][j] = cvt<T>(a.vals[(static_cast<std::size_t>(k) * bs + i) * bs + j]);
+                    xb[q][j] = ld_relaxed_bits(src[q] + j);
+                }
+            }
+        }
+        for (int it = 0;; ++it) {
+            bool pending = false;
+#pragma unroll
+            for (int q = 0; q < kQ; ++q)
+#pragma unroll
+                for (int j = 0; j < kMaxBlock; ++j)
+                    pending |= on[q] && j < bs && xb[q][j] == Bits<T>::kSentinel;
+            if (!pending) break;
+            if (it >= kSpinLimit) {
+                atomicOr(a.status, kErrTimeout);
+                break;
+            }
+            if ((it & 1023) == 1023 && (*reinterpret_cast<volatile unsigned*>(a.status) & kErrTimeout)) break;
+            if (it >= 256) __nanosleep(32);
+#pragma unroll
+            for (int q = 0; q < kQ; ++q)
+#pragma unroll
+                for (int j = 0; j < kMaxBlock; ++j)
+                    if (on[q] && j < bs && xb[q][j] == Bits<T>::kSentinel) xb[q][j] = ld_relaxed_bits(src[q] + j);
+        }
+#pragma unroll
+        for (int q = 0; q < kQ; ++q) {
+            if (!on[q]) continue;
+            T sum = 0;
+#pragma unroll
+            for (int j = 0; j < kMaxBlock; ++j) {
+                if (j < bs) {
+                    xv[q][j] = from_bits(xb[q][j]);
+                    sum = add_rn(sum, mul_rn(co[q][j], xv[q][j]));
+                }
+            }
+            acc = sub_rn(acc, sum);
+        }
+    }
+    return acc;
+}
+
+// In-place Gauss-Jordan inverse of a bs x bs block with partial pivoting
+// (the dense-block ILU's diagonal); returns false on a zero pivot.
+__device__ bool block_inverse(int bs, const double* a, double* inv)
+{
+    double m[kMaxBlock * kMaxBlock], r[kMaxBlock * kMaxBlock];
+    for (int i = 0; i < bs * bs; ++i) { m[i] = a[i]; r[i] = 0.0; }
+    for (int i = 0; i < bs; ++i) r[i * bs + i] = 1.0;
+    for (int c = 0; c < bs; ++c) {
+        int p = c;
+        for (int i = c + 1; i < bs; ++i)
+            if (fabs(m[i * bs + c]) > fabs(m[p * bs + c])) p = i;
+        if (!isfinite(m[p * bs + c]) || fabs(m[p * bs + c]) <= 64.0 * DBL_EPSILON) return false;
+        if (p != c) {
+            for (int j = 0; j < bs; ++j) {
+                double t = m[c * bs + j]; m[c * bs + j] = m[p * bs + j]; m[p * bs + j] = t;
+                t = r[c * bs + j]; r[c * bs + j] = r[p * bs + j]; r[p * bs + j] = t;
+            }
+        }
+        const double piv = m[c * bs + c];
+        for (int j = 0; j < bs; ++j) {
+            m[c * bs + j] = div_rn(m[c * bs + j], piv);
+            r[c * bs + j] = div_rn(r[c * bs + j], piv);
+        }
+        for (int i = 0; i < bs; ++i) {
+            if (i == c) continue;
+            const double f = m[i * bs + c];
+            for (int j = 0; j < bs; ++j) {
+                m[i * bs + j] = sub_rn(m[i * bs + j], mul_rn(f, m[c * bs + j]));
+                r[i * bs + j] = sub_rn(r[i * bs + j], mul_rn(f, r[c * bs + j]));
+            }
+        }
+    }
+    for (int i = 0; i < bs * bs; ++i) inv[i] = r[i];
+    return true;
+}
+
+template<class T, class F, int MODE>
+__device__ __forceinline__ T row_body(const SweepArgs<T, F>& a, int row, int c0, int cstep)
 {
     const int bs = a.bs;
     const std::size_t rb = static_cast<std::size_t>(row) * bs;
     // Row-local operands are loaded before the dependency wait so their
     // latency is not added to the level-to-level critical path.
-    if (MODE == kIluForward) {          // in -> work (unit lower solve)
+    if constexpr (MODE == kIluForward) {          // in -> work (unit lower solve)
         const int b = a.rowptr[row], d = a.diagpos[row];
         for (int c = c0; c < bs; c += cstep) {
             const T own = a.in[rb + c];
-            publish(a.work + rb + c, eliminate<T, 0, false, true>(own, a, a.work, b, d, row, c));
+            publish(a.work + rb + c, eliminate<T, F, 0, false, true>(own, a, a.work, b, d, row, c));
         }
-    } else if (MODE == kIluBackward) {  // work -> out (upper solve, times the inverse diagonal)
+    } else if constexpr (MODE == kIluBackward) {  // work -> out (upper solve, times the inverse diagonal)
         const int d = a.diagpos[row], end = a.rowptr[row + 1];
         for (int c = c0; c < bs; c += cstep) {
-            const T own = a.work[rb + c], inv = a.inv[rb + c];
-            publish(a.out + rb + c, mul_rn(eliminate<T, 0, false, true>(own, a, a.out, d + 1, end, row, c), inv));
+            const T own = a.work[rb + c], inv = cvt<T>(a.inv[rb + c]);
+            publish(a.out + rb + c, mul_rn(eliminate<T, F, 0, false, true>(own, a, a.out, d + 1, end, row, c), inv));
         }
-    } else if (MODE == kSsorForward) {  // in -> work
+    } else if constexpr (MODE == kSsorForward) {  // in -> work
         const int b = a.rowptr[row], end = a.rowptr[row + 1];
         for (int c = c0; c < bs; c += cstep) {
             const T own = a.in[rb + c], dg = a.diag[rb + c];
-            publish(a.work + rb + c, div_rn(eliminate<T, 1, true, true>(own, a, a.work, b, end, row, c), dg));
+            publish(a.work + rb + c, div_rn(eliminate<T, F, 1, true, true>(own, a, a.work, b, end, row, c), dg));
         }
-    } else if (MODE == kSsorBackward) { // work -> out
+    } else if constexpr (MODE == kSsorBackward) { // work -> out
         const int b = a.rowptr[row], end = a.rowptr[row + 1];
         for (int c = c0; c < bs; c += cstep) {
             const T dg = a.diag[rb + c];
             const T z0 = mul_rn(dg, a.work[rb + c]);
-            publish(a.out + rb + c, div_rn(eliminate<T, 2, true, true>(z0, a, a.out, b, end, row, c), dg));
+            publish(a.out + rb + c, div_rn(eliminate<T, F, 2, true, true>(z0, a, a.out, b, end, row, c), dg));
         }
-    } else {  // kIluFactor: IKJ elimination of one row (preconditioner.hpp:442-469)
+    } else if constexpr (MODE == kBlockForward) {  // in -> work, block row c0 of the row
+        const int b = a.rowptr[row], d = a.diagpos[row];
+        const T own = a.in[rb + c0];
+        publish(a.work + rb + c0, block_eliminate<T, F>(own, a, a.work, b, d, c0));
+    } else if constexpr (MODE == kBlockBackward) { // returns w = y - sum U x; the caller applies Dinv
+        const int d = a.diagpos[row], end = a.rowptr[row + 1];
+        const T own = a.work[rb + c0];
+        return block_eliminate<T, F>(own, a, a.out, d + 1, end, c0);
+    } else if constexpr (MODE == kBlockFactor) {   // block IKJ of one row; lane = block row c0
+        const int b = a.rowptr[row], d = a.diagpos[row];
+        wait_deps<0>(a.flags, a.cols, b, d, row, a.owned, a.epoch, a.status);
+        const int i = c0;
+        const std::size_t b2 = static_cast<std::size_t>(bs) * bs;
+        for (int l = b; l < d; ++l) {
+            const int p = a.cols[l];
+            T arow[kMaxBlock], lrow[kMaxBlock];
+            for (int j = 0; j < bs; ++j) arow[j] = a.vals[l * b2 + i * bs + j];
+            const F* dp = a.inv + static_cast<std::size_t>(p) * b2;
+            for (int k = 0; k < bs; ++k) {
+                T sum = 0;
+                for (int j = 0; j < bs; ++j) sum = add_rn(sum, mul_rn(arow[j], __ldcg(dp + j * bs + k)));
+                lrow[k] = sum;
+            }
+            for (int k = 0; k < bs; ++k) a.vals[l * b2 + i * bs + k] = lrow[k];
+            for (int u = a.upd_start[l]; u < a.upd_start[l + 1]; ++u) {
+                const F* ub = a.vals + static_cast<std::size_t>(a.upd_upper[u]) * b2;
+                F* tb = a.vals + static_cast<std::size_t>(a.upd_target[u]) * b2 + i * bs;
+                for (int k = 0; k < bs; ++k) {
+                    T sum = 0;
+                    for (int j = 0; j < bs; ++j) sum = add_rn(sum, mul_rn(lrow[j], __ldcg(ub + j * bs + k)));
+                    tb[k] = sub_rn(tb[k], sum);
+                }
+            }
+        }
+    } else if constexpr (MODE == kIluFactor) {  // IKJ elimination of one row (preconditioner.hpp:442-469)
         const int b = a.rowptr[row], d = a.diagpos[row];
         wait_deps<0>(a.flags, a.cols, b, d, row, a.owned, a.epoch, a.status);
         const T tol = pivot_tolerance<T>();
@@ -285,10 +433,11 @@ __device__ __forceinline__ void row_body(const SweepArgs<T>& a, int row, int c0,
             a.inv[rb + c] = div_rn(T(1), dv);
         }
     }
+    return T(0);
 }
 
-template<class T, int MODE>
-__global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T> a)
+template<class T, class F, int MODE>
+__global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T, F> a)
 {
     const int lane = threadIdx.x & 31;
     const int bs = a.bs;
@@ -312,8 +461,34 @@ __global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T> a)
         if (lane == 0) next = atomicAdd(a.ticket, 1ull) - a.base;
         const int s = a.task_start[t], nrows = a.task_start[t + 1] - s;
         const int row = rl < nrows ? a.order[s + rl] : -1;
-        if (row >= 0) row_body<T, MODE>(a, row, c0, cstep);
-        if (MODE == kIluFactor) {
+        T w = 0;
+        if (row >= 0) w = row_body<T, F, MODE>(a, row, c0, cstep);
+        if constexpr (MODE == kBlockBackward) {
+            // x_r[i] = sum_j Dinv_r[i][j] w_j: the row's w_j live in the
+            // lanes rl*bs + j of this warp.
+            __syncwarp();
+            const int base = (rl * bs) & 31;
+            T x = 0;
+            for (int j = 0; j < bs; ++j) {
+                const T wj = __shfl_sync(0xffffffffu, w, (base + j) & 31);
+                if (row >= 0)
+                    x = add_rn(x, mul_rn(cvt<T>(a.inv[static_cast<std::size_t>(row) * bs * bs + c0 * bs + j]), wj));
+            }
+            if (row >= 0) publish(a.out + static_cast<std::size_t>(row) * bs + c0, x);
+        }
+        if constexpr (MODE == kBlockFactor) {
+            // The row's diagonal block is final: invert it (one lane per row).
+            __syncwarp();
+            if (row >= 0 && c0 == 0) {
+                const std::size_t b2 = static_cast<std::size_t>(bs) * bs;
+                double blk[kMaxBlock * kMaxBlock], inv[kMaxBlock * kMaxBlock];
+                const F* dblk = a.vals + static_cast<std::size_t>(a.diagpos[row]) * b2;
+                for (std::size_t q = 0; q < b2; ++q) blk[q] = static_cast<double>(dblk[q]);
+                if (!block_inverse(bs, blk, inv)) atomicOr(a.status, kErrZeroPivot);
+                for (std::size_t q = 0; q < b2; ++q) a.inv[static_cast<std::size_t>(row) * b2 + q] = static_cast<F>(inv[q]);
+            }
+        }
+        if constexpr (is_factor(MODE)) {
             __syncwarp();
             if (lane < nrows) {
                 __threadfence();
@@ -340,11 +515,11 @@ int sweep_warps(const Context& c, const Sweep& s)
     return static_cast<int>(warps);
 }
 
-template<class T, int MODE>
-void launch(Context& c, Preconditioner& p, Sweep& s, SweepArgs<T>& a)
+template<class T, class F, int MODE>
+void launch(Context& c, Preconditioner& p, Sweep& s, SweepArgs<T, F>& a)
 {
     if (s.tasks == 0) return;
-    if (MODE == kIluFactor && ++p.epoch == 0xffffffffu) {
+    if (is_factor(MODE) && ++p.epoch == 0xffffffffu) {
         OWTK_CUDA(cudaMemsetAsync(p.flags.ptr, 0, p.owned * sizeof(unsigned), c.stream));
         p.epoch = 1;
     }
@@ -360,7 +535,7 @@ void launch(Context& c, Preconditioner& p, Sweep& s, SweepArgs<T>& a)
     a.status = c.status.as<unsigned>();
     a.owned = static_cast<int>(p.owned);
     a.bs = static_cast<int>(p.bs);
-    k_sweep<T, MODE><<<blocks, kThreads, 0, c.stream>>>(a);
+    k_sweep<T, F, MODE><<<blocks, kThreads, 0, c.stream>>>(a);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
     p.ticket_base += static_cast<unsigned long long>(s.tasks)
@@ -384,7 +559,7 @@ template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* mat
     a.upd_start = p.d_upd_start.as<int>();
     a.upd_target = p.d_upd_target.as<int>();
     a.upd_upper = p.d_upd_upper.as<int>();
-    launch<T, kIluFactor>(c, p, p.lower, a);
+    launch<T, T, kIluFactor>(c, p, p.lower, a);
 }
 
 template<class T> void fill_sentinel(Context& c, std::size_t n, T* x)
@@ -410,9 +585,9 @@ template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* 
     a.work = p.work.as<T>();
     const std::size_t n = p.owned * p.bs;
     fill_sentinel<T>(c, n, a.work);
-    launch<T, kIluForward>(c, p, p.lower, a);
+    launch<T, T, kIluForward>(c, p, p.lower, a);
     fill_sentinel<T>(c, n, out);
-    launch<T, kIluBackward>(c, p, p.upper, a);
+    launch<T, T, kIluBackward>(c, p, p.upper, a);
 }
 
 template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T* out)
@@ -429,13 +604,77 @@ template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T*
     a.omega = static_cast<T>(p.parameter);
     const std::size_t n = p.owned * p.bs;
     fill_sentinel<T>(c, n, a.work);
-    launch<T, kSsorForward>(c, p, p.lower, a);
+    launch<T, T, kSsorForward>(c, p, p.lower, a);
     fill_sentinel<T>(c, n, out);
-    launch<T, kSsorBackward>(c, p, p.upper, a);
+    launch<T, T, kSsorBackward>(c, p, p.upper, a);
     const T omega = static_cast<T>(p.parameter);
     if (omega != T(1)) scale<T>(c, p.owned * p.bs, omega * (T(2) - omega), out);
 }
 
+// ILU(k) with low-precision factor storage F (float or bf16) and FP32
+// vectors / arithmetic: the inner preconditioner of mixed-precision solves.
+template<class F> void ilu_apply_lp(Context& c, Preconditioner& p, const float* in, float* out)
+{
+    SweepArgs<float, F> a{};
+    a.rowptr = p.d_frowptr.as<int>();
+    a.cols = p.d_fcols.as<int>();
+    a.diagpos = p.d_fdiagpos.as<int>();
+    a.vals = p.lp_vals.as<F>();
+    a.inv = p.lp_inv.as<F>();
+    a.in = in;
+    a.out = out;
+    a.work = p.work32.as<float>();
+    const std::size_t n = p.owned * p.bs;
+    fill_sentinel<float>(c, n, a.work);
+    if (p.block) {
+        launch<float, F, kBlockForward>(c, p, p.lower, a);
+        fill_sentinel<float>(c, n, out);
+        launch<float, F, kBlockBackward>(c, p, p.upper, a);
+    } else {
+        launch<float, F, kIluForward>(c, p, p.lower, a);
+        fill_sentinel<float>(c, n, out);
+        launch<float, F, kIluBackward>(c, p, p.upper, a);
+    }
+}
+
+// Dense-block ILU(0): FP64 factorisation (bs <= 4) reusing the symbolic
+// pattern, update lists and level sets of the component-diagonal ILU.
+void block_ilu_factorize(Context& c, Preconditioner& p, const double* matrix_values)
+{
+    gather_values<double>(c, p.f_cols.size(), p.bs * p.bs, p.d_fsource.as<std::int64_t>(), matrix_values,
+                          p.d_fvalues.as<double>());
+    SweepArgs<double> a{};
+    a.rowptr = p.d_frowptr.as<int>();
+    a.cols = p.d_fcols.as<int>();
+    a.diagpos = p.d_fdiagpos.as<int>();
+    a.vals = p.d_fvalues.as<double>();
+    a.inv = p.inv_diag.as<double>();
+    a.upd_start = p.d_upd_start.as<int>();
+    a.upd_target = p.d_upd_target.as<int>();
+    a.upd_upper = p.d_upd_upper.as<int>();
+    launch<double, double, kBlockFactor>(c, p, p.lower, a);
+}
+
+void block_ilu_apply(Context& c, Preconditioner& p, const double* in, double* out)
+{
+    SweepArgs<double> a{};
+    a.rowptr = p.d_frowptr.as<int>();
+    a.cols = p.d_fcols.as<int>();
+    a.diagpos = p.d_fdiagpos.as<int>();
+    a.vals = p.d_fvalues.as<double>();
+    a.inv = p.inv_diag.as<double>();
+    a.in = in;
+    a.out = out;
+    a.work = p.work.as<double>();
+    const std::size_t n = p.owned * p.bs;
+    fill_sentinel<double>(c, n, a.work);
+    launch<double, double, kBlockForward>(c, p, p.lower, a);
+    fill_sentinel<double>(c, n, out);
+    launch<double, double, kBlockBackward>(c, p, p.upper, a);
+}
+
+template void ilu_apply_lp<float>(Context&, Preconditioner&, const float*, float*);
+template void ilu_apply_lp<__nv_bfloat16>(Context&, Preconditioner&, const float*, float*);
 template void ilu_factorize<double>(Context&, Preconditioner&, const double*);
 template void ilu_factorize<float>(Context&, Preconditioner&, const float*);
 template void ilu_apply<double>(Context&, Preconditioner&, const double*, double*);

@@ -118,6 +118,17 @@ struct Matrix {
     std::size_t local_size() const { return (owned + ghost) * bs; }
 };
 
+struct Workspace {
+    Context* ctx = nullptr;
+    std::vector<std::unique_ptr<Vector>> vectors;
+    std::vector<std::unique_ptr<Vector>> stage;   // host-buffer solve staging (rhs, x)
+    std::size_t scalar_capacity = 0;              // host scalar arrays (Hessenberg etc.)
+    std::uint64_t epochs = 0;
+    // core.hpp:405-423: (re)allocate when the layout changes or more vectors /
+    // scalars are needed; each growth counts one allocation epoch.
+    void prepare(const Vector& layout, std::size_t count, std::size_t scalars = 0);
+};
+
 // A scheduled triangular sweep: rows ordered by (level, row), cut into warp
 // tasks that never straddle a level; dependencies are the row's entries whose
 // column lies on the solved side.
@@ -155,18 +166,19 @@ struct Preconditioner {
     DeviceBuffer ticket;       // uint64 monotone task counter
     std::uint32_t epoch = 0;
     std::uint64_t ticket_base = 0;
+    // Dense-block ILU: bs x bs factor blocks, inverse diagonal blocks.
+    bool block = false;
+    // Factor storage precision; F32 / BF16 copies are applied to FP32 vectors.
+    owtk_dtype storage = OWTK_F64;
+    DeviceBuffer lp_vals, lp_inv, work32;
+    // Mixed-precision wrapper: FP64 in/out, FP32 inner solve.
+    std::unique_ptr<Matrix> m32;
+    std::unique_ptr<Preconditioner> inner;
+    std::unique_ptr<Workspace> inner_ws;
+    unsigned inner_iterations = 0;
+    DeviceBuffer v32, z32;
 };
 
-struct Workspace {
-    Context* ctx = nullptr;
-    std::vector<std::unique_ptr<Vector>> vectors;
-    std::vector<std::unique_ptr<Vector>> stage;   // host-buffer solve staging (rhs, x)
-    std::size_t scalar_capacity = 0;              // host scalar arrays (Hessenberg etc.)
-    std::uint64_t epochs = 0;
-    // core.hpp:405-423: (re)allocate when the layout changes or more vectors /
-    // scalars are needed; each growth counts one allocation epoch.
-    void prepare(const Vector& layout, std::size_t count, std::size_t scalars = 0);
-};
 
 // ---------------------------------------------------------------- setup (setup.cpp)
 void build_tile_plan(Matrix& m);
@@ -229,6 +241,10 @@ template<class T> void reciprocal_checked(Context& c, std::size_t n, const T* d,
 template<class T> void bsr_diagonal(Context& c, const Matrix& m, T* out);
 
 template<class T> void scaled_copy(Context& c, std::size_t n, const T* x, T s, T* out);
+template<class To, class From> void convert(Context& c, std::size_t n, const From* src, To* dst);
+template<class F> void ilu_apply_lp(Context& c, Preconditioner& p, const float* in, float* out);
+void block_ilu_factorize(Context& c, Preconditioner& p, const double* matrix_values);
+void block_ilu_apply(Context& c, Preconditioner& p, const double* in, double* out);
 
 }  // namespace kern
 

@@ -14,8 +14,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libowtk_b200.so")
 
-F64, F32 = 0, 1
-PC_IDENTITY, PC_JACOBI, PC_SSOR, PC_SPLIT_SSOR, PC_ILU = 0, 1, 2, 3, 4
+F64, F32, BF16 = 0, 1, 2
+PC_IDENTITY, PC_JACOBI, PC_SSOR, PC_SPLIT_SSOR, PC_ILU, PC_BLOCK_ILU, PC_MIXED = 0, 1, 2, 3, 4, 5, 6
 FGMRES, BICGSTAB, PIPELINED_BICGSTAB, COMM_HIDING_BICGSTAB, IDRS = 0, 1, 2, 3, 4
 
 STATUS = {0: "ok", 1: "invalid_argument", 2: "zero_pivot", 3: "out_of_range", 4: "cuda_error",
@@ -101,6 +101,8 @@ def lib():
             "owtk_matrix_diagonal": (c_int, [vp, vp]),
             "owtk_pc_create": (c_int, [vp, c_int, c_double, POINTER(vp)]),
             "owtk_pc_destroy": (c_int, [vp]),
+            "owtk_pc_create_stored": (c_int, [vp, c_int, c_double, c_int, POINTER(vp)]),
+            "owtk_pc_create_mixed": (c_int, [vp, c_int, c_double, c_int, ctypes.c_uint32, POINTER(vp)]),
             "owtk_pc_apply": (c_int, [vp, vp, vp]),
             "owtk_pc_update_values": (c_int, [vp, vp]),
             "owtk_pc_numeric_updates": (c_uint64, [vp]),
@@ -325,9 +327,19 @@ class Matrix:
 
 
 class Preconditioner:
-    def __init__(self, matrix: Matrix, kind: int, parameter: float = 0.0):
+    """storage F32/BF16: factors kept in that precision (FP32 applies);
+    mixed_inner >= 0: FP64 wrapper around an FP32 inner solve of that many
+    GMRES steps (0: one factor apply)."""
+
+    def __init__(self, matrix: Matrix, kind: int, parameter: float = 0.0, storage: int = F64,
+                 mixed_inner: int | None = None):
         h = c_void_p()
-        check(lib().owtk_pc_create(matrix.h, kind, parameter, ctypes.byref(h)))
+        if mixed_inner is not None:
+            check(lib().owtk_pc_create_mixed(matrix.h, kind, parameter, storage, mixed_inner, ctypes.byref(h)))
+        elif storage != F64:
+            check(lib().owtk_pc_create_stored(matrix.h, kind, parameter, storage, ctypes.byref(h)))
+        else:
+            check(lib().owtk_pc_create(matrix.h, kind, parameter, ctypes.byref(h)))
         self.h, self.matrix, self.kind = h, matrix, kind
 
     def apply(self, x: Vector, y: Vector):
@@ -344,10 +356,11 @@ class Preconditioner:
         n = c_uint64()
         check(lib().owtk_ilu_factors(self.h, ctypes.byref(n), None, None, None, None))
         m = self.matrix
+        per = m.bs * m.bs if self.kind == PC_BLOCK_ILU else m.bs
         rp = np.empty(m.owned + 1, dtype=np.uint64)
         ci = np.empty(max(1, n.value), dtype=np.uint64)
-        vals = np.empty(n.value * m.bs, dtype=m.dtype)
-        inv = np.empty(m.owned * m.bs, dtype=m.dtype)
+        vals = np.empty(n.value * per, dtype=m.dtype)
+        inv = np.empty(m.owned * per, dtype=m.dtype)
         check(lib().owtk_ilu_factors(self.h, ctypes.byref(n), _ptr(rp), _ptr(ci), _ptr(vals), _ptr(inv)))
         return rp, ci[:n.value], vals, inv
 
