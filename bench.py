@@ -41,6 +41,20 @@ def parse():
     p.add_argument("--vertices", type=int, default=2_000_000)
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernels", action="store_true",
+                   help="standalone kernel throughput sweep (one JSON line per kernel) instead of the solve")
+    p.add_argument("--bs", default="3", help="block sizes of the kernel sweep, comma separated")
+    p.add_argument("--orders", default="rcm", help="vertex orders of the kernel sweep: rcm,hilbert")
+    p.add_argument("--only", default="", help="kernel sweep: comma-separated subset of "
+                   "spmv,split,spmv32,ilu,ssor,dot,norm,axpy")
+    p.add_argument("--reps", type=int, default=20, help="kernel sweep: timed launches per kernel")
+    p.add_argument("--form", choices=["plain", "mixed", "batching", "learned"], default="plain",
+                   help="plain: the FP64 GMRES(30)+ILU(0) headline; mixed / batching / learned: the three "
+                        "other forms, one JSON line each")
+    p.add_argument("--systems", type=int, default=256, help="batching: number of systems")
+    p.add_argument("--draws", type=int, default=32, help="learned: coefficient draws of the training mesh")
+    p.add_argument("--train-vertices", type=int, default=200_000, help="learned: training mesh size")
+    p.add_argument("--epochs", type=int, default=4, help="learned: passes over the training pairs")
     return p.parse_args()
 
 
@@ -68,9 +82,10 @@ class Clocks:
                "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-               "--format=csv,noheader,nounits", "-lms", "200"]
+               "--format=csv,noheader,nounits", "-lms", "50"]
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)   # the sampler is running before the timed region starts
         except OSError:
             self.proc = None
         return self
@@ -109,12 +124,7 @@ def build_system(n_vertices: int, seed: int):
 
 def algorithmic_bytes(s, ilu_entries: int):
     n, bs, nnz = s.owned, s.bs, s.nnz
-    spmv = nnz * (bs * 8 + 4) + (n + 1) * 4 + 2 * n * bs * 8
-    # Forward + backward ILU sweep: factor values + columns once, row offsets
-    # and diagonal positions, inverse diagonal, input read, output written and
-    # re-read by the backward sweep.
-    ilu = ilu_entries * (bs * 8 + 4) + 2 * (n + 1) * 4 + n * 4 + n * bs * 8 + 3 * n * bs * 8
-    return spmv, ilu
+    return kernel_bytes("spmv", n, bs, nnz), kernel_bytes("ilu", n, bs, nnz, factor_entries=ilu_entries)
 
 
 def cpu_reference_solve(s, reps: int, native_build: bool = False):
@@ -306,10 +316,379 @@ def run_ours(args):
     return 0
 
 
+def kernel_bytes(kind: str, n: int, bs: int, nnz: int, sv: int = 8, factor_entries: int = 0, k: int = 16,
+                 off_entries: int = 0) -> int:
+    """Algorithmic HBM bytes of one launch (values, 32-bit indices, vectors
+    each read or written once)."""
+    vec = n * bs * sv
+    if kind in ("spmv", "spmv32"):
+        return nnz * (bs * sv + 4) + (n + 1) * 4 + 2 * vec
+    if kind == "split":
+        return vec + off_entries * (bs * sv + 4) + (n + 1) * 4 + 2 * vec
+    if kind == "ilu":
+        return algorithmic_bytes_ilu(n, bs, factor_entries)
+    if kind == "ssor":
+        return 2 * (nnz * (bs * sv + 4) + (n + 1) * 4) + 3 * vec
+    if kind == "dot":
+        return (k + 1) * vec
+    if kind == "norm":
+        return vec
+    if kind == "axpy":
+        return 3 * vec
+    raise ValueError(kind)
+
+
+def algorithmic_bytes_ilu(n: int, bs: int, factor_entries: int) -> int:
+    # Forward + backward ILU sweep: factor values + columns once, row offsets
+    # and diagonal positions, inverse diagonal, input read, output written and
+    # re-read by the backward sweep.
+    return factor_entries * (bs * 8 + 4) + 2 * (n + 1) * 4 + n * 4 + n * bs * 8 + 3 * n * bs * 8
+
+
+def run_kernels(args):
+    """Standalone throughput sweep of the hot kernels on the Poisson-disk /
+    Delaunay disk mesh: each kernel launched `--reps` times back to back on the
+    library's stream and timed with CUDA events; the matrices exceed L2, so
+    every launch streams them from HBM.  One JSON line per (order, bs, kernel)."""
+    import torch
+    from owtk_b200 import native, problems
+
+    peak, peak_kind = measured_peaks()
+    only = set(filter(None, args.only.split(","))) or {"spmv", "split", "spmv32", "ilu", "ssor", "dot", "norm", "axpy"}
+    t = time.time()
+    xy, edges = problems.disk_mesh(args.vertices, args.seed)
+    gen_s = time.time() - t
+    ctx = native.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+
+    def timed(fn, reps):
+        fn()
+        ctx.synchronize()
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        c.record(stream)
+        c.synchronize()
+        return a.elapsed_time(c) / reps * 1e3   # microseconds per launch
+
+    for order in args.orders.split(","):
+        for bs in [int(b) for b in args.bs.split(",")]:
+            s = problems.component_diagonal_system(xy, edges, bs, np.random.default_rng(args.seed), order=order)
+            n, nnz = s.owned, s.nnz
+            m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
+            x = native.Vector(ctx, n, 0, bs).upload(s.rhs)
+            y = native.Vector(ctx, n, 0, bs)
+            results = []
+
+            def emit(kind, us, nbytes, **extra):
+                gbs = nbytes / (us * 1e-6) / 1e9
+                line = {"kernel": kind, "order": order, "block_size": bs, "vertices": n, "entries": nnz,
+                        "us_per_launch": round(us, 2), "bytes_per_launch": int(nbytes), "achieved_gbs": round(gbs, 1),
+                        "peak_gbs": peak, "frac": round(gbs / peak, 4), "peak_source": peak_kind,
+                        "reps": args.reps, "mesh_gen_s": round(gen_s, 1)}
+                line.update(extra)
+                results.append(line)
+                print(json.dumps(line), flush=True)
+
+            if "spmv" in only:
+                emit("spmv", timed(lambda: m.apply(x, y), args.reps), kernel_bytes("spmv", n, bs, nnz))
+            if "split" in only:
+                orp, oci, diag, off = s.split()
+                d = native.Vector(ctx, n, 0, bs).upload(diag)
+                o = native.Vector(ctx, max(off.size // bs, 1), 0, bs).upload(off)
+                sm = native.Matrix(ctx, "split", n, 0, bs, orp, oci, diag_ptr=d.data_ptr, off_ptr=o.data_ptr)
+                emit("split", timed(lambda: sm.apply(x, y), args.reps),
+                     kernel_bytes("split", n, bs, nnz, off_entries=int(orp[-1])))
+            if "spmv32" in only:
+                m32 = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals, dtype=np.float32)
+                x32 = native.Vector(ctx, n, 0, bs, dtype=np.float32).upload(s.rhs)
+                y32 = native.Vector(ctx, n, 0, bs, dtype=np.float32)
+                emit("spmv32", timed(lambda: m32.apply(x32, y32), args.reps), kernel_bytes("spmv32", n, bs, nnz, sv=4))
+            if "ilu" in only:
+                pc = native.Preconditioner(m, native.PC_ILU, 0)
+                fe = int(pc.ilu_factors()[1].size)
+                _, _, depth_lower, depth_upper = pc.levels()
+                emit("ilu", timed(lambda: pc.apply(x, y), max(2, args.reps // 4)),
+                     kernel_bytes("ilu", n, bs, nnz, factor_entries=fe),
+                     lower_levels=int(depth_lower), upper_levels=int(depth_upper))
+            if "ssor" in only:
+                ps = native.Preconditioner(m, native.PC_SSOR, 1.0)
+                emit("ssor", timed(lambda: ps.apply(x, y), max(2, args.reps // 4)), kernel_bytes("ssor", n, bs, nnz))
+            if "dot" in only:
+                basis = [native.Vector(ctx, n, 0, bs).upload(s.rhs) for _ in range(16)]
+                emit("dot", timed(lambda: native.dot_batch(x, basis), args.reps), kernel_bytes("dot", n, bs, nnz, k=16),
+                     note="16 dot products against one vector, result read on the host")
+            if "norm" in only:
+                emit("norm", timed(lambda: native.norm(x), args.reps), kernel_bytes("norm", n, bs, nnz),
+                     note="one-pass scaled norm, result read on the host")
+            if "axpy" in only:
+                emit("axpy", timed(lambda: native.axpy(0.5, x, y), args.reps), kernel_bytes("axpy", n, bs, nnz))
+            ctx.synchronize()
+    return 0
+
+# ---------------------------------------------------------------- other forms
+def _event_time(stream, fn, steps):
+    import torch
+
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    c.record(stream)
+    c.synchronize()
+    return a.elapsed_time(c) / steps
+
+
+def _line(args, workload, value_s, e2e_s, cfg, dtype, extra):
+    line = {"metric": METRIC, "value": value_s, "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value_s * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": dict({"workload": workload}, **cfg)}
+    if e2e_s is not None:
+        line["e2e"] = e2e_s
+    line.update(extra)
+    return line
+
+
+def run_batching(args):
+    """256 uneven systems (log-uniform 5k-200k vertices, aspect U(1,4), bs in
+    {1,2,3,4}) by BiCGSTAB + Jacobi to rtol 1e-8 in one persistent,
+    graph-captured launch after the autotuner picked the launch shape."""
+    import torch
+    from owtk_b200 import native, problems
+
+    t = time.time()
+    systems = problems.batch_systems(count=args.systems, seed=3)
+    gen_s = time.time() - t
+    ctx = native.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    t = time.time()
+    batch = native.Batch(ctx, systems)
+    create_s = time.time() - t
+    t = time.time()
+    bps, vpw = batch.autotune()
+    tune_s = time.time() - t
+    rhs = np.concatenate([y.rhs for y in systems])
+    rv = native.Vector(ctx, rhs.size, 0, 1).upload(rhs)
+    xv = native.Vector(ctx, rhs.size, 0, 1)
+    opts = native.default_options()
+    res = None
+
+    def step():
+        nonlocal res
+        xv.fill(0.0)
+        res = batch.solve(rv, xv, opts)
+
+    for _ in range(args.warmup):
+        step()
+    launches0 = ctx.kernel_launches
+    with Clocks(0) as clk:
+        ms = _event_time(stream, step, args.steps)
+    launches = (ctx.kernel_launches - launches0) // args.steps
+    status = [r.status for r in res]
+    its = np.array([r.iterations for r in res])
+    # e2e: pinned host rhs / x copied in and x copied out inside the call.
+    hb = torch.from_numpy(rhs).pin_memory()
+    hx = torch.zeros(rhs.size, dtype=torch.float64).pin_memory()
+
+    def host_step():
+        hx.zero_()
+        batch.solve_host(hb.data_ptr(), hx.data_ptr(), opts)
+
+    host_step()
+    e2e_ms = _event_time(stream, host_step, args.steps)
+    # Algorithmic bytes: per iteration two SpMV passes and ~21 vector passes
+    # (element-wise phases and the fused dot operands); setup SpMV + 3 passes.
+    total = 0
+    for y, k in zip(systems, its):
+        n, bs, nnz = y.owned, y.bs, y.nnz
+        spmv = nnz * (bs * 8 + 4) + (n + 1) * 4 + 2 * n * bs * 8
+        total += int(k) * (2 * spmv + 21 * n * bs * 8) + spmv + 3 * n * bs * 8
+    peak, peak_kind = measured_peaks()
+    achieved = total / (ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = _cpu_batch_sample(systems, its)
+    extra = {"e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * rhs.size * 8,
+                     "d2h_bytes_per_step": rhs.size * 8},
+             "roofline": {"bound": "hbm", "kernel": "k_batch_bicgstab (whole persistent launch)", "achieved": achieved,
+                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                          "bytes_per_launch": total, "ms_per_launch": ms, "peak_source": peak_kind},
+             "batch": {"systems": len(systems), "vertices": int(sum(y.owned for y in systems)),
+                       "unknowns": int(rhs.size), "entries": int(sum(y.nnz for y in systems)),
+                       "converged": int(sum(1 for v in status if v == 0)), "iterations_min": int(its.min()),
+                       "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
+                       "blocks_per_sm": bps, "vertices_per_warp": {str(b): vpw[b] for b in (1, 2, 3, 4)},
+                       "generate_s": gen_s, "create_s": create_s, "autotune_s": tune_s,
+                       "graph_captures_launches": list(batch.graph_counts())},
+             "gpu_launches": int(launches), "clocks": clk.summary()}
+    if cpu is not None:
+        extra["cpu_baseline"] = cpu
+    print(json.dumps(_line(args, "batch-256-bicgstab-jacobi", ms / 1e3, None,
+                           {"systems": len(systems), "solver": "bicgstab+jacobi", "rtol": 1e-8,
+                            "l2": "inputs larger than L2 (matrices 2.8 GB)"}, "f64", extra)))
+    return 0
+
+
+def _cpu_batch_sample(systems, its, budget_s: float = 20.0):
+    """The reference's bicgstab + Jacobi (oracle/_ref, one thread) on the first
+    systems until ~budget_s, extrapolated to the whole batch by
+    sum(unknowns x iterations)."""
+    import oracle
+
+    try:
+        ref = oracle.Reference()
+    except FileNotFoundError:
+        return None
+    spent, work_done, done = 0.0, 0, 0
+    for y, k in zip(systems, its):
+        m = ref.matrix("bsr", y.owned, 0, y.bs, y.rowptr, y.cols, y.vals)
+        pc = ref.pc("jacobi", m, 0.0)
+        t = time.time()
+        r, _ = ref.solve("bicgstab", m, pc, oracle.default_options(), y.rhs, np.zeros(y.owned * y.bs))
+        spent += time.time() - t
+        work_done += y.owned * y.bs * int(r.iterations)
+        done += 1
+        if spent >= budget_s:
+            break
+    total_work = sum(y.owned * y.bs * int(k) for y, k in zip(systems, its))
+    value = spent * total_work / max(work_done, 1)
+    return {"value": value, "unit": "s", "cores": 1, "kind": "reference",
+            "sample": f"reference bicgstab+jacobi on the first {done} of {len(systems)} systems ({spent:.1f} s), "
+                      f"scaled by unknowns x iterations to the whole batch"}
+
+
+def run_mixed(args):
+    """Dense 3x3 blocks on the 2M-vertex disk mesh: FP64 FGMRES(30) outer
+    refinement to rtol 1e-10 around block-ILU(0) factors stored in FP32 and in
+    BF16 with an FP32 inner solve, against the plain FP64 block-ILU(0) FGMRES;
+    errors against the FP64 solution."""
+    import torch
+    from owtk_b200 import native, problems
+
+    t = time.time()
+    s = problems.config2(args.vertices)
+    gen_s = time.time() - t
+    n, bs = s.owned, s.bs
+    ctx = native.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    m = native.Matrix(ctx, "dense", n, 0, bs, s.rowptr, s.cols, s.vals)
+    b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
+    opts = native.default_options(relative_tolerance=1e-10, restart=30)
+    out = {}
+    xref = None
+    for name, storage, inner in (("fp64", native.F64, None), ("fp32", native.F32, 4), ("bf16", native.BF16, 4)):
+        t = time.time()
+        pc = native.Preconditioner(m, native.PC_BLOCK_ILU, 0, storage=storage, mixed_inner=inner)
+        ctx.synchronize()
+        setup_s = time.time() - t
+        x = native.Vector(ctx, n, 0, bs)
+        ws = native.Workspace(ctx)
+        res = None
+
+        def step():
+            nonlocal res
+            x.fill(0.0)
+            res = native.solve(native.FGMRES, m, pc, b, x, opts, ws)
+
+        for _ in range(args.warmup):
+            step()
+        ms = _event_time(stream, step, args.steps)
+        xs = x.download()
+        if xref is None:
+            xref = xs
+        out[name] = {"ms": ms, "iterations": int(res.iterations), "status": int(res.status),
+                     "true_relative_residual": float(res.true_residual_norm / np.linalg.norm(s.rhs)),
+                     "error_vs_fp64": float(np.linalg.norm(xs - xref) / np.linalg.norm(xref)), "setup_s": setup_s}
+    best = min(out["fp32"]["ms"], out["bf16"]["ms"])
+    extra = {"mixed": out, "speedup_vs_fp64": out["fp64"]["ms"] / best}
+    print(json.dumps(_line(args, "mixed-dense3x3-fgmres-blockilu0", best / 1e3, None,
+                           {"vertices": n, "entries": s.nnz, "block_size": bs, "rtol": 1e-10,
+                            "solver": "fgmres(30) fp64 outer, block-ilu(0) fp32/bf16 factors, fp32 inner",
+                            "mesh_gen_s": gen_s}, "f64+f32", extra)))
+    return 0
+
+
+def run_learned(args):
+    """Anisotropic unit-square mesh (--vertices, default 8M): the network is
+    trained on the GPU on ILU(0)-GMRES residual/error pairs of --draws
+    coefficient draws of a --train-vertices mesh, then FGMRES(30) with the
+    network (ILU(0) fallback; FP64 outer, BF16/FP32 network) is timed against
+    plain FP64 ILU(0)-GMRES(30) on the same system, both to rtol 1e-8."""
+    import torch
+    from owtk_b200 import learned, native, problems
+
+    ctx = native.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    # Training.
+    t = time.time()
+    train = [sys_ for _, sys_ in problems.anisotropic_draws(args.train_vertices, 41, range(args.draws))]
+    gen_train_s = time.time() - t
+    m0 = native.Matrix(ctx, "bsr", train[0].owned, 0, 3, train[0].rowptr, train[0].cols, train[0].vals)
+    net = native.Learned(m0, seed=1)
+    t = time.time()
+    hist = learned.train(ctx, net, train, epochs=args.epochs, learning_rate=1e-3, pairs_per_system=4)
+    train_s = time.time() - t
+    weights = net.parameters()
+    # The large system.
+    t = time.time()
+    s = problems.config4(args.vertices)
+    gen_s = time.time() - t
+    n, bs = s.owned, s.bs
+    m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
+    t = time.time()
+    ilu = native.Preconditioner(m, native.PC_ILU, 0)
+    ctx.synchronize()
+    ilu_setup_s = time.time() - t
+    netL = native.Learned(m, seed=1)
+    netL.set_parameters(weights)
+    pcl = native.LearnedPreconditioner(netL, ilu)
+    b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
+    x = native.Vector(ctx, n, 0, bs)
+    ws = native.Workspace(ctx)
+    opts = native.default_options(relative_tolerance=1e-8, restart=30)
+    results = {}
+    for name, pc in (("ilu0_gmres_fp64", ilu), ("learned_fgmres", pcl)):
+        res = None
+
+        def step():
+            nonlocal res
+            x.fill(0.0)
+            res = native.solve(native.FGMRES, m, pc, b, x, opts, ws)
+
+        step()
+        ms = _event_time(stream, step, max(1, args.steps))
+        results[name] = {"ms": ms, "iterations": int(res.iterations), "status": int(res.status),
+                         "true_relative_residual": float(res.true_residual_norm / np.linalg.norm(s.rhs))}
+    apps, falls = pcl.counts()
+    results["learned_fgmres"]["network_applications"] = apps
+    results["learned_fgmres"]["fallbacks"] = falls
+    speed = results["ilu0_gmres_fp64"]["ms"] / results["learned_fgmres"]["ms"]
+    extra = {"learned": results, "speedup_vs_plain_fp64_ilu_gmres": speed,
+             "training": {"draws": args.draws, "vertices": train[0].owned, "epochs": args.epochs,
+                          "loss_history": hist, "train_s": train_s, "generate_s": gen_train_s},
+             "setup": {"mesh_gen_s": gen_s, "ilu_setup_s": ilu_setup_s}}
+    print(json.dumps(_line(args, "learned-anisotropic-fgmres", results["learned_fgmres"]["ms"] / 1e3, None,
+                           {"vertices": n, "entries": s.nnz, "block_size": bs, "rtol": 1e-8,
+                            "solver": "fgmres(30) + learned network (ilu(0) fallback) vs gmres(30)+ilu(0)"},
+                           "f64+bf16", extra)))
+    return 0
+
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernels:
+        return run_kernels(args)
+    if args.form == "batching":
+        return run_batching(args)
+    if args.form == "mixed":
+        return run_mixed(args)
+    if args.form == "learned":
+        return run_learned(args)
     return run_ours(args)
 
 

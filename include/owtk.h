@@ -134,7 +134,9 @@ typedef enum owtk_pc_kind {
      * IKJ factorisation with inverted diagonal blocks; parameter unused. */
     OWTK_PC_BLOCK_ILU = 5,
     /* Created only by owtk_pc_create_mixed. */
-    OWTK_PC_MIXED = 6
+    OWTK_PC_MIXED = 6,
+    /* Created only by owtk_pc_create_learned. */
+    OWTK_PC_LEARNED = 7
 } owtk_pc_kind;
 
 owtk_status owtk_pc_create(owtk_matrix* m, owtk_pc_kind kind, double parameter,
@@ -263,6 +265,96 @@ owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_precondi
  * current, so make it before any stream capture. */
 owtk_status owtk_dot_batch_f64_noalloc(const double* w, const double* const* basis, size_t k,
                                        size_t n, double* results, void* stream);
+
+/* ---------------------------------------------------------------- batching
+ * Many independent FP64 component-diagonal block-CSR systems (uneven sizes,
+ * block sizes 1..32, ghosts 0) solved together by BiCGSTAB with a Jacobi
+ * preconditioner in ONE persistent cooperative launch with per-system
+ * convergence masks, captured once in a CUDA graph and replayed.  No single
+ * reference counterpart: each system follows the reference's bicgstab
+ * (krylov_solvers.hpp:546-745) with JacobiPreconditioner
+ * (preconditioner.hpp:25-113), result counters included; the structure of each
+ * system is validated like BlockCsrMatrix (block_csr.hpp:281-300). */
+typedef struct owtk_batch owtk_batch;
+
+typedef struct owtk_batch_system {
+    size_t owned;               /* vertices (rows) */
+    size_t bs;                  /* block size, 1..32 */
+    const uint64_t* rowptr;     /* host, owned + 1 */
+    const uint64_t* cols;       /* host, rowptr[owned] local columns < owned */
+    const double* values;       /* host, rowptr[owned] * bs, [entry][component] */
+} owtk_batch_system;
+
+owtk_status owtk_batch_create(owtk_context* ctx, size_t count, const owtk_batch_system* systems, owtk_batch** out);
+owtk_status owtk_batch_destroy(owtk_batch* batch);
+/* Total unknowns and the first unknown of each system (count + 1 entries):
+ * right-hand sides and solutions are single device arrays in system order. */
+owtk_status owtk_batch_layout(const owtk_batch* batch, size_t* unknowns, uint64_t* offsets);
+/* Current launch shape: resident blocks per SM and vertices per warp pass for
+ * block sizes 0..32 (33 entries; index = block size). */
+owtk_status owtk_batch_config(const owtk_batch* batch, uint32_t* blocks_per_sm, uint32_t* vertices_per_warp);
+/* Override the shape (0 leaves a field unchanged). */
+owtk_status owtk_batch_set_config(owtk_batch* batch, uint32_t blocks_per_sm, size_t bs, uint32_t vertices_per_warp);
+/* Autotuner: times one SpMV pass per vertices-per-warp candidate and block
+ * size present, then a few solver iterations per blocks-per-SM candidate, and
+ * keeps the fastest; outputs as owtk_batch_config (either may be NULL). */
+owtk_status owtk_batch_autotune(owtk_batch* batch, const owtk_solver_options* options, uint32_t* blocks_per_sm,
+                                uint32_t* vertices_per_warp);
+/* 1 (default): each solve replays a CUDA graph holding the whole launch
+ * (re-captured when the vectors, options or shape change); 0: plain launches. */
+owtk_status owtk_batch_use_graph(owtk_batch* batch, int enable);
+owtk_status owtk_batch_graph_counts(const owtk_batch* batch, uint64_t* captures, uint64_t* launches);
+/* Solve every system from the initial guess in x; results has count entries.
+ * Device arrays of owtk_batch_layout's total length. */
+owtk_status owtk_batch_solve(owtk_batch* batch, const double* device_rhs, double* device_x,
+                             const owtk_solver_options* options, owtk_solver_result* results);
+/* Same with host arrays (copied in and out inside the call). */
+owtk_status owtk_batch_solve_host(owtk_batch* batch, const double* host_rhs, double* host_x,
+                                  const owtk_solver_options* options, owtk_solver_result* results);
+
+/* ---------------------------------------------------------------- tensor cores
+ * D (m x n, FP32, row-major) = A (m x k, BF16, row-major) * B (n x k, BF16,
+ * row-major)^T on the sm_100a tensor cores (tcgen05.mma, FP32 accumulation in
+ * tensor memory); m % 128 == 0, n in {64, 128}, k % 64 == 0, 16-byte aligned
+ * device pointers.  The building block of the learned preconditioner's dense
+ * products, exposed to check that path in isolation.  No reference
+ * counterpart. */
+owtk_status owtk_bf16_gemm_nt(owtk_context* ctx, size_t m, size_t n, size_t k, const void* device_a,
+                              const void* device_b, float* device_d);
+
+/* ---------------------------------------------------------------- learned preconditioner
+ * A message-passing network on the graph of an FP64 component-diagonal BSR
+ * matrix (ghosts 0, block size <= 8): hidden width 64, 4 layers, BF16 weights
+ * and activations on the tensor cores with FP32 accumulation, no biases (so
+ * M(a r) = a M(r) for a > 0); its decoder adds the Jacobi step, so untrained
+ * weights give the Jacobi preconditioner.  The FP64 restatement of the
+ * network is oracle/gnn.py.  No reference counterpart.  The matrix is
+ * borrowed and must outlive the network. */
+typedef struct owtk_learned owtk_learned;
+
+owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** out);
+owtk_status owtk_learned_destroy(owtk_learned* net);
+/* Re-read the coefficients of a matrix with the same pattern (edge weights
+ * and diagonal of the graph); the weights are kept. */
+owtk_status owtk_learned_update_matrix(owtk_learned* net, owtk_matrix* m);
+/* Flat FP32 parameters: encoder 64x16, 4 layers 64x128, decoder 8x64. */
+size_t owtk_learned_parameter_count(void);
+owtk_status owtk_learned_get_parameters(owtk_learned* net, float* host, size_t count);
+owtk_status owtk_learned_set_parameters(owtk_learned* net, const float* host, size_t count);
+/* out = M(in), FP64 vectors of the matrix layout. */
+owtk_status owtk_learned_apply(owtk_learned* net, owtk_vector* in, owtk_vector* out);
+/* Forward + backward of one training pair: loss ||M(r) - e||^2 / ||e||^2 and
+ * its gradient, kept on the device for owtk_learned_adam_step (and copied
+ * to host_grads when it is not NULL). */
+owtk_status owtk_learned_loss_grad(owtk_learned* net, owtk_vector* r, owtk_vector* e, double* loss,
+                                   float* host_grads);
+owtk_status owtk_learned_adam_step(owtk_learned* net, double learning_rate);
+/* The network as a preconditioner of its matrix: each application z = M(v)
+ * is judged by the FP64 residual ||v - A z||; when that does not fall below
+ * ||v|| the fallback (e.g. ILU(0), may be NULL) computes z instead.  Both
+ * handles are borrowed. */
+owtk_status owtk_pc_create_learned(owtk_learned* net, owtk_preconditioner* fallback, owtk_preconditioner** out);
+owtk_status owtk_pc_learned_counts(owtk_preconditioner* p, uint64_t* applications, uint64_t* fallbacks);
 
 #ifdef __cplusplus
 }

@@ -111,11 +111,6 @@ namespace {
 
 std::size_t dsize(owtk_dtype d) { return d == OWTK_F64 ? 8 : (d == OWTK_F32 ? 4 : 2); }
 
-void require(bool ok, const char* message)
-{
-    if (!ok) fail(OWTK_ERR_INVALID_ARGUMENT, message);
-}
-
 // Validate a host CSR structure as block_csr.hpp:281-300 does and narrow it
 // to int32 for the device.
 void ingest_structure(Matrix& m, std::size_t owned, std::size_t ghost, std::size_t bs,
@@ -380,24 +375,6 @@ void numeric_update(Preconditioner& p, Matrix& m)
     ++p.numeric_updates;
 }
 
-template<class F>
-owtk_status guarded(F&& f)
-{
-    try {
-        f();
-        return OWTK_OK;
-    } catch (const Error& e) {
-        g_last_error = e.message;
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        g_last_error = "host allocation failed";
-        return OWTK_ERR_RUNTIME;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-        return OWTK_ERR_RUNTIME;
-    }
-}
-
 }  // namespace
 
 // ------------------------------------------------------------ shared ops
@@ -419,6 +396,14 @@ void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out)
     if (!in.same_layout(out)) fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
     Context& c = *in.ctx;
     const std::size_t n = in.owned_size();
+    if (p != nullptr && p->kind == OWTK_PC_LEARNED) {
+        if (in.owned != p->owned || in.ghost != p->ghost || in.bs != p->bs)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
+        if (in.dtype != OWTK_F64 || out.dtype != OWTK_F64)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "the learned preconditioner applies to FP64 vectors");
+        learned_apply(*p, in, out);
+        return;
+    }
     if (p != nullptr && (p->kind == OWTK_PC_MIXED || p->storage != OWTK_F64 || p->block)) {
         if (in.owned != p->owned || in.ghost != p->ghost || in.bs != p->bs)
             fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
@@ -740,6 +725,11 @@ owtk_status owtk_split_view_create(owtk_context* ctx, owtk_dtype dtype, size_t o
         if (owned == 0 || bs == 0 || rowptr == nullptr || device_diagonal == nullptr
             || (device_off_diagonal == nullptr && rowptr[owned] != 0))
             fail(OWTK_ERR_INVALID_ARGUMENT, "invalid split CSR storage");
+        const auto misaligned = [&](const void* p) {
+            return reinterpret_cast<std::uintptr_t>(p) % dsize(dtype) != 0;
+        };
+        if (misaligned(device_diagonal) || misaligned(device_off_diagonal))
+            fail(OWTK_ERR_INVALID_ARGUMENT, "split coefficients are not aligned to their element size");
         auto m = std::make_unique<owtk_matrix>();
         m->ctx = ctx;
         m->kind = 1;

@@ -1,0 +1,1241 @@
+// Learned preconditioner: a message-passing network on the matrix graph
+// (hidden 64, 4 layers, no biases) whose dense products run on the sm_100a
+// tensor cores (tcgen05.mma, BF16 operands in shared memory, FP32
+// accumulators in TMEM), with hand-written forward, backward and Adam
+// kernels.  The network (FP64 restatement in oracle/gnn.py):
+//
+//   q = r/d (the Jacobi step);  x_v = [r_v/rms(r), q_v/rms(q), 0...] (16 features)
+//   h0 = x We^T;  per layer: m_v = sum_u w_vu h_u,  h += relu([h | m] Wl^T)
+//   out = q + rms(q) * (h4 Wd^T)       (an untrained decoder is Jacobi)
+//
+// Device layouts: node features h are BF16 rows of 64 (128 bytes); the layer
+// kernel gathers a 128-row tile of [h | m] into swizzled shared memory, runs
+// eight K=16 MMAs against the resident layer weight and applies the
+// ReLU/residual epilogue straight from TMEM.
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+#include "owtk_internal.h"
+#include "umma.cuh"
+
+namespace owtk {
+namespace gnn {
+
+using namespace dev;
+using bf16 = __nv_bfloat16;
+
+constexpr int kH = 64;             // hidden width
+constexpr int kF = 16;             // input features
+constexpr int kLayers = 4;
+constexpr int kTile = 128;         // rows per tensor-core tile
+constexpr int kMmaSpin = 1 << 22;
+
+// ---------------------------------------------------------------- shared pieces
+__device__ __forceinline__ std::uint32_t align1024(std::uint32_t a) { return (a + 1023u) & ~1023u; }
+
+// Bounded wait on an mbarrier phase; false if it gave up.
+__device__ __forceinline__ bool wait_phase(std::uint32_t bar, std::uint32_t parity)
+{
+    return mbar_wait_bounded(bar, parity, kMmaSpin);
+}
+
+// 16 bytes of a BF16 row (8 features) to / from FP32.
+__device__ __forceinline__ void bf16x8_to_f32(const uint4& u, float (&f)[8])
+{
+    const bf16* b = reinterpret_cast<const bf16*>(&u);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = __bfloat162float(b[i]);
+}
+
+__device__ __forceinline__ uint4 f32_to_bf16x8(const float (&f)[8])
+{
+    uint4 u;
+    bf16* b = reinterpret_cast<bf16*>(&u);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) b[i] = __float2bfloat16_rn(f[i]);
+    return u;
+}
+
+// ---------------------------------------------------------------- generic GEMM
+// D (M x N, FP32, row-major) = A (M x K, BF16, row-major) * B (N x K, BF16,
+// row-major)^T with M % 128 == 0, N in {64, 128}, K % 64 == 0.  One CTA (4
+// warps) per 128-row tile; K in 64-element blocks staged through swizzled
+// shared memory.  Used to check the tensor-core path in isolation.
+template<int N>
+__global__ void __launch_bounds__(128, 1) k_umma_gemm_nt(int K, const bf16* __restrict__ A,
+                                                          const bf16* __restrict__ B, float* __restrict__ D,
+                                                          unsigned* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) std::uint64_t bar_storage;
+    __shared__ std::uint32_t tmem_base_s;
+    const std::uint32_t base = align1024(smem_u32(smem_raw));
+    const std::uint32_t a_tile = base, b_tile = base + kTile * 128;
+    unsigned char* gen = smem_raw + (base - smem_u32(smem_raw));
+    const std::uint32_t bar = smem_u32(&bar_storage);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long row0 = static_cast<long long>(blockIdx.x) * kTile;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async_smem();
+    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), N);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const std::uint32_t tmem = tmem_base_s;
+    constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, N);
+    bool ok = true;
+    for (int kb = 0; kb < K / 64; ++kb) {
+        // Stage A (128 x 64) and B (N x 64): thread t copies 16-byte chunks.
+        for (int i = threadIdx.x; i < kTile * 8; i += 128) {
+            const int r = i >> 3, c = i & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(A + (row0 + r) * K + kb * 64 + c * 8);
+            *reinterpret_cast<uint4*>(gen + sw128(r, c)) = v;
+        }
+        for (int i = threadIdx.x; i < N * 8; i += 128) {
+            const int r = i >> 3, c = i & 7;
+            const uint4 v = *reinterpret_cast<const uint4*>(B + static_cast<long long>(r) * K + kb * 64 + c * 8);
+            *reinterpret_cast<uint4*>(gen + kTile * 128 + sw128(r, c)) = v;
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tmem_fence_after_sync();
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                umma_bf16(tmem, umma_desc_sw128(a_tile + 32 * k), umma_desc_sw128(b_tile + 32 * k), idesc,
+                          kb > 0 || k > 0);
+            umma_commit(bar);
+        }
+        ok = ok && wait_phase(bar, kb & 1);
+        tmem_fence_after_sync();
+        if (!__syncthreads_and(ok)) break;
+    }
+    if (ok) {
+        // Epilogue: warp w reads TMEM lanes 32w..32w+31 = rows of the tile.
+#pragma unroll
+        for (int c0 = 0; c0 < N; c0 += 32) {
+            float v[32];
+            tmem_ld32(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + c0, v);
+            float* out = D + (row0 + 32 * warp + lane) * N + c0;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) out[i] = v[i];
+        }
+    } else if (threadIdx.x == 0) {
+        atomicOr(status, kErrTimeout);
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, N);
+}
+
+// ---------------------------------------------------------------- network kernels
+struct GraphArgs {
+    int n, bs;
+    const int* nb_ptr;       // off-diagonal neighbours of v (row v of the matrix)
+    const int* nb_col;
+    const float* nb_w;       // w_vu = -mean_c a_vu,c / d_v,c
+    const int* tr_ptr;       // transposed: the v with u in N(v), for vertex u
+    const int* tr_col;
+    const float* tr_w;       // w_vu of that edge
+    const float* dinv;       // 1 / diagonal, n * bs
+};
+
+// q = r / d in FP32 (the Jacobi step; its norm scales the network's output).
+template<class T>
+__global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* __restrict__ r,
+                                                     const float* __restrict__ dinv, float* __restrict__ q)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) q[i] = static_cast<float>(r[i]) * dinv[i];
+}
+
+// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...].
+template<class T>
+__global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
+                                                    const double* norms, const float* __restrict__ we,
+                                                    bf16* __restrict__ h0)
+{
+    __shared__ float w[kH * kF];
+    for (int i = threadIdx.x; i < kH * kF; i += blockDim.x) w[i] = we[i];
+    __syncthreads();
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.n) return;
+    const double root = sqrt(static_cast<double>(g.n) * g.bs), nr = norms[0], nq = norms[2];
+    const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
+    const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
+    float x[kF];
+#pragma unroll
+    for (int f = 0; f < kF; ++f) x[f] = 0.0f;
+    for (int c = 0; c < g.bs; ++c) {
+        const long long o = static_cast<long long>(v) * g.bs + c;
+        x[c] = static_cast<float>(r[o]) * inv_r;
+        x[g.bs + c] = q[o] * inv_q;
+    }
+    uint4* out = reinterpret_cast<uint4*>(h0 + static_cast<long long>(v) * kH);
+#pragma unroll
+    for (int c8 = 0; c8 < kH / 8; ++c8) {
+        float o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int f = 0; f < kF; ++f) acc = fmaf(w[(c8 * 8 + i) * kF + f], x[f], acc);
+            o[i] = acc;
+        }
+        out[c8] = f32_to_bf16x8(o);
+    }
+}
+
+// Decoder: out = q + rms(q) * (h Wd^T).
+template<class O>
+__global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __restrict__ q, const double* norms,
+                                                    const float* __restrict__ wd, const bf16* __restrict__ h,
+                                                    O* __restrict__ out)
+{
+    __shared__ float w[8 * kH];
+    for (int i = threadIdx.x; i < 8 * kH; i += blockDim.x) w[i] = wd[i];
+    __syncthreads();
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.n) return;
+    const float s = static_cast<float>(norms[2] / sqrt(static_cast<double>(g.n) * g.bs));
+    float hv[kH];
+    const uint4* hr = reinterpret_cast<const uint4*>(h + static_cast<long long>(v) * kH);
+#pragma unroll
+    for (int c8 = 0; c8 < kH / 8; ++c8) {
+        float f[8];
+        bf16x8_to_f32(hr[c8], f);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) hv[c8 * 8 + i] = f[i];
+    }
+    for (int c = 0; c < g.bs; ++c) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kH; ++k) acc = fmaf(w[c * kH + k], hv[k], acc);
+        const long long o = static_cast<long long>(v) * g.bs + c;
+        out[o] = static_cast<O>(norms[0] > 0.0 ? q[o] + s * acc : 0.0f);
+    }
+}
+
+// One message-passing layer, fused: for each 128-row tile, gather [h | m]
+// (m_v = sum_u w_vu h_u in FP32, rounded to BF16) into swizzled shared
+// memory, Y = [h | m] Wl^T by eight K=16 tensor-core MMAs into TMEM, then
+// h_out = h + relu(Y) from TMEM.  Training also keeps m (BF16) and the sign
+// mask of Y (one 64-bit word per row) for the backward pass.
+constexpr int kLayerThreads = 128;
+constexpr int kLayerSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128;   // A: [h | m], B: Wl
+
+template<bool TRAIN>
+__global__ void __launch_bounds__(kLayerThreads, 4)
+    k_gnn_layer(GraphArgs g, const bf16* __restrict__ h_in, const bf16* __restrict__ wl, bf16* __restrict__ h_out,
+                bf16* __restrict__ m_out, unsigned long long* __restrict__ mask_out, unsigned* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) std::uint64_t bar_storage;
+    __shared__ std::uint32_t tmem_base_s;
+    const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
+    unsigned char* tile = smem_raw + (base - raw);                 // A0 (h), A1 (m), B0, B1
+    const std::uint32_t a0 = base, a1 = base + kTile * 128, b0 = base + 2 * kTile * 128, b1 = b0 + kH * 128;
+    const std::uint32_t bar = smem_u32(&bar_storage);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (g.n + kTile - 1) / kTile;
+
+    // Layer weight (64 x 128, row-major = K-major) into the two B blocks.
+    for (int i = threadIdx.x; i < kH * 16; i += kLayerThreads) {
+        const int r = i >> 4, c16 = i & 15;
+        const uint4 v = *reinterpret_cast<const uint4*>(wl + r * 128 + c16 * 8);
+        *reinterpret_cast<uint4*>(tile + 2 * kTile * 128 + (c16 >> 3) * kH * 128 + sw128(r, c16 & 7)) = v;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async_smem();
+    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kH);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const std::uint32_t tmem = tmem_base_s;
+    constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, kH);
+    const int grp = lane >> 3, chunk = lane & 7;   // 4 rows at a time, 8 lanes x 16 bytes per row
+    int iter = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++iter) {
+        const int row0 = t * kTile;
+        // ---- gather [h | m]
+        for (int it = 0; it < 8; ++it) {
+            const int r = 32 * warp + 4 * it + grp, v = row0 + r;
+            uint4 hv = make_uint4(0, 0, 0, 0), mv = make_uint4(0, 0, 0, 0);
+            if (v < g.n) {
+                hv = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(v) * kH + chunk * 8);
+                float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                const int e0 = g.nb_ptr[v], e1 = g.nb_ptr[v + 1];
+                for (int e = e0; e < e1; e += 4) {
+                    uint4 nv[4];
+                    float nw[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        nw[q] = 0.0f;
+                        nv[q] = make_uint4(0, 0, 0, 0);
+                        if (e + q < e1) {
+                            const int u = g.nb_col[e + q];
+                            nw[q] = g.nb_w[e + q];
+                            nv[q] = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float f[8];
+                        bf16x8_to_f32(nv[q], f);
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) acc[i] = fmaf(nw[q], f[i], acc[i]);
+                    }
+                }
+                mv = f32_to_bf16x8(acc);
+                if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
+            }
+            *reinterpret_cast<uint4*>(tile + sw128(r, chunk)) = hv;
+            *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, chunk)) = mv;
+        }
+        fence_proxy_async_smem();
+        tmem_fence_before_sync();
+        __syncthreads();
+        // ---- Y = [h | m] Wl^T
+        if (threadIdx.x == 0) {
+            tmem_fence_after_sync();
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                umma_bf16(tmem, umma_desc_sw128(a0 + 32 * k), umma_desc_sw128(b0 + 32 * k), idesc, k > 0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                umma_bf16(tmem, umma_desc_sw128(a1 + 32 * k), umma_desc_sw128(b1 + 32 * k), idesc, true);
+            umma_commit(bar);
+        }
+        ok = wait_phase(bar, iter & 1);
+        tmem_fence_after_sync();
+        if (!__syncthreads_and(ok)) break;
+        // ---- epilogue: row = tile row 32*warp + lane
+        const int r = 32 * warp + lane, v = row0 + r;
+        unsigned long long mask = 0;
+        uint4 outv[8];
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            float y[32];
+            tmem_ld32(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + 32 * half, y);
+#pragma unroll
+            for (int c4 = 0; c4 < 4; ++c4) {
+                const int c8 = half * 4 + c4;
+                float hf[8];
+                bf16x8_to_f32(*reinterpret_cast<const uint4*>(tile + sw128(r, c8)), hf);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float yv = y[c4 * 8 + i];
+                    if (yv > 0.0f) mask |= 1ull << (c8 * 8 + i);
+                    hf[i] += fmaxf(yv, 0.0f);
+                }
+                outv[c8] = f32_to_bf16x8(hf);
+            }
+        }
+        if (v < g.n) {
+            uint4* o = reinterpret_cast<uint4*>(h_out + static_cast<long long>(v) * kH);
+#pragma unroll
+            for (int c8 = 0; c8 < 8; ++c8) o[c8] = outv[c8];
+            if (TRAIN) mask_out[v] = mask;
+        }
+        tmem_fence_before_sync();
+        __syncthreads();
+    }
+    if (!ok && threadIdx.x == 0) atomicOr(status, kErrTimeout);
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, kH);
+}
+
+// ---------------------------------------------------------------- backward kernels
+// Loss ||out - e||^2 / ||e||^2 (partials per block, combined in block order by
+// the last block) and dz = s * 2 (out - e) / ||e||^2.
+__global__ void __launch_bounds__(256) k_gnn_out_grad(long long count, const float* __restrict__ out,
+                                                      const double* __restrict__ e, const double* enorm,
+                                                      const double* rnorm, double scale_n, float* __restrict__ dz,
+                                                      double* partials, unsigned* ticket, double* loss)
+{
+    const double ee = (*enorm) * (*enorm);
+    const double s = rnorm[2] / scale_n;   // rms of the Jacobi step
+    const float g = ee > 0.0 ? static_cast<float>(2.0 * s / ee) : 0.0f;
+    double acc = 0.0;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const double d = static_cast<double>(out[i]) - e[i];
+        acc += d * d;
+        dz[i] = g * static_cast<float>(d);
+    }
+    acc = warp_sum(acc);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < 8; ++w) b += red[w];
+        partials[blockIdx.x] = b;
+        __threadfence();
+        if (atomicAdd(ticket, 1u) == gridDim.x - 1) {
+            __threadfence();
+            double t = 0.0;
+            for (unsigned k = 0; k < gridDim.x; ++k) t += __ldcg(partials + k);
+            *loss = ee > 0.0 ? t / ee : 0.0;
+            *ticket = 0;
+        }
+    }
+}
+
+// dh4 = dz Wd (FP32 rows of 64).
+__global__ void __launch_bounds__(256) k_gnn_decode_bwd(int n, int bs, const float* __restrict__ dz,
+                                                        const float* __restrict__ wd, float* __restrict__ dh)
+{
+    __shared__ float w[8 * kH];
+    for (int i = threadIdx.x; i < 8 * kH; i += blockDim.x) w[i] = wd[i];
+    __syncthreads();
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    float d[8];
+    for (int c = 0; c < 8; ++c) d[c] = c < bs ? dz[static_cast<long long>(v) * bs + c] : 0.0f;
+    float4* o = reinterpret_cast<float4*>(dh + static_cast<long long>(v) * kH);
+#pragma unroll
+    for (int k4 = 0; k4 < kH / 4; ++k4) {
+        float r[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float acc = 0.0f;
+            for (int c = 0; c < bs; ++c) acc = fmaf(d[c], w[c * kH + k4 * 4 + i], acc);
+            r[i] = acc;
+        }
+        o[k4] = make_float4(r[0], r[1], r[2], r[3]);
+    }
+}
+
+// Per-block partials of G[i][j] = sum_v a[v][i] * b[v][j] (a: FP32 rows of pa,
+// b: rows of pb in BF16 or FP32), i < pa, j < pb, pa * pb <= 1024; rows split
+// into contiguous block ranges, summed in row order.
+template<class B>
+__global__ void __launch_bounds__(256) k_gnn_outer(int n, int pa, int pb, const float* __restrict__ a,
+                                                   const B* __restrict__ b, float* __restrict__ partials)
+{
+    const int rows = (n + gridDim.x - 1) / gridDim.x;
+    const int v0 = blockIdx.x * rows, v1 = min(n, v0 + rows);
+    for (int t = threadIdx.x; t < pa * pb; t += blockDim.x) {
+        const int i = t / pb, j = t - i * pb;
+        float acc = 0.0f;
+        for (int v = v0; v < v1; ++v)
+            acc = fmaf(a[static_cast<long long>(v) * pa + i], static_cast<float>(b[static_cast<long long>(v) * pb + j]),
+                       acc);
+        partials[static_cast<long long>(blockIdx.x) * pa * pb + t] = acc;
+    }
+}
+
+// Sum `blocks` partial arrays of `count` floats in block order into out[]
+// (optionally transposed: out[j * rows + i] for element i * cols + j).
+__global__ void k_gnn_reduce(int blocks, int count, const float* __restrict__ partials, float* __restrict__ out,
+                             int rows, int cols, int transpose)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    float acc = 0.0f;
+    for (int b = 0; b < blocks; ++b) acc += partials[static_cast<long long>(b) * count + t];
+    if (transpose) {
+        const int i = t / cols, j = t - i * cols;
+        out[j * rows + i] = acc;
+    } else {
+        out[t] = acc;
+    }
+}
+
+// Layer backward, part 1 (tensor cores): dy = dh (.) [y > 0] (kept in BF16
+// for the weight gradient), dcat = dy Wl (128 x 128 per tile, K = 64), then
+// dh += dcat[:, :64] in place and dm = dcat[:, 64:].
+constexpr int kBwdSmem = 1024 + kTile * 128 + 2 * kH * 128;
+
+__global__ void __launch_bounds__(kLayerThreads, 4)
+    k_gnn_layer_bwd(int n, float* __restrict__ dh, const unsigned long long* __restrict__ mask,
+                    const bf16* __restrict__ wlt, bf16* __restrict__ dy_out, float* __restrict__ dm, unsigned* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) std::uint64_t bar_storage;
+    __shared__ std::uint32_t tmem_base_s;
+    const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
+    unsigned char* tile = smem_raw + (base - raw);     // A: dy (128 x 64), B: Wl^T (128 x 64)
+    const std::uint32_t a0 = base, b0 = base + kTile * 128;
+    const std::uint32_t bar = smem_u32(&bar_storage);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (n + kTile - 1) / kTile;
+    for (int i = threadIdx.x; i < 2 * kH * 8; i += kLayerThreads) {
+        const int r = i >> 3, c = i & 7;
+        *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, c)) =
+            *reinterpret_cast<const uint4*>(wlt + r * kH + c * 8);
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async_smem();
+    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), 2 * kH);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const std::uint32_t tmem = tmem_base_s;
+    constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, 2 * kH);
+    int iter = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++iter) {
+        const int row0 = t * kTile;
+        // dy tile: thread handles (row, chunk) pairs.
+        for (int i = threadIdx.x; i < kTile * 8; i += kLayerThreads) {
+            const int r = i >> 3, c = i & 7, v = row0 + r;
+            float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (v < n) {
+                const unsigned long long mk = mask[v];
+                const float4* src = reinterpret_cast<const float4*>(dh + static_cast<long long>(v) * kH + c * 8);
+                const float4 p = src[0], q = src[1];
+                const float x[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int k = 0; k < 8; ++k) f[k] = ((mk >> (c * 8 + k)) & 1ull) ? x[k] : 0.0f;
+            }
+            const uint4 u = f32_to_bf16x8(f);
+            *reinterpret_cast<uint4*>(tile + sw128(r, c)) = u;
+            if (v < n) *reinterpret_cast<uint4*>(dy_out + static_cast<long long>(v) * kH + c * 8) = u;
+        }
+        fence_proxy_async_smem();
+        tmem_fence_before_sync();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tmem_fence_after_sync();
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                umma_bf16(tmem, umma_desc_sw128(a0 + 32 * k), umma_desc_sw128(b0 + 32 * k), idesc, k > 0);
+            umma_commit(bar);
+        }
+        ok = wait_phase(bar, iter & 1);
+        tmem_fence_after_sync();
+        if (!__syncthreads_and(ok)) break;
+        const int v = row0 + 32 * warp + lane;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float y[32];
+            tmem_ld32(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + 32 * q, y);
+            if (v < n) {
+                float* dst = q < 2 ? dh + static_cast<long long>(v) * kH + 32 * q
+                                   : dm + static_cast<long long>(v) * kH + 32 * (q - 2);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) dst[i] = q < 2 ? dst[i] + y[i] : y[i];
+            }
+        }
+        tmem_fence_before_sync();
+        __syncthreads();
+    }
+    if (!ok && threadIdx.x == 0) atomicOr(status, kErrTimeout);
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, 2 * kH);
+}
+
+// Layer backward, part 2: dh_u += sum over edges (v -> u) of w_vu dm_v, a
+// gather over the transposed graph (deterministic).
+__global__ void __launch_bounds__(256) k_gnn_agg_t(GraphArgs g, const float* __restrict__ dm, float* __restrict__ dh)
+{
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int u = static_cast<int>(t >> 4), c4 = static_cast<int>(t & 15);
+    if (u >= g.n) return;
+    float4 acc = reinterpret_cast<const float4*>(dh + static_cast<long long>(u) * kH)[c4];
+    for (int k = g.tr_ptr[u]; k < g.tr_ptr[u + 1]; ++k) {
+        const float w = g.tr_w[k];
+        const float4 d = reinterpret_cast<const float4*>(dm + static_cast<long long>(g.tr_col[k]) * kH)[c4];
+        acc.x = fmaf(w, d.x, acc.x);
+        acc.y = fmaf(w, d.y, acc.y);
+        acc.z = fmaf(w, d.z, acc.z);
+        acc.w = fmaf(w, d.w, acc.w);
+    }
+    reinterpret_cast<float4*>(dh + static_cast<long long>(u) * kH)[c4] = acc;
+}
+
+// Layer weight gradient on the tensor cores: dWl^T (128 x 64) = [h | m]^T dy,
+// K = vertices.  Each CTA accumulates its tiles in TMEM (operands transposed
+// into K-major shared tiles) and writes one FP32 partial; k_gnn_reduce sums
+// the partials in CTA order.
+constexpr int kWgradSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128;
+
+__global__ void __launch_bounds__(kLayerThreads, 4)
+    k_gnn_wgrad(int n, const bf16* __restrict__ h, const bf16* __restrict__ m, const bf16* __restrict__ dy,
+                float* __restrict__ partials, unsigned* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) std::uint64_t bar_storage;
+    __shared__ std::uint32_t tmem_base_s;
+    const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
+    unsigned char* tile = smem_raw + (base - raw);
+    // A: 128 feature rows x 128 vertices (two K blocks of 64); B: 64 rows x 128.
+    const std::uint32_t a0 = base, b0 = base + 2 * kTile * 128;
+    const std::uint32_t bar = smem_u32(&bar_storage);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (n + kTile - 1) / kTile;
+    const int t0 = static_cast<int>(static_cast<long long>(ntiles) * blockIdx.x / gridDim.x);
+    const int t1 = static_cast<int>(static_cast<long long>(ntiles) * (blockIdx.x + 1) / gridDim.x);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async_smem();
+    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kH);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const std::uint32_t tmem = tmem_base_s;
+    constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, kH);
+    bf16* sa = reinterpret_cast<bf16*>(tile);
+    bf16* sb = reinterpret_cast<bf16*>(tile + 2 * kTile * 128);
+    int iter = 0;
+    bool ok = true;
+    for (int t = t0; t < t1; ++t, ++iter) {
+        const int row0 = t * kTile;
+        // Transpose: vertex k of the tile becomes K index k; feature f a row.
+        for (int i = threadIdx.x; i < kTile * 16; i += kLayerThreads) {
+            const int k = i >> 4, c16 = i & 15, v = row0 + k;     // c16: 16-byte chunk of [h | m] (8 features)
+            uint4 u = make_uint4(0, 0, 0, 0);
+            if (v < n) u = *reinterpret_cast<const uint4*>((c16 < 8 ? h : m) + static_cast<long long>(v) * kH
+                                                          + (c16 & 7) * 8);
+            const bf16* e = reinterpret_cast<const bf16*>(&u);
+            const int kb = k >> 6, kc = (k & 63) >> 3, ke = k & 7;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int f = c16 * 8 + q;
+                sa[(kb * kTile * 128 + sw128(f, kc)) / 2 + ke] = e[q];
+            }
+        }
+        for (int i = threadIdx.x; i < kTile * 8; i += kLayerThreads) {
+            const int k = i >> 3, c8 = i & 7, v = row0 + k;
+            uint4 u = make_uint4(0, 0, 0, 0);
+            if (v < n) u = *reinterpret_cast<const uint4*>(dy + static_cast<long long>(v) * kH + c8 * 8);
+            const bf16* e = reinterpret_cast<const bf16*>(&u);
+            const int kb = k >> 6, kc = (k & 63) >> 3, ke = k & 7;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int o = c8 * 8 + q;
+                sb[(kb * kH * 128 + sw128(o, kc)) / 2 + ke] = e[q];
+            }
+        }
+        fence_proxy_async_smem();
+        tmem_fence_before_sync();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tmem_fence_after_sync();
+#pragma unroll
+            for (int kb = 0; kb < 2; ++kb)
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    umma_bf16(tmem, umma_desc_sw128(a0 + kb * kTile * 128 + 32 * k),
+                              umma_desc_sw128(b0 + kb * kH * 128 + 32 * k), idesc, iter > 0 || kb > 0 || k > 0);
+            umma_commit(bar);
+        }
+        ok = wait_phase(bar, iter & 1);
+        tmem_fence_after_sync();
+        if (!__syncthreads_and(ok)) break;
+    }
+    // Partial of this CTA (zero if it had no tiles).
+    const int f = 32 * warp + lane;
+    float* out = partials + static_cast<long long>(blockIdx.x) * (2 * kH) * kH + static_cast<long long>(f) * kH;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        float y[32];
+        if (iter > 0 && ok) {
+            tmem_ld32(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + 32 * half, y);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) y[i] = 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) out[32 * half + i] = y[i];
+    }
+    if (!ok && threadIdx.x == 0) atomicOr(status, kErrTimeout);
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, kH);
+}
+
+// Adam (bias-corrected) on the flat FP32 parameters; refreshes the BF16
+// copies of the layer weights (Wl and Wl^T) used by the tensor cores.
+__global__ void __launch_bounds__(256) k_gnn_adam(int count, float* __restrict__ p, const float* __restrict__ g,
+                                                  float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                                                  float b2, float eps, float c1, float c2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_gnn_pack(const float* __restrict__ wl, bf16* __restrict__ wl16, bf16* __restrict__ wlt16)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;    // over kLayers * 64 * 128
+    if (i >= kLayers * kH * 2 * kH) return;
+    const int l = i / (kH * 2 * kH), r = (i / (2 * kH)) % kH, c = i % (2 * kH);
+    const bf16 b = __float2bfloat16_rn(wl[i]);
+    wl16[i] = b;
+    wlt16[l * kH * 2 * kH + c * kH + r] = b;
+}
+
+// Matrix graph: weights w_vu = -mean_c a_vu,c / d_v,c of the off-diagonal
+// entries and 1 / diagonal.
+__global__ void k_gnn_graph(int n, int bs, const int* __restrict__ nb_ptr, const int* __restrict__ nb_entry,
+                            const double* __restrict__ vals, const double* __restrict__ diag, float* __restrict__ nb_w,
+                            float* __restrict__ dinv)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    for (int c = 0; c < bs; ++c)
+        dinv[static_cast<long long>(v) * bs + c] = static_cast<float>(1.0 / diag[static_cast<long long>(v) * bs + c]);
+    for (int k = nb_ptr[v]; k < nb_ptr[v + 1]; ++k) {
+        const long long e = nb_entry[k];
+        double acc = 0.0;
+        for (int c = 0; c < bs; ++c) acc += vals[e * bs + c] / diag[static_cast<long long>(v) * bs + c];
+        nb_w[k] = static_cast<float>(-acc / bs);
+    }
+}
+
+__global__ void k_gnn_gather_w(int count, const int* __restrict__ idx, const float* __restrict__ src,
+                               float* __restrict__ dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) dst[i] = src[idx[i]];
+}
+
+}  // namespace gnn
+
+// ====================================================================== host
+struct Gnn {
+    static constexpr int kOffWe = 0;
+    static constexpr int kOffWl = gnn::kH * gnn::kF;
+    static constexpr int kLayerW = gnn::kH * 2 * gnn::kH;
+    static constexpr int kOffWd = kOffWl + gnn::kLayers * kLayerW;
+    static constexpr int kParams = kOffWd + 8 * gnn::kH;
+
+    Context* ctx = nullptr;
+    Matrix* matrix = nullptr;
+    int n = 0, bs = 0;
+    DeviceBuffer nb_ptr, nb_col, nb_w, nb_entry, tr_ptr, tr_col, tr_w, tr_edge, dinv;
+    DeviceBuffer params, grads, adam_m, adam_v, wl16, wlt16;
+    DeviceBuffer h[gnn::kLayers + 1], m[gnn::kLayers], mask[gnn::kLayers], x;   // training activations
+    DeviceBuffer ha, hb;                                                       // inference ping-pong
+    DeviceBuffer norm_r, norm_e, out32, dz, dh, dm, dy, partials, loss_partials, ticket, loss;
+    DeviceBuffer qbuf;   // q = r / d (FP32); norm_r holds |r|, |q| at [0], [2]
+    int adam_t = 0;
+    bool train_ready = false;
+    std::uint64_t applications = 0;
+
+    gnn::GraphArgs graph() const
+    {
+        gnn::GraphArgs g;
+        g.n = n;
+        g.bs = bs;
+        g.nb_ptr = nb_ptr.as<int>();
+        g.nb_col = nb_col.as<int>();
+        g.nb_w = nb_w.as<float>();
+        g.tr_ptr = tr_ptr.as<int>();
+        g.tr_col = tr_col.as<int>();
+        g.tr_w = tr_w.as<float>();
+        g.dinv = dinv.as<float>();
+        return g;
+    }
+    unsigned blocks(long long count, int threads = 256) const
+    {
+        return static_cast<unsigned>((count + threads - 1) / threads);
+    }
+    unsigned layer_grid() const
+    {
+        const int tiles = (n + gnn::kTile - 1) / gnn::kTile;
+        return static_cast<unsigned>(std::min(tiles, ctx->sm_count * 4));
+    }
+};
+
+namespace {
+
+void gnn_pack(Gnn& G)
+{
+    gnn::k_gnn_pack<<<G.blocks(gnn::kLayers * Gnn::kLayerW), 256, 0, G.ctx->stream>>>(
+        G.params.as<float>() + Gnn::kOffWl, G.wl16.as<gnn::bf16>(), G.wlt16.as<gnn::bf16>());
+    OWTK_CUDA(cudaGetLastError());
+    G.ctx->launched();
+}
+
+void gnn_set_attrs()
+{
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kLayerSmem));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kLayerSmem));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kBwdSmem));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kWgradSmem));
+}
+
+// Seeded initial weights: normal draws from std::mt19937_64, scaled per
+// matrix; the decoder starts at zero (the network starts as Jacobi).
+std::vector<float> gnn_initial_weights(int bs, std::uint64_t seed)
+{
+    std::vector<float> w(Gnn::kParams, 0.0f);
+    std::mt19937_64 gen(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    const double se = 1.0 / std::sqrt(2.0 * bs), sl = 0.5 / std::sqrt(2.0 * gnn::kH);
+    for (int k = 0; k < gnn::kH; ++k)
+        for (int f = 0; f < gnn::kF; ++f) {
+            const double z = nd(gen);
+            w[Gnn::kOffWe + k * gnn::kF + f] = f < 2 * bs ? static_cast<float>(se * z) : 0.0f;
+        }
+    for (int i = 0; i < gnn::kLayers * Gnn::kLayerW; ++i) w[Gnn::kOffWl + i] = static_cast<float>(sl * nd(gen));
+    return w;
+}
+
+// Forward from r (device, T) into out (device, O).  TRAIN keeps activations.
+template<class T, class O, bool TRAIN>
+void gnn_forward(Gnn& G, const T* r, O* out)
+{
+    Context& c = *G.ctx;
+    const gnn::GraphArgs g = G.graph();
+    const long long nb = static_cast<long long>(G.n) * G.bs;
+    double* norms = G.norm_r.as<double>();
+    gnn::k_gnn_prepare<T><<<G.blocks(nb), 256, 0, c.stream>>>(nb, r, G.dinv.as<float>(), G.qbuf.as<float>());
+    kern::norm<T>(c, static_cast<std::size_t>(nb), r, norms, norms + 1);
+    kern::norm<float>(c, static_cast<std::size_t>(nb), G.qbuf.as<float>(), norms + 2, norms + 3);
+    gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
+    gnn::k_gnn_encode<T><<<G.blocks(G.n), 256, 0, c.stream>>>(g, r, G.qbuf.as<float>(), norms,
+                                                               G.params.as<float>() + Gnn::kOffWe, h0);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched(2);
+    const gnn::bf16* hin = h0;
+    for (int l = 0; l < gnn::kLayers; ++l) {
+        gnn::bf16* hout = TRAIN ? G.h[l + 1].as<gnn::bf16>() : (l % 2 == 0 ? G.hb : G.ha).as<gnn::bf16>();
+        gnn::k_gnn_layer<TRAIN><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
+            g, hin, G.wl16.as<gnn::bf16>() + l * Gnn::kLayerW, hout, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
+            TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, c.status.as<unsigned>());
+        OWTK_CUDA(cudaGetLastError());
+        c.launched();
+        hin = hout;
+    }
+    gnn::k_gnn_decode<O><<<G.blocks(G.n), 256, 0, c.stream>>>(g, G.qbuf.as<float>(), norms,
+                                                               G.params.as<float>() + Gnn::kOffWd, hin, out);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+    ++G.applications;
+}
+
+void gnn_train_buffers(Gnn& G)
+{
+    if (G.train_ready) return;
+    const std::size_t rows = static_cast<std::size_t>(G.n);
+    for (auto& b : G.h) b.allocate(rows * gnn::kH * 2 + 16);
+    for (auto& b : G.m) b.allocate(rows * gnn::kH * 2 + 16);
+    for (auto& b : G.mask) b.allocate(rows * 8 + 16);
+    G.x.allocate(rows * gnn::kF * 4 + 16);
+    G.out32.allocate(rows * G.bs * 4 + 16);
+    G.dz.allocate(rows * G.bs * 4 + 16);
+    G.dh.allocate(rows * gnn::kH * 4 + 16);
+    G.dm.allocate(rows * gnn::kH * 4 + 16);
+    G.dy.allocate(rows * gnn::kH * 2 + 16);
+    G.partials.allocate(static_cast<std::size_t>(std::max(G.ctx->sm_count * 4, 256)) * 2 * gnn::kH * gnn::kH * 4);
+    G.loss_partials.allocate(1024 * 8);
+    G.ticket.allocate(16);
+    OWTK_CUDA(cudaMemsetAsync(G.ticket.ptr, 0, 16, G.ctx->stream));
+    G.loss.allocate(16);
+    G.norm_e.allocate(16);
+    G.train_ready = true;
+}
+
+// Features x of every vertex (kept for the encoder gradient).
+__global__ void k_gnn_features(gnn::GraphArgs g, const double* __restrict__ r, const float* __restrict__ q,
+                               const double* norms, float* __restrict__ x)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.n) return;
+    const double root = sqrt(static_cast<double>(g.n) * g.bs), nr = norms[0], nq = norms[2];
+    const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
+    const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
+    float* xv = x + static_cast<long long>(v) * gnn::kF;
+    for (int f = 0; f < gnn::kF; ++f) xv[f] = 0.0f;
+    for (int c = 0; c < g.bs; ++c) {
+        const long long o = static_cast<long long>(v) * g.bs + c;
+        xv[c] = static_cast<float>(r[o]) * inv_r;
+        xv[g.bs + c] = q[o] * inv_q;
+    }
+}
+
+// Loss and gradient of one (r, e) pair into G.grads; returns the loss.
+double gnn_loss_grad(Gnn& G, const double* r, const double* e)
+{
+    Context& c = *G.ctx;
+    gnn_train_buffers(G);
+    const gnn::GraphArgs g = G.graph();
+    const long long nb = static_cast<long long>(G.n) * G.bs;
+    gnn_forward<double, float, true>(G, r, G.out32.as<float>());
+    k_gnn_features<<<G.blocks(G.n), 256, 0, c.stream>>>(g, r, G.qbuf.as<float>(), G.norm_r.as<double>(),
+                                                        G.x.as<float>());
+    kern::norm<double>(c, static_cast<std::size_t>(nb), e, G.norm_e.as<double>(), G.norm_e.as<double>() + 1);
+    const unsigned lb = 512;
+    gnn::k_gnn_out_grad<<<lb, 256, 0, c.stream>>>(nb, G.out32.as<float>(), e, G.norm_e.as<double>(),
+                                                   G.norm_r.as<double>(), std::sqrt(static_cast<double>(nb)),
+                                                   G.dz.as<float>(), G.loss_partials.as<double>(),
+                                                   G.ticket.as<unsigned>(), G.loss.as<double>());
+    gnn::k_gnn_decode_bwd<<<G.blocks(G.n), 256, 0, c.stream>>>(G.n, G.bs, G.dz.as<float>(),
+                                                                G.params.as<float>() + Gnn::kOffWd, G.dh.as<float>());
+    float* grads = G.grads.as<float>();
+    OWTK_CUDA(cudaMemsetAsync(grads, 0, Gnn::kParams * sizeof(float), c.stream));
+    const unsigned ob = 256;
+    gnn::k_gnn_outer<gnn::bf16><<<ob, 256, 0, c.stream>>>(G.n, G.bs, gnn::kH, G.dz.as<float>(),
+                                                           G.h[gnn::kLayers].as<gnn::bf16>(), G.partials.as<float>());
+    gnn::k_gnn_reduce<<<G.blocks(G.bs * gnn::kH), 256, 0, c.stream>>>(ob, G.bs * gnn::kH, G.partials.as<float>(),
+                                                                       grads + Gnn::kOffWd, 0, 0, 0);
+    c.launched(6);
+    for (int l = gnn::kLayers - 1; l >= 0; --l) {
+        gnn::k_gnn_layer_bwd<<<G.layer_grid(), gnn::kLayerThreads, gnn::kBwdSmem, c.stream>>>(
+            G.n, G.dh.as<float>(), G.mask[l].as<unsigned long long>(), G.wlt16.as<gnn::bf16>() + l * Gnn::kLayerW,
+            G.dy.as<gnn::bf16>(), G.dm.as<float>(), c.status.as<unsigned>());
+        const unsigned wg = G.layer_grid();
+        gnn::k_gnn_wgrad<<<wg, gnn::kLayerThreads, gnn::kWgradSmem, c.stream>>>(
+            G.n, G.h[l].as<gnn::bf16>(), G.m[l].as<gnn::bf16>(), G.dy.as<gnn::bf16>(), G.partials.as<float>(),
+            c.status.as<unsigned>());
+        gnn::k_gnn_reduce<<<G.blocks(2 * gnn::kH * gnn::kH), 256, 0, c.stream>>>(
+            wg, 2 * gnn::kH * gnn::kH, G.partials.as<float>(), grads + Gnn::kOffWl + l * Gnn::kLayerW, 2 * gnn::kH,
+            gnn::kH, 1);
+        gnn::k_gnn_agg_t<<<G.blocks(static_cast<long long>(G.n) * 16), 256, 0, c.stream>>>(g, G.dm.as<float>(),
+                                                                                            G.dh.as<float>());
+        OWTK_CUDA(cudaGetLastError());
+        c.launched(4);
+    }
+    gnn::k_gnn_outer<float><<<ob, 256, 0, c.stream>>>(G.n, gnn::kH, gnn::kF, G.dh.as<float>(), G.x.as<float>(),
+                                                       G.partials.as<float>());
+    gnn::k_gnn_reduce<<<G.blocks(gnn::kH * gnn::kF), 256, 0, c.stream>>>(ob, gnn::kH * gnn::kF, G.partials.as<float>(),
+                                                                          grads + Gnn::kOffWe, 0, 0, 0);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched(3);
+    double loss = 0.0;
+    OWTK_CUDA(cudaMemcpyAsync(&loss, G.loss.ptr, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    c.check_device_status();
+    return loss;
+}
+
+void gnn_adam(Gnn& G, double lr)
+{
+    Context& c = *G.ctx;
+    ++G.adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, static_cast<float>(G.adam_t));
+    const float c2 = 1.0f - std::pow(b2, static_cast<float>(G.adam_t));
+    gnn::k_gnn_adam<<<G.blocks(Gnn::kParams), 256, 0, c.stream>>>(Gnn::kParams, G.params.as<float>(),
+                                                                    G.grads.as<float>(), G.adam_m.as<float>(),
+                                                                    G.adam_v.as<float>(), static_cast<float>(lr), b1,
+                                                                    b2, 1e-8f, c1, c2);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+    gnn_pack(G);
+}
+
+}  // namespace
+
+namespace gnn {
+}  // namespace gnn
+}  // namespace owtk
+
+// ====================================================================== C ABI
+namespace owtk {
+
+// z = M(v); judged by ||v - A z|| against ||v||, the fallback steps in when
+// the network does not reduce the residual.
+void learned_apply(Preconditioner& p, Vector& in, Vector& out)
+{
+    Gnn& G = *p.net;
+    Context& c = *G.ctx;
+    const std::size_t n = static_cast<std::size_t>(G.n) * G.bs;
+    const double* x = static_cast<const double*>(in.data);
+    double* y = static_cast<double*>(out.data);
+    if (x == y) {
+        if (!p.alias_copy.ptr) p.alias_copy.allocate(n * sizeof(double) + 16);
+        kern::copy<double>(c, n, x, p.alias_copy.as<double>());
+        x = p.alias_copy.as<double>();
+    }
+    gnn_forward<double, double, false>(G, x, y);
+    ++p.learned_applications;
+    if (p.fallback == nullptr) return;
+    if (!p.check_work.ptr) p.check_work.allocate(n * sizeof(double) + 16);
+    double* w = p.check_work.as<double>();
+    kern::spmv<double>(c, *G.matrix, y, w);
+    kern::sub<double>(c, n, x, w, w);
+    constexpr int kSlot = kScalarSlots - 4;
+    kern::norm<double>(c, n, w, c.dev_scalar_copy.as<double>() + kSlot, c.dev_scalars + kSlot);
+    kern::norm<double>(c, n, x, c.dev_scalar_copy.as<double>() + kSlot + 1, c.dev_scalars + kSlot + 1);
+    c.sync();
+    const double rho = c.host_scalars[kSlot], nu = c.host_scalars[kSlot + 1];
+    if (!(rho < nu)) {
+        ++p.learned_fallbacks;
+        Vector src;        // non-owning description of the (possibly copied) input
+        src.ctx = in.ctx;
+        src.dtype = in.dtype;
+        src.owned = in.owned;
+        src.ghost = in.ghost;
+        src.bs = in.bs;
+        src.data = const_cast<double*>(x);
+        src.is_view = true;
+        apply_preconditioner(p.fallback, src, out);
+    }
+}
+
+namespace {
+
+void gnn_bind_matrix(Gnn& G, Matrix& m)
+{
+    Context& c = *G.ctx;
+    DeviceBuffer diag(static_cast<std::size_t>(G.n) * G.bs * sizeof(double) + 16);
+    kern::bsr_diagonal<double>(c, m, diag.as<double>());
+    c.sync();
+    try {
+        c.check_device_status();
+    } catch (const Error&) {
+        fail(OWTK_ERR_INVALID_ARGUMENT, "BlockCsrMatrix row has no diagonal");
+    }
+    gnn::k_gnn_graph<<<G.blocks(G.n), 256, 0, c.stream>>>(G.n, G.bs, G.nb_ptr.as<int>(), G.nb_entry.as<int>(),
+                                                           static_cast<const double*>(m.values.ptr), diag.as<double>(),
+                                                           G.nb_w.as<float>(), G.dinv.as<float>());
+    const int ne = static_cast<int>(G.tr_col.bytes / sizeof(int));
+    if (ne > 0)
+        gnn::k_gnn_gather_w<<<G.blocks(ne), 256, 0, c.stream>>>(ne, G.tr_edge.as<int>(), G.nb_w.as<float>(),
+                                                                G.tr_w.as<float>());
+    OWTK_CUDA(cudaGetLastError());
+    c.launched(2);
+    c.sync();
+    G.matrix = &m;
+}
+
+}  // namespace
+}  // namespace owtk
+
+struct owtk_learned : owtk::Gnn {};
+
+extern "C" {
+
+owtk_status owtk_bf16_gemm_nt(owtk_context* ctx, size_t m, size_t n, size_t k, const void* device_a,
+                              const void* device_b, float* device_d)
+{
+    return owtk::guarded([&] {
+        owtk::require(ctx != nullptr && device_a != nullptr && device_b != nullptr && device_d != nullptr,
+                      "null argument");
+        if (m == 0 || m % 128 != 0 || (n != 64 && n != 128) || k == 0 || k % 64 != 0 || k > (1u << 20)
+            || m > (1ull << 31))
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "bf16 gemm shape: m % 128 == 0, n in {64, 128}, k % 64 == 0");
+        const auto aligned = [](const void* p) { return (reinterpret_cast<std::uintptr_t>(p) & 15u) == 0; };
+        if (!aligned(device_a) || !aligned(device_b) || !aligned(device_d))
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "bf16 gemm operands must be 16-byte aligned");
+        const int smem = 1024 + owtk::gnn::kTile * 128 + static_cast<int>(n) * 128;
+        const auto* A = static_cast<const owtk::gnn::bf16*>(device_a);
+        const auto* B = static_cast<const owtk::gnn::bf16*>(device_b);
+        const unsigned grid = static_cast<unsigned>(m / 128);
+        if (n == 64) {
+            OWTK_CUDA(cudaFuncSetAttribute(owtk::gnn::k_umma_gemm_nt<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           smem));
+            owtk::gnn::k_umma_gemm_nt<64><<<grid, 128, smem, ctx->stream>>>(static_cast<int>(k), A, B, device_d,
+                                                                             ctx->status.as<unsigned>());
+        } else {
+            OWTK_CUDA(cudaFuncSetAttribute(owtk::gnn::k_umma_gemm_nt<128>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            owtk::gnn::k_umma_gemm_nt<128><<<grid, 128, smem, ctx->stream>>>(static_cast<int>(k), A, B, device_d,
+                                                                              ctx->status.as<unsigned>());
+        }
+        OWTK_CUDA(cudaGetLastError());
+        ctx->launched();
+        ctx->sync();
+        ctx->check_device_status();
+    });
+}
+
+owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** out)
+{
+    return owtk::guarded([&] {
+        owtk::require(m != nullptr && out != nullptr, "null handle");
+        if (m->kind != 0 || m->dtype != OWTK_F64 || m->ghost != 0 || m->bs == 0 || m->bs > 8)
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT,
+                       "the learned preconditioner needs an FP64 component-diagonal BSR matrix, no ghosts, bs <= 8");
+        auto G = std::make_unique<owtk_learned>();
+        G->ctx = m->ctx;
+        G->n = static_cast<int>(m->owned);
+        G->bs = static_cast<int>(m->bs);
+        // Off-diagonal neighbour lists and their transpose (host structure).
+        std::vector<std::int32_t> nb_ptr(G->n + 1, 0), nb_col, nb_entry, tr_count(G->n + 1, 0);
+        for (int v = 0; v < G->n; ++v) {
+            for (int e = m->h_rowptr[v]; e < m->h_rowptr[v + 1]; ++e) {
+                const int u = m->h_cols[e];
+                if (u == v) continue;
+                nb_col.push_back(u);
+                nb_entry.push_back(e);
+                ++tr_count[u + 1];
+            }
+            nb_ptr[v + 1] = static_cast<std::int32_t>(nb_col.size());
+        }
+        std::vector<std::int32_t> tr_ptr(G->n + 1, 0);
+        for (int u = 0; u < G->n; ++u) tr_ptr[u + 1] = tr_ptr[u] + tr_count[u + 1];
+        std::vector<std::int32_t> tr_col(nb_col.size()), tr_edge(nb_col.size()), fill(tr_ptr.begin(), tr_ptr.end() - 1);
+        for (int v = 0; v < G->n; ++v)
+            for (int k = nb_ptr[v]; k < nb_ptr[v + 1]; ++k) {
+                const int u = nb_col[k];
+                tr_col[fill[u]] = v;
+                tr_edge[fill[u]] = k;
+                ++fill[u];
+            }
+        cudaStream_t st = G->ctx->stream;
+        G->nb_ptr = owtk::upload(st, nb_ptr);
+        G->nb_col = owtk::upload(st, nb_col);
+        G->nb_entry = owtk::upload(st, nb_entry);
+        G->tr_ptr = owtk::upload(st, tr_ptr);
+        G->tr_col = owtk::upload(st, tr_col);
+        G->tr_col.bytes = tr_col.size() * sizeof(int);
+        G->tr_edge = owtk::upload(st, tr_edge);
+        G->nb_w.allocate(nb_col.size() * sizeof(float) + 16);
+        G->tr_w.allocate(nb_col.size() * sizeof(float) + 16);
+        G->dinv.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
+        const std::vector<float> w0 = owtk::gnn_initial_weights(G->bs, seed);
+        G->params = owtk::upload(st, w0);
+        G->grads.allocate(owtk::Gnn::kParams * sizeof(float) + 16);
+        G->adam_m.allocate(owtk::Gnn::kParams * sizeof(float) + 16);
+        G->adam_v.allocate(owtk::Gnn::kParams * sizeof(float) + 16);
+        OWTK_CUDA(cudaMemsetAsync(G->adam_m.ptr, 0, owtk::Gnn::kParams * sizeof(float), st));
+        OWTK_CUDA(cudaMemsetAsync(G->adam_v.ptr, 0, owtk::Gnn::kParams * sizeof(float), st));
+        G->wl16.allocate(owtk::gnn::kLayers * owtk::Gnn::kLayerW * 2 + 16);
+        G->wlt16.allocate(owtk::gnn::kLayers * owtk::Gnn::kLayerW * 2 + 16);
+        G->ha.allocate(static_cast<std::size_t>(G->n) * owtk::gnn::kH * 2 + 16);
+        G->hb.allocate(static_cast<std::size_t>(G->n) * owtk::gnn::kH * 2 + 16);
+        G->norm_r.allocate(64);
+        G->qbuf.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
+        owtk::gnn_set_attrs();
+        owtk::gnn_pack(*G);
+        owtk::gnn_bind_matrix(*G, *m);
+        *out = G.release();
+    });
+}
+
+owtk_status owtk_learned_destroy(owtk_learned* net)
+{
+    return owtk::guarded([&] { delete net; });
+}
+
+owtk_status owtk_learned_update_matrix(owtk_learned* net, owtk_matrix* m)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && m != nullptr, "null handle");
+        if (m->kind != 0 || m->dtype != OWTK_F64 || static_cast<int>(m->owned) != net->n
+            || static_cast<int>(m->bs) != net->bs || m->entries != net->matrix->entries)
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "matrix pattern differs from the network's graph");
+        owtk::gnn_bind_matrix(*net, *m);
+    });
+}
+
+size_t owtk_learned_parameter_count(void) { return owtk::Gnn::kParams; }
+
+owtk_status owtk_learned_get_parameters(owtk_learned* net, float* host, size_t count)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && host != nullptr && count == owtk::Gnn::kParams, "parameter count");
+        OWTK_CUDA(cudaMemcpyAsync(host, net->params.ptr, count * sizeof(float), cudaMemcpyDeviceToHost,
+                                  net->ctx->stream));
+        net->ctx->sync();
+    });
+}
+
+owtk_status owtk_learned_set_parameters(owtk_learned* net, const float* host, size_t count)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && host != nullptr && count == owtk::Gnn::kParams, "parameter count");
+        OWTK_CUDA(cudaMemcpyAsync(net->params.ptr, host, count * sizeof(float), cudaMemcpyHostToDevice,
+                                  net->ctx->stream));
+        owtk::gnn_pack(*net);
+        net->ctx->sync();
+    });
+}
+
+owtk_status owtk_learned_apply(owtk_learned* net, owtk_vector* in, owtk_vector* out)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && in != nullptr && out != nullptr, "null handle");
+        if (in->dtype != OWTK_F64 || out->dtype != OWTK_F64 || static_cast<int>(in->owned) != net->n
+            || static_cast<int>(in->bs) != net->bs || !in->same_layout(*out))
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "learned preconditioner vector layout mismatch");
+        if (in->data == out->data) owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "in and out must differ");
+        owtk::gnn_forward<double, double, false>(*net, static_cast<const double*>(in->data),
+                                                 static_cast<double*>(out->data));
+        net->ctx->sync();
+        net->ctx->check_device_status();
+    });
+}
+
+owtk_status owtk_learned_loss_grad(owtk_learned* net, owtk_vector* r, owtk_vector* e, double* loss,
+                                   float* host_grads)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && r != nullptr && e != nullptr && loss != nullptr, "null argument");
+        if (r->dtype != OWTK_F64 || e->dtype != OWTK_F64 || static_cast<int>(r->owned) != net->n
+            || static_cast<int>(r->bs) != net->bs || !r->same_layout(*e))
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "training pair layout mismatch");
+        *loss = owtk::gnn_loss_grad(*net, static_cast<const double*>(r->data), static_cast<const double*>(e->data));
+        if (host_grads) {
+            OWTK_CUDA(cudaMemcpyAsync(host_grads, net->grads.ptr, owtk::Gnn::kParams * sizeof(float),
+                                      cudaMemcpyDeviceToHost, net->ctx->stream));
+            net->ctx->sync();
+        }
+    });
+}
+
+owtk_status owtk_learned_adam_step(owtk_learned* net, double learning_rate)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && learning_rate > 0 && std::isfinite(learning_rate), "invalid learning rate");
+        owtk::gnn_adam(*net, learning_rate);
+        net->ctx->sync();
+    });
+}
+
+owtk_status owtk_pc_create_learned(owtk_learned* net, owtk_preconditioner* fallback, owtk_preconditioner** out)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && out != nullptr, "null handle");
+        if (fallback && (fallback->owned != static_cast<std::size_t>(net->n)
+                         || fallback->bs != static_cast<std::size_t>(net->bs) || fallback->dtype != OWTK_F64))
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "fallback preconditioner layout differs from the network's");
+        auto p = std::make_unique<owtk_preconditioner>();
+        p->ctx = net->ctx;
+        p->kind = OWTK_PC_LEARNED;
+        p->dtype = OWTK_F64;
+        p->matrix = net->matrix;
+        p->owned = static_cast<std::size_t>(net->n);
+        p->bs = static_cast<std::size_t>(net->bs);
+        p->net = net;
+        p->fallback = fallback;
+        *out = p.release();
+    });
+}
+
+owtk_status owtk_pc_learned_counts(owtk_preconditioner* p, uint64_t* applications, uint64_t* fallbacks)
+{
+    return owtk::guarded([&] {
+        owtk::require(p != nullptr && p->kind == OWTK_PC_LEARNED, "not a learned preconditioner");
+        if (applications) *applications = p->learned_applications;
+        if (fallbacks) *fallbacks = p->learned_fallbacks;
+    });
+}
+
+}  // extern "C"

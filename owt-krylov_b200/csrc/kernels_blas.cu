@@ -499,53 +499,6 @@ __global__ void __launch_bounds__(kThreads) k_cgs_update_dot(std::size_t n, int 
 // to scale) and rescales when a larger magnitude arrives; pairs combine the
 // same way.  NaN anywhere gives NaN and an infinite entry gives infinity,
 // as the reference's two-pass scaled norm does (reduction.hpp:64-89).
-struct ScaledSum {
-    double scale, ssq;
-    int nan;
-};
-
-__device__ __forceinline__ void norm_push(ScaledSum& a, double x)
-{
-    const double m = fabs(x);
-    if (isnan(m)) { a.nan = 1; return; }
-    if (m == 0.0 || isinf(a.scale)) return;
-    if (m > a.scale) {
-        if (isinf(m)) { a.scale = m; a.ssq = 1.0; return; }
-        const double r = a.scale / m;
-        a.ssq = 1.0 + a.ssq * r * r;
-        a.scale = m;
-    } else {
-        const double r = m / a.scale;
-        a.ssq += r * r;
-    }
-}
-
-__device__ __forceinline__ ScaledSum norm_merge(ScaledSum a, ScaledSum b)
-{
-    ScaledSum r;
-    r.nan = a.nan | b.nan;
-    if (a.scale < b.scale) { const ScaledSum t = a; a = b; b = t; }
-    r.scale = a.scale;
-    if (a.scale == 0.0) { r.ssq = 0.0; return r; }
-    if (isinf(a.scale)) { r.ssq = 1.0; return r; }
-    const double q = b.scale / a.scale;
-    r.ssq = a.ssq + b.ssq * q * q;
-    return r;
-}
-
-__device__ __forceinline__ ScaledSum norm_warp(ScaledSum a)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        ScaledSum b;
-        b.scale = __shfl_xor_sync(0xffffffffu, a.scale, o);
-        b.ssq = __shfl_xor_sync(0xffffffffu, a.ssq, o);
-        b.nan = __shfl_xor_sync(0xffffffffu, a.nan, o);
-        a = norm_merge(a, b);
-    }
-    return a;
-}
-
 template<class T>
 __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __restrict__ x, double* partials,
                                                    unsigned* ticket, double* out_dev, double* out_host)

@@ -19,6 +19,7 @@
 // blocks such as bs = 1296).
 
 #include <algorithm>
+#include <cstdint>
 
 #include "device_common.cuh"
 #include "owtk_internal.h"
@@ -28,8 +29,11 @@ namespace {
 
 using namespace dev;
 
-constexpr int kStage = 1024;      // staged values (products) per tile: 4 per thread
-constexpr int kRowCap = 1024;     // rows per tile (outputs are bounded by kStage too)
+#ifndef OWTK_SPMV_STAGE
+#define OWTK_SPMV_STAGE 1024
+#endif
+constexpr int kStage = OWTK_SPMV_STAGE;   // staged values (products) per tile
+constexpr int kRowCap = kStage < 1024 ? kStage : 1024;   // rows per tile (outputs are bounded by kStage too)
 
 template<class T>
 struct SpmvArgs {
@@ -51,7 +55,7 @@ __device__ __forceinline__ int div_bs(int k, unsigned long long magic)
 
 // KIND 0: component-diagonal BSR, 1: split view, 2: dense BSR.
 template<class T, int KIND>
-__global__ void __launch_bounds__(kThreads, 8) k_spmv_tiles(SpmvArgs<T> a)
+__global__ void __launch_bounds__(kThreads, 4) k_spmv_tiles(SpmvArgs<T> a)
 {
     constexpr int kPer = kStage / kThreads;   // staged units per thread
     __shared__ T prod[kStage];
@@ -145,52 +149,276 @@ __global__ void __launch_bounds__(kThreads, 8) k_spmv_tiles(SpmvArgs<T> a)
     }
 }
 
-// Persistent variant for the component-diagonal and split forms: each CTA
-// walks tiles blockIdx.x, +gridDim.x, ... and issues the next tile's value and
-// column loads before the current tile's gather/sum/store phases, so the HBM
-// stream never waits for the shared-memory phases.  Same arithmetic as
-// k_spmv_tiles (bit-identical results).
-template<class T, int KIND>
-__global__ void __launch_bounds__(kThreads, 4) k_spmv_stream(SpmvArgs<T> a, const int4* __restrict__ meta,
-                                                              int ntiles)
-{
-    constexpr int kPer = kStage / kThreads;
-    __shared__ T prod[kStage];
-    int tile = blockIdx.x;
-    if (tile >= ntiles) return;
-    const int bs = a.bs;
-    int4 m = meta[tile];   // r0, r1, e0, e1
-    T pv[kPer];
-    int pc[kPer];          // column of value k (times bs plus component below)
+// ------------------------------------------------------------------ bulk
+// Persistent bulk-copy pipeline for the component-diagonal and split forms.
+//
+// A CTA owns a contiguous run of tiles.  Its producer warp streams each tile's
+// value run, column run and row offsets into a kBulkStages-deep shared-memory
+// ring with cp.async.bulk (completion counted in bytes on the stage's "full"
+// mbarrier; L2 evict-first on the streams so that x stays L2-resident), while
+// the eight consumer warps of the previous stages gather x, form the rounded
+// products in place and add them per output in entry order (the same
+// arithmetic as k_spmv_tiles, bit-identical results), then release the stage
+// on its "empty" mbarrier.  Every copy covers whole 16-byte granules: the
+// granule-aligned superset of the tile's runs, clipped to the last whole
+// granule of each array, with the at most 15 trailing bytes of an array read
+// by plain loads.  Every wait is bounded; a wait that gives up sets the
+// timeout bit and the consumers leave together at their next named barrier.
+#ifndef OWTK_BULK_STAGES
+#define OWTK_BULK_STAGES 3
+#endif
+#ifndef OWTK_BULK_CONSUMERS
+#define OWTK_BULK_CONSUMERS 128
+#endif
+#ifndef OWTK_BULK_CTAS_PER_SM
+#define OWTK_BULK_CTAS_PER_SM 4
+#endif
+constexpr int kBulkStages = OWTK_BULK_STAGES;
+constexpr int kBulkConsumers = OWTK_BULK_CONSUMERS;
+constexpr int kBulkThreads = kBulkConsumers + 32;
+constexpr int kBulkCtasPerSm = OWTK_BULK_CTAS_PER_SM;
+constexpr int kBulkSpin = 1 << 20;
 
-#define OWTK_SPMV_ISSUE(t)                                                         \
-    do {                                                                           \
-        const int iu = ((t).w - (t).z) * bs;                                       \
-        if (iu <= kStage && ((t).y - (t).x) * bs <= kStage) {                      \
-            const T* iv = a.vals + static_cast<std::size_t>((t).z) * bs;           \
-            _Pragma("unroll") for (int j = 0; j < kPer; ++j) {                     \
-                const int k = threadIdx.x + j * kThreads;                          \
-                if (k < iu) {                                                      \
-                    const int e = div_bs(k, a.magic);                              \
-                    pv[j] = __ldcs(iv + k);                                        \
-                    pc[j] = __ldg(a.cols + (t).z + e) * bs + (k - e * bs);         \
-                }                                                                  \
-            }                                                                      \
-        }                                                                          \
-    } while (0)
-    OWTK_SPMV_ISSUE(m);
-    for (;;) {
-        const int next = tile + static_cast<int>(gridDim.x);
-        int4 mn = make_int4(0, 0, 0, 0);
-        if (next < ntiles) mn = meta[next];
-        const int r0 = m.x, r1 = m.y, e0 = m.z;
-        const int units = (m.w - e0) * bs;
-        const int outs = (r1 - r0) * bs;
-        const bool longtile = units > kStage || outs > kStage;
-        if (longtile) {
+struct BulkHead {          // written by the producer before the stage's arrival
+    int r0, r1, e0, e1;
+    int voff, vavail;      // value k of the tile sits at vals[voff + k] if k < vavail
+    int coff, cavail;
+    int roff, ravail;
+    int longtile, pad;
+};
+
+template<class T>
+struct BulkLayout {
+    static constexpr int round128(int b) { return (b + 127) / 128 * 128; }
+    static constexpr int kVals = round128(kStage * static_cast<int>(sizeof(T)) + 16);
+    static constexpr int kCols = round128(kStage * 4 + 16);
+    static constexpr int kRows = round128((kRowCap + 1) * 4 + 16);
+    static constexpr int kHead = 128;
+    static constexpr int kStageBytes = kVals + kCols + kRows + kHead;
+    static constexpr int kBars = 128;    // 2 * kBulkStages mbarriers
+    static constexpr int kTotal = kBars + kBulkStages * kStageBytes;
+    static_assert(2 * kBulkStages * 8 <= kBars, "mbarrier area");
+};
+
+// Granule-aligned copy of elements [b, e) of an array of `total` elements of
+// `sz` bytes starting at a 16-byte aligned base.  Returns the bytes to copy
+// (0: nothing), the copy's first byte `lo`, the index of element b in the
+// destination and how many of the run's elements the copy holds.
+__device__ __forceinline__ std::uint32_t bulk_segment(std::size_t b, std::size_t e, std::size_t total, int sz,
+                                                      std::size_t& lo, int& off, int& avail)
+{
+    const std::size_t bb = b * sz, eb = e * sz, tb = (total * sz) & ~std::size_t(15);
+    lo = bb & ~std::size_t(15);
+    std::size_t hi = (eb + 15) & ~std::size_t(15);
+    if (hi > tb) hi = tb;
+    off = static_cast<int>((bb - lo) / sz);
+    if (hi <= bb) {
+        avail = 0;
+        return 0;
+    }
+    avail = static_cast<int>((hi - bb) / sz);
+    return static_cast<std::uint32_t>(hi - lo);
+}
+
+// Products of one staged tile, written in place over the staged values.
+// BS > 0: block size known at compile time; thread t takes entries t, t+C, ...
+// and all BS components of each (one column load per entry, BS independent
+// gathers).  BS == 0: any block size; thread t takes values t, t+C, ...
+template<class T, int BS>
+__device__ __forceinline__ void bulk_products(const SpmvArgs<T>& a, const BulkHead* h, T* sv, const int* sc, int t)
+{
+    const int e0 = h->e0, ne = h->e1 - e0;
+    const int voff = h->voff, vavail = h->vavail, coff = h->coff, cavail = h->cavail;
+    const std::size_t vbase = static_cast<std::size_t>(e0) * (BS > 0 ? BS : a.bs);
+    if constexpr (BS > 0) {
+        constexpr int kEpt = (kStage / BS + kBulkConsumers - 1) / kBulkConsumers;
+        T pv[kEpt][BS], px[kEpt][BS];
+#pragma unroll
+        for (int j = 0; j < kEpt; ++j) {
+            const int el = t + j * kBulkConsumers;
+            if (el < ne) {
+                const int col = el < cavail ? sc[coff + el] : a.cols[e0 + el];
+                const T* xs = a.x + col * BS;
+#pragma unroll
+                for (int c = 0; c < BS; ++c) {
+                    const int k = el * BS + c;
+                    pv[j][c] = k < vavail ? sv[voff + k] : a.vals[vbase + k];
+                    px[j][c] = __ldg(xs + c);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kEpt; ++j) {
+            const int el = t + j * kBulkConsumers;
+            if (el < ne) {
+#pragma unroll
+                for (int c = 0; c < BS; ++c) sv[voff + el * BS + c] = mul_rn(pv[j][c], px[j][c]);
+            }
+        }
+    } else {
+        constexpr int kPer = (kStage + kBulkConsumers - 1) / kBulkConsumers;
+        const int bs = a.bs, units = ne * bs;
+        T pv[kPer], px[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = t + j * kBulkConsumers;
+            if (k < units) {
+                const int e = div_bs(k, a.magic);
+                pv[j] = k < vavail ? sv[voff + k] : a.vals[vbase + k];
+                const int col = e < cavail ? sc[coff + e] : a.cols[e0 + e];
+                px[j] = __ldg(a.x + col * bs + (k - e * bs));
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = t + j * kBulkConsumers;
+            if (k < units) sv[voff + k] = mul_rn(pv[j], px[j]);
+        }
+    }
+}
+
+// Sums of one staged tile: thread t owns outputs (row, component) t, t+C, ...
+// and adds its row's staged products in entry order (eight loaded ahead of
+// the add chain), the reference's summation sequence.
+template<class T, int KIND, int BS>
+__device__ __forceinline__ void bulk_sums(const SpmvArgs<T>& a, const BulkHead* h, const T* sv, const int* sr, int t)
+{
+    const int bs = BS > 0 ? BS : a.bs;
+    const int r0 = h->r0, e0 = h->e0, outs = (h->r1 - r0) * bs;
+    const int voff = h->voff, roff = h->roff, ravail = h->ravail;
+    const std::size_t ybase = static_cast<std::size_t>(r0) * bs;
+    for (int o = t; o < outs; o += kBulkConsumers) {
+        const int rl = BS > 0 ? o / BS : div_bs(o, a.magic), c = o - rl * bs;
+        const int b0 = (rl < ravail ? sr[roff + rl] : a.rowptr[r0 + rl]) - e0;
+        const int b1 = (rl + 1 < ravail ? sr[roff + rl + 1] : a.rowptr[r0 + rl + 1]) - e0;
+        T acc = T(0);
+        if constexpr (KIND == 1) acc = mul_rn(a.diag[ybase + o], a.x[ybase + o]);
+        const T* p = sv + voff + c;
+        for (int e = b0; e < b1; e += 8) {
+            T q[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (e + i < b1) q[i] = p[(e + i) * bs];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (e + i < b1) acc = add_rn(acc, q[i]);
+        }
+        a.y[ybase + o] = acc;
+    }
+}
+
+template<class T, int KIND, int BS>
+__global__ void __launch_bounds__(kBulkThreads, kBulkCtasPerSm)
+    k_spmv_bulk(SpmvArgs<T> a, const int4* __restrict__ meta, int ntiles, std::size_t entries, std::size_t owned,
+                unsigned* status)
+{
+    using L = BulkLayout<T>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const std::uint32_t bars = smem_u32(smem);     // full[0..S), empty[0..S)
+    unsigned char* stages = smem + L::kBars;
+    const int bs = BS > 0 ? BS : a.bs;
+    const long long nb = gridDim.x;
+    const int t_begin = static_cast<int>(static_cast<long long>(ntiles) * blockIdx.x / nb);
+    const int t_end = static_cast<int>(static_cast<long long>(ntiles) * (blockIdx.x + 1) / nb);
+    const int count = t_end - t_begin;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kBulkStages; ++s) {
+            mbar_init(bars + 8 * s, 1);
+            mbar_init(bars + 8 * (kBulkStages + s), kBulkConsumers / 32);
+        }
+        fence_proxy_async_smem();
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == kBulkConsumers / 32) {
+        // ------------------------------------------------------------ producer
+        const std::uint64_t policy = l2_policy_evict_first();
+        bool ok = true;
+        int issued = 0;
+        for (int i0 = 0; i0 < count && ok; i0 += 32) {
+            int4 mine = make_int4(0, 0, 0, 0);
+            if (i0 + lane < count) mine = meta[t_begin + i0 + lane];
+            const int batch = min(32, count - i0);
+            for (int j = 0; j < batch; ++j) {
+                int4 m;
+                m.x = __shfl_sync(0xffffffffu, mine.x, j);
+                m.y = __shfl_sync(0xffffffffu, mine.y, j);
+                m.z = __shfl_sync(0xffffffffu, mine.z, j);
+                m.w = __shfl_sync(0xffffffffu, mine.w, j);
+                const int it = i0 + j, s = it % kBulkStages, use = it / kBulkStages;
+                int good = 1;
+                if (lane == 0) {
+                    const std::uint32_t full = bars + 8 * s, empty = bars + 8 * (kBulkStages + s);
+                    if (!mbar_wait_bounded(empty, (use & 1) ^ 1, kBulkSpin)) {
+                        atomicOr(status, kErrTimeout);
+                        good = 0;
+                    } else {
+                        unsigned char* st = stages + static_cast<std::size_t>(s) * L::kStageBytes;
+                        BulkHead* h = reinterpret_cast<BulkHead*>(st + L::kVals + L::kCols + L::kRows);
+                        const int units = (m.w - m.z) * bs, outs = (m.y - m.x) * bs;
+                        h->r0 = m.x;
+                        h->r1 = m.y;
+                        h->e0 = m.z;
+                        h->e1 = m.w;
+                        h->longtile = units > kStage || outs > kStage;
+                        std::uint32_t bytes = 0, bv = 0, bc = 0, br = 0;
+                        std::size_t lv = 0, lc = 0, lr = 0;
+                        if (!h->longtile) {
+                            bv = bulk_segment(static_cast<std::size_t>(m.z) * bs, static_cast<std::size_t>(m.w) * bs,
+                                              entries * bs, sizeof(T), lv, h->voff, h->vavail);
+                            bc = bulk_segment(m.z, m.w, entries, 4, lc, h->coff, h->cavail);
+                            br = bulk_segment(m.x, static_cast<std::size_t>(m.y) + 1, owned + 1, 4, lr, h->roff,
+                                              h->ravail);
+                            bytes = bv + bc + br;
+                        }
+                        if (bytes == 0) {
+                            mbar_arrive(full);
+                        } else {
+                            mbar_arrive_expect_tx(full, bytes);
+                            if (bv) bulk_load(smem_u32(st), reinterpret_cast<const unsigned char*>(a.vals) + lv, bv,
+                                              full, policy);
+                            if (bc) bulk_load(smem_u32(st + L::kVals),
+                                              reinterpret_cast<const unsigned char*>(a.cols) + lc, bc, full, policy);
+                            if (br) bulk_load(smem_u32(st + L::kVals + L::kCols),
+                                              reinterpret_cast<const unsigned char*>(a.rowptr) + lr, br, full, policy);
+                        }
+                        ++issued;
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, good, 0) != 0;
+                if (!ok) break;
+            }
+        }
+        // Leave only after every issued copy has landed.
+        if (lane == 0) {
+            for (int it = max(0, issued - kBulkStages); it < issued; ++it)
+                if (!mbar_wait_bounded(bars + 8 * (it % kBulkStages), (it / kBulkStages) & 1, kBulkSpin))
+                    atomicOr(status, kErrTimeout);
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    // All consumers of the CTA meet at one named barrier per tile (products
+    // visible before the sums); a wait that gives up is reported through that
+    // barrier, so they leave together.
+    const int t = threadIdx.x;
+    for (int it = 0; it < count; ++it) {
+        const int s = it % kBulkStages, use = it / kBulkStages;
+        const bool ready = mbar_wait_bounded(bars + 8 * s, use & 1, kBulkSpin);
+        unsigned char* st = stages + static_cast<std::size_t>(s) * L::kStageBytes;
+        T* sv = reinterpret_cast<T*>(st);
+        const int* sc = reinterpret_cast<const int*>(st + L::kVals);
+        const int* sr = reinterpret_cast<const int*>(st + L::kVals + L::kCols);
+        const BulkHead* h = reinterpret_cast<const BulkHead*>(st + L::kVals + L::kCols + L::kRows);
+        const int longtile = ready ? h->longtile : 0;
+        if (ready && longtile) {
+            const int r0 = h->r0, r1 = h->r1;
             for (int r = r0; r < r1; ++r) {
                 const int b0 = a.rowptr[r], b1 = a.rowptr[r + 1];
-                for (int c = threadIdx.x; c < bs; c += kThreads) {
+                for (int c = t; c < bs; c += kBulkConsumers) {
                     const std::size_t o = static_cast<std::size_t>(r) * bs + c;
                     T acc = KIND == 1 ? mul_rn(a.diag[o], a.x[o]) : T(0);
                     for (int e = b0; e < b1; ++e)
@@ -199,46 +427,43 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmv_stream(SpmvArgs<T> a, cons
                     a.y[o] = acc;
                 }
             }
-            if (next >= ntiles) break;
-            tile = next;
-            m = mn;
-            OWTK_SPMV_ISSUE(m);
-            continue;
+        } else if (ready) {
+            bulk_products<T, BS>(a, h, sv, sc, t);
         }
-        int ob[kPer], oe[kPer];
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const int o = threadIdx.x + j * kThreads;
-            if (o < outs) {
-                const int rl = div_bs(o, a.magic);
-                ob[j] = a.rowptr[r0 + rl] - e0;
-                oe[j] = a.rowptr[r0 + rl + 1] - e0;
-            }
+        if (bar_any(1, kBulkConsumers, !ready)) {
+            if (t == 0) atomicOr(status, kErrTimeout);
+            return;
         }
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const int k = threadIdx.x + j * kThreads;
-            if (k < units) prod[k] = mul_rn(pv[j], __ldg(a.x + pc[j]));
-        }
-        if (next < ntiles) OWTK_SPMV_ISSUE(mn);   // next tile's stream flies during the phases below
-        __syncthreads();
-        const std::size_t ybase = static_cast<std::size_t>(r0) * bs;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const int o = threadIdx.x + j * kThreads;
-            if (o < outs) {
-                const int c = o - div_bs(o, a.magic) * bs;
-                T acc = KIND == 1 ? mul_rn(a.diag[ybase + o], a.x[ybase + o]) : T(0);
-                for (int e = ob[j]; e < oe[j]; ++e) acc = add_rn(acc, prod[e * bs + c]);
-                a.y[ybase + o] = acc;
-            }
-        }
-        __syncthreads();
-        if (next >= ntiles) break;
-        tile = next;
-        m = mn;
+        if (!longtile) bulk_sums<T, KIND, BS>(a, h, sv, sr, t);
+        // The next fill of this stage is an async-proxy write after our
+        // generic-proxy product writes.
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bars + 8 * (kBulkStages + s));
     }
-#undef OWTK_SPMV_ISSUE
+}
+
+template<class T, int KIND, int BS>
+void launch_bulk(Context& c, const SpmvArgs<T>& a, const Matrix& m)
+{
+    const int smem = BulkLayout<T>::kTotal;
+    const unsigned grid = std::min<unsigned>(static_cast<unsigned>(m.plan.tiles),
+                                             static_cast<unsigned>(c.sm_count) * kBulkCtasPerSm);
+    OWTK_CUDA(cudaFuncSetAttribute(k_spmv_bulk<T, KIND, BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_spmv_bulk<T, KIND, BS><<<grid, kBulkThreads, smem, c.stream>>>(
+        a, m.plan.tile_meta.as<int4>(), m.plan.tiles, m.entries, m.owned, c.status.as<unsigned>());
+}
+
+template<class T, int KIND>
+void launch_bulk_bs(Context& c, const SpmvArgs<T>& a, const Matrix& m)
+{
+    switch (m.bs) {
+    case 1: launch_bulk<T, KIND, 1>(c, a, m); break;
+    case 2: launch_bulk<T, KIND, 2>(c, a, m); break;
+    case 3: launch_bulk<T, KIND, 3>(c, a, m); break;
+    case 4: launch_bulk<T, KIND, 4>(c, a, m); break;
+    default: launch_bulk<T, KIND, 0>(c, a, m); break;
+    }
 }
 
 // First diagonal entry of every row (block_csr.hpp:217-236).
@@ -287,11 +512,17 @@ template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
     a.bs = static_cast<int>(m.bs);
     a.magic = ((1ull << 32) + m.bs - 1) / m.bs;
     const unsigned grid = static_cast<unsigned>(m.plan.tiles);
-    const unsigned persistent = std::min<unsigned>(grid, static_cast<unsigned>(c.sm_count) * 4);
-    const int4* meta = m.plan.tile_meta.as<int4>();
-    if (m.kind == 0) k_spmv_stream<T, 0><<<persistent, kThreads, 0, c.stream>>>(a, meta, m.plan.tiles);
-    else if (m.kind == 1) k_spmv_stream<T, 1><<<persistent, kThreads, 0, c.stream>>>(a, meta, m.plan.tiles);
-    else k_spmv_tiles<T, 2><<<grid, kThreads, 0, c.stream>>>(a);
+    const auto aligned = [](const void* p) { return (reinterpret_cast<std::uintptr_t>(p) & 15u) == 0; };
+    if (m.kind != 2 && aligned(a.vals) && aligned(a.cols) && aligned(a.rowptr)) {
+        if (m.kind == 0) launch_bulk_bs<T, 0>(c, a, m);
+        else launch_bulk_bs<T, 1>(c, a, m);
+    } else if (m.kind == 0) {
+        k_spmv_tiles<T, 0><<<grid, kThreads, 0, c.stream>>>(a);
+    } else if (m.kind == 1) {
+        k_spmv_tiles<T, 1><<<grid, kThreads, 0, c.stream>>>(a);
+    } else {
+        k_spmv_tiles<T, 2><<<grid, kThreads, 0, c.stream>>>(a);
+    }
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }

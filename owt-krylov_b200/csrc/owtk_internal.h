@@ -6,7 +6,9 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <exception>
 #include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -22,6 +24,31 @@ struct Error {
 [[noreturn]] void fail(owtk_status code, const std::string& message);
 void cuda_check(cudaError_t e, const char* what);
 #define OWTK_CUDA(call) ::owtk::cuda_check((call), #call)
+void record_error(const std::string& message);   // text returned by owtk_last_error()
+
+inline void require(bool ok, const char* message)
+{
+    if (!ok) fail(OWTK_ERR_INVALID_ARGUMENT, message);
+}
+
+// Runs an entry point's body, mapping exceptions to status codes.
+template<class F>
+owtk_status guarded(F&& f)
+{
+    try {
+        f();
+        return OWTK_OK;
+    } catch (const Error& e) {
+        record_error(e.message);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        record_error("host allocation failed");
+        return OWTK_ERR_RUNTIME;
+    } catch (const std::exception& e) {
+        record_error(e.what());
+        return OWTK_ERR_RUNTIME;
+    }
+}
 
 // ---------------------------------------------------------------- device buffers
 // Owning device allocation (cudaMalloc) released on destruction.
@@ -177,7 +204,15 @@ struct Preconditioner {
     std::unique_ptr<Workspace> inner_ws;
     unsigned inner_iterations = 0;
     DeviceBuffer v32, z32;
+    // Learned preconditioner: the network (borrowed) and the preconditioner
+    // that takes a step whenever the network's step does not reduce the FP64
+    // residual (borrowed, may be null).
+    struct Gnn* net = nullptr;
+    Preconditioner* fallback = nullptr;
+    std::uint64_t learned_applications = 0, learned_fallbacks = 0;
+    DeviceBuffer check_work, alias_copy;
 };
+void learned_apply(Preconditioner& p, struct Vector& in, struct Vector& out);   // gnn.cu
 
 
 // ---------------------------------------------------------------- setup (setup.cpp)

@@ -15,7 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libowtk_b200.so")
 
 F64, F32, BF16 = 0, 1, 2
-PC_IDENTITY, PC_JACOBI, PC_SSOR, PC_SPLIT_SSOR, PC_ILU, PC_BLOCK_ILU, PC_MIXED = 0, 1, 2, 3, 4, 5, 6
+PC_IDENTITY, PC_JACOBI, PC_SSOR, PC_SPLIT_SSOR, PC_ILU, PC_BLOCK_ILU, PC_MIXED, PC_LEARNED = 0, 1, 2, 3, 4, 5, 6, 7
 FGMRES, BICGSTAB, PIPELINED_BICGSTAB, COMM_HIDING_BICGSTAB, IDRS = 0, 1, 2, 3, 4
 
 STATUS = {0: "ok", 1: "invalid_argument", 2: "zero_pivot", 3: "out_of_range", 4: "cuda_error",
@@ -57,6 +57,11 @@ class SolverResult(ctypes.Structure):
         d["status_name"] = SOLVER_STATUS[self.status] if 0 <= self.status < 5 else str(self.status)
         d["breakdown_name"] = BREAKDOWN[self.breakdown_reason] if 0 <= self.breakdown_reason < 10 else "?"
         return d
+
+
+class BatchSystem(ctypes.Structure):
+    _fields_ = [("owned", c_size_t), ("bs", c_size_t), ("rowptr", c_void_p), ("cols", c_void_p),
+                ("values", c_void_p)]
 
 
 _lib = None
@@ -119,6 +124,29 @@ def lib():
             "owtk_workspace_vector": (vp, [vp, sz]),
             "owtk_solve": (c_int, [c_int, vp, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
             "owtk_solve_host": (c_int, [c_int, vp, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
+            "owtk_batch_create": (c_int, [vp, sz, POINTER(BatchSystem), POINTER(vp)]),
+            "owtk_batch_destroy": (c_int, [vp]),
+            "owtk_batch_layout": (c_int, [vp, POINTER(sz), vp]),
+            "owtk_batch_config": (c_int, [vp, POINTER(ctypes.c_uint32), POINTER(ctypes.c_uint32)]),
+            "owtk_batch_set_config": (c_int, [vp, ctypes.c_uint32, sz, ctypes.c_uint32]),
+            "owtk_batch_autotune": (c_int, [vp, POINTER(SolverOptions), POINTER(ctypes.c_uint32),
+                                            POINTER(ctypes.c_uint32)]),
+            "owtk_batch_use_graph": (c_int, [vp, c_int]),
+            "owtk_batch_graph_counts": (c_int, [vp, u64p, u64p]),
+            "owtk_batch_solve": (c_int, [vp, vp, vp, POINTER(SolverOptions), POINTER(SolverResult)]),
+            "owtk_batch_solve_host": (c_int, [vp, vp, vp, POINTER(SolverOptions), POINTER(SolverResult)]),
+            "owtk_bf16_gemm_nt": (c_int, [vp, sz, sz, sz, vp, vp, vp]),
+            "owtk_learned_create": (c_int, [vp, c_uint64, POINTER(vp)]),
+            "owtk_learned_destroy": (c_int, [vp]),
+            "owtk_learned_update_matrix": (c_int, [vp, vp]),
+            "owtk_learned_parameter_count": (sz, []),
+            "owtk_learned_get_parameters": (c_int, [vp, vp, sz]),
+            "owtk_learned_set_parameters": (c_int, [vp, vp, sz]),
+            "owtk_learned_apply": (c_int, [vp, vp, vp]),
+            "owtk_learned_loss_grad": (c_int, [vp, vp, vp, POINTER(c_double), vp]),
+            "owtk_learned_adam_step": (c_int, [vp, c_double]),
+            "owtk_pc_create_learned": (c_int, [vp, vp, POINTER(vp)]),
+            "owtk_pc_learned_counts": (c_int, [vp, u64p, u64p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -430,6 +458,166 @@ def solve_host(kind: int, matrix: Matrix, pc: Preconditioner | None, rhs_ptr: in
     check(lib().owtk_solve_host(kind, matrix.h, pc.h if pc else None, c_void_p(rhs_ptr), c_void_p(x_ptr),
                                 ctypes.byref(o), workspace.h if workspace else None, ctypes.byref(r)))
     return r
+
+
+# ---------------------------------------------------------------- tensor cores
+def bf16_gemm_nt(ctx: Context, a_ptr: int, b_ptr: int, d_ptr: int, m: int, n: int, k: int):
+    """D (m x n FP32) = A (m x k BF16) * B (n x k BF16)^T on the tensor cores;
+    device pointers (e.g. torch tensors' data_ptr())."""
+    check(lib().owtk_bf16_gemm_nt(ctx.h, m, n, k, c_void_p(a_ptr), c_void_p(b_ptr), c_void_p(d_ptr)))
+
+
+# ---------------------------------------------------------------- learned preconditioner
+class Learned:
+    """The message-passing network on a matrix's graph (owtk_learned_* in
+    include/owtk.h): forward, loss/gradient, Adam, and its use as a
+    preconditioner with a fallback."""
+
+    def __init__(self, matrix: Matrix, seed: int = 0):
+        self.matrix = matrix
+        self.h = None
+        h = c_void_p()
+        check(lib().owtk_learned_create(matrix.h, seed, ctypes.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def parameter_count() -> int:
+        return int(lib().owtk_learned_parameter_count())
+
+    def update_matrix(self, matrix: Matrix):
+        check(lib().owtk_learned_update_matrix(self.h, matrix.h))
+        self.matrix = matrix
+
+    def parameters(self) -> np.ndarray:
+        out = np.empty(self.parameter_count(), dtype=np.float32)
+        check(lib().owtk_learned_get_parameters(self.h, _ptr(out), out.size))
+        return out
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().owtk_learned_set_parameters(self.h, _ptr(p), p.size))
+
+    def apply(self, x: Vector, y: Vector):
+        check(lib().owtk_learned_apply(self.h, x.h, y.h))
+
+    def loss_grad(self, r: Vector, e: Vector, want_grads: bool = False):
+        loss = c_double()
+        g = np.empty(self.parameter_count(), dtype=np.float32) if want_grads else None
+        check(lib().owtk_learned_loss_grad(self.h, r.h, e.h, ctypes.byref(loss), _ptr(g) if g is not None else None))
+        return (loss.value, g) if want_grads else loss.value
+
+    def adam_step(self, learning_rate: float):
+        check(lib().owtk_learned_adam_step(self.h, learning_rate))
+
+    def close(self):
+        if self.h is not None:
+            lib().owtk_learned_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LearnedPreconditioner(Preconditioner):
+    """owtk_pc_create_learned: the network judged by the FP64 residual, the
+    fallback (e.g. an ILU(0) Preconditioner) taking the steps it fails."""
+
+    def __init__(self, net: Learned, fallback: "Preconditioner | None" = None):
+        self.matrix = net.matrix
+        self.net = net
+        self.fallback = fallback
+        self.kind = PC_LEARNED
+        self.h = None
+        h = c_void_p()
+        check(lib().owtk_pc_create_learned(net.h, fallback.h if fallback else None, ctypes.byref(h)))
+        self.h = h
+
+    def counts(self):
+        a, f = c_uint64(), c_uint64()
+        check(lib().owtk_pc_learned_counts(self.h, ctypes.byref(a), ctypes.byref(f)))
+        return a.value, f.value
+
+
+# ---------------------------------------------------------------- batching
+class Batch:
+    """Many independent FP64 component-diagonal systems solved together by
+    BiCGSTAB + Jacobi in one persistent graph-captured launch
+    (owtk_batch_* in include/owtk.h).  `systems` holds objects with owned, bs,
+    rowptr, cols, vals (a BlockSystem) or (owned, bs, rowptr, cols, vals) tuples."""
+
+    MAX_BS = 32
+
+    def __init__(self, ctx: Context, systems):
+        self.ctx = ctx
+        self.h = None
+        keep, descs = [], []
+        for y in systems:
+            owned, bs, rp, ci, vals = ((y.owned, y.bs, y.rowptr, y.cols, y.vals) if hasattr(y, "owned") else y)
+            rp, ci = _u64(rp), _u64(ci)
+            vals = np.ascontiguousarray(vals, dtype=np.float64)
+            keep += [rp, ci, vals]
+            descs.append(BatchSystem(owned, bs, _ptr(rp), _ptr(ci), _ptr(vals)))
+        arr = (BatchSystem * len(descs))(*descs)
+        h = c_void_p()
+        check(lib().owtk_batch_create(ctx.h, len(descs), arr, ctypes.byref(h)))
+        self.h = h
+        self.count = len(descs)
+        self.unknowns, self.offsets = self.layout()
+
+    def layout(self):
+        n = c_size_t()
+        off = np.empty(self.count + 1, dtype=np.uint64)
+        check(lib().owtk_batch_layout(self.h, ctypes.byref(n), _ptr(off)))
+        return n.value, off.astype(np.int64)
+
+    def config(self):
+        bps = ctypes.c_uint32()
+        vpw = (ctypes.c_uint32 * (self.MAX_BS + 1))()
+        check(lib().owtk_batch_config(self.h, ctypes.byref(bps), vpw))
+        return bps.value, list(vpw)
+
+    def set_config(self, blocks_per_sm: int = 0, bs: int = 0, vertices_per_warp: int = 0):
+        check(lib().owtk_batch_set_config(self.h, blocks_per_sm, bs, vertices_per_warp))
+
+    def autotune(self, options: SolverOptions | None = None):
+        bps = ctypes.c_uint32()
+        vpw = (ctypes.c_uint32 * (self.MAX_BS + 1))()
+        check(lib().owtk_batch_autotune(self.h, ctypes.byref(options) if options else None, ctypes.byref(bps), vpw))
+        return bps.value, list(vpw)
+
+    def use_graph(self, enable: bool):
+        check(lib().owtk_batch_use_graph(self.h, int(enable)))
+
+    def graph_counts(self):
+        c, l = c_uint64(), c_uint64()
+        check(lib().owtk_batch_graph_counts(self.h, ctypes.byref(c), ctypes.byref(l)))
+        return c.value, l.value
+
+    def solve(self, rhs: Vector, x: Vector, options: SolverOptions | None = None) -> list:
+        o = options or default_options()
+        res = (SolverResult * self.count)()
+        check(lib().owtk_batch_solve(self.h, c_void_p(rhs.data_ptr), c_void_p(x.data_ptr), ctypes.byref(o), res))
+        return list(res)
+
+    def solve_host(self, rhs_ptr: int, x_ptr: int, options: SolverOptions | None = None) -> list:
+        o = options or default_options()
+        res = (SolverResult * self.count)()
+        check(lib().owtk_batch_solve_host(self.h, c_void_p(rhs_ptr), c_void_p(x_ptr), ctypes.byref(o), res))
+        return list(res)
+
+    def close(self):
+        if self.h is not None:
+            lib().owtk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------- host setup

@@ -153,6 +153,11 @@ def component_diagonal_system(xy, edges, bs, rng, order: str = "natural") -> Blo
     n = xy.shape[0]
     a_fwd, a_bwd, diag = _coefficients(n, edges, bs, rng)
     rhs = rng.uniform(-1.0, 1.0, size=n * bs)
+    return _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order)
+
+
+def _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order) -> BlockSystem:
+    n = xy.shape[0]
     meta = {"order": order}
     if order != "natural":
         from . import native
@@ -175,6 +180,57 @@ def component_diagonal_system(xy, edges, bs, rng, order: str = "natural") -> Blo
                        meta=meta)
 
 
+def angle_field(xy: np.ndarray, rng, modes: int = 6) -> np.ndarray:
+    """Smooth random angle field: pi * sum of `modes` low-frequency sine modes
+    with N(0, 1)/modes amplitudes, integer wave numbers in [-3, 3]."""
+    k = rng.integers(-3, 4, size=(modes, 2))
+    amp = rng.normal(0.0, 1.0, size=modes) / modes
+    phase = rng.uniform(0.0, 2.0 * np.pi, size=modes)
+    theta = np.zeros(xy.shape[0])
+    for (kx, ky), a, ph in zip(k, amp, phase):
+        theta += a * np.sin(2.0 * np.pi * (kx * xy[:, 0] + ky * xy[:, 1]) + ph)
+    return np.pi * theta
+
+
+def anisotropic_system(xy, edges, bs, rng, strength: float = 1e4, order: str = "rcm") -> BlockSystem:
+    """w_ij = 1 + strength (e_ij . d(x_ij))^2 per edge, with e_ij the unit edge
+    vector and d the unit direction rotated by the smooth angle field at the
+    edge midpoint; per component a skew s ~ U(-0.3, 0.3) (s_ji = -s_ij),
+    a_ij = -w (1 + s); diagonal 1.05 sum |a| + U(0, 0.1); rhs U(-1, 1)."""
+    n = xy.shape[0]
+    i, j = edges[:, 0], edges[:, 1]
+    mid = 0.5 * (xy[i] + xy[j])
+    theta = angle_field(mid, rng)
+    d = np.stack([np.cos(theta), np.sin(theta)], axis=1)
+    ev = xy[j] - xy[i]
+    ev /= np.linalg.norm(ev, axis=1, keepdims=True)
+    w = 1.0 + strength * np.einsum("ij,ij->i", ev, d) ** 2
+    s = rng.uniform(-0.3, 0.3, size=(edges.shape[0], bs))
+    a_fwd = -w[:, None] * (1.0 + s)
+    a_bwd = -w[:, None] * (1.0 - s)
+    absum = np.empty((n, bs))
+    for c in range(bs):
+        absum[:, c] = (np.bincount(i, weights=np.abs(a_fwd[:, c]), minlength=n)
+                       + np.bincount(j, weights=np.abs(a_bwd[:, c]), minlength=n))
+    diag = 1.05 * absum + rng.uniform(0.0, 0.1, size=(n, bs))
+    rhs = rng.uniform(-1.0, 1.0, size=n * bs)
+    return _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order)
+
+
+def config4(n_target: int = 8_000_000, seed: int = 4, bs: int = 3, draw: int = 0,
+            order: str = "rcm") -> BlockSystem:
+    """Poisson-disk points in the unit square, Delaunay, anisotropic
+    coefficients (draw `draw` of the coefficient stream), RCM-ordered, bs 3."""
+    def build():
+        xy, edges = disk_mesh(n_target, seed, domain="square")
+        rng = np.random.default_rng([seed, draw])
+        return anisotropic_system(xy, edges, bs, rng, order=order)
+
+    sysm = _cached(f"square-{n_target}-{seed}-{bs}-{draw}-{order}", build)
+    sysm.meta.update(config=f"poisson-square-{sysm.owned}-delaunay-anisotropic-{order}-bs{bs}", seed=seed, draw=draw)
+    return sysm
+
+
 def config0(seed: int = 0, side: int = 64, bs: int = 3) -> BlockSystem:
     """64x64 jittered triangulated lattice (4096 vertices), bs 3."""
     rng = np.random.default_rng(seed)
@@ -182,6 +238,32 @@ def config0(seed: int = 0, side: int = 64, bs: int = 3) -> BlockSystem:
     sysm = component_diagonal_system(xy, edges, bs, rng)
     sysm.meta.update(config="lattice-64x64-bs3", seed=seed)
     return sysm
+
+
+def batch_systems(count: int = 256, seed: int = 3, n_min: int = 5_000, n_max: int = 200_000,
+                  block_sizes=(1, 2, 3, 4)) -> list:
+    """The batching workload: `count` independent systems with vertex counts
+    log-uniform in [n_min, n_max] on jittered triangulated lattices of aspect
+    ratio U(1, 4), block sizes drawn from `block_sizes`, coefficients and
+    right-hand sides as config0.  System i draws from its own stream
+    (seed, i), so any subset regenerates identically."""
+    rng = np.random.default_rng(seed)
+    spec = []
+    for _ in range(count):
+        n = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        aspect = float(rng.uniform(1.0, 4.0))
+        bs = int(rng.choice(block_sizes))
+        spec.append((n, aspect, bs))
+    out = []
+    for i, (n, aspect, bs) in enumerate(spec):
+        ny = max(2, int(round(np.sqrt(n / aspect))))
+        nx = max(2, int(round(n / ny)))
+        srng = np.random.default_rng([seed, i])
+        xy, edges = lattice(nx, ny, 0.2, srng, aspect)
+        s = component_diagonal_system(xy, edges, bs, srng)
+        s.meta.update(index=i, aspect=aspect, config=f"batch-{count}-{seed}")
+        out.append(s)
+    return out
 
 
 def disk_mesh(n_target: int, seed: int, domain: str = "disk"):
@@ -215,6 +297,30 @@ def config1(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = 
     sysm = _cached(f"disk-{n_target}-{seed}-{bs}-{order}", build)
     sysm.meta.update(config=f"poisson-disk-{sysm.owned}-delaunay-{order}-bs{bs}", seed=seed)
     return sysm
+
+
+def config2(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm") -> BlockSystem:
+    """The config-1 disk mesh with dense bs x bs blocks (see dense_block_system)."""
+    def build():
+        xy, edges = disk_mesh(n_target, seed)
+        rng = np.random.default_rng([seed, 2])
+        return dense_block_system(xy, edges, bs, rng, order=order)
+
+    sysm = _cached(f"disk-dense-{n_target}-{seed}-{bs}-{order}", build)
+    sysm.kind = "dense"
+    sysm.meta.update(config=f"poisson-disk-{sysm.owned}-delaunay-{order}-dense{bs}x{bs}", seed=seed)
+    return sysm
+
+
+def anisotropic_draws(n_target: int, seed: int, draws, bs: int = 3, order: str = "rcm"):
+    """Coefficient draws of one anisotropic unit-square mesh (mesh and
+    ordering built once); yields (draw, BlockSystem)."""
+    xy, edges = disk_mesh(n_target, seed, domain="square")
+    for d in draws:
+        rng = np.random.default_rng([seed, d])
+        s = anisotropic_system(xy, edges, bs, rng, order=order)
+        s.meta.update(draw=d)
+        yield d, s
 
 
 def dense_block_system(xy, edges, bs: int, rng, order: str = "natural") -> BlockSystem:

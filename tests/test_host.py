@@ -111,3 +111,27 @@ def test_context_without_device_reports_no_device(native):
     with pytest.raises(native.OwtkError) as e:
         native.Context(0)
     assert e.value.kind in ("no_device", "cuda_error")
+
+
+def test_bindings_marshal_with_null_handles(native):
+    # Every binding of the batching, tensor-core and learned entry points
+    # converts its arguments and reaches the library, which rejects the null
+    # handle with a status (no GPU needed).
+    b = native.Batch.__new__(native.Batch)
+    b.h, b.count = None, 2
+    net = native.Learned.__new__(native.Learned)
+    net.h = None
+    ctx = native.Context.__new__(native.Context)
+    ctx.h = None
+    v = native.Vector.__new__(native.Vector)
+    v.h = None
+    calls = [b.layout, b.config, lambda: b.set_config(1, 3, 4), b.autotune, lambda: b.use_graph(True),
+             b.graph_counts, lambda: b.solve_host(0, 0), lambda: native.Batch(ctx, [(2, 1, [0, 1, 2], [0, 1], [1.0, 1.0])]),
+             net.parameters, lambda: net.set_parameters(np.zeros(native.Learned.parameter_count())),
+             lambda: net.loss_grad(v, v, want_grads=True), lambda: net.adam_step(1e-3), lambda: net.apply(v, v),
+             lambda: native.bf16_gemm_nt(ctx, 0, 0, 0, 128, 64, 64)]
+    for call in calls:
+        with pytest.raises(native.OwtkError):
+            call()
+    assert native.Learned.parameter_count() == 64 * 16 + 4 * 64 * 128 + 8 * 64
+    b.h = net.h = None

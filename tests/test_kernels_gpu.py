@@ -61,6 +61,48 @@ def test_spmv_bitwise(native, ctx, golden, name):
     assert_bitwise(y.download()[: n * bs], golden[f"{name}/split_spmv"], "split spmv")
 
 
+@pytest.mark.parametrize("side,bs", [(420, 3), (300, 2), (161, 5)])
+def test_spmv_bitwise_many_tiles_per_cta(native, ctx, restatement, side, bs):
+    # Thousands of 2048-value tiles: every persistent CTA streams several
+    # tiles through its shared-memory ring (wrap-around of the stages), and
+    # array lengths that are not whole 16-byte granules end in plain loads.
+    c = cases.lattice_case(side=side, bs=bs, seed=side)
+    n = c["owned"]
+    expect = restatement.bsr_spmv(n, bs, c["rowptr"], c["cols"], c["vals"], c["x"])
+    m = bsr(native, ctx, c)
+    x = dvec(native, ctx, c, c["x"])
+    y = dvec(native, ctx, c, fill=5.0)
+    m.apply(x, y)
+    assert_bitwise(y.download()[: n * bs], expect, "bsr spmv")
+    orp, oci, diag, off = cases.split_of(c)
+    expect = restatement.split_spmv(n, bs, orp, oci, diag, off, c["x"])
+    keep = []
+    sm, _, _ = split_matrix(native, ctx, c, keep)
+    sm.apply(x, y)
+    assert_bitwise(y.download()[: n * bs], expect, "split spmv")
+    # Borrowed coefficients that are 8-byte but not 16-byte aligned take the
+    # per-tile kernel; the result is the same.
+    d = device_array(native, ctx, diag)
+    o = device_array(native, ctx, np.concatenate([[0.0], off]))
+    shifted = native.Matrix(ctx, "split", n, 0, bs, orp, oci, diag_ptr=d.data_ptr, off_ptr=o.data_ptr + 8)
+    shifted.apply(x, y)
+    assert_bitwise(y.download()[: n * bs], expect, "split spmv, unaligned coefficients")
+    with pytest.raises(native.OwtkError):   # not even element-aligned
+        native.Matrix(ctx, "split", n, 0, bs, orp, oci, diag_ptr=d.data_ptr, off_ptr=o.data_ptr + 4)
+    # FP32 values through the same pipeline (4096-byte-smaller stages).
+    m32 = bsr(native, ctx, c, dtype=np.float32)
+    x32 = native.Vector(ctx, n, 0, bs, dtype=np.float32).upload(c["x"])
+    y32 = native.Vector(ctx, n, 0, bs, dtype=np.float32)
+    m32.apply(x32, y32)
+    got = y32.download().astype(np.float64)
+    ref = restatement.bsr_spmv(n, bs, c["rowptr"], c["cols"], c["vals"].astype(np.float32).astype(np.float64),
+                               c["x"].astype(np.float32).astype(np.float64))
+    bound = restatement.bsr_spmv(n, bs, c["rowptr"], c["cols"], np.abs(c["vals"]), np.abs(c["x"]))
+    deg = np.repeat(np.diff(c["rowptr"]), bs)
+    assert (np.abs(got - ref) <= (deg + 2) * np.finfo(np.float32).eps * bound + 1e-30).all()
+    ctx.synchronize()
+
+
 @pytest.mark.parametrize("name", list(cases.DENSE_CASES))
 def test_dense_spmv_bitwise(native, ctx, golden, name):
     c = cases.dense_case(**cases.DENSE_CASES[name])
