@@ -238,6 +238,17 @@ uint64_t owtk_workspace_allocation_epochs(owtk_workspace* ws);
 /* Workspace vector `index` (same slot order as the reference solver), or NULL. */
 owtk_vector* owtk_workspace_vector(owtk_workspace* ws, size_t index);
 
+/* solve_specwave_native (specwave_compat.hpp:99-249) for the legacy SpecWave
+ * solver IDs: 3, 4, 10, 22 communication-hiding BiCGSTAB + SSOR (4: residual
+ * replacement 50 when unset); 5, 8, 11 BiCGSTAB + SSOR; 7 GMRES + SSOR;
+ * 9, 13 BiCGSTAB + ILU(0); 12, 15 pipelined BiCGSTAB + SSOR; 14 IDR(s) + SSOR;
+ * 21 pipelined BiCGSTAB + ILU(0); SSOR with omega = options->relaxation.  ID 6
+ * (PETSc) returns the default result (invalid_input); the stationary and
+ * multigrid IDs are rejected with OWTK_ERR_INVALID_ARGUMENT. */
+owtk_status owtk_solve_specwave(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
+                                const owtk_solver_options* options, owtk_workspace* workspace,
+                                owtk_solver_result* result);
+
 /* Device-resident solve: rhs and x are device vectors with the matrix layout.
  * pc may be NULL (identity); workspace may be NULL (a temporary is used). */
 owtk_status owtk_solve(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,

@@ -1189,6 +1189,53 @@ owtk_status owtk_solve(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditione
     });
 }
 
+// solve_specwave_native (specwave_compat.hpp:99-249): the legacy SpecWave
+// solver IDs mapped onto the device solvers and preconditioners exactly as the
+// reference maps them.  IDs 10 and 22 select the reference's mixed-precision
+// and compensated serial reductions; on the device every reduction is the
+// two-stage FP64 reduction.  Stationary and multigrid IDs are not on this path.
+owtk_status owtk_solve_specwave(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
+                                const owtk_solver_options* options, owtk_workspace* workspace,
+                                owtk_solver_result* result)
+{
+    return guarded([&] {
+        require(m != nullptr && rhs != nullptr && x != nullptr && options != nullptr && result != nullptr,
+                "null handle");
+        owtk_solver_options o = *options;
+        owtk_solver_kind kind = OWTK_SOLVER_BICGSTAB;
+        owtk_pc_kind pck = OWTK_PC_SSOR;
+        double parameter = o.relaxation;
+        switch (solver_id) {
+        case 3: case 10: case 22: kind = OWTK_SOLVER_COMM_HIDING_BICGSTAB; break;
+        case 4:
+            kind = OWTK_SOLVER_COMM_HIDING_BICGSTAB;
+            if (o.residual_replacement_interval == 0) o.residual_replacement_interval = 50;
+            break;
+        case 5: case 8: case 11: kind = OWTK_SOLVER_BICGSTAB; break;
+        case 7: kind = OWTK_SOLVER_FGMRES; break;
+        case 9: case 13: kind = OWTK_SOLVER_BICGSTAB; pck = OWTK_PC_ILU; parameter = 0; break;
+        case 12: case 15: kind = OWTK_SOLVER_PIPELINED_BICGSTAB; break;
+        case 14: kind = OWTK_SOLVER_IDRS; break;
+        case 21: kind = OWTK_SOLVER_PIPELINED_BICGSTAB; pck = OWTK_PC_ILU; parameter = 0; break;
+        case 6: {   // the PETSc adapter: a default SolverResult
+            owtk_solver_result r{};
+            r.status = 4;
+            const double nan = std::numeric_limits<double>::quiet_NaN();
+            r.initial_residual_norm = r.recursive_residual_norm = r.true_residual_norm = r.relative_residual_norm = nan;
+            *result = r;
+            return;
+        }
+        default:
+            fail(OWTK_ERR_INVALID_ARGUMENT, "SpecWave solver id is not on the device path (stationary or multigrid)");
+        }
+        auto pc = make_pc(m, pck, parameter, OWTK_F64);
+        owtk_workspace local;
+        local.ctx = m->ctx;
+        Workspace& ws = workspace ? static_cast<Workspace&>(*workspace) : static_cast<Workspace&>(local);
+        solve(kind, *m, pc.get(), *rhs, *x, o, ws, *result);
+    });
+}
+
 owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,
                             const void* host_rhs, void* host_x, const owtk_solver_options* options,
                             owtk_workspace* workspace, owtk_solver_result* result)

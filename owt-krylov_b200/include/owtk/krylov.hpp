@@ -711,7 +711,10 @@ JacobiPreconditioner(const SplitBlockCsrMatrixView<T, Index>&) -> JacobiPrecondi
 template<std::floating_point T, std::integral Index = std::size_t>
 class LocalSsorPreconditioner : public detail::DevicePc {
 public:
-    explicit LocalSsorPreconditioner(BlockCsrMatrix<T, Index>& matrix, T omega = T(1)) : matrix_(&matrix)
+    // The reference keeps a pointer to the (const) matrix; update_values()
+    // re-reads its host values.
+    explicit LocalSsorPreconditioner(const BlockCsrMatrix<T, Index>& matrix, T omega = T(1))
+        : matrix_(const_cast<BlockCsrMatrix<T, Index>*>(&matrix))
     {
         create(matrix.device(), OWTK_PC_SSOR, static_cast<double>(omega));
     }
@@ -926,6 +929,69 @@ template<std::floating_point T, class Operator, class Preconditioner = IdentityP
 {
     return detail::device_solve<T>(OWTK_SOLVER_IDRS, op, rhs, solution, options, preconditioner,
                                    static_cast<SolverWorkspace<T>*>(nullptr));
+}
+
+// ------------------------------------------------------------------ SpecWave compatibility
+// Legacy SpecWave solver IDs (specwave_compat.hpp:24-48), exact numeric labels.
+enum class SpecWaveSolver : int {
+    jacobi = 0, gauss_seidel = 1, chebyshev_srj = 2, pipelined_stable = 3, pipelined_residual_replacement = 4,
+    bicgstab_ssor = 5, petsc = 6, gmres_ssor = 7, bicgstab_pure_ssor = 8, bicgstab_ilu0 = 9,
+    pipelined_mixed_precision = 10, bicgstab_full_system = 11, pipelined_full_system = 12,
+    bicgstab_full_system_ilu0 = 13, idrs = 14, communication_hiding_bicgstab = 15, asynchronous_gauss_seidel = 16,
+    multigrid_v_jacobi = 17, multigrid_v_red_black = 18, multigrid_w = 19, full_multigrid = 20,
+    pipelined_bicgstab_ilu0 = 21, async_pipe_stable = 22,
+};
+
+// solve_specwave_native (specwave_compat.hpp:99-249) with the device solvers:
+// the same ID -> solver / preconditioner selection.  IDs 10 and 22 choose the
+// mixed-precision and compensated serial reductions in the reference; device
+// reductions are two-stage FP64 for every ID.  The stationary and multigrid
+// IDs are not on the device path and throw std::invalid_argument; PETSc (6)
+// returns a default SolverResult as the reference does.
+template<std::floating_point T, std::integral Index, class Operator, class Halo,
+         class Reduction = SerialReduction<T>>
+[[nodiscard]] SolverResult<T> solve_specwave_native(SpecWaveSolver solver, const BlockCsrMatrix<T, Index>& matrix,
+                                                    Operator& linear_operator, Halo&, const BlockVector<T>& rhs,
+                                                    BlockVector<T>& solution, SolverOptions<T> options = {},
+                                                    Reduction reduction = {})
+{
+    using S = SpecWaveSolver;
+    switch (solver) {
+    case S::pipelined_stable:
+    case S::pipelined_mixed_precision:
+    case S::async_pipe_stable:
+        return communication_hiding_bicgstab(linear_operator, rhs, solution, options,
+                                             LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::pipelined_residual_replacement:
+        if (options.residual_replacement_interval == 0) options.residual_replacement_interval = 50;
+        return communication_hiding_bicgstab(linear_operator, rhs, solution, options,
+                                             LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::bicgstab_ssor:
+    case S::bicgstab_pure_ssor:
+    case S::bicgstab_full_system:
+        return bicgstab(linear_operator, rhs, solution, options,
+                        LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::gmres_ssor:
+        return gmres(linear_operator, rhs, solution, options,
+                     LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::bicgstab_ilu0:
+    case S::bicgstab_full_system_ilu0:
+        return bicgstab(linear_operator, rhs, solution, options, Ilu0Preconditioner<T, Index>(matrix), reduction);
+    case S::pipelined_full_system:
+    case S::communication_hiding_bicgstab:
+        return pipelined_bicgstab(linear_operator, rhs, solution, options,
+                                  LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::idrs:
+        return idrs(linear_operator, rhs, solution, options,
+                    LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::pipelined_bicgstab_ilu0:
+        return pipelined_bicgstab(linear_operator, rhs, solution, options, Ilu0Preconditioner<T, Index>(matrix),
+                                  reduction);
+    case S::petsc:
+        return {};
+    default:
+        throw std::invalid_argument("SpecWave solver is not on the device path (stationary or multigrid)");
+    }
 }
 
 // ------------------------------------------------------------------ orderings

@@ -136,6 +136,7 @@ def lib():
             "owtk_batch_solve": (c_int, [vp, vp, vp, POINTER(SolverOptions), POINTER(SolverResult)]),
             "owtk_batch_solve_host": (c_int, [vp, vp, vp, POINTER(SolverOptions), POINTER(SolverResult)]),
             "owtk_bf16_gemm_nt": (c_int, [vp, sz, sz, sz, vp, vp, vp]),
+            "owtk_solve_specwave": (c_int, [c_int, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
             "owtk_learned_create": (c_int, [vp, c_uint64, POINTER(vp)]),
             "owtk_learned_destroy": (c_int, [vp]),
             "owtk_learned_update_matrix": (c_int, [vp, vp]),
@@ -448,6 +449,16 @@ def solve(kind: int, matrix: Matrix, pc: Preconditioner | None, rhs: Vector, x: 
     r = SolverResult()
     check(lib().owtk_solve(kind, matrix.h, pc.h if pc else None, rhs.h, x.h, ctypes.byref(o),
                            workspace.h if workspace else None, ctypes.byref(r)))
+    return r
+
+
+def solve_specwave(solver_id: int, matrix: Matrix, rhs: Vector, x: Vector, options: SolverOptions | None = None,
+                   workspace: Workspace | None = None) -> SolverResult:
+    """solve_specwave_native: a legacy SpecWave solver id (owtk_solve_specwave)."""
+    o = options or default_options()
+    r = SolverResult()
+    check(lib().owtk_solve_specwave(solver_id, matrix.h, rhs.h, x.h, ctypes.byref(o),
+                                    workspace.h if workspace else None, ctypes.byref(r)))
     return r
 
 

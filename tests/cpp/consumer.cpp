@@ -107,6 +107,20 @@ int main(int argc, char** argv)
     ssor.apply(rhs, z);
     write(dir + "/split_ssor.f64", std::vector<double>(z.owned().begin(), z.owned().end()));
 
+    // The SpecWave dispatcher with the same operator (legacy id 9).
+    NoHaloExchange halo;
+    BlockVector<double> x4 = rhs.clone_layout();
+    const auto r4 = solve_specwave_native(SpecWaveSolver::bicgstab_ilu0, A, op, halo, rhs, x4, options);
+    report(results, "specwave_bicgstab_ilu0", r4);
+    write(dir + "/x_specwave.f64", std::vector<double>(x4.owned().begin(), x4.owned().end()));
+    try {
+        BlockVector<double> x5 = rhs.clone_layout();
+        (void)solve_specwave_native(SpecWaveSolver::multigrid_w, A, op, halo, rhs, x5, options);
+        results << "specwave_multigrid accepted\n";
+    } catch (const std::invalid_argument&) {
+        results << "specwave_multigrid invalid_argument\n";
+    }
+
     const auto order = reverse_cuthill_mckee_order(A);
     write(dir + "/rcm.u64", order);
     results << "epochs " << workspace.allocation_epochs() << '\n';

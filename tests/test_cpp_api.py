@@ -60,6 +60,7 @@ def test_consumer_matches_oracle(native, restatement, tmp_path):
     for key, solver, pck, opts, xfile in [
         ("gmres_ilu0", "gmres", "ilu", {}, "x_gmres.f64"),
         ("bicgstab_jacobi", "bicgstab", "jacobi", {"convergence_check_interval": 1}, "x_bicgstab.f64"),
+        ("specwave_bicgstab_ilu0", "bicgstab", "ilu", {}, "x_specwave.f64"),
     ]:
         pc = restatement.make_pc(pck, mat, 0.0, ilu if pck == "ilu" else None)
         r, xr = restatement.solve(solver, mat, pc, oracle.default_options(**opts), rhs, np.zeros(n * bs))
@@ -77,3 +78,4 @@ def test_consumer_matches_oracle(native, restatement, tmp_path):
     assert res["epochs"] == ["2"]          # GMRES sized the workspace; BiCGSTAB reused it
     assert res["ilu_updates"] == ["1"]
     assert res["layout_error"] == ["invalid_argument"]
+    assert res["specwave_multigrid"] == ["invalid_argument"]

@@ -177,3 +177,45 @@ def test_float32_solve(native, ctx, problems):
     r = native.solve(native.FGMRES, m, pc, b, x, native.default_options(relative_tolerance=1e-5))
     assert r.status == 0
     assert r.true_residual_norm <= 1e-5 * np.linalg.norm(rhs) * 1.01
+
+
+SPECWAVE = {3: ("COMM_HIDING_BICGSTAB", "SSOR"), 4: ("COMM_HIDING_BICGSTAB", "SSOR"),
+            5: ("BICGSTAB", "SSOR"), 7: ("FGMRES", "SSOR"), 8: ("BICGSTAB", "SSOR"), 9: ("BICGSTAB", "ILU"),
+            10: ("COMM_HIDING_BICGSTAB", "SSOR"), 11: ("BICGSTAB", "SSOR"), 12: ("PIPELINED_BICGSTAB", "SSOR"),
+            13: ("BICGSTAB", "ILU"), 14: ("IDRS", "SSOR"), 15: ("PIPELINED_BICGSTAB", "SSOR"),
+            21: ("PIPELINED_BICGSTAB", "ILU"), 22: ("COMM_HIDING_BICGSTAB", "SSOR")}
+
+
+@pytest.mark.parametrize("solver_id", sorted(SPECWAVE))
+def test_specwave_dispatch_matches_direct_calls(native, ctx, solver_id):
+    # specwave_compat.hpp:99-249: each legacy id is the named solver with the
+    # named preconditioner (SSOR omega = options.relaxation, ILU(0)).
+    c = cases.lattice_case(side=20, bs=3, seed=21)
+    n, bs = c["owned"], c["bs"]
+    m = native.Matrix(ctx, "bsr", n, 0, bs, c["rowptr"], c["cols"], c["vals"])
+    b = native.Vector(ctx, n, 0, bs).upload(c["rhs"][: n * bs])
+    opts = native.default_options(relaxation=1.2, residual_replacement_interval=0 if solver_id == 4 else 50)
+    x1, x2 = native.Vector(ctx, n, 0, bs), native.Vector(ctx, n, 0, bs)
+    r1 = native.solve_specwave(solver_id, m, b, x1, opts)
+    kind, pck = SPECWAVE[solver_id]
+    pc = native.Preconditioner(m, getattr(native, "PC_" + pck), 1.2 if pck == "SSOR" else 0)
+    direct = native.default_options(relaxation=1.2, residual_replacement_interval=50)
+    r2 = native.solve(getattr(native, kind), m, pc, b, x2, direct)
+    d1, d2 = r1.as_dict(), r2.as_dict()
+    d1.pop("solve_seconds", None)
+    d2.pop("solve_seconds", None)
+    assert d1 == d2
+    assert np.array_equal(x1.download().view(np.uint64), x2.download().view(np.uint64))
+
+
+def test_specwave_petsc_and_rejected_ids(native, ctx):
+    c = cases.lattice_case(side=8, bs=3, seed=21)
+    n, bs = c["owned"], c["bs"]
+    m = native.Matrix(ctx, "bsr", n, 0, bs, c["rowptr"], c["cols"], c["vals"])
+    b = native.Vector(ctx, n, 0, bs).upload(c["rhs"][: n * bs])
+    x = native.Vector(ctx, n, 0, bs)
+    r = native.solve_specwave(6, m, b, x)
+    assert r.status == 4 and np.isnan(r.true_residual_norm)      # default SolverResult
+    for sid in (0, 1, 2, 16, 17, 18, 19, 20, 23, -1):
+        with pytest.raises(native.OwtkError):
+            native.solve_specwave(sid, m, b, x)
