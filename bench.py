@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--bs", default="3", help="block sizes of the kernel sweep, comma separated")
     p.add_argument("--orders", default="rcm", help="vertex orders of the kernel sweep: rcm,hilbert")
     p.add_argument("--only", default="", help="kernel sweep: comma-separated subset of "
-                   "spmv,split,spmv32,ilu,ssor,dot,norm,axpy")
+                   "spmv,split,spmv32,ilu,ssor,dot,norm,axpy,gnn")
     p.add_argument("--reps", type=int, default=20, help="kernel sweep: timed launches per kernel")
     p.add_argument("--form", choices=["plain", "mixed", "batching", "learned"], default="plain",
                    help="plain: the FP64 GMRES(30)+ILU(0) headline; mixed / batching / learned: the three "
@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--systems", type=int, default=256, help="batching: number of systems")
     p.add_argument("--draws", type=int, default=32, help="learned: coefficient draws of the training mesh")
     p.add_argument("--train-vertices", type=int, default=200_000, help="learned: training mesh size")
-    p.add_argument("--epochs", type=int, default=4, help="learned: passes over the training pairs")
+    p.add_argument("--epochs", type=int, default=10, help="learned: passes over the training pairs")
     return p.parse_args()
 
 
@@ -354,7 +354,8 @@ def run_kernels(args):
     from owtk_b200 import native, problems
 
     peak, peak_kind = measured_peaks()
-    only = set(filter(None, args.only.split(","))) or {"spmv", "split", "spmv32", "ilu", "ssor", "dot", "norm", "axpy"}
+    only = set(filter(None, args.only.split(","))) or {"spmv", "split", "spmv32", "ilu", "ssor", "dot", "norm", "axpy",
+                                                        "gnn"}
     t = time.time()
     xy, edges = problems.disk_mesh(args.vertices, args.seed)
     gen_s = time.time() - t
@@ -424,6 +425,21 @@ def run_kernels(args):
                      note="one-pass scaled norm, result read on the host")
             if "axpy" in only:
                 emit("axpy", timed(lambda: native.axpy(0.5, x, y), args.reps), kernel_bytes("axpy", n, bs, nnz))
+            if "gnn" in only and bs <= 8:
+                # One application of the learned preconditioner (prepare, two
+                # norms, encoder, four fused tensor-core layers, decoder).
+                # Algorithmic bytes per vertex: FP64 r read three times, FP32
+                # 1/d and q, BF16 features (128 B) written by the encoder, read
+                # and written by each layer with its neighbour list (column +
+                # weight per entry), read by the decoder; FP64 output.
+                net = native.Learned(m, seed=1)
+                deg = (nnz - n) / n
+                per_vertex = (3 * bs * 8 + 2 * bs * 4 + bs * 4 + 128 + 4 * (2 * 128 + 4 + deg * 8) + 128 + bs * 4
+                              + bs * 8)
+                flops = 4 * 2 * 2 * 64 * 64 * n
+                us = timed(lambda: net.apply(x, y), max(2, args.reps // 2))
+                emit("gnn", us, per_vertex * n, tensor_tflops=round(flops / (us * 1e-6) / 1e12, 2),
+                     note="one learned-preconditioner application; HBM-bound (65 kFLOP vs ~1.6 kB per vertex)")
             ctx.synchronize()
     return 0
 
@@ -628,7 +644,7 @@ def run_learned(args):
     m0 = native.Matrix(ctx, "bsr", train[0].owned, 0, 3, train[0].rowptr, train[0].cols, train[0].vals)
     net = native.Learned(m0, seed=1)
     t = time.time()
-    hist = learned.train(ctx, net, train, epochs=args.epochs, learning_rate=1e-3, pairs_per_system=4)
+    hist = learned.train(ctx, net, train, epochs=args.epochs, learning_rate=1e-3, pairs_per_system=6)
     train_s = time.time() - t
     weights = net.parameters()
     # The large system.

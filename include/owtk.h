@@ -354,12 +354,15 @@ owtk_status owtk_learned_get_parameters(owtk_learned* net, float* host, size_t c
 owtk_status owtk_learned_set_parameters(owtk_learned* net, const float* host, size_t count);
 /* out = M(in), FP64 vectors of the matrix layout. */
 owtk_status owtk_learned_apply(owtk_learned* net, owtk_vector* in, owtk_vector* out);
-/* Forward + backward of one training pair: loss ||M(r) - e||^2 / ||e||^2 and
+/* Forward + backward of one training pair: the loss (weights below) and
  * its gradient, kept on the device for owtk_learned_adam_step (and copied
  * to host_grads when it is not NULL). */
 owtk_status owtk_learned_loss_grad(owtk_learned* net, owtk_vector* r, owtk_vector* e, double* loss,
                                    float* host_grads);
 owtk_status owtk_learned_adam_step(owtk_learned* net, double learning_rate);
+/* Loss = error_weight ||M(r) - e||^2 / ||e||^2
+ *      + residual_weight ||r - A M(r)||^2 / ||r||^2   (default 0.1 and 1). */
+owtk_status owtk_learned_set_loss_weights(owtk_learned* net, double error_weight, double residual_weight);
 /* The network as a preconditioner of its matrix: each application z = M(v)
  * is judged by the FP64 residual ||v - A z||; when that does not fall below
  * ||v|| the fallback (e.g. ILU(0), may be NULL) computes z instead.  Both

@@ -149,6 +149,7 @@ struct GraphArgs {
     const int* tr_ptr;       // transposed: the v with u in N(v), for vertex u
     const int* tr_col;
     const float* tr_w;       // w_vu of that edge
+    const int* tr_edge;      // index of that edge in the forward (nb) order
     const float* dinv;       // 1 / diagonal, n * bs
 };
 
@@ -273,33 +274,66 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++iter) {
         const int row0 = t * kTile;
         // ---- gather [h | m]
+        // Lane L of the warp holds the neighbour range of the warp's row L;
+        // 8-lane groups take one row per step (lane `chunk` owns features
+        // 8*chunk..8*chunk+7), load the row's first 8 neighbour indices and
+        // weights cooperatively (one lane each) and broadcast them; the next
+        // step's index loads are issued before this step's feature gathers.
+        const int wrow0 = row0 + 32 * warp;
+        int p0 = 0, p1 = 0;
+        if (wrow0 + lane < g.n) {
+            p0 = g.nb_ptr[wrow0 + lane];
+            p1 = g.nb_ptr[wrow0 + lane + 1];
+        }
+        auto load_idx = [&](int it, int& col, float& w, int& e0, int& e1) {
+            const int src = 4 * it + grp;
+            e0 = __shfl_sync(0xffffffffu, p0, src);
+            e1 = __shfl_sync(0xffffffffu, p1, src);
+            col = 0;
+            w = 0.0f;
+            if (e0 + chunk < e1) {
+                col = g.nb_col[e0 + chunk];
+                w = g.nb_w[e0 + chunk];
+            }
+        };
+        int ncol, ne0, ne1;
+        float nw;
+        load_idx(0, ncol, nw, ne0, ne1);
         for (int it = 0; it < 8; ++it) {
             const int r = 32 * warp + 4 * it + grp, v = row0 + r;
+            const int col = ncol, e0 = ne0, e1 = ne1;
+            const float wgt = nw;
+            if (it + 1 < 8) load_idx(it + 1, ncol, nw, ne0, ne1);
             uint4 hv = make_uint4(0, 0, 0, 0), mv = make_uint4(0, 0, 0, 0);
+            const int deg = e1 - e0;
+            uint4 nv[8];
+            float ws[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int u = __shfl_sync(0xffffffffu, col, (lane & ~7) + q);
+                ws[q] = __shfl_sync(0xffffffffu, wgt, (lane & ~7) + q);
+                nv[q] = make_uint4(0, 0, 0, 0);
+                if (q < deg) nv[q] = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8);
+            }
             if (v < g.n) {
                 hv = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(v) * kH + chunk * 8);
                 float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                const int e0 = g.nb_ptr[v], e1 = g.nb_ptr[v + 1];
-                for (int e = e0; e < e1; e += 4) {
-                    uint4 nv[4];
-                    float nw[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        nw[q] = 0.0f;
-                        nv[q] = make_uint4(0, 0, 0, 0);
-                        if (e + q < e1) {
-                            const int u = g.nb_col[e + q];
-                            nw[q] = g.nb_w[e + q];
-                            nv[q] = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8);
-                        }
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < 8; ++q) {
+                    if (q < deg) {
                         float f[8];
                         bf16x8_to_f32(nv[q], f);
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) acc[i] = fmaf(nw[q], f[i], acc[i]);
+                        for (int i = 0; i < 8; ++i) acc[i] = fmaf(ws[q], f[i], acc[i]);
                     }
+                }
+                for (int e = e0 + 8; e < e1; ++e) {   // rows with more than 8 neighbours
+                    const int u = g.nb_col[e];
+                    const float we = g.nb_w[e];
+                    float f[8];
+                    bf16x8_to_f32(*reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8), f);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[i] = fmaf(we, f[i], acc[i]);
                 }
                 mv = f32_to_bf16x8(acc);
                 if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
@@ -362,40 +396,64 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
 }
 
 // ---------------------------------------------------------------- backward kernels
-// Loss ||out - e||^2 / ||e||^2 (partials per block, combined in block order by
-// the last block) and dz = s * 2 (out - e) / ||e||^2.
+// Loss  we ||out - e||^2 / ||e||^2 + wr ||r - A out||^2 / ||r||^2  (partials
+// per block, combined in block order by the last block) and
+// dz = s * (2 we (out - e) / ||e||^2 - 2 wr A^T (r - A out) / ||r||^2), where
+// res = r - A out and g = A^T res are precomputed.
 __global__ void __launch_bounds__(256) k_gnn_out_grad(long long count, const float* __restrict__ out,
-                                                      const double* __restrict__ e, const double* enorm,
-                                                      const double* rnorm, double scale_n, float* __restrict__ dz,
-                                                      double* partials, unsigned* ticket, double* loss)
+                                                      const double* __restrict__ e, const float* __restrict__ res,
+                                                      const float* __restrict__ g, const double* enorm,
+                                                      const double* norms, double scale_n, double we, double wr,
+                                                      float* __restrict__ dz, double* partials, unsigned* ticket,
+                                                      double* loss)
 {
-    const double ee = (*enorm) * (*enorm);
-    const double s = rnorm[2] / scale_n;   // rms of the Jacobi step
-    const float g = ee > 0.0 ? static_cast<float>(2.0 * s / ee) : 0.0f;
-    double acc = 0.0;
+    const double ee = (*enorm) * (*enorm), rr = norms[0] * norms[0];
+    const double s = norms[2] / scale_n;   // rms of the Jacobi step
+    const float ge = ee > 0.0 ? static_cast<float>(2.0 * we * s / ee) : 0.0f;
+    const float gr = rr > 0.0 ? static_cast<float>(2.0 * wr * s / rr) : 0.0f;
+    double acc_e = 0.0, acc_r = 0.0;
     for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
         const double d = static_cast<double>(out[i]) - e[i];
-        acc += d * d;
-        dz[i] = g * static_cast<float>(d);
+        acc_e += d * d;
+        acc_r += static_cast<double>(res[i]) * res[i];
+        dz[i] = ge * static_cast<float>(d) - gr * g[i];
     }
-    acc = warp_sum(acc);
-    __shared__ double red[8];
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    acc_e = warp_sum(acc_e);
+    acc_r = warp_sum(acc_r);
+    __shared__ double red[2][8];
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = acc_e;
+        red[1][threadIdx.x >> 5] = acc_r;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double b = 0.0;
-        for (int w = 0; w < 8; ++w) b += red[w];
-        partials[blockIdx.x] = b;
+        double be = 0.0, br = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            be += red[0][w];
+            br += red[1][w];
+        }
+        partials[2 * blockIdx.x] = be;
+        partials[2 * blockIdx.x + 1] = br;
         __threadfence();
         if (atomicAdd(ticket, 1u) == gridDim.x - 1) {
             __threadfence();
-            double t = 0.0;
-            for (unsigned k = 0; k < gridDim.x; ++k) t += __ldcg(partials + k);
-            *loss = ee > 0.0 ? t / ee : 0.0;
+            double te = 0.0, tr = 0.0;
+            for (unsigned k = 0; k < gridDim.x; ++k) {
+                te += __ldcg(partials + 2 * k);
+                tr += __ldcg(partials + 2 * k + 1);
+            }
+            *loss = (ee > 0.0 ? we * te / ee : 0.0) + (rr > 0.0 ? wr * tr / rr : 0.0);
             *ticket = 0;
         }
     }
+}
+
+__global__ void k_gnn_residual(long long count, const double* __restrict__ r, const float* __restrict__ ax,
+                               float* __restrict__ res)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) res[i] = static_cast<float>(r[i] - static_cast<double>(ax[i]));
 }
 
 // dh4 = dz Wd (FP32 rows of 64).
@@ -694,21 +752,56 @@ __global__ void k_gnn_pack(const float* __restrict__ wl, bf16* __restrict__ wl16
 }
 
 // Matrix graph: weights w_vu = -mean_c a_vu,c / d_v,c of the off-diagonal
-// entries and 1 / diagonal.
+// entries, 1 / diagonal, and FP32 copies of the coefficients (for A x and
+// A^T x in the residual term of the training loss).
 __global__ void k_gnn_graph(int n, int bs, const int* __restrict__ nb_ptr, const int* __restrict__ nb_entry,
                             const double* __restrict__ vals, const double* __restrict__ diag, float* __restrict__ nb_w,
-                            float* __restrict__ dinv)
+                            float* __restrict__ dinv, float* __restrict__ nb_a, float* __restrict__ diag_f)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
-    for (int c = 0; c < bs; ++c)
-        dinv[static_cast<long long>(v) * bs + c] = static_cast<float>(1.0 / diag[static_cast<long long>(v) * bs + c]);
+    for (int c = 0; c < bs; ++c) {
+        const double d = diag[static_cast<long long>(v) * bs + c];
+        dinv[static_cast<long long>(v) * bs + c] = static_cast<float>(1.0 / d);
+        diag_f[static_cast<long long>(v) * bs + c] = static_cast<float>(d);
+    }
     for (int k = nb_ptr[v]; k < nb_ptr[v + 1]; ++k) {
         const long long e = nb_entry[k];
         double acc = 0.0;
-        for (int c = 0; c < bs; ++c) acc += vals[e * bs + c] / diag[static_cast<long long>(v) * bs + c];
+        for (int c = 0; c < bs; ++c) {
+            const double a = vals[e * bs + c];
+            acc += a / diag[static_cast<long long>(v) * bs + c];
+            nb_a[static_cast<long long>(k) * bs + c] = static_cast<float>(a);
+        }
         nb_w[k] = static_cast<float>(-acc / bs);
     }
+}
+
+// y = A x (transpose = false) or A^T x (true) in FP32 over the graph:
+// (A x)_v = d_v x_v + sum_{u in N(v)} a_vu x_u;  (A^T x)_u = d_u x_u + sum over
+// edges (v -> u) of a_vu x_v.
+template<bool TRANSPOSE>
+__global__ void __launch_bounds__(256) k_gnn_matvec(GraphArgs g, const float* __restrict__ nb_a,
+                                                    const float* __restrict__ diag_f, const float* __restrict__ x,
+                                                    float* __restrict__ y)
+{
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<long long>(g.n) * g.bs) return;
+    const int v = static_cast<int>(t / g.bs), c = static_cast<int>(t - static_cast<long long>(v) * g.bs);
+    float acc = diag_f[t] * x[t];
+    if (TRANSPOSE) {
+        for (int k = g.tr_ptr[v]; k < g.tr_ptr[v + 1]; ++k) {
+            // tr_w's edge: the transposed slot stores the forward edge index in nb order
+            const int src = g.tr_col[k];
+            acc = fmaf(nb_a[static_cast<long long>(g.tr_edge[k]) * g.bs + c], x[static_cast<long long>(src) * g.bs + c],
+                       acc);
+        }
+    } else {
+        for (int k = g.nb_ptr[v]; k < g.nb_ptr[v + 1]; ++k)
+            acc = fmaf(nb_a[static_cast<long long>(k) * g.bs + c], x[static_cast<long long>(g.nb_col[k]) * g.bs + c],
+                       acc);
+    }
+    y[t] = acc;
 }
 
 __global__ void k_gnn_gather_w(int count, const int* __restrict__ idx, const float* __restrict__ src,
@@ -737,6 +830,8 @@ struct Gnn {
     DeviceBuffer ha, hb;                                                       // inference ping-pong
     DeviceBuffer norm_r, norm_e, out32, dz, dh, dm, dy, partials, loss_partials, ticket, loss;
     DeviceBuffer qbuf;   // q = r / d (FP32); norm_r holds |r|, |q| at [0], [2]
+    DeviceBuffer nb_a, diag_f, ax, res, gres;   // FP32 coefficients; A out, r - A out, A^T (r - A out)
+    double loss_error_weight = 0.1, loss_residual_weight = 1.0;
     int adam_t = 0;
     bool train_ready = false;
     std::uint64_t applications = 0;
@@ -752,6 +847,7 @@ struct Gnn {
         g.tr_ptr = tr_ptr.as<int>();
         g.tr_col = tr_col.as<int>();
         g.tr_w = tr_w.as<float>();
+        g.tr_edge = tr_edge.as<int>();
         g.dinv = dinv.as<float>();
         return g;
     }
@@ -847,6 +943,9 @@ void gnn_train_buffers(Gnn& G)
     for (auto& b : G.mask) b.allocate(rows * 8 + 16);
     G.x.allocate(rows * gnn::kF * 4 + 16);
     G.out32.allocate(rows * G.bs * 4 + 16);
+    G.ax.allocate(rows * G.bs * 4 + 16);
+    G.res.allocate(rows * G.bs * 4 + 16);
+    G.gres.allocate(rows * G.bs * 4 + 16);
     G.dz.allocate(rows * G.bs * 4 + 16);
     G.dh.allocate(rows * gnn::kH * 4 + 16);
     G.dm.allocate(rows * gnn::kH * 4 + 16);
@@ -889,11 +988,19 @@ double gnn_loss_grad(Gnn& G, const double* r, const double* e)
     k_gnn_features<<<G.blocks(G.n), 256, 0, c.stream>>>(g, r, G.qbuf.as<float>(), G.norm_r.as<double>(),
                                                         G.x.as<float>());
     kern::norm<double>(c, static_cast<std::size_t>(nb), e, G.norm_e.as<double>(), G.norm_e.as<double>() + 1);
+    gnn::k_gnn_matvec<false><<<G.blocks(nb), 256, 0, c.stream>>>(g, G.nb_a.as<float>(), G.diag_f.as<float>(),
+                                                                 G.out32.as<float>(), G.ax.as<float>());
+    gnn::k_gnn_residual<<<G.blocks(nb), 256, 0, c.stream>>>(nb, r, G.ax.as<float>(), G.res.as<float>());
+    gnn::k_gnn_matvec<true><<<G.blocks(nb), 256, 0, c.stream>>>(g, G.nb_a.as<float>(), G.diag_f.as<float>(),
+                                                                G.res.as<float>(), G.gres.as<float>());
     const unsigned lb = 512;
-    gnn::k_gnn_out_grad<<<lb, 256, 0, c.stream>>>(nb, G.out32.as<float>(), e, G.norm_e.as<double>(),
-                                                   G.norm_r.as<double>(), std::sqrt(static_cast<double>(nb)),
-                                                   G.dz.as<float>(), G.loss_partials.as<double>(),
-                                                   G.ticket.as<unsigned>(), G.loss.as<double>());
+    gnn::k_gnn_out_grad<<<lb, 256, 0, c.stream>>>(nb, G.out32.as<float>(), e, G.res.as<float>(), G.gres.as<float>(),
+                                                   G.norm_e.as<double>(), G.norm_r.as<double>(),
+                                                   std::sqrt(static_cast<double>(nb)), G.loss_error_weight,
+                                                   G.loss_residual_weight, G.dz.as<float>(),
+                                                   G.loss_partials.as<double>(), G.ticket.as<unsigned>(),
+                                                   G.loss.as<double>());
+    c.launched(4);
     gnn::k_gnn_decode_bwd<<<G.blocks(G.n), 256, 0, c.stream>>>(G.n, G.bs, G.dz.as<float>(),
                                                                 G.params.as<float>() + Gnn::kOffWd, G.dh.as<float>());
     float* grads = G.grads.as<float>();
@@ -1013,7 +1120,8 @@ void gnn_bind_matrix(Gnn& G, Matrix& m)
     }
     gnn::k_gnn_graph<<<G.blocks(G.n), 256, 0, c.stream>>>(G.n, G.bs, G.nb_ptr.as<int>(), G.nb_entry.as<int>(),
                                                            static_cast<const double*>(m.values.ptr), diag.as<double>(),
-                                                           G.nb_w.as<float>(), G.dinv.as<float>());
+                                                           G.nb_w.as<float>(), G.dinv.as<float>(), G.nb_a.as<float>(),
+                                                           G.diag_f.as<float>());
     const int ne = static_cast<int>(G.tr_col.bytes / sizeof(int));
     if (ne > 0)
         gnn::k_gnn_gather_w<<<G.blocks(ne), 256, 0, c.stream>>>(ne, G.tr_edge.as<int>(), G.nb_w.as<float>(),
@@ -1109,6 +1217,8 @@ owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** ou
         G->nb_w.allocate(nb_col.size() * sizeof(float) + 16);
         G->tr_w.allocate(nb_col.size() * sizeof(float) + 16);
         G->dinv.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
+        G->diag_f.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
+        G->nb_a.allocate(nb_col.size() * G->bs * sizeof(float) + 16);
         const std::vector<float> w0 = owtk::gnn_initial_weights(G->bs, seed);
         G->params = owtk::upload(st, w0);
         G->grads.allocate(owtk::Gnn::kParams * sizeof(float) + 16);
@@ -1146,6 +1256,18 @@ owtk_status owtk_learned_update_matrix(owtk_learned* net, owtk_matrix* m)
 }
 
 size_t owtk_learned_parameter_count(void) { return owtk::Gnn::kParams; }
+
+owtk_status owtk_learned_set_loss_weights(owtk_learned* net, double error_weight, double residual_weight)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr, "null handle");
+        if (!(error_weight >= 0) || !(residual_weight >= 0) || !std::isfinite(error_weight)
+            || !std::isfinite(residual_weight) || error_weight + residual_weight <= 0)
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "loss weights must be finite, non-negative, not both zero");
+        net->loss_error_weight = error_weight;
+        net->loss_residual_weight = residual_weight;
+    });
+}
 
 owtk_status owtk_learned_get_parameters(owtk_learned* net, float* host, size_t count)
 {

@@ -276,7 +276,6 @@ __device__ __forceinline__ void bulk_products(const SpmvArgs<T>& a, const BulkHe
         }
     }
 }
-
 // Sums of one staged tile: thread t owns outputs (row, component) t, t+C, ...
 // and adds its row's staged products in entry order (eight loaded ahead of
 // the add chain), the reference's summation sequence.

@@ -146,6 +146,7 @@ def lib():
             "owtk_learned_apply": (c_int, [vp, vp, vp]),
             "owtk_learned_loss_grad": (c_int, [vp, vp, vp, POINTER(c_double), vp]),
             "owtk_learned_adam_step": (c_int, [vp, c_double]),
+            "owtk_learned_set_loss_weights": (c_int, [vp, c_double, c_double]),
             "owtk_pc_create_learned": (c_int, [vp, vp, POINTER(vp)]),
             "owtk_pc_learned_counts": (c_int, [vp, u64p, u64p]),
         }
@@ -519,6 +520,9 @@ class Learned:
 
     def adam_step(self, learning_rate: float):
         check(lib().owtk_learned_adam_step(self.h, learning_rate))
+
+    def set_loss_weights(self, error_weight: float = 1.0, residual_weight: float = 1.0):
+        check(lib().owtk_learned_set_loss_weights(self.h, error_weight, residual_weight))
 
     def close(self):
         if self.h is not None:

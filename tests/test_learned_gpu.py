@@ -5,8 +5,9 @@ fallback, and what training gains over the untrained (Jacobi) network.
 
 Tolerances: activations and layer weights are BF16 (8-bit mantissa) with
 FP32 accumulation, through four layers; the network's correction is held to
-5% relative error and gradients to cosine similarity >= 0.99 with <= 10%
-relative error per weight tensor.  Exact properties are checked exactly:
+5% relative error; with the error loss gradients are held to cosine
+similarity >= 0.99 and <= 10% relative error per weight tensor (the residual
+term, which multiplies the output by A, to 0.98 and 20%).  Exact properties are checked exactly:
 positive homogeneity (scaling by 2 is exact in every rounding), the untrained
 network equals Jacobi, and a network whose every step fails hands each step
 to ILU(0), reproducing ILU(0)-FGMRES bit for bit.
@@ -82,19 +83,24 @@ def test_forward_matches_restatement(native, ctx):
     np.testing.assert_allclose(y.download(), jac, rtol=2e-7)
 
 
-def test_gradients_match_restatement(native, ctx):
+@pytest.mark.parametrize("weights,loss_tol,cos_min,rel_max", [((1.0, 0.0), 5e-2, 0.99, 0.1),
+                                                             ((0.1, 1.0), 0.15, 0.98, 0.2)])
+def test_gradients_match_restatement(native, ctx, weights, loss_tol, cos_min, rel_max):
+    # The residual term multiplies the network output by A, which roughly
+    # doubles the relative BF16 error of the loss and its gradient.
     from oracle import gnn
     c, m, net, g = setup(native, ctx, side=20)
     n, bs = c["owned"], c["bs"]
     v = bf16_weights(bs, 11)
     net.set_parameters(v)
+    net.set_loss_weights(*weights)
     rng = np.random.default_rng(13)
     r = rng.uniform(-1, 1, n * bs)
     e = rng.uniform(-1, 1, n * bs)
     loss, grads = net.loss_grad(native.Vector(ctx, n, 0, bs).upload(r), native.Vector(ctx, n, 0, bs).upload(e),
                                 want_grads=True)
-    rl, rg = gnn.loss_and_grad(g, unflat(v, bs), r, e)
-    assert abs(loss - rl) <= 5e-2 * rl, (loss, rl)
+    rl, rg = gnn.loss_and_grad(g, unflat(v, bs), r, e, we=weights[0], wr=weights[1])
+    assert abs(loss - rl) <= loss_tol * rl, (loss, rl)
     got = unflat(grads, bs)
     pairs = [("we", got["we"], rg["we"]), ("wd", got["wd"], rg["wd"])]
     pairs += [(f"wl{l}", got["wl"][l], rg["wl"][l]) for l in range(4)]
@@ -102,7 +108,7 @@ def test_gradients_match_restatement(native, ctx):
         a, b = a.reshape(-1), b.reshape(-1)
         cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-        assert cos >= 0.99 and rel <= 0.1, (name, cos, rel)
+        assert cos >= cos_min and rel <= rel_max, (name, cos, rel)
 
 
 def test_training_reduces_the_loss(native, ctx):
@@ -145,12 +151,12 @@ def test_trained_network_beats_untrained(native, ctx):
     # iterations with the trained network against the untrained one (the
     # Jacobi preconditioner) on a held-out draw.
     from owtk_b200 import learned
-    systems = [learned.training_system(3000, seed=41, draw=d) for d in range(5)]
+    systems = [learned.training_system(3000, seed=41, draw=d) for d in range(8)]
     held = learned.training_system(3000, seed=41, draw=99)
     s0 = systems[0]
     m0 = native.Matrix(ctx, "bsr", s0.owned, 0, s0.bs, s0.rowptr, s0.cols, s0.vals)
     net = native.Learned(m0, seed=1)
-    hist = learned.train(ctx, net, systems, epochs=6, learning_rate=1e-3, pairs_per_system=4)
+    hist = learned.train(ctx, net, systems, epochs=10, learning_rate=1e-3, pairs_per_system=6)
     assert hist[-1] < hist[0]
     mh = native.Matrix(ctx, "bsr", held.owned, 0, held.bs, held.rowptr, held.cols, held.vals)
     net.update_matrix(mh)
@@ -158,3 +164,5 @@ def test_trained_network_beats_untrained(native, ctx):
     net.set_parameters(np.where(np.arange(net.parameter_count()) >= 1024 + 4 * 8192, 0.0, net.parameters()))
     untrained = learned.fgmres_iterations(ctx, mh, native.LearnedPreconditioner(net), held.rhs)
     assert trained < untrained, (trained, untrained)
+    ilu = learned.fgmres_iterations(ctx, mh, native.Preconditioner(mh, native.PC_ILU, 0), held.rhs)
+    assert trained <= ilu + 2, (trained, ilu)   # as good as ILU(0) in iterations
