@@ -29,6 +29,13 @@ for _p in (REPO, PKG):
 import numpy as np  # noqa: E402
 
 METRIC = "time-to-rtol 1e-8 on B200, learned/mixed vs plain FP64 ILU-GMRES; SpMV HBM GB/s"
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per vertex from one
+# ncu capture on the 1M-vertex disk mesh (profiles/ilu0_sweeps_fp64_1m_vertices.md,
+# profiles/spmv_bulk_bsr3_fp64_1m_vertices.md); traffic grows with the vertex
+# count, so the benchmark's per-launch traffic is this times its vertices.
+PROFILED_TRAFFIC_PER_VERTEX = {"ilu0 sweep pair": (255.98e6 + 20.89e6 + 279.87e6 + 21.80e6) / 999_573,
+                               "spmv": (224.46e6 + 5.60e6) / 999_573}
 WORKLOAD = "plain-fp64-gmres30-ilu0"
 
 
@@ -298,11 +305,12 @@ def run_ours(args):
                     "d2h_bytes_per_step": n * bs * 8},
             "roofline": {"bound": "hbm", "kernel": "ilu0 forward+backward sweep", "achieved": ilu_bytes / (ilu_ms * 1e-3) / 1e9,
                          "peak": peak, "unit": "GB/s", "frac": ilu_bytes / (ilu_ms * 1e-3) / 1e9 / peak,
-                         "traffic": None, "bytes_per_launch": ilu_bytes, "ms_per_launch": ilu_ms,
-                         "peak_source": peak_kind},
+                         "traffic": PROFILED_TRAFFIC_PER_VERTEX["ilu0 sweep pair"] * n,
+                         "traffic_source": "ncu DRAM bytes per vertex on the 1M-vertex mesh, scaled to this mesh",
+                         "bytes_per_launch": ilu_bytes, "ms_per_launch": ilu_ms, "peak_source": peak_kind},
             "spmv": {"achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "unit": "GB/s",
                      "frac": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak, "us_per_launch": spmv_ms * 1e3,
-                     "bytes_per_launch": spmv_bytes},
+                     "bytes_per_launch": spmv_bytes, "traffic": PROFILED_TRAFFIC_PER_VERTEX["spmv"] * n},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
