@@ -348,6 +348,10 @@ owtk_status owtk_learned_destroy(owtk_learned* net);
 /* Re-read the coefficients of a matrix with the same pattern (edge weights
  * and diagonal of the graph); the weights are kept. */
 owtk_status owtk_learned_update_matrix(owtk_learned* net, owtk_matrix* m);
+/* 1 when the layers gather neighbours with TMA (tile::gather4) into shared
+ * memory (environment OWTK_GNN_TMA=1 at creation, with tensor-map support),
+ * 0 for the default register-gather path; both give bit-identical results. */
+int owtk_learned_uses_tma(const owtk_learned* net);
 /* Flat FP32 parameters: encoder 64x16, 4 layers 64x128, decoder 8x64. */
 size_t owtk_learned_parameter_count(void);
 owtk_status owtk_learned_get_parameters(owtk_learned* net, float* host, size_t count);

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 namespace owtk::dev {
@@ -167,6 +168,26 @@ __device__ __forceinline__ void bulk_load(std::uint32_t dst, const void* src, st
         " [%0], [%1], %2, [%3], %4;" ::"r"(dst),
         "l"(src), "r"(bytes), "r"(bar), "l"(policy)
         : "memory");
+}
+
+// Granule-aligned copy of elements [b, e) of an array of `total` elements of
+// `sz` bytes starting at a 16-byte aligned base.  Returns the bytes to copy
+// (0: nothing), the copy's first byte `lo`, the index of element b in the
+// destination and how many of the run's elements the copy holds.
+__device__ __forceinline__ std::uint32_t bulk_segment(std::size_t b, std::size_t e, std::size_t total, int sz,
+                                                      std::size_t& lo, int& off, int& avail)
+{
+    const std::size_t bb = b * sz, eb = e * sz, tb = (total * sz) & ~std::size_t(15);
+    lo = bb & ~std::size_t(15);
+    std::size_t hi = (eb + 15) & ~std::size_t(15);
+    if (hi > tb) hi = tb;
+    off = static_cast<int>((bb - lo) / sz);
+    if (hi <= bb) {
+        avail = 0;
+        return 0;
+    }
+    avail = static_cast<int>((hi - bb) / sz);
+    return static_cast<std::uint32_t>(hi - lo);
 }
 
 // OR of `pred` over the `count` threads that meet at named barrier `id`.

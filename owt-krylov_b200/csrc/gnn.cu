@@ -13,11 +13,14 @@
 // eight K=16 MMAs against the resident layer weight and applies the
 // ReLU/residual epilogue straight from TMEM.
 
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -162,7 +165,8 @@ __global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* _
     if (i < count) q[i] = static_cast<float>(r[i]) * dinv[i];
 }
 
-// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...].
+// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...], one thread
+// per vertex (the weights are read as shared-memory broadcasts).
 template<class T>
 __global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
                                                     const double* norms, const float* __restrict__ we,
@@ -177,13 +181,10 @@ __global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __rest
     const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
     const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
     float x[kF];
+    const long long vb = static_cast<long long>(v) * g.bs;
 #pragma unroll
-    for (int f = 0; f < kF; ++f) x[f] = 0.0f;
-    for (int c = 0; c < g.bs; ++c) {
-        const long long o = static_cast<long long>(v) * g.bs + c;
-        x[c] = static_cast<float>(r[o]) * inv_r;
-        x[g.bs + c] = q[o] * inv_q;
-    }
+    for (int f = 0; f < kF; ++f)
+        x[f] = f < g.bs ? static_cast<float>(r[vb + f]) * inv_r : (f < 2 * g.bs ? q[vb + f - g.bs] * inv_q : 0.0f);
     uint4* out = reinterpret_cast<uint4*>(h0 + static_cast<long long>(v) * kH);
 #pragma unroll
     for (int c8 = 0; c8 < kH / 8; ++c8) {
@@ -199,33 +200,37 @@ __global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __rest
     }
 }
 
-// Decoder: out = q + rms(q) * (h Wd^T).
+// Decoder: out = q + rms(q) * (h Wd^T).  An 8-lane group per vertex reads the
+// row as one coalesced 128-byte load; each lane's partial dot products are
+// summed across the group with three shuffles.
 template<class O>
 __global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __restrict__ q, const double* norms,
                                                     const float* __restrict__ wd, const bf16* __restrict__ h,
                                                     O* __restrict__ out)
 {
-    __shared__ float w[8 * kH];
-    for (int i = threadIdx.x; i < 8 * kH; i += blockDim.x) w[i] = wd[i];
+    // Row c, features 8*c8..8*c8+7 at c * 72 + c8 * 9: conflict-free across a group.
+    __shared__ float w[8 * 72];
+    for (int i = threadIdx.x; i < 8 * kH; i += blockDim.x) w[(i / kH) * 72 + ((i % kH) / 8) * 9 + i % 8] = wd[i];
     __syncthreads();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= g.n) return;
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int v = static_cast<int>(t >> 3), c8 = static_cast<int>(t & 7);
+    const bool live = v < g.n;
     const float s = static_cast<float>(norms[2] / sqrt(static_cast<double>(g.n) * g.bs));
-    float hv[kH];
-    const uint4* hr = reinterpret_cast<const uint4*>(h + static_cast<long long>(v) * kH);
-#pragma unroll
-    for (int c8 = 0; c8 < kH / 8; ++c8) {
-        float f[8];
-        bf16x8_to_f32(hr[c8], f);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) hv[c8 * 8 + i] = f[i];
-    }
+    float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (live) bf16x8_to_f32(reinterpret_cast<const uint4*>(h + static_cast<long long>(v) * kH)[c8], f);
+    float mine = 0.0f;
     for (int c = 0; c < g.bs; ++c) {
         float acc = 0.0f;
 #pragma unroll
-        for (int k = 0; k < kH; ++k) acc = fmaf(w[c * kH + k], hv[k], acc);
-        const long long o = static_cast<long long>(v) * g.bs + c;
-        out[o] = static_cast<O>(norms[0] > 0.0 ? q[o] + s * acc : 0.0f);
+        for (int i = 0; i < 8; ++i) acc = fmaf(w[c * 72 + c8 * 9 + i], f[i], acc);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        if (c8 == c) mine = acc;
+    }
+    if (live && c8 < g.bs) {
+        const long long o = static_cast<long long>(v) * g.bs + c8;
+        out[o] = static_cast<O>(norms[0] > 0.0 ? q[o] + s * mine : 0.0f);
     }
 }
 
@@ -285,49 +290,66 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
             p0 = g.nb_ptr[wrow0 + lane];
             p1 = g.nb_ptr[wrow0 + lane + 1];
         }
-        auto load_idx = [&](int it, int& col, float& w, int& e0, int& e1) {
-            const int src = 4 * it + grp;
-            e0 = __shfl_sync(0xffffffffu, p0, src);
-            e1 = __shfl_sync(0xffffffffu, p1, src);
-            col = 0;
-            w = 0.0f;
-            if (e0 + chunk < e1) {
-                col = g.nb_col[e0 + chunk];
-                w = g.nb_w[e0 + chunk];
-            }
+        // Software pipeline over the 8 row-steps: indices two steps ahead,
+        // neighbour features one step ahead of the accumulation.
+        struct Idx {
+            int col, e0, e1;
+            float w;
         };
-        int ncol, ne0, ne1;
-        float nw;
-        load_idx(0, ncol, nw, ne0, ne1);
-        for (int it = 0; it < 8; ++it) {
-            const int r = 32 * warp + 4 * it + grp, v = row0 + r;
-            const int col = ncol, e0 = ne0, e1 = ne1;
-            const float wgt = nw;
-            if (it + 1 < 8) load_idx(it + 1, ncol, nw, ne0, ne1);
-            uint4 hv = make_uint4(0, 0, 0, 0), mv = make_uint4(0, 0, 0, 0);
-            const int deg = e1 - e0;
+        struct Got {
             uint4 nv[8];
-            float ws[8];
+            uint4 hv;
+        };
+        auto load_idx = [&](int it) {
+            Idx x;
+            const int src = 4 * it + grp;
+            x.e0 = __shfl_sync(0xffffffffu, p0, src);
+            x.e1 = __shfl_sync(0xffffffffu, p1, src);
+            x.col = 0;
+            x.w = 0.0f;
+            if (x.e0 + chunk < x.e1) {
+                x.col = g.nb_col[x.e0 + chunk];
+                x.w = g.nb_w[x.e0 + chunk];
+            }
+            return x;
+        };
+        auto gather = [&](int it, const Idx& x, Got& d) {
+            const int v = row0 + 32 * warp + 4 * it + grp, deg = x.e1 - x.e0;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int u = __shfl_sync(0xffffffffu, col, (lane & ~7) + q);
-                ws[q] = __shfl_sync(0xffffffffu, wgt, (lane & ~7) + q);
-                nv[q] = make_uint4(0, 0, 0, 0);
-                if (q < deg) nv[q] = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8);
+                const int u = __shfl_sync(0xffffffffu, x.col, (lane & ~7) + q);
+                d.nv[q] = make_uint4(0, 0, 0, 0);
+                if (q < deg) d.nv[q] = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8);
             }
+            d.hv = make_uint4(0, 0, 0, 0);
+            if (v < g.n) d.hv = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(v) * kH + chunk * 8);
+        };
+        Idx ia = load_idx(0), ib = load_idx(1);
+        Got da, db;
+        gather(0, ia, da);
+#pragma unroll 1
+        for (int it = 0; it < 8; ++it) {
+            Idx ic = ia;
+            if (it + 2 < 8) ic = load_idx(it + 2);
+            if (it + 1 < 8) gather(it + 1, ib, db);
+            const int r = 32 * warp + 4 * it + grp, v = row0 + r;
+            const int deg = ia.e1 - ia.e0;
+            uint4 mv = make_uint4(0, 0, 0, 0);
+            float ws[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) ws[q] = __shfl_sync(0xffffffffu, ia.w, (lane & ~7) + q);
             if (v < g.n) {
-                hv = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(v) * kH + chunk * 8);
                 float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     if (q < deg) {
                         float f[8];
-                        bf16x8_to_f32(nv[q], f);
+                        bf16x8_to_f32(da.nv[q], f);
 #pragma unroll
                         for (int i = 0; i < 8; ++i) acc[i] = fmaf(ws[q], f[i], acc[i]);
                     }
                 }
-                for (int e = e0 + 8; e < e1; ++e) {   // rows with more than 8 neighbours
+                for (int e = ia.e0 + 8; e < ia.e1; ++e) {   // rows with more than 8 neighbours
                     const int u = g.nb_col[e];
                     const float we = g.nb_w[e];
                     float f[8];
@@ -338,8 +360,11 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
                 mv = f32_to_bf16x8(acc);
                 if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
             }
-            *reinterpret_cast<uint4*>(tile + sw128(r, chunk)) = hv;
+            *reinterpret_cast<uint4*>(tile + sw128(r, chunk)) = da.hv;
             *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, chunk)) = mv;
+            ia = ib;
+            ib = ic;
+            da = db;
         }
         fence_proxy_async_smem();
         tmem_fence_before_sync();
@@ -392,6 +417,276 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     if (!ok && threadIdx.x == 0) atomicOr(status, kErrTimeout);
     tmem_fence_before_sync();
     __syncthreads();
+    if (warp == 0) tmem_free(tmem, kH);
+}
+
+// ---------------------------------------------------------------- TMA-fed layer
+// The same layer, warp-specialised.  A producer warp streams, per 16-row
+// sub-tile, the neighbours' feature rows with TMA gathers (tile::gather4, box
+// one row high) into a 3-stage shared-memory ring together with the rows'
+// gather plan entries and edge weights (bulk copies), and per 128-row tile the
+// tile's own rows with one 2D TMA load whose 128-byte swizzle is exactly the
+// K-major operand layout of the MMA.  The four consumer warps aggregate m from
+// shared memory (no global loads on the common path), write the swizzled m
+// block, run the eight MMAs and the epilogue.  Rows whose neighbours do not fit
+// a sub-tile's 128 slots are gathered from global memory by the consumers.
+constexpr int kSubRows = 16;                     // rows per gather sub-tile
+constexpr int kSubsPerTile = kTile / kSubRows;   // 8
+constexpr int kSlots = 128;                      // staged neighbour rows per sub-tile
+constexpr int kGStages = 3;
+constexpr int kSubWeights = 512;                 // staged edge weights per sub-tile
+constexpr int kTmaThreads = 160;                 // 4 consumer warps + 1 producer warp
+constexpr int kStageSlots = kSlots * 128;                        // 16 KB
+constexpr int kStageMeta = kStageSlots;                          // 16 int4 = 256 B
+constexpr int kStageHead = kStageMeta + 256;                     // woff, wavail, nq
+constexpr int kStageW = kStageHead + 64;                         // weights
+constexpr int kStageBytes = (kStageW + kSubWeights * 4 + 16 + 1023) / 1024 * 1024;
+constexpr int kTmaSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128 + kGStages * kStageBytes;
+
+template<bool TRAIN>
+__global__ void __launch_bounds__(kTmaThreads, 2)
+    k_gnn_layer_tma(GraphArgs g, const __grid_constant__ CUtensorMap gmap, const __grid_constant__ CUtensorMap tmap,
+                    const bf16* __restrict__ h_in, const bf16* __restrict__ wl, bf16* __restrict__ h_out,
+                    bf16* __restrict__ m_out, unsigned long long* __restrict__ mask_out, const int4* __restrict__ quads,
+                    const int* __restrict__ quad_ptr, const int4* __restrict__ metas, int edges, unsigned* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) std::uint64_t bars[2 * kGStages + 3];   // full, empty, a_full, a_free, mma
+    __shared__ std::uint32_t tmem_base_s;
+    const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
+    unsigned char* sm = smem_raw + (base - raw);
+    const std::uint32_t a0 = base, a1 = base + kTile * 128, b0 = base + 2 * kTile * 128, b1 = b0 + kH * 128;
+    const std::uint32_t st0 = b0 + 2 * kH * 128;
+    unsigned char* stg = sm + (st0 - base);
+    const std::uint32_t bar0 = smem_u32(bars);
+    const auto full = [&](int s) { return bar0 + 8 * s; };
+    const auto empty = [&](int s) { return bar0 + 8 * (kGStages + s); };
+    const std::uint32_t a_full = bar0 + 8 * (2 * kGStages), a_free = a_full + 8, mma_bar = a_full + 16;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (g.n + kTile - 1) / kTile;
+
+    // Layer weight into the two B blocks.
+    for (int i = threadIdx.x; i < kH * 16; i += kTmaThreads) {
+        const int r = i >> 4, c16 = i & 15;
+        *reinterpret_cast<uint4*>(sm + 2 * kTile * 128 + (c16 >> 3) * kH * 128 + sw128(r, c16 & 7)) =
+            *reinterpret_cast<const uint4*>(wl + r * 128 + c16 * 8);
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kGStages; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 4);
+        }
+        mbar_init(a_full, 1);
+        mbar_init(a_free, 1);
+        mbar_init(mma_bar, 1);
+        fence_proxy_async_smem();
+    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kH);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const std::uint32_t tmem = tmem_base_s;
+
+    if (warp == 4) {
+        // ------------------------------------------------------------ producer
+        const std::uint64_t policy = l2_policy_evict_normal();
+        int gsub = 0, it = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
+            const int row0 = t * kTile;
+            // The tile's plan in one round of loads: lane s < 9 holds sub-tile
+            // s's first quad and first edge; lane q holds quad q of each
+            // sub-tile (at most 32 per sub-tile).
+            int my_q = 0, my_e = 0;
+            if (lane <= kSubsPerTile) {
+                const int sub = min(t * kSubsPerTile + lane, (g.n + kSubRows - 1) / kSubRows);
+                my_q = quad_ptr[sub];
+                my_e = g.nb_ptr[min(row0 + lane * kSubRows, g.n)];
+            }
+            int4 myquad[kSubsPerTile];
+            int qs[kSubsPerTile + 1], es[kSubsPerTile + 1];
+#pragma unroll
+            for (int s = 0; s <= kSubsPerTile; ++s) {
+                qs[s] = __shfl_sync(0xffffffffu, my_q, s);
+                es[s] = __shfl_sync(0xffffffffu, my_e, s);
+            }
+#pragma unroll
+            for (int s = 0; s < kSubsPerTile; ++s) {
+                myquad[s] = make_int4(0, 0, 0, 0);
+                if (lane < qs[s + 1] - qs[s]) myquad[s] = quads[qs[s] + lane];
+            }
+#pragma unroll
+            for (int s = 0; s < kSubsPerTile; ++s, ++gsub) {
+                if (!ok) break;
+                const int st = gsub % kGStages, use = gsub / kGStages;
+                const int sub = t * kSubsPerTile + s;
+                const int r0 = row0 + s * kSubRows;
+                unsigned char* sp = stg + st * kStageBytes;
+                const std::uint32_t sb = st0 + st * kStageBytes;
+                const int nq = r0 < g.n ? qs[s + 1] - qs[s] : 0;
+                int good = 1;
+                if (lane == 0) {
+                    if (!mbar_wait_bounded(empty(st), (use & 1) ^ 1, kMmaSpin)) {
+                        good = 0;
+                    } else if (r0 >= g.n) {
+                        mbar_arrive(full(st));
+                    } else {
+                        const int e_first = es[s], e_last = es[s + 1];
+                        std::size_t lo = 0;
+                        int woff = 0, wavail = 0;
+                        std::uint32_t wb = bulk_segment(e_first, e_last, edges, 4, lo, woff, wavail);
+                        if (wb > static_cast<std::uint32_t>(kSubWeights * 4 + 16)) {   // keep within the stage
+                            wb = 0;
+                            wavail = 0;
+                        }
+                        int* head = reinterpret_cast<int*>(sp + kStageHead);
+                        head[0] = woff;
+                        head[1] = wavail;
+                        head[2] = e_first;
+                        mbar_arrive_expect_tx(full(st), static_cast<std::uint32_t>(nq) * 512u + 256u + wb);
+                        bulk_load(sb + kStageMeta, metas + static_cast<std::size_t>(sub) * kSubRows, 256, full(st),
+                                  policy);
+                        if (wb) bulk_load(sb + kStageW, reinterpret_cast<const unsigned char*>(g.nb_w) + lo, wb, full(st),
+                                          policy);
+                    }
+                }
+                good = __shfl_sync(0xffffffffu, good, 0);
+                if (!good) {
+                    atomicOr(status, kErrTimeout);
+                    ok = false;
+                    break;
+                }
+                if (lane < nq) {
+                    const int4 q = myquad[s];
+                    tma_gather4(sb + lane * 512, &gmap, 0, q.x, q.y, q.z, q.w, full(st), policy);
+                }
+                __syncwarp();
+            }
+            if (!ok) break;
+            // The tile's own rows (swizzled) once the previous tile's epilogue is done.
+            if (lane == 0) {
+                if (it > 0 && !mbar_wait_bounded(a_free, (it - 1) & 1, kMmaSpin)) {
+                    atomicOr(status, kErrTimeout);
+                    ok = false;
+                } else {
+                    mbar_arrive_expect_tx(a_full, kTile * 128);
+                    tma_load_2d(a0, &tmap, 0, row0, a_full);
+                }
+            }
+            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        }
+        // Leave after the last copies landed.
+        if (lane == 0) {
+            for (int k = max(0, gsub - kGStages); k < gsub; ++k)
+                mbar_wait_bounded(full(k % kGStages), (k / kGStages) & 1, kMmaSpin);
+            if (it > 0) mbar_wait_bounded(a_full, (it - 1) & 1, kMmaSpin);
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, kH);
+    const int grp = lane >> 3, chunk = lane & 7;
+    int gsub = 0, it = 0;
+    bool failed = false;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int row0 = t * kTile;
+        for (int s = 0; s < kSubsPerTile; ++s, ++gsub) {
+            const int st = gsub % kGStages, use = gsub / kGStages;
+            const unsigned char* sp = stg + st * kStageBytes;
+            const bool ready = !failed && __all_sync(0xffffffffu, mbar_wait_bounded(full(st), use & 1, kMmaSpin));
+            failed = failed || !ready;
+            const int rl = 4 * warp + grp;                 // row within the sub-tile
+            const int r = s * kSubRows + rl, v = row0 + r;
+            uint4 mv = make_uint4(0, 0, 0, 0);
+            if (ready && v < g.n) {
+                const int4 meta = reinterpret_cast<const int4*>(sp + kStageMeta)[rl];
+                const int* head = reinterpret_cast<const int*>(sp + kStageHead);
+                const int woff = head[0], wavail = head[1], e_first = head[2];
+                const float* sw = reinterpret_cast<const float*>(sp + kStageW);
+                float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int k = 0; k < meta.y; ++k) {
+                    const int wi = meta.z + k;
+                    const float w = wi < wavail ? sw[woff + wi] : g.nb_w[e_first + wi];
+                    uint4 u;
+                    if (meta.x >= 0) u = *reinterpret_cast<const uint4*>(sp + (meta.x + k) * 128 + chunk * 16);
+                    else u = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(g.nb_col[e_first + wi]) * kH
+                                                             + chunk * 8);
+                    float f[8];
+                    bf16x8_to_f32(u, f);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[i] = fmaf(w, f[i], acc[i]);
+                }
+                mv = f32_to_bf16x8(acc);
+                if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
+            }
+            *reinterpret_cast<uint4*>(sm + kTile * 128 + sw128(r, chunk)) = mv;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty(st));
+        }
+        fence_proxy_async_smem();
+        tmem_fence_before_sync();
+        if (bar_any(1, 128, failed)) {
+            failed = true;
+            break;
+        }
+        if (threadIdx.x == 0) {
+            bool aok = mbar_wait_bounded(a_full, it & 1, kMmaSpin);
+            if (aok) {
+                tmem_fence_after_sync();
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    umma_bf16(tmem, umma_desc_sw128(a0 + 32 * k), umma_desc_sw128(b0 + 32 * k), idesc, k > 0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    umma_bf16(tmem, umma_desc_sw128(a1 + 32 * k), umma_desc_sw128(b1 + 32 * k), idesc, true);
+                umma_commit(mma_bar);
+            } else {
+                atomicOr(status, kErrTimeout);
+                mbar_arrive(mma_bar);
+            }
+        }
+        const bool mok = mbar_wait_bounded(mma_bar, it & 1, kMmaSpin);
+        tmem_fence_after_sync();
+        if (bar_any(1, 128, !mok)) {
+            failed = true;
+            break;
+        }
+        // Epilogue: row = 32*warp + lane; h_old from the swizzled A0 block.
+        const int r = 32 * warp + lane, v = row0 + r;
+        unsigned long long mask = 0;
+        uint4 outv[8];
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            float y[32];
+            tmem_ld32(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + 32 * half, y);
+#pragma unroll
+            for (int c4 = 0; c4 < 4; ++c4) {
+                const int c8 = half * 4 + c4;
+                float hf[8];
+                bf16x8_to_f32(*reinterpret_cast<const uint4*>(sm + sw128(r, c8)), hf);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float yv = y[c4 * 8 + i];
+                    if (yv > 0.0f) mask |= 1ull << (c8 * 8 + i);
+                    hf[i] += fmaxf(yv, 0.0f);
+                }
+                outv[c8] = f32_to_bf16x8(hf);
+            }
+        }
+        if (v < g.n) {
+            uint4* o = reinterpret_cast<uint4*>(h_out + static_cast<long long>(v) * kH);
+#pragma unroll
+            for (int c8 = 0; c8 < 8; ++c8) o[c8] = outv[c8];
+            if (TRAIN) mask_out[v] = mask;
+        }
+        tmem_fence_before_sync();
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (threadIdx.x == 0) mbar_arrive(a_free);
+    }
+    if (failed && threadIdx.x == 0) atomicOr(status, kErrTimeout);
+    tmem_fence_before_sync();
+    asm volatile("bar.sync 1, 128;" ::: "memory");
     if (warp == 0) tmem_free(tmem, kH);
 }
 
@@ -830,6 +1125,12 @@ struct Gnn {
     DeviceBuffer ha, hb;                                                       // inference ping-pong
     DeviceBuffer norm_r, norm_e, out32, dz, dh, dm, dy, partials, loss_partials, ticket, loss;
     DeviceBuffer qbuf;   // q = r / d (FP32); norm_r holds |r|, |q| at [0], [2]
+    // Gather plan of the TMA-fed layer (per 16-row sub-tile: neighbour rows in
+    // quads, per row {slot or -1, degree, edge offset, 1}) and the tensor maps
+    // of every feature buffer (gather: box 64 x 1; tile: box 64 x 128, swizzled).
+    DeviceBuffer quads, quad_ptr, metas;
+    bool tma = false;
+    CUtensorMap gmap_a{}, tmap_a{}, gmap_b{}, tmap_b{}, gmap_h[gnn::kLayers + 1]{}, tmap_h[gnn::kLayers + 1]{};
     DeviceBuffer nb_a, diag_f, ax, res, gres;   // FP32 coefficients; A out, r - A out, A^T (r - A out)
     double loss_error_weight = 0.1, loss_residual_weight = 1.0;
     int adam_t = 0;
@@ -882,6 +1183,38 @@ void gnn_set_attrs()
                                    gnn::kBwdSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kWgradSmem));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kTmaSmem));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kTmaSmem));
+}
+
+// Tensor maps of a feature buffer (n rows of 64 BF16).
+bool gnn_encode_maps(const void* h, int n, CUtensorMap& gmap, CUtensorMap& tmap)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess
+            || q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(gnn::kH), static_cast<cuuint64_t>(n)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(gnn::kH * 2)};
+    const cuuint32_t one[2] = {1, 1};
+    const cuuint32_t gbox[2] = {static_cast<cuuint32_t>(gnn::kH), 1};
+    const cuuint32_t tbox[2] = {static_cast<cuuint32_t>(gnn::kH), static_cast<cuuint32_t>(gnn::kTile)};
+    void* addr = const_cast<void*>(h);
+    if (encode(&gmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, addr, dims, strides, gbox, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+        != CUDA_SUCCESS)
+        return false;
+    return encode(&tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, addr, dims, strides, tbox, one,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+        == CUDA_SUCCESS;
 }
 
 // Seeded initial weights: normal draws from std::mt19937_64, scaled per
@@ -920,14 +1253,26 @@ void gnn_forward(Gnn& G, const T* r, O* out)
     const gnn::bf16* hin = h0;
     for (int l = 0; l < gnn::kLayers; ++l) {
         gnn::bf16* hout = TRAIN ? G.h[l + 1].as<gnn::bf16>() : (l % 2 == 0 ? G.hb : G.ha).as<gnn::bf16>();
-        gnn::k_gnn_layer<TRAIN><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
-            g, hin, G.wl16.as<gnn::bf16>() + l * Gnn::kLayerW, hout, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
-            TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, c.status.as<unsigned>());
+        if (G.tma) {
+            const CUtensorMap& gm = TRAIN ? G.gmap_h[l] : (l % 2 == 0 ? G.gmap_a : G.gmap_b);
+            const CUtensorMap& tm = TRAIN ? G.tmap_h[l] : (l % 2 == 0 ? G.tmap_a : G.tmap_b);
+            const int tiles = (G.n + gnn::kTile - 1) / gnn::kTile;
+            const unsigned grid = static_cast<unsigned>(std::min(tiles, c.sm_count * 2));
+            gnn::k_gnn_layer_tma<TRAIN><<<grid, gnn::kTmaThreads, gnn::kTmaSmem, c.stream>>>(
+                g, gm, tm, hin, G.wl16.as<gnn::bf16>() + l * Gnn::kLayerW, hout,
+                TRAIN ? G.m[l].as<gnn::bf16>() : nullptr, TRAIN ? G.mask[l].as<unsigned long long>() : nullptr,
+                G.quads.as<int4>(), G.quad_ptr.as<int>(), G.metas.as<int4>(),
+                static_cast<int>(G.nb_col.bytes / sizeof(int)), c.status.as<unsigned>());
+        } else {
+            gnn::k_gnn_layer<TRAIN><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
+                g, hin, G.wl16.as<gnn::bf16>() + l * Gnn::kLayerW, hout, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
+                TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, c.status.as<unsigned>());
+        }
         OWTK_CUDA(cudaGetLastError());
         c.launched();
         hin = hout;
     }
-    gnn::k_gnn_decode<O><<<G.blocks(G.n), 256, 0, c.stream>>>(g, G.qbuf.as<float>(), norms,
+    gnn::k_gnn_decode<O><<<G.blocks(8ll * G.n), 256, 0, c.stream>>>(g, G.qbuf.as<float>(), norms,
                                                                G.params.as<float>() + Gnn::kOffWd, hin, out);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
@@ -939,6 +1284,9 @@ void gnn_train_buffers(Gnn& G)
     if (G.train_ready) return;
     const std::size_t rows = static_cast<std::size_t>(G.n);
     for (auto& b : G.h) b.allocate(rows * gnn::kH * 2 + 16);
+    if (G.tma)
+        for (int l = 0; l <= gnn::kLayers; ++l)
+            if (!gnn_encode_maps(G.h[l].ptr, G.n, G.gmap_h[l], G.tmap_h[l])) G.tma = false;
     for (auto& b : G.m) b.allocate(rows * gnn::kH * 2 + 16);
     for (auto& b : G.mask) b.allocate(rows * 8 + 16);
     G.x.allocate(rows * gnn::kF * 4 + 16);
@@ -1085,10 +1433,8 @@ void learned_apply(Preconditioner& p, Vector& in, Vector& out)
     if (!p.check_work.ptr) p.check_work.allocate(n * sizeof(double) + 16);
     double* w = p.check_work.as<double>();
     kern::spmv<double>(c, *G.matrix, y, w);
-    kern::sub<double>(c, n, x, w, w);
     constexpr int kSlot = kScalarSlots - 4;
-    kern::norm<double>(c, n, w, c.dev_scalar_copy.as<double>() + kSlot, c.dev_scalars + kSlot);
-    kern::norm<double>(c, n, x, c.dev_scalar_copy.as<double>() + kSlot + 1, c.dev_scalars + kSlot + 1);
+    kern::residual_norms(c, n, x, w, c.dev_scalar_copy.as<double>() + kSlot, c.dev_scalars + kSlot);
     c.sync();
     const double rho = c.host_scalars[kSlot], nu = c.host_scalars[kSlot + 1];
     if (!(rho < nu)) {
@@ -1231,6 +1577,43 @@ owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** ou
         G->ha.allocate(static_cast<std::size_t>(G->n) * owtk::gnn::kH * 2 + 16);
         G->hb.allocate(static_cast<std::size_t>(G->n) * owtk::gnn::kH * 2 + 16);
         G->norm_r.allocate(64);
+        // Gather plan of the TMA-fed layer.
+        {
+            const int subs = (G->n + owtk::gnn::kSubRows - 1) / owtk::gnn::kSubRows;
+            std::vector<std::int32_t> quads, quad_ptr(subs + 1, 0), metas(static_cast<std::size_t>(subs) * 16 * 4, 0);
+            for (int sub = 0; sub < subs; ++sub) {
+                const int r0 = sub * owtk::gnn::kSubRows;
+                int slots = 0;
+                for (int r = r0; r < std::min(r0 + owtk::gnn::kSubRows, G->n); ++r) {
+                    const int e0 = nb_ptr[r], deg = nb_ptr[r + 1] - e0, need = (deg + 3) / 4 * 4;
+                    std::int32_t* meta = &metas[(static_cast<std::size_t>(r)) * 4];
+                    meta[1] = deg;
+                    meta[2] = e0 - nb_ptr[r0];
+                    meta[3] = 1;
+                    if (deg == 0) {
+                        meta[0] = 0;
+                    } else if (slots + need <= owtk::gnn::kSlots) {
+                        meta[0] = slots;
+                        for (int j = 0; j < need; ++j) quads.push_back(nb_col[e0 + (j < deg ? j : 0)]);
+                        slots += need;
+                    } else {
+                        meta[0] = -1;
+                    }
+                }
+                quad_ptr[sub + 1] = static_cast<std::int32_t>(quads.size() / 4);
+            }
+            if (quads.empty()) quads.assign(4, 0);
+            G->quads = owtk::upload(st, quads);
+            G->quad_ptr = owtk::upload(st, quad_ptr);
+            G->metas = owtk::upload(st, metas);
+        }
+        G->nb_col.bytes = nb_col.size() * sizeof(int);
+        // The register-gather layer is the default: on the 2M-vertex mesh the
+        // TMA-fed layer measured about twice its time per launch.
+        const char* tma_env = std::getenv("OWTK_GNN_TMA");
+        G->tma = tma_env && tma_env[0] == '1'
+            && owtk::gnn_encode_maps(G->ha.ptr, G->n, G->gmap_a, G->tmap_a)
+            && owtk::gnn_encode_maps(G->hb.ptr, G->n, G->gmap_b, G->tmap_b);
         G->qbuf.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
         owtk::gnn_set_attrs();
         owtk::gnn_pack(*G);
@@ -1256,6 +1639,8 @@ owtk_status owtk_learned_update_matrix(owtk_learned* net, owtk_matrix* m)
 }
 
 size_t owtk_learned_parameter_count(void) { return owtk::Gnn::kParams; }
+
+int owtk_learned_uses_tma(const owtk_learned* net) { return net != nullptr && net->tma ? 1 : 0; }
 
 owtk_status owtk_learned_set_loss_weights(owtk_learned* net, double error_weight, double residual_weight)
 {

@@ -556,6 +556,65 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
     }
 }
 
+// ||x - w|| and ||x|| in one pass (the learned preconditioner's residual
+// check), same one-pass scaled sums and fixed combine order as k_norm.
+__global__ void __launch_bounds__(kThreads) k_residual_norms(std::size_t n, const double* __restrict__ x,
+                                                              const double* __restrict__ w, double* partials,
+                                                              unsigned* ticket, double* out_dev, double* out_host)
+{
+    ScaledSum a{0.0, 0.0, 0}, b{0.0, 0.0, 0};
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+        const double xv = x[i];
+        norm_push(a, xv - w[i]);
+        norm_push(b, xv);
+    }
+    a = norm_warp(a);
+    b = norm_warp(b);
+    __shared__ ScaledSum red[2][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ScaledSum s0 = red[0][0], s1 = red[1][0];
+        for (int k = 1; k < kThreads / 32; ++k) {
+            s0 = norm_merge(s0, red[0][k]);
+            s1 = norm_merge(s1, red[1][k]);
+        }
+        double* p = partials + 6 * blockIdx.x;
+        p[0] = s0.scale;
+        p[1] = s0.ssq;
+        p[2] = s0.nan;
+        p[3] = s1.scale;
+        p[4] = s1.ssq;
+        p[5] = s1.nan;
+        __threadfence();
+        if (atomicAdd(ticket, 1u) == gridDim.x - 1) {
+            __threadfence();
+            ScaledSum t0{0.0, 0.0, 0}, t1{0.0, 0.0, 0};
+            for (unsigned k = 0; k < gridDim.x; ++k) {
+                const double* q = partials + 6 * k;
+                t0 = norm_merge(t0, ScaledSum{__ldcg(q), __ldcg(q + 1), __ldcg(q + 2) != 0.0});
+                t1 = norm_merge(t1, ScaledSum{__ldcg(q + 3), __ldcg(q + 4), __ldcg(q + 5) != 0.0});
+            }
+            const ScaledSum ts[2] = {t0, t1};
+            for (int k = 0; k < 2; ++k) {
+                const ScaledSum& t = ts[k];
+                double r;
+                if (t.nan) r = __longlong_as_double(0x7ff8000000000000LL);
+                else if (t.scale == 0.0 || isinf(t.scale)) r = t.scale;
+                else r = t.scale * sqrt(t.ssq);
+                out_dev[k] = r;
+                out_host[k] = r;
+            }
+            *ticket = 0;
+        }
+    }
+}
+
 inline PtrPack pack(const void* const* p, int k)
 {
     PtrPack pk{};
@@ -682,6 +741,14 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
 {
     const unsigned blocks = reduce_blocks(c, n);
     k_norm<T><<<blocks, kThreads, 0, c.stream>>>(n, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+void residual_norms(Context& c, std::size_t n, const double* x, const double* w, double* out_dev, double* out_host)
+{
+    const unsigned blocks = reduce_blocks(c, n);
+    k_residual_norms<<<blocks, kThreads, 0, c.stream>>>(n, x, w, partials_of(c), ticket_of(c), out_dev, out_host);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }

@@ -264,6 +264,8 @@ template<class T> void gmres_update(Context& c, std::size_t n, int k, const T* c
 template<class T> void multidot(Context& c, std::size_t n, int k, const T* const* a,
                                 const T* const* b, double* out_dev, double* out_host);
 template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_dev, double* out_host);
+// ||x - w|| and ||x|| (two results) in one pass.
+void residual_norms(Context& c, std::size_t n, const double* x, const double* w, double* out_dev, double* out_host);
 template<class T> void jacobi(Context& c, std::size_t n, const T* inv, const T* in, T* out);
 template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y);
 template<class T> void gather_values(Context& c, std::size_t entries, std::size_t bs,

@@ -113,4 +113,34 @@ __device__ __forceinline__ void tmem_ld32(std::uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// ---------------------------------------------------------------- tensor loads
+// TMA tensor copies global -> shared through a CUtensorMap (a __grid_constant__
+// kernel parameter), completing on an mbarrier.  x is the innermost
+// coordinate (elements; here always 0, so 16-byte aligned).  No multicast.
+__device__ __forceinline__ void tma_load_2d(std::uint32_t dst, const void* tmap, int x, int y, std::uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(tmap), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// Four rows r0..r3 (box one row high) into 4 consecutive box-sized slots.
+__device__ __forceinline__ void tma_gather4(std::uint32_t dst, const void* tmap, int x, int r0, int r1, int r2, int r3,
+                                            std::uint32_t bar, std::uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(dst),
+        "l"(tmap), "r"(x), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(bar), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ std::uint64_t l2_policy_evict_normal()
+{
+    std::uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 }  // namespace owtk::dev

@@ -141,6 +141,7 @@ def lib():
             "owtk_learned_destroy": (c_int, [vp]),
             "owtk_learned_update_matrix": (c_int, [vp, vp]),
             "owtk_learned_parameter_count": (sz, []),
+            "owtk_learned_uses_tma": (c_int, [vp]),
             "owtk_learned_get_parameters": (c_int, [vp, vp, sz]),
             "owtk_learned_set_parameters": (c_int, [vp, vp, sz]),
             "owtk_learned_apply": (c_int, [vp, vp, vp]),
@@ -491,6 +492,10 @@ class Learned:
         h = c_void_p()
         check(lib().owtk_learned_create(matrix.h, seed, ctypes.byref(h)))
         self.h = h
+
+    @property
+    def uses_tma(self) -> bool:
+        return bool(lib().owtk_learned_uses_tma(self.h))
 
     @staticmethod
     def parameter_count() -> int:

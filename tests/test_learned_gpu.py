@@ -83,6 +83,31 @@ def test_forward_matches_restatement(native, ctx):
     np.testing.assert_allclose(y.download(), jac, rtol=2e-7)
 
 
+def test_tma_and_register_gather_agree_bitwise(native, ctx, monkeypatch):
+    # Both layer kernels aggregate neighbours in edge order with the same FP32
+    # operations, so forward outputs and gradients are identical.
+    c, m, net, g = setup(native, ctx, side=40, seed=37)
+    n, bs = c["owned"], c["bs"]
+    assert not net.uses_tma
+    monkeypatch.setenv("OWTK_GNN_TMA", "1")
+    net2 = native.Learned(m, seed=3)
+    monkeypatch.delenv("OWTK_GNN_TMA")
+    assert net2.uses_tma
+    v = bf16_weights(bs, 5)
+    net.set_parameters(v)
+    net2.set_parameters(v)
+    rng = np.random.default_rng(3)
+    r = native.Vector(ctx, n, 0, bs).upload(rng.uniform(-1, 1, n * bs))
+    e = native.Vector(ctx, n, 0, bs).upload(rng.uniform(-1, 1, n * bs))
+    y1, y2 = native.Vector(ctx, n, 0, bs), native.Vector(ctx, n, 0, bs)
+    net.apply(r, y1)
+    net2.apply(r, y2)
+    assert_bitwise(y1.download(), y2.download(), "network output")
+    l1, g1 = net.loss_grad(r, e, want_grads=True)
+    l2, g2 = net2.loss_grad(r, e, want_grads=True)
+    assert l1 == l2 and np.array_equal(g1, g2)
+
+
 @pytest.mark.parametrize("weights,loss_tol,cos_min,rel_max", [((1.0, 0.0), 5e-2, 0.99, 0.1),
                                                              ((0.1, 1.0), 0.15, 0.98, 0.2)])
 def test_gradients_match_restatement(native, ctx, weights, loss_tol, cos_min, rel_max):
