@@ -391,6 +391,21 @@ void apply_operator(Matrix& m, Vector& in, Vector& out)
 
 void mixed_apply(Preconditioner& p, Vector& in, Vector& out);
 
+void matrix_layout_check_f64(Matrix& m, Vector& in, Vector& out) { matrix_layout_check<double>(m, in, out); }
+
+bool apply_preconditioner_product(Preconditioner* p, Vector& in, Vector& out, double* product)
+{
+    if (p == nullptr || p->kind != OWTK_PC_LEARNED) {
+        apply_preconditioner(p, in, out);
+        return false;
+    }
+    if (!in.same_layout(out) || in.owned != p->owned || in.ghost != p->ghost || in.bs != p->bs)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
+    if (in.dtype != OWTK_F64 || out.dtype != OWTK_F64)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "the learned preconditioner applies to FP64 vectors");
+    return learned_apply(*p, in, out, product);
+}
+
 void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out)
 {
     if (!in.same_layout(out)) fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");

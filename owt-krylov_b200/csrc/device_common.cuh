@@ -160,6 +160,12 @@ __device__ __forceinline__ std::uint64_t l2_policy_evict_first()
     return p;
 }
 
+// Hint: bring `bytes` (a multiple of 16) from a 16-byte aligned address into L2.
+__device__ __forceinline__ void prefetch_l2(const void* src, std::uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void bulk_load(std::uint32_t dst, const void* src, std::uint32_t bytes,
                                           std::uint32_t bar, std::uint64_t policy)
 {

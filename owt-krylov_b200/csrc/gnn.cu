@@ -69,6 +69,32 @@ __device__ __forceinline__ uint4 f32_to_bf16x8(const float (&f)[8])
     return u;
 }
 
+// w * x + s on the two features held by one 32-bit word of BF16 pairs.
+__device__ __forceinline__ float2 fma_bf16x2(float w, std::uint32_t x, float2 s)
+{
+    return __ffma2_rn(make_float2(w, w), make_float2(__uint_as_float(x << 16), __uint_as_float(x & 0xffff0000u)), s);
+}
+
+__device__ __forceinline__ void accumulate_row(float w, const uint4& f, float2 (&acc)[4])
+{
+    acc[0] = fma_bf16x2(w, f.x, acc[0]);
+    acc[1] = fma_bf16x2(w, f.y, acc[1]);
+    acc[2] = fma_bf16x2(w, f.z, acc[2]);
+    acc[3] = fma_bf16x2(w, f.w, acc[3]);
+}
+
+__device__ __forceinline__ uint4 pack_bf16x8(const float2 (&acc)[4])
+{
+    uint4 u;
+    std::uint32_t* p = reinterpret_cast<std::uint32_t*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const __nv_bfloat162 b = __floats2bfloat162_rn(acc[k].x, acc[k].y);
+        p[k] = *reinterpret_cast<const std::uint32_t*>(&b);
+    }
+    return u;
+}
+
 // ---------------------------------------------------------------- generic GEMM
 // D (M x N, FP32, row-major) = A (M x K, BF16, row-major) * B (N x K, BF16,
 // row-major)^T with M % 128 == 0, N in {64, 128}, K % 64 == 0.  One CTA (4
@@ -154,6 +180,9 @@ struct GraphArgs {
     const float* tr_w;       // w_vu of that edge
     const int* tr_edge;      // index of that edge in the forward (nb) order
     const float* dinv;       // 1 / diagonal, n * bs
+    const int* ell_col;      // first 8 neighbours of v at 8 v.. (padding: -1)
+    const float* ell_w;      // their weights (padding: 0)
+    const unsigned char* tile_ovf;   // 128-row tile holds a row with more than 8 neighbours
 };
 
 // q = r / d in FP32 (the Jacobi step; its norm scales the network's output).
@@ -165,38 +194,43 @@ __global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* _
     if (i < count) q[i] = static_cast<float>(r[i]) * dinv[i];
 }
 
-// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...], one thread
-// per vertex (the weights are read as shared-memory broadcasts).
+// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...].  An 8-lane
+// group per vertex, lane `c8` computing features 8*c8..8*c8+7 (one coalesced
+// 16-byte store each) as packed f32x2 FMAs over the 2 bs nonzero inputs in
+// ascending order; the zero inputs are skipped, which leaves every sum
+// bit-identical to the full 16-term one (fma(w, 0, s) = s, s never -0).
 template<class T>
 __global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
                                                     const double* norms, const float* __restrict__ we,
                                                     bf16* __restrict__ h0)
 {
-    __shared__ float w[kH * kF];
-    for (int i = threadIdx.x; i < kH * kF; i += blockDim.x) w[i] = we[i];
+    __shared__ __align__(16) float wt[kF * kH];   // transposed: wt[f * 64 + k] = We[k][f]
+    for (int j = threadIdx.x; j < kH * kF; j += blockDim.x) wt[j] = we[(j % kH) * kF + j / kH];
     __syncthreads();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= g.n) return;
     const double root = sqrt(static_cast<double>(g.n) * g.bs), nr = norms[0], nq = norms[2];
     const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
     const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
-    float x[kF];
-    const long long vb = static_cast<long long>(v) * g.bs;
+    const int nf = 2 * g.bs;
+    const long long total = 8ll * g.n, stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const int v = static_cast<int>(t >> 3), c8 = static_cast<int>(t & 7);
+        const long long vb = static_cast<long long>(v) * g.bs;
+        float2 acc[4] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f),
+                         make_float2(0.0f, 0.0f)};
 #pragma unroll
-    for (int f = 0; f < kF; ++f)
-        x[f] = f < g.bs ? static_cast<float>(r[vb + f]) * inv_r : (f < 2 * g.bs ? q[vb + f - g.bs] * inv_q : 0.0f);
-    uint4* out = reinterpret_cast<uint4*>(h0 + static_cast<long long>(v) * kH);
-#pragma unroll
-    for (int c8 = 0; c8 < kH / 8; ++c8) {
-        float o[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int f = 0; f < kF; ++f) acc = fmaf(w[(c8 * 8 + i) * kF + f], x[f], acc);
-            o[i] = acc;
+        for (int f = 0; f < kF; ++f) {
+            if (f < nf) {
+                const float x = f < g.bs ? static_cast<float>(r[vb + f]) * inv_r : q[vb + f - g.bs] * inv_q;
+                const float4* wp = reinterpret_cast<const float4*>(wt + f * kH + c8 * 8);
+                const float4 wa = wp[0], wb = wp[1];
+                const float2 xx = make_float2(x, x);
+                acc[0] = __ffma2_rn(make_float2(wa.x, wa.y), xx, acc[0]);
+                acc[1] = __ffma2_rn(make_float2(wa.z, wa.w), xx, acc[1]);
+                acc[2] = __ffma2_rn(make_float2(wb.x, wb.y), xx, acc[2]);
+                acc[3] = __ffma2_rn(make_float2(wb.z, wb.w), xx, acc[3]);
+            }
         }
-        out[c8] = f32_to_bf16x8(o);
+        reinterpret_cast<uint4*>(h0 + static_cast<long long>(v) * kH)[c8] = pack_bf16x8(acc);
     }
 }
 
@@ -230,30 +264,80 @@ __global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __
     }
     if (live && c8 < g.bs) {
         const long long o = static_cast<long long>(v) * g.bs + c8;
-        out[o] = static_cast<O>(norms[0] > 0.0 ? q[o] + s * mine : 0.0f);
+        out[o] = static_cast<O>(norms[0] > 0.0 ? fmaf(s, mine, q[o]) : 0.0f);
     }
 }
 
-// One message-passing layer, fused: for each 128-row tile, gather [h | m]
-// (m_v = sum_u w_vu h_u in FP32, rounded to BF16) into swizzled shared
-// memory, Y = [h | m] Wl^T by eight K=16 tensor-core MMAs into TMEM, then
-// h_out = h + relu(Y) from TMEM.  Training also keeps m (BF16) and the sign
-// mask of Y (one 64-bit word per row) for the backward pass.
+// One message-passing layer, fused.  Per 128-row tile:
+//  * the tile's own rows h arrive by one 2D TMA load whose 128-byte swizzle
+//    is the MMA's K-major operand layout, issued while the previous tile
+//    finishes (and the tile after next has its index rows prefetched to L2);
+//  * each warp aggregates m_v = sum_u w_vu h_u for 32 rows, four at a time
+//    (an 8-lane group per row, lane `chunk` owning features 8*chunk..+7), over
+//    the rows' padded 8-slot neighbour lists: lane `chunk` loads slot
+//    `chunk`'s index and weight two row steps ahead and the group shares them
+//    by shuffles; the neighbours' 16-byte feature chunks are gathered in
+//    quarter steps of two slots through a register ring kGatherDepth quarter
+//    steps ahead of their use; the FP32 sums run as packed f32x2 FMAs and m
+//    is rounded to BF16 into the swizzled second operand block;
+//  * eight K=16 MMAs give Y = [h | m] Wl^T in TMEM and the epilogue writes
+//    h + relu(Y) (or, for the last layer of an inference pass, the decoder's
+//    output straight from the rounded rows).
+// Padding slots (index -1) load nothing and carry weight 0: fma(0, x, s) = s
+// for the finite chunk x their registers still hold and a running sum that
+// is never -0, so the sums are bit-identical to skipping the slot.  Rows with
+// more than 8 neighbours continue from their CSR list in the same edge order
+// (their tiles are flagged on the host).  Training also keeps m (BF16) and
+// the sign mask of Y (one 64-bit word per row) for the backward pass.
+constexpr int kEll = 8;            // padded neighbour slots per row
+#ifndef OWTK_GNN_DEPTH
+#define OWTK_GNN_DEPTH 8
+#endif
+constexpr int kGatherDepth = OWTK_GNN_DEPTH;   // quarter steps (2 slots) in flight per warp
 constexpr int kLayerThreads = 128;
 constexpr int kLayerSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128;   // A: [h | m], B: Wl
 
-template<bool TRAIN>
+#ifndef OWTK_GNN_LDOP
+#define OWTK_GNN_LDOP ".nc"
+#endif
+// Chunk `chunk` of feature row u into d when u >= 0 (a padding slot, u < 0,
+// leaves d as it is).
+__device__ __forceinline__ void load_slot(uint4& d, const bf16* h, int u, int chunk)
+{
+    const uint4* p = reinterpret_cast<const uint4*>(h + static_cast<long long>(u) * kH) + chunk;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ge.s32 p, %4, 0;\n\t"
+        "@p ld.global" OWTK_GNN_LDOP ".v4.u32 {%0, %1, %2, %3}, [%5];\n\t}"
+        : "+r"(d.x), "+r"(d.y), "+r"(d.z), "+r"(d.w)
+        : "r"(u), "l"(p));
+}
+
+// The decoder fused into the last layer (inference): out = q + rms(q) (h Wd^T)
+// from the epilogue's rounded rows, with the sums of k_gnn_decode in the same
+// order (per 8-feature chunk, then the pairwise tree over the chunks).
+template<class O>
+struct DecodeArgs {
+    const float* q;
+    const double* norms;
+    const float* wd;
+    O* out;
+};
+
+template<bool TRAIN, bool DECODE = false, class O = float>
 __global__ void __launch_bounds__(kLayerThreads, 4)
-    k_gnn_layer(GraphArgs g, const bf16* __restrict__ h_in, const bf16* __restrict__ wl, bf16* __restrict__ h_out,
-                bf16* __restrict__ m_out, unsigned long long* __restrict__ mask_out, unsigned* status)
+    k_gnn_layer(GraphArgs g, const __grid_constant__ CUtensorMap tmap_in, const __grid_constant__ CUtensorMap tmap_out,
+                const bf16* __restrict__ h_in, const bf16* __restrict__ wl, bf16* __restrict__ m_out,
+                unsigned long long* __restrict__ mask_out, DecodeArgs<O> dec, unsigned* status)
 {
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) std::uint64_t bar_storage;
+    __shared__ __align__(8) std::uint64_t bar_storage[2];   // [0] MMAs done, [1] own rows landed
     __shared__ std::uint32_t tmem_base_s;
+    __shared__ float wd_s[DECODE ? 8 * kH : 1];
     const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
     unsigned char* tile = smem_raw + (base - raw);                 // A0 (h), A1 (m), B0, B1
     const std::uint32_t a0 = base, a1 = base + kTile * 128, b0 = base + 2 * kTile * 128, b1 = b0 + kH * 128;
-    const std::uint32_t bar = smem_u32(&bar_storage);
+    const std::uint32_t bar = smem_u32(&bar_storage[0]), bar_h = smem_u32(&bar_storage[1]);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = (g.n + kTile - 1) / kTile;
 
@@ -263,8 +347,16 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         const uint4 v = *reinterpret_cast<const uint4*>(wl + r * 128 + c16 * 8);
         *reinterpret_cast<uint4*>(tile + 2 * kTile * 128 + (c16 >> 3) * kH * 128 + sw128(r, c16 & 7)) = v;
     }
+    float dec_scale = 0.0f;
+    bool dec_live = false;
+    if (DECODE) {
+        for (int i = threadIdx.x; i < g.bs * kH; i += kLayerThreads) wd_s[i] = dec.wd[i];
+        dec_scale = static_cast<float>(dec.norms[2] / sqrt(static_cast<double>(g.n) * g.bs));
+        dec_live = dec.norms[0] > 0.0;
+    }
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
+        mbar_init(bar_h, 1);
         fence_proxy_async_smem();
     }
     if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kH);
@@ -273,102 +365,102 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     tmem_fence_after_sync();
     const std::uint32_t tmem = tmem_base_s;
     constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, kH);
+    // Own rows of `t` into A0 (rows past n read as zeros); the index rows of
+    // the tile after it towards L2.
+    const auto stage_tile = [&](int t) {
+        if (t < ntiles) {
+            mbar_arrive_expect_tx(bar_h, kTile * 128);
+            tma_load_2d(a0, &tmap_in, 0, t * kTile, bar_h);
+        }
+        const int tn = t + static_cast<int>(gridDim.x);
+        if (tn < ntiles) {
+            const std::uint32_t bytes = static_cast<std::uint32_t>(min(kTile, g.n - tn * kTile)) * kEll * 4;
+            prefetch_l2(g.ell_col + static_cast<long long>(tn) * kTile * kEll, bytes);
+            prefetch_l2(g.ell_w + static_cast<long long>(tn) * kTile * kEll, bytes);
+        }
+    };
+    if (threadIdx.x == 0) stage_tile(blockIdx.x);
     const int grp = lane >> 3, chunk = lane & 7;   // 4 rows at a time, 8 lanes x 16 bytes per row
     int iter = 0;
-    bool ok = true;
+    bool ok = true, h_pending = blockIdx.x < ntiles;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++iter) {
         const int row0 = t * kTile;
-        // ---- gather [h | m]
-        // Lane L of the warp holds the neighbour range of the warp's row L;
-        // 8-lane groups take one row per step (lane `chunk` owns features
-        // 8*chunk..8*chunk+7), load the row's first 8 neighbour indices and
-        // weights cooperatively (one lane each) and broadcast them; the next
-        // step's index loads are issued before this step's feature gathers.
-        const int wrow0 = row0 + 32 * warp;
-        int p0 = 0, p1 = 0;
-        if (wrow0 + lane < g.n) {
-            p0 = g.nb_ptr[wrow0 + lane];
-            p1 = g.nb_ptr[wrow0 + lane + 1];
+        const bool overflow = g.tile_ovf[t] != 0;
+        // ---- m: row step s (0..7) covers rows 32*warp + 4*s + grp; its 8
+        // slots are gathered as 4 quarter steps of 2 slots, issued kGatherDepth
+        // quarter steps ahead of their accumulation through a register ring.
+        // Lane `chunk` of a group loads the row's slot `chunk` (index and
+        // weight, two row steps ahead of its first gather) and shares it by
+        // shuffles.
+        const int first = row0 + 32 * warp + grp;
+        const auto ell_at = [&](int s) { return static_cast<long long>(min(first + 4 * s, g.n - 1)) * kEll + chunk; };
+        constexpr int kQuarters = 4 * 8;
+        int ecol[8];
+        float ew[8];
+        // A padding slot loads nothing (weight 0): it keeps a chunk gathered
+        // earlier in this tile or these zeros.
+        uint4 ring[kGatherDepth + 1][2];
+#pragma unroll
+        for (int i = 0; i <= kGatherDepth; ++i) ring[i][0] = ring[i][1] = make_uint4(0, 0, 0, 0);
+        const auto load_ell = [&](int s) {
+            ecol[s & 7] = __ldg(g.ell_col + ell_at(s));
+            ew[s & 7] = __ldg(g.ell_w + ell_at(s));
+        };
+        const auto issue = [&](int k) {   // quarter k: slots 2*(k&3), +1 of row step k>>2
+            const int s = k >> 2;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int u = __shfl_sync(0xffffffffu, ecol[s & 7], (lane & ~7) + 2 * (k & 3) + j);
+                load_slot(ring[k % (kGatherDepth + 1)][j], h_in, u, chunk);
+            }
+        };
+        static_assert(kGatherDepth >= 1 && kGatherDepth <= 20, "index ring holds 8 row steps");
+        load_ell(0);
+        load_ell(1);
+        load_ell(2);
+#pragma unroll
+        for (int k = 0; k < kGatherDepth; ++k) {
+            if ((k & 3) == 0 && k > 0 && (k >> 2) + 2 < 8) load_ell((k >> 2) + 2);
+            issue(k);
         }
-        // Software pipeline over the 8 row-steps: indices two steps ahead,
-        // neighbour features one step ahead of the accumulation.
-        struct Idx {
-            int col, e0, e1;
-            float w;
-        };
-        struct Got {
-            uint4 nv[8];
-            uint4 hv;
-        };
-        auto load_idx = [&](int it) {
-            Idx x;
-            const int src = 4 * it + grp;
-            x.e0 = __shfl_sync(0xffffffffu, p0, src);
-            x.e1 = __shfl_sync(0xffffffffu, p1, src);
-            x.col = 0;
-            x.w = 0.0f;
-            if (x.e0 + chunk < x.e1) {
-                x.col = g.nb_col[x.e0 + chunk];
-                x.w = g.nb_w[x.e0 + chunk];
+        float2 acc[4];
+#pragma unroll
+        for (int k = 0; k < kQuarters; ++k) {
+            const int kn = k + kGatherDepth;
+            if (kn < kQuarters) {
+                if ((kn & 3) == 0 && (kn >> 2) + 2 < 8) load_ell((kn >> 2) + 2);
+                issue(kn);
             }
-            return x;
-        };
-        auto gather = [&](int it, const Idx& x, Got& d) {
-            const int v = row0 + 32 * warp + 4 * it + grp, deg = x.e1 - x.e0;
+            const int s = k >> 2;
+            if ((k & 3) == 0)
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int u = __shfl_sync(0xffffffffu, x.col, (lane & ~7) + q);
-                d.nv[q] = make_uint4(0, 0, 0, 0);
-                if (q < deg) d.nv[q] = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8);
-            }
-            d.hv = make_uint4(0, 0, 0, 0);
-            if (v < g.n) d.hv = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(v) * kH + chunk * 8);
-        };
-        Idx ia = load_idx(0), ib = load_idx(1);
-        Got da, db;
-        gather(0, ia, da);
-#pragma unroll 1
-        for (int it = 0; it < 8; ++it) {
-            Idx ic = ia;
-            if (it + 2 < 8) ic = load_idx(it + 2);
-            if (it + 1 < 8) gather(it + 1, ib, db);
-            const int r = 32 * warp + 4 * it + grp, v = row0 + r;
-            const int deg = ia.e1 - ia.e0;
-            uint4 mv = make_uint4(0, 0, 0, 0);
-            float ws[8];
+                for (int i = 0; i < 4; ++i) acc[i] = make_float2(0.0f, 0.0f);
 #pragma unroll
-            for (int q = 0; q < 8; ++q) ws[q] = __shfl_sync(0xffffffffu, ia.w, (lane & ~7) + q);
-            if (v < g.n) {
-                float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    if (q < deg) {
-                        float f[8];
-                        bf16x8_to_f32(da.nv[q], f);
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) acc[i] = fmaf(ws[q], f[i], acc[i]);
-                    }
+            for (int j = 0; j < 2; ++j)
+                accumulate_row(__shfl_sync(0xffffffffu, ew[s & 7], (lane & ~7) + 2 * (k & 3) + j),
+                               ring[k % (kGatherDepth + 1)][j], acc);
+            if ((k & 3) == 3) {
+                const int r = 32 * warp + 4 * s + grp, v = row0 + r;
+                if (overflow && v < g.n) {   // rows with more than 8 neighbours
+                    const int e1 = g.nb_ptr[v + 1];
+                    for (int e = g.nb_ptr[v] + kEll; e < e1; ++e)
+                        accumulate_row(g.nb_w[e], __ldg(reinterpret_cast<const uint4*>(
+                                                            h_in + static_cast<long long>(g.nb_col[e]) * kH) + chunk),
+                                       acc);
                 }
-                for (int e = ia.e0 + 8; e < ia.e1; ++e) {   // rows with more than 8 neighbours
-                    const int u = g.nb_col[e];
-                    const float we = g.nb_w[e];
-                    float f[8];
-                    bf16x8_to_f32(*reinterpret_cast<const uint4*>(h_in + static_cast<long long>(u) * kH + chunk * 8), f);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) acc[i] = fmaf(we, f[i], acc[i]);
+                uint4 mv = make_uint4(0, 0, 0, 0);
+                if (v < g.n) {
+                    mv = pack_bf16x8(acc);
+                    if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
                 }
-                mv = f32_to_bf16x8(acc);
-                if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
+                *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, chunk)) = mv;
             }
-            *reinterpret_cast<uint4*>(tile + sw128(r, chunk)) = da.hv;
-            *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, chunk)) = mv;
-            ia = ib;
-            ib = ic;
-            da = db;
         }
         fence_proxy_async_smem();
+        ok = wait_phase(bar_h, iter & 1);
+        h_pending = !ok;
         tmem_fence_before_sync();
-        __syncthreads();
+        if (!__syncthreads_and(ok)) break;
         // ---- Y = [h | m] Wl^T
         if (threadIdx.x == 0) {
             tmem_fence_after_sync();
@@ -406,15 +498,52 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
             }
         }
         if (v < g.n) {
-            uint4* o = reinterpret_cast<uint4*>(h_out + static_cast<long long>(v) * kH);
+            if (DECODE) {
+                const long long o0 = static_cast<long long>(v) * g.bs;
+#pragma unroll 1
+                for (int c = 0; c < g.bs; ++c) {
+                    float part[8];   // per 8-feature chunk, then the pairwise tree
 #pragma unroll
-            for (int c8 = 0; c8 < 8; ++c8) o[c8] = outv[c8];
-            if (TRAIN) mask_out[v] = mask;
+                    for (int c8 = 0; c8 < 8; ++c8) {
+                        float f[8];
+                        bf16x8_to_f32(outv[c8], f);
+                        float p = 0.0f;
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) p = fmaf(wd_s[c * kH + c8 * 8 + i], f[i], p);
+                        part[c8] = p;
+                    }
+                    const float y = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
+                    dec.out[o0 + c] = static_cast<O>(dec_live ? fmaf(dec_scale, y, dec.q[o0 + c]) : 0.0f);
+                }
+            } else if (TRAIN) {
+                mask_out[v] = mask;
+            }
+        }
+        if (!DECODE) {
+            // The new rows replace the old ones in A0 (each thread its own
+            // row) and leave as one TMA tile store.
+#pragma unroll
+            for (int c8 = 0; c8 < 8; ++c8) *reinterpret_cast<uint4*>(tile + sw128(r, c8)) = outv[c8];
+            fence_proxy_async_smem();
         }
         tmem_fence_before_sync();
         __syncthreads();
+        // A0 is free once the store has read it: the next tile's own rows.
+        if (threadIdx.x == 0) {
+            if (!DECODE) {
+                tma_store_2d(&tmap_out, a0, 0, row0);
+                bulk_wait_read();
+            }
+            fence_proxy_async_smem();
+            stage_tile(t + static_cast<int>(gridDim.x));
+        }
+        h_pending = t + static_cast<int>(gridDim.x) < ntiles;
     }
-    if (!ok && threadIdx.x == 0) atomicOr(status, kErrTimeout);
+    if (!ok && threadIdx.x == 0) {
+        atomicOr(status, kErrTimeout);
+        if (h_pending) wait_phase(bar_h, iter & 1);   // let an own-row copy in flight land
+    }
+    if (!DECODE && threadIdx.x == 0) bulk_wait_all();
     tmem_fence_before_sync();
     __syncthreads();
     if (warp == 0) tmem_free(tmem, kH);
@@ -1103,7 +1232,7 @@ __global__ void k_gnn_gather_w(int count, const int* __restrict__ idx, const flo
                                float* __restrict__ dst)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) dst[i] = src[idx[i]];
+    if (i < count) dst[i] = idx[i] >= 0 ? src[idx[i]] : 0.0f;
 }
 
 }  // namespace gnn
@@ -1120,6 +1249,7 @@ struct Gnn {
     Matrix* matrix = nullptr;
     int n = 0, bs = 0;
     DeviceBuffer nb_ptr, nb_col, nb_w, nb_entry, tr_ptr, tr_col, tr_w, tr_edge, dinv;
+    DeviceBuffer ell_col, ell_src, ell_w, tile_ovf;   // padded 8-slot neighbour lists (forward layer)
     DeviceBuffer params, grads, adam_m, adam_v, wl16, wlt16;
     DeviceBuffer h[gnn::kLayers + 1], m[gnn::kLayers], mask[gnn::kLayers], x;   // training activations
     DeviceBuffer ha, hb;                                                       // inference ping-pong
@@ -1150,6 +1280,9 @@ struct Gnn {
         g.tr_w = tr_w.as<float>();
         g.tr_edge = tr_edge.as<int>();
         g.dinv = dinv.as<float>();
+        g.ell_col = ell_col.as<int>();
+        g.ell_w = ell_w.as<float>();
+        g.tile_ovf = tile_ovf.as<unsigned char>();
         return g;
     }
     unsigned blocks(long long count, int threads = 256) const
@@ -1178,6 +1311,8 @@ void gnn_set_attrs()
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kLayerSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kLayerSmem));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<false, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kLayerSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kBwdSmem));
@@ -1242,14 +1377,12 @@ void gnn_forward(Gnn& G, const T* r, O* out)
     const gnn::GraphArgs g = G.graph();
     const long long nb = static_cast<long long>(G.n) * G.bs;
     double* norms = G.norm_r.as<double>();
-    gnn::k_gnn_prepare<T><<<G.blocks(nb), 256, 0, c.stream>>>(nb, r, G.dinv.as<float>(), G.qbuf.as<float>());
-    kern::norm<T>(c, static_cast<std::size_t>(nb), r, norms, norms + 1);
-    kern::norm<float>(c, static_cast<std::size_t>(nb), G.qbuf.as<float>(), norms + 2, norms + 3);
+    kern::prepare_norms<T>(c, static_cast<std::size_t>(nb), r, G.dinv.as<float>(), G.qbuf.as<float>(), norms);
     gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
-    gnn::k_gnn_encode<T><<<G.blocks(G.n), 256, 0, c.stream>>>(g, r, G.qbuf.as<float>(), norms,
-                                                               G.params.as<float>() + Gnn::kOffWe, h0);
+    gnn::k_gnn_encode<T><<<std::min(G.blocks(8ll * G.n), static_cast<unsigned>(c.sm_count * 8)), 256, 0, c.stream>>>(
+        g, r, G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
     OWTK_CUDA(cudaGetLastError());
-    c.launched(2);
+    c.launched();
     const gnn::bf16* hin = h0;
     for (int l = 0; l < gnn::kLayers; ++l) {
         gnn::bf16* hout = TRAIN ? G.h[l + 1].as<gnn::bf16>() : (l % 2 == 0 ? G.hb : G.ha).as<gnn::bf16>();
@@ -1264,9 +1397,24 @@ void gnn_forward(Gnn& G, const T* r, O* out)
                 G.quads.as<int4>(), G.quad_ptr.as<int>(), G.metas.as<int4>(),
                 static_cast<int>(G.nb_col.bytes / sizeof(int)), c.status.as<unsigned>());
         } else {
+            const CUtensorMap& tm = TRAIN ? G.tmap_h[l] : (l % 2 == 0 ? G.tmap_a : G.tmap_b);
+            const gnn::bf16* wl = G.wl16.as<gnn::bf16>() + l * Gnn::kLayerW;
+            if constexpr (!TRAIN) {
+              if (l == gnn::kLayers - 1) {   // last layer with the decoder fused
+                const gnn::DecodeArgs<O> dec{G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWd, out};
+                gnn::k_gnn_layer<false, true, O><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
+                    g, tm, tm, hin, wl, nullptr, nullptr, dec, c.status.as<unsigned>());
+                OWTK_CUDA(cudaGetLastError());
+                c.launched();
+                ++G.applications;
+                return;
+              }
+            }
+            const CUtensorMap& tmo = TRAIN ? G.tmap_h[l + 1] : (l % 2 == 0 ? G.tmap_b : G.tmap_a);
             gnn::k_gnn_layer<TRAIN><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
-                g, hin, G.wl16.as<gnn::bf16>() + l * Gnn::kLayerW, hout, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
-                TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, c.status.as<unsigned>());
+                g, tm, tmo, hin, wl, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
+                TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, gnn::DecodeArgs<float>{},
+                c.status.as<unsigned>());
         }
         OWTK_CUDA(cudaGetLastError());
         c.launched();
@@ -1284,9 +1432,9 @@ void gnn_train_buffers(Gnn& G)
     if (G.train_ready) return;
     const std::size_t rows = static_cast<std::size_t>(G.n);
     for (auto& b : G.h) b.allocate(rows * gnn::kH * 2 + 16);
-    if (G.tma)
-        for (int l = 0; l <= gnn::kLayers; ++l)
-            if (!gnn_encode_maps(G.h[l].ptr, G.n, G.gmap_h[l], G.tmap_h[l])) G.tma = false;
+    for (int l = 0; l <= gnn::kLayers; ++l)
+        if (!gnn_encode_maps(G.h[l].ptr, G.n, G.gmap_h[l], G.tmap_h[l]))
+            fail(OWTK_ERR_CUDA, "tensor-map encoding of the training activations failed");
     for (auto& b : G.m) b.allocate(rows * gnn::kH * 2 + 16);
     for (auto& b : G.mask) b.allocate(rows * 8 + 16);
     G.x.allocate(rows * gnn::kF * 4 + 16);
@@ -1415,7 +1563,7 @@ namespace owtk {
 
 // z = M(v); judged by ||v - A z|| against ||v||, the fallback steps in when
 // the network does not reduce the residual.
-void learned_apply(Preconditioner& p, Vector& in, Vector& out)
+bool learned_apply(Preconditioner& p, Vector& in, Vector& out, double* product)
 {
     Gnn& G = *p.net;
     Context& c = *G.ctx;
@@ -1429,9 +1577,14 @@ void learned_apply(Preconditioner& p, Vector& in, Vector& out)
     }
     gnn_forward<double, double, false>(G, x, y);
     ++p.learned_applications;
-    if (p.fallback == nullptr) return;
-    if (!p.check_work.ptr) p.check_work.allocate(n * sizeof(double) + 16);
-    double* w = p.check_work.as<double>();
+    if (p.fallback == nullptr) return false;
+    // The check's product A z is the solver's next operator application: it
+    // lands in `product` when the caller asks for it.
+    double* w = product;
+    if (w == nullptr) {
+        if (!p.check_work.ptr) p.check_work.allocate(n * sizeof(double) + 16);
+        w = p.check_work.as<double>();
+    }
     kern::spmv<double>(c, *G.matrix, y, w);
     constexpr int kSlot = kScalarSlots - 4;
     kern::residual_norms(c, n, x, w, c.dev_scalar_copy.as<double>() + kSlot, c.dev_scalars + kSlot);
@@ -1448,8 +1601,12 @@ void learned_apply(Preconditioner& p, Vector& in, Vector& out)
         src.data = const_cast<double*>(x);
         src.is_view = true;
         apply_preconditioner(p.fallback, src, out);
+        return false;
     }
+    return product != nullptr;
 }
+
+const Matrix* learned_matrix(const Preconditioner& p) { return p.net ? p.net->matrix : nullptr; }
 
 namespace {
 
@@ -1472,8 +1629,11 @@ void gnn_bind_matrix(Gnn& G, Matrix& m)
     if (ne > 0)
         gnn::k_gnn_gather_w<<<G.blocks(ne), 256, 0, c.stream>>>(ne, G.tr_edge.as<int>(), G.nb_w.as<float>(),
                                                                 G.tr_w.as<float>());
+    const int slots = G.n * gnn::kEll;
+    gnn::k_gnn_gather_w<<<G.blocks(slots), 256, 0, c.stream>>>(slots, G.ell_src.as<int>(), G.nb_w.as<float>(),
+                                                               G.ell_w.as<float>());
     OWTK_CUDA(cudaGetLastError());
-    c.launched(2);
+    c.launched(3);
     c.sync();
     G.matrix = &m;
 }
@@ -1608,12 +1768,36 @@ owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** ou
             G->metas = owtk::upload(st, metas);
         }
         G->nb_col.bytes = nb_col.size() * sizeof(int);
-        // The register-gather layer is the default: on the 2M-vertex mesh the
-        // TMA-fed layer measured about twice its time per launch.
+        // Padded 8-slot neighbour lists of the forward layer: the first 8
+        // neighbours in edge order, padding slots -1 (weight 0; the weights
+        // are filled from the edge weights on every matrix bind).
+        {
+            const int tiles = (G->n + owtk::gnn::kTile - 1) / owtk::gnn::kTile;
+            std::vector<std::int32_t> ell_col(static_cast<std::size_t>(G->n) * owtk::gnn::kEll),
+                ell_src(ell_col.size());
+            std::vector<std::uint8_t> tile_ovf(tiles, 0);
+            for (int v = 0; v < G->n; ++v) {
+                const int e0 = nb_ptr[v], deg = nb_ptr[v + 1] - e0;
+                for (int q = 0; q < owtk::gnn::kEll; ++q) {
+                    const std::size_t i = static_cast<std::size_t>(v) * owtk::gnn::kEll + q;
+                    ell_col[i] = q < deg ? nb_col[e0 + q] : -1;
+                    ell_src[i] = q < deg ? e0 + q : -1;
+                }
+                if (deg > owtk::gnn::kEll) tile_ovf[v / owtk::gnn::kTile] = 1;
+            }
+            G->ell_col = owtk::upload(st, ell_col);
+            G->ell_src = owtk::upload(st, ell_src);
+            G->tile_ovf = owtk::upload(st, tile_ovf);
+            G->ell_w.allocate(ell_col.size() * sizeof(float) + 16);
+        }
+        // Tensor maps of the ping-pong feature buffers (own-row tiles of the
+        // layer).  The register-gather layer is the default: on the 2M-vertex
+        // mesh the TMA-gather layer measured about twice its time per launch.
+        if (!owtk::gnn_encode_maps(G->ha.ptr, G->n, G->gmap_a, G->tmap_a)
+            || !owtk::gnn_encode_maps(G->hb.ptr, G->n, G->gmap_b, G->tmap_b))
+            owtk::fail(OWTK_ERR_CUDA, "tensor-map encoding of the feature buffers failed");
         const char* tma_env = std::getenv("OWTK_GNN_TMA");
-        G->tma = tma_env && tma_env[0] == '1'
-            && owtk::gnn_encode_maps(G->ha.ptr, G->n, G->gmap_a, G->tmap_a)
-            && owtk::gnn_encode_maps(G->hb.ptr, G->n, G->gmap_b, G->tmap_b);
+        G->tma = tma_env && tma_env[0] == '1';
         G->qbuf.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
         owtk::gnn_set_attrs();
         owtk::gnn_pack(*G);

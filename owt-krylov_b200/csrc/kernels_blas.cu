@@ -556,6 +556,94 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
     }
 }
 
+// q = r / d (FP32) with ||r|| and ||q|| in the same pass: the learned
+// preconditioner's input scaling.  Same per-thread order, CTA merge and fixed
+// combine order as k_norm over each array, so both norms equal k_norm's.
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_prepare_norms(std::size_t n, const T* __restrict__ r,
+                                                            const float* __restrict__ dinv, float* __restrict__ q,
+                                                            double* partials, unsigned* ticket, double* norms)
+{
+    ScaledSum a{0.0, 0.0, 0}, b{0.0, 0.0, 0};
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    constexpr int kU = 8;
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += kU * stride) {
+        double va[kU], vb[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const std::size_t idx = i + u * stride;
+            va[u] = 0.0;
+            vb[u] = 0.0;
+            if (idx < n) {
+                const T rv = r[idx];
+                const float qv = static_cast<float>(rv) * dinv[idx];
+                q[idx] = qv;
+                va[u] = static_cast<double>(rv);
+                vb[u] = static_cast<double>(qv);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            norm_push(a, va[u]);
+            norm_push(b, vb[u]);
+        }
+    }
+    a = norm_warp(a);
+    b = norm_warp(b);
+    __shared__ ScaledSum red[2][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ScaledSum s0 = red[0][0], s1 = red[1][0];
+        for (int w = 1; w < kThreads / 32; ++w) {
+            s0 = norm_merge(s0, red[0][w]);
+            s1 = norm_merge(s1, red[1][w]);
+        }
+        double* p = partials + 6 * blockIdx.x;
+        p[0] = s0.scale;
+        p[1] = s0.ssq;
+        p[2] = s0.nan;
+        p[3] = s1.scale;
+        p[4] = s1.ssq;
+        p[5] = s1.nan;
+    }
+    if (last_block(ticket)) {
+        __threadfence();
+        ScaledSum t0{0.0, 0.0, 0}, t1{0.0, 0.0, 0};
+        for (unsigned k = threadIdx.x; k < gridDim.x; k += kThreads) {
+            const double* p = partials + 6 * k;
+            t0 = norm_merge(t0, ScaledSum{__ldcg(p), __ldcg(p + 1), __ldcg(p + 2) != 0.0});
+            t1 = norm_merge(t1, ScaledSum{__ldcg(p + 3), __ldcg(p + 4), __ldcg(p + 5) != 0.0});
+        }
+        t0 = norm_warp(t0);
+        t1 = norm_warp(t1);
+        __syncthreads();
+        if (lane == 0) {
+            red[0][warp] = t0;
+            red[1][warp] = t1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                ScaledSum s = red[j][0];
+                for (int w = 1; w < kThreads / 32; ++w) s = norm_merge(s, red[j][w]);
+                double v;
+                if (s.nan) v = __longlong_as_double(0x7ff8000000000000LL);
+                else if (s.scale == 0.0 || isinf(s.scale)) v = s.scale;
+                else v = s.scale * sqrt(s.ssq);
+                norms[2 * j] = v;
+                norms[2 * j + 1] = v;
+            }
+            *ticket = 0;
+        }
+    }
+}
+
 // ||x - w|| and ||x|| in one pass (the learned preconditioner's residual
 // check), same one-pass scaled sums and fixed combine order as k_norm.
 __global__ void __launch_bounds__(kThreads) k_residual_norms(std::size_t n, const double* __restrict__ x,
@@ -744,6 +832,16 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }
+
+template<class T>
+void prepare_norms(Context& c, std::size_t n, const T* r, const float* dinv, float* q, double* norms)
+{
+    const unsigned blocks = reduce_blocks(c, n);
+    k_prepare_norms<T><<<blocks, kThreads, 0, c.stream>>>(n, r, dinv, q, partials_of(c), ticket_of(c), norms);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+template void prepare_norms<double>(Context&, std::size_t, const double*, const float*, float*, double*);
 
 void residual_norms(Context& c, std::size_t n, const double* x, const double* w, double* out_dev, double* out_host)
 {

@@ -212,7 +212,10 @@ struct Preconditioner {
     std::uint64_t learned_applications = 0, learned_fallbacks = 0;
     DeviceBuffer check_work, alias_copy;
 };
-void learned_apply(Preconditioner& p, struct Vector& in, struct Vector& out);   // gnn.cu
+// gnn.cu.  With `product` non-null, returns true when it also holds A z for
+// the network's own matrix (no fallback was taken).
+bool learned_apply(Preconditioner& p, struct Vector& in, struct Vector& out, double* product = nullptr);
+const Matrix* learned_matrix(const Preconditioner& p);
 
 
 // ---------------------------------------------------------------- setup (setup.cpp)
@@ -266,6 +269,9 @@ template<class T> void multidot(Context& c, std::size_t n, int k, const T* const
 template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_dev, double* out_host);
 // ||x - w|| and ||x|| (two results) in one pass.
 void residual_norms(Context& c, std::size_t n, const double* x, const double* w, double* out_dev, double* out_host);
+// q = r / d (FP32 q, FP32 1/d) with norms[0] = norms[1] = ||r||, norms[2] = norms[3] = ||q||.
+template<class T>
+void prepare_norms(Context& c, std::size_t n, const T* r, const float* dinv, float* q, double* norms);
 template<class T> void jacobi(Context& c, std::size_t n, const T* inv, const T* in, T* out);
 template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y);
 template<class T> void gather_values(Context& c, std::size_t entries, std::size_t bs,
@@ -288,6 +294,9 @@ void block_ilu_apply(Context& c, Preconditioner& p, const double* in, double* ou
 // Operator / preconditioner application on device vectors (capi.cu).
 void apply_operator(Matrix& m, Vector& in, Vector& out);
 void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out);
+// apply_preconditioner that may also return A out (see learned_apply).
+bool apply_preconditioner_product(Preconditioner* p, Vector& in, Vector& out, double* product);
+void matrix_layout_check_f64(Matrix& m, Vector& in, Vector& out);
 
 // Solver recurrences (solvers.cpp).
 void solve(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& rhs, Vector& x,

@@ -49,6 +49,25 @@ struct Engine {
 
     void op(Vector& in, Vector& out) { apply_operator(A, in, out); ++res.operator_applications; }
     void pc(Vector& in, Vector& out) { apply_preconditioner(M, in, out); ++res.preconditioner_applications; }
+    // out = M in, then az = A out.  The learned preconditioner bound to this
+    // operator forms A out for its residual check; it then writes it to az
+    // (the same SpMV, so the same bits) and the second product is skipped.
+    void pc_op(Vector& in, Vector& out, Vector& az)
+    {
+        if (M != nullptr && M->kind == OWTK_PC_LEARNED && learned_matrix(*M) == &A && A.dtype == OWTK_F64
+            && az.dtype == OWTK_F64 && az.same_layout(in)) {
+            matrix_layout_check_f64(A, out, az);
+            ++res.preconditioner_applications;
+            if (apply_preconditioner_product(M, in, out, static_cast<double*>(az.data))) {
+                ++res.operator_applications;
+                return;
+            }
+            op(out, az);
+            return;
+        }
+        pc(in, out);
+        op(out, az);
+    }
 
     // k dot products of (a[j], b[j]) in one pass; values in slots [slot, slot+k).
     void dots(int k, Vector* const* a, Vector* const* b, int slot = kSlotA)
@@ -542,8 +561,7 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         std::size_t cols = 0;
         bool arnoldi_breakdown = false;
         for (; cols < R && res.iterations < o.maximum_iterations; ++cols, ++res.iterations) {
-            e.pc(*V[cols], *Z[cols]);
-            e.op(*Z[cols], w);
+            e.pc_op(*V[cols], *Z[cols], w);
             const std::size_t k = cols + 1;
             const T* vb[kMaxBatch];
             for (std::size_t j = 0; j < k; ++j) vb[j] = vptr[j];

@@ -125,6 +125,28 @@ __device__ __forceinline__ void tma_load_2d(std::uint32_t dst, const void* tmap,
         : "memory");
 }
 
+// Shared -> global tile store through a tensor map (rows past the tensor's
+// extent are not written); completion is tracked by bulk groups.
+__device__ __forceinline__ void tma_store_2d(const void* tmap, std::uint32_t src, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(tmap),
+                 "r"(src), "r"(x), "r"(y)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Wait until every committed bulk store has finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Wait until every committed bulk store has completed.
+__device__ __forceinline__ void bulk_wait_all()
+{
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // Four rows r0..r3 (box one row high) into 4 consecutive box-sized slots.
 __device__ __forceinline__ void tma_gather4(std::uint32_t dst, const void* tmap, int x, int r0, int r1, int r2, int r3,
                                             std::uint32_t bar, std::uint64_t policy)
