@@ -69,18 +69,22 @@ __device__ __forceinline__ uint4 f32_to_bf16x8(const float (&f)[8])
     return u;
 }
 
-// w * x + s on the two features held by one 32-bit word of BF16 pairs.
-__device__ __forceinline__ float2 fma_bf16x2(float w, std::uint32_t x, float2 s)
-{
-    return __ffma2_rn(make_float2(w, w), make_float2(__uint_as_float(x << 16), __uint_as_float(x & 0xffff0000u)), s);
-}
+// Edge weights enter the aggregation rounded to BF16: the product of a BF16
+// weight and a BF16 feature is exact in FP32, so s = fma(w, x, s) in FP32 is
+// the same operation as the mixed-precision fma.rn.f32.bf16 used here.
+__device__ __forceinline__ float bf16_round(float w) { return __bfloat162float(__float2bfloat16_rn(w)); }
 
-__device__ __forceinline__ void accumulate_row(float w, const uint4& f, float2 (&acc)[4])
+// acc += w * f for the 8 BF16 features of f; w holds BF16 bits.
+__device__ __forceinline__ void accumulate_row(unsigned short w, const uint4& f, float2 (&acc)[4])
 {
-    acc[0] = fma_bf16x2(w, f.x, acc[0]);
-    acc[1] = fma_bf16x2(w, f.y, acc[1]);
-    acc[2] = fma_bf16x2(w, f.z, acc[2]);
-    acc[3] = fma_bf16x2(w, f.w, acc[3]);
+    const std::uint32_t x[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+            "fma.rn.f32.bf16 %0, lo, %3, %0;\n\t"
+            "fma.rn.f32.bf16 %1, hi, %3, %1;\n\t}"
+            : "+f"(acc[k].x), "+f"(acc[k].y)
+            : "r"(x[k]), "h"(w));
 }
 
 __device__ __forceinline__ uint4 pack_bf16x8(const float2 (&acc)[4])
@@ -181,7 +185,7 @@ struct GraphArgs {
     const int* tr_edge;      // index of that edge in the forward (nb) order
     const float* dinv;       // 1 / diagonal, n * bs
     const int* ell_col;      // first 8 neighbours of v at 8 v.. (padding: -1)
-    const float* ell_w;      // their weights (padding: 0)
+    const unsigned short* ell_w;   // their weights as BF16 bits (padding: 0)
     const unsigned char* tile_ovf;   // 128-row tile holds a row with more than 8 neighbours
 };
 
@@ -196,41 +200,83 @@ __global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* _
 
 // Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...].  An 8-lane
 // group per vertex, lane `c8` computing features 8*c8..8*c8+7 (one coalesced
-// 16-byte store each) as packed f32x2 FMAs over the 2 bs nonzero inputs in
+// 16-byte store each) as packed f32x2 FMAs over the 2 BS nonzero inputs in
 // ascending order; the zero inputs are skipped, which leaves every sum
-// bit-identical to the full 16-term one (fma(w, 0, s) = s, s never -0).
-template<class T>
+// bit-identical to the full 16-term one (fma(w, 0, s) = s, s never -0).  Each
+// thread takes 4 vertices per pass (their inputs loaded first) and reads each
+// weight pair once for all 4; the transposed weights are laid out so that the
+// 8 lanes of a group read 8 distinct bank quads.
+template<class T, int BS>
 __global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
                                                     const double* norms, const float* __restrict__ we,
                                                     bf16* __restrict__ h0)
 {
-    __shared__ __align__(16) float wt[kF * kH];   // transposed: wt[f * 64 + k] = We[k][f]
-    for (int j = threadIdx.x; j < kH * kF; j += blockDim.x) wt[j] = we[(j % kH) * kF + j / kH];
+    constexpr int NF = 2 * BS, U = 4;
+    // wt[f * 64 + half * 32 + c8 * 4 + i] = We[8 * c8 + 4 * half + i][f]
+    __shared__ __align__(16) float wt[NF * kH];
+    for (int j = threadIdx.x; j < NF * kH; j += blockDim.x) {
+        const int f = j / kH, k = j % kH, half = k / 32, c8 = (k % 32) / 4, i = k % 4;
+        wt[j] = we[(8 * c8 + 4 * half + i) * kF + f];
+    }
     __syncthreads();
     const double root = sqrt(static_cast<double>(g.n) * g.bs), nr = norms[0], nq = norms[2];
     const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
     const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
-    const int nf = 2 * g.bs;
+    const int c8 = threadIdx.x & 7;
+    const float4* w4 = reinterpret_cast<const float4*>(wt);
     const long long total = 8ll * g.n, stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-        const int v = static_cast<int>(t >> 3), c8 = static_cast<int>(t & 7);
-        const long long vb = static_cast<long long>(v) * g.bs;
-        float2 acc[4] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f),
-                         make_float2(0.0f, 0.0f)};
+    for (long long t0 = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t0 < total; t0 += U * stride) {
+        float x[U][NF];
 #pragma unroll
-        for (int f = 0; f < kF; ++f) {
-            if (f < nf) {
-                const float x = f < g.bs ? static_cast<float>(r[vb + f]) * inv_r : q[vb + f - g.bs] * inv_q;
-                const float4* wp = reinterpret_cast<const float4*>(wt + f * kH + c8 * 8);
-                const float4 wa = wp[0], wb = wp[1];
-                const float2 xx = make_float2(x, x);
-                acc[0] = __ffma2_rn(make_float2(wa.x, wa.y), xx, acc[0]);
-                acc[1] = __ffma2_rn(make_float2(wa.z, wa.w), xx, acc[1]);
-                acc[2] = __ffma2_rn(make_float2(wb.x, wb.y), xx, acc[2]);
-                acc[3] = __ffma2_rn(make_float2(wb.z, wb.w), xx, acc[3]);
+        for (int u = 0; u < U; ++u) {
+            const long long t = min(t0 + u * stride, total - 1);
+            const long long vb = (t >> 3) * BS;
+#pragma unroll
+            for (int c = 0; c < BS; ++c) {
+                x[u][c] = static_cast<float>(r[vb + c]) * inv_r;
+                x[u][BS + c] = q[vb + c] * inv_q;
             }
         }
-        reinterpret_cast<uint4*>(h0 + static_cast<long long>(v) * kH)[c8] = pack_bf16x8(acc);
+        float2 acc[U][4];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[u][i] = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            const float4 wa = w4[f * 16 + c8], wb = w4[f * 16 + 8 + c8];
+            const float2 w0 = make_float2(wa.x, wa.y), w1 = make_float2(wa.z, wa.w), w2 = make_float2(wb.x, wb.y),
+                         w3 = make_float2(wb.z, wb.w);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const float2 xx = make_float2(x[u][f], x[u][f]);
+                acc[u][0] = __ffma2_rn(w0, xx, acc[u][0]);
+                acc[u][1] = __ffma2_rn(w1, xx, acc[u][1]);
+                acc[u][2] = __ffma2_rn(w2, xx, acc[u][2]);
+                acc[u][3] = __ffma2_rn(w3, xx, acc[u][3]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long t = t0 + u * stride;
+            if (t < total) reinterpret_cast<uint4*>(h0 + (t >> 3) * kH)[c8] = pack_bf16x8(acc[u]);
+        }
+    }
+}
+
+template<class T>
+void launch_encode(unsigned grid, cudaStream_t st, const GraphArgs& g, const T* r, const float* q, const double* norms,
+                   const float* we, bf16* h0)
+{
+    switch (g.bs) {
+    case 1: k_gnn_encode<T, 1><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    case 2: k_gnn_encode<T, 2><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    case 3: k_gnn_encode<T, 3><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    case 4: k_gnn_encode<T, 4><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    case 5: k_gnn_encode<T, 5><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    case 6: k_gnn_encode<T, 6><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    case 7: k_gnn_encode<T, 7><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
+    default: k_gnn_encode<T, 8><<<grid, 256, 0, st>>>(g, r, q, norms, we, h0); break;
     }
 }
 
@@ -275,14 +321,16 @@ __global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __
 //  * each warp aggregates m_v = sum_u w_vu h_u for 32 rows, four at a time
 //    (an 8-lane group per row, lane `chunk` owning features 8*chunk..+7), over
 //    the rows' padded 8-slot neighbour lists: lane `chunk` loads slot
-//    `chunk`'s index and weight two row steps ahead and the group shares them
-//    by shuffles; the neighbours' 16-byte feature chunks are gathered in
+//    `chunk`'s index and BF16 weight two row steps ahead and the group shares
+//    them by shuffles; the neighbours' 16-byte feature chunks are gathered in
 //    quarter steps of two slots through a register ring kGatherDepth quarter
-//    steps ahead of their use; the FP32 sums run as packed f32x2 FMAs and m
-//    is rounded to BF16 into the swizzled second operand block;
-//  * eight K=16 MMAs give Y = [h | m] Wl^T in TMEM and the epilogue writes
-//    h + relu(Y) (or, for the last layer of an inference pass, the decoder's
-//    output straight from the rounded rows).
+//    steps ahead of their use; the sums run in FP32 as mixed-precision FMAs
+//    straight from the BF16 halves (each product exact) and m is rounded to
+//    BF16 into the swizzled second operand block;
+//  * eight K=16 MMAs give Y = [h | m] Wl^T in TMEM; the epilogue writes
+//    h + relu(Y) into A0 and one TMA tile store moves it out (for the last
+//    layer of an inference pass, four more MMAs of the rounded rows against
+//    the BF16 decoder weights, N = 16, give out = q + rms(q) (h Wd^T)).
 // Padding slots (index -1) load nothing and carry weight 0: fma(0, x, s) = s
 // for the finite chunk x their registers still hold and a running sum that
 // is never -0, so the sums are bit-identical to skipping the slot.  Rows with
@@ -291,11 +339,13 @@ __global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __
 // the sign mask of Y (one 64-bit word per row) for the backward pass.
 constexpr int kEll = 8;            // padded neighbour slots per row
 #ifndef OWTK_GNN_DEPTH
-#define OWTK_GNN_DEPTH 8
+#define OWTK_GNN_DEPTH 4
 #endif
 constexpr int kGatherDepth = OWTK_GNN_DEPTH;   // quarter steps (2 slots) in flight per warp
 constexpr int kLayerThreads = 128;
 constexpr int kLayerSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128;   // A: [h | m], B: Wl
+constexpr int kDecodeRows = 16;                                      // Wd padded to N = 16
+constexpr int kLayerSmemDec = kLayerSmem + kDecodeRows * 128;        // + Wd (BF16, swizzled)
 
 #ifndef OWTK_GNN_LDOP
 #define OWTK_GNN_LDOP ".nc"
@@ -333,7 +383,6 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     extern __shared__ unsigned char smem_raw[];
     __shared__ __align__(8) std::uint64_t bar_storage[2];   // [0] MMAs done, [1] own rows landed
     __shared__ std::uint32_t tmem_base_s;
-    __shared__ float wd_s[DECODE ? 8 * kH : 1];
     const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
     unsigned char* tile = smem_raw + (base - raw);                 // A0 (h), A1 (m), B0, B1
     const std::uint32_t a0 = base, a1 = base + kTile * 128, b0 = base + 2 * kTile * 128, b1 = b0 + kH * 128;
@@ -349,8 +398,16 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     }
     float dec_scale = 0.0f;
     bool dec_live = false;
+    const std::uint32_t wdt = b1 + kH * 128;   // decoder weight tile (DECODE)
     if (DECODE) {
-        for (int i = threadIdx.x; i < g.bs * kH; i += kLayerThreads) wd_s[i] = dec.wd[i];
+        // Wd (bs x 64, FP32) as a 16-row BF16 operand, rows past bs zero.
+        for (int i = threadIdx.x; i < kDecodeRows * 8; i += kLayerThreads) {
+            const int c = i >> 3, c8 = i & 7;
+            float f[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) f[k] = c < g.bs ? dec.wd[c * kH + c8 * 8 + k] : 0.0f;
+            *reinterpret_cast<uint4*>(tile + (wdt - base) + sw128(c, c8)) = f32_to_bf16x8(f);
+        }
         dec_scale = static_cast<float>(dec.norms[2] / sqrt(static_cast<double>(g.n) * g.bs));
         dec_live = dec.norms[0] > 0.0;
     }
@@ -359,12 +416,15 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         mbar_init(bar_h, 1);
         fence_proxy_async_smem();
     }
-    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kH);
+    constexpr std::uint32_t kCols = DECODE ? 2 * kH : kH;   // Y (64) and the decoder's 16
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kCols);
     tmem_fence_before_sync();
     __syncthreads();
     tmem_fence_after_sync();
     const std::uint32_t tmem = tmem_base_s;
     constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, kH);
+    constexpr std::uint32_t idesc_dec = umma_idesc_bf16(kTile, kDecodeRows);
+    std::uint32_t mma_waits = 0;   // completions of `bar` so far
     // Own rows of `t` into A0 (rows past n read as zeros); the index rows of
     // the tile after it towards L2.
     const auto stage_tile = [&](int t) {
@@ -374,9 +434,9 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         }
         const int tn = t + static_cast<int>(gridDim.x);
         if (tn < ntiles) {
-            const std::uint32_t bytes = static_cast<std::uint32_t>(min(kTile, g.n - tn * kTile)) * kEll * 4;
-            prefetch_l2(g.ell_col + static_cast<long long>(tn) * kTile * kEll, bytes);
-            prefetch_l2(g.ell_w + static_cast<long long>(tn) * kTile * kEll, bytes);
+            const std::uint32_t rows = static_cast<std::uint32_t>(min(kTile, g.n - tn * kTile));
+            prefetch_l2(g.ell_col + static_cast<long long>(tn) * kTile * kEll, rows * kEll * 4);
+            prefetch_l2(g.ell_w + static_cast<long long>(tn) * kTile * kEll, rows * kEll * 2);
         }
     };
     if (threadIdx.x == 0) stage_tile(blockIdx.x);
@@ -396,7 +456,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         const auto ell_at = [&](int s) { return static_cast<long long>(min(first + 4 * s, g.n - 1)) * kEll + chunk; };
         constexpr int kQuarters = 4 * 8;
         int ecol[8];
-        float ew[8];
+        unsigned ew[8];   // BF16 weight bits
         // A padding slot loads nothing (weight 0): it keeps a chunk gathered
         // earlier in this tile or these zeros.
         uint4 ring[kGatherDepth + 1][2];
@@ -437,14 +497,16 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
                 for (int i = 0; i < 4; ++i) acc[i] = make_float2(0.0f, 0.0f);
 #pragma unroll
             for (int j = 0; j < 2; ++j)
-                accumulate_row(__shfl_sync(0xffffffffu, ew[s & 7], (lane & ~7) + 2 * (k & 3) + j),
+                accumulate_row(static_cast<unsigned short>(
+                                   __shfl_sync(0xffffffffu, ew[s & 7], (lane & ~7) + 2 * (k & 3) + j)),
                                ring[k % (kGatherDepth + 1)][j], acc);
             if ((k & 3) == 3) {
                 const int r = 32 * warp + 4 * s + grp, v = row0 + r;
                 if (overflow && v < g.n) {   // rows with more than 8 neighbours
                     const int e1 = g.nb_ptr[v + 1];
                     for (int e = g.nb_ptr[v] + kEll; e < e1; ++e)
-                        accumulate_row(g.nb_w[e], __ldg(reinterpret_cast<const uint4*>(
+                        accumulate_row(__bfloat16_as_ushort(__float2bfloat16_rn(g.nb_w[e])),
+                                       __ldg(reinterpret_cast<const uint4*>(
                                                             h_in + static_cast<long long>(g.nb_col[e]) * kH) + chunk),
                                        acc);
                 }
@@ -472,7 +534,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
                 umma_bf16(tmem, umma_desc_sw128(a1 + 32 * k), umma_desc_sw128(b1 + 32 * k), idesc, true);
             umma_commit(bar);
         }
-        ok = wait_phase(bar, iter & 1);
+        ok = wait_phase(bar, mma_waits++ & 1);
         tmem_fence_after_sync();
         if (!__syncthreads_and(ok)) break;
         // ---- epilogue: row = tile row 32*warp + lane
@@ -497,34 +559,34 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
                 outv[c8] = f32_to_bf16x8(hf);
             }
         }
-        if (v < g.n) {
-            if (DECODE) {
-                const long long o0 = static_cast<long long>(v) * g.bs;
-#pragma unroll 1
-                for (int c = 0; c < g.bs; ++c) {
-                    float part[8];   // per 8-feature chunk, then the pairwise tree
+        if (TRAIN && v < g.n) mask_out[v] = mask;
+        // The new rows replace the old ones in A0 (each thread its own row):
+        // the operand of the decoder's MMA, or the source of one TMA store.
 #pragma unroll
-                    for (int c8 = 0; c8 < 8; ++c8) {
-                        float f[8];
-                        bf16x8_to_f32(outv[c8], f);
-                        float p = 0.0f;
+        for (int c8 = 0; c8 < 8; ++c8) *reinterpret_cast<uint4*>(tile + sw128(r, c8)) = outv[c8];
+        fence_proxy_async_smem();
+        if constexpr (DECODE) {
+            // out = q + rms(q) (h Wd^T): four K=16 MMAs into TMEM columns 64..79.
+            tmem_fence_before_sync();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tmem_fence_after_sync();
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) p = fmaf(wd_s[c * kH + c8 * 8 + i], f[i], p);
-                        part[c8] = p;
-                    }
-                    const float y = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
-                    dec.out[o0 + c] = static_cast<O>(dec_live ? fmaf(dec_scale, y, dec.q[o0 + c]) : 0.0f);
-                }
-            } else if (TRAIN) {
-                mask_out[v] = mask;
+                for (int k = 0; k < 4; ++k)
+                    umma_bf16(tmem + kH, umma_desc_sw128(a0 + 32 * k), umma_desc_sw128(wdt + 32 * k), idesc_dec, k > 0);
+                umma_commit(bar);
             }
-        }
-        if (!DECODE) {
-            // The new rows replace the old ones in A0 (each thread its own
-            // row) and leave as one TMA tile store.
+            ok = wait_phase(bar, mma_waits++ & 1);
+            tmem_fence_after_sync();
+            if (!__syncthreads_and(ok)) break;
+            float y[kDecodeRows];
+            tmem_ld16(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + kH, y);
+            if (v < g.n) {
+                const long long o0 = static_cast<long long>(v) * g.bs;
 #pragma unroll
-            for (int c8 = 0; c8 < 8; ++c8) *reinterpret_cast<uint4*>(tile + sw128(r, c8)) = outv[c8];
-            fence_proxy_async_smem();
+                for (int c = 0; c < 8; ++c)
+                    if (c < g.bs) dec.out[o0 + c] = static_cast<O>(dec_live ? fmaf(dec_scale, y[c], dec.q[o0 + c]) : 0.0f);
+            }
         }
         tmem_fence_before_sync();
         __syncthreads();
@@ -546,7 +608,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     if (!DECODE && threadIdx.x == 0) bulk_wait_all();
     tmem_fence_before_sync();
     __syncthreads();
-    if (warp == 0) tmem_free(tmem, kH);
+    if (warp == 0) tmem_free(tmem, kCols);
 }
 
 // ---------------------------------------------------------------- TMA-fed layer
@@ -736,7 +798,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
                 float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 for (int k = 0; k < meta.y; ++k) {
                     const int wi = meta.z + k;
-                    const float w = wi < wavail ? sw[woff + wi] : g.nb_w[e_first + wi];
+                    const float w = bf16_round(wi < wavail ? sw[woff + wi] : g.nb_w[e_first + wi]);
                     uint4 u;
                     if (meta.x >= 0) u = *reinterpret_cast<const uint4*>(sp + (meta.x + k) * 128 + chunk * 16);
                     else u = *reinterpret_cast<const uint4*>(h_in + static_cast<long long>(g.nb_col[e_first + wi]) * kH
@@ -1232,7 +1294,15 @@ __global__ void k_gnn_gather_w(int count, const int* __restrict__ idx, const flo
                                float* __restrict__ dst)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) dst[i] = idx[i] >= 0 ? src[idx[i]] : 0.0f;
+    if (i < count) dst[i] = src[idx[i]];
+}
+
+// Padded slot weights as BF16 bits (padding, idx < 0: zero).
+__global__ void k_gnn_gather_wb(int count, const int* __restrict__ idx, const float* __restrict__ src,
+                                unsigned short* __restrict__ dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) dst[i] = idx[i] >= 0 ? __bfloat16_as_ushort(__float2bfloat16_rn(src[idx[i]])) : 0;
 }
 
 }  // namespace gnn
@@ -1281,7 +1351,7 @@ struct Gnn {
         g.tr_edge = tr_edge.as<int>();
         g.dinv = dinv.as<float>();
         g.ell_col = ell_col.as<int>();
-        g.ell_w = ell_w.as<float>();
+        g.ell_w = ell_w.as<unsigned short>();
         g.tile_ovf = tile_ovf.as<unsigned char>();
         return g;
     }
@@ -1313,7 +1383,7 @@ void gnn_set_attrs()
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kLayerSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<false, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   gnn::kLayerSmem));
+                                   gnn::kLayerSmemDec));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kBwdSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1379,8 +1449,8 @@ void gnn_forward(Gnn& G, const T* r, O* out)
     double* norms = G.norm_r.as<double>();
     kern::prepare_norms<T>(c, static_cast<std::size_t>(nb), r, G.dinv.as<float>(), G.qbuf.as<float>(), norms);
     gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
-    gnn::k_gnn_encode<T><<<std::min(G.blocks(8ll * G.n), static_cast<unsigned>(c.sm_count * 8)), 256, 0, c.stream>>>(
-        g, r, G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
+    gnn::launch_encode<T>(std::min(G.blocks(8ll * G.n), static_cast<unsigned>(c.sm_count * 8)), c.stream, g, r,
+                          G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
     const gnn::bf16* hin = h0;
@@ -1402,7 +1472,7 @@ void gnn_forward(Gnn& G, const T* r, O* out)
             if constexpr (!TRAIN) {
               if (l == gnn::kLayers - 1) {   // last layer with the decoder fused
                 const gnn::DecodeArgs<O> dec{G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWd, out};
-                gnn::k_gnn_layer<false, true, O><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
+                gnn::k_gnn_layer<false, true, O><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmemDec, c.stream>>>(
                     g, tm, tm, hin, wl, nullptr, nullptr, dec, c.status.as<unsigned>());
                 OWTK_CUDA(cudaGetLastError());
                 c.launched();
@@ -1630,8 +1700,8 @@ void gnn_bind_matrix(Gnn& G, Matrix& m)
         gnn::k_gnn_gather_w<<<G.blocks(ne), 256, 0, c.stream>>>(ne, G.tr_edge.as<int>(), G.nb_w.as<float>(),
                                                                 G.tr_w.as<float>());
     const int slots = G.n * gnn::kEll;
-    gnn::k_gnn_gather_w<<<G.blocks(slots), 256, 0, c.stream>>>(slots, G.ell_src.as<int>(), G.nb_w.as<float>(),
-                                                               G.ell_w.as<float>());
+    gnn::k_gnn_gather_wb<<<G.blocks(slots), 256, 0, c.stream>>>(slots, G.ell_src.as<int>(), G.nb_w.as<float>(),
+                                                                G.ell_w.as<unsigned short>());
     OWTK_CUDA(cudaGetLastError());
     c.launched(3);
     c.sync();
@@ -1788,7 +1858,7 @@ owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** ou
             G->ell_col = owtk::upload(st, ell_col);
             G->ell_src = owtk::upload(st, ell_src);
             G->tile_ovf = owtk::upload(st, tile_ovf);
-            G->ell_w.allocate(ell_col.size() * sizeof(float) + 16);
+            G->ell_w.allocate(ell_col.size() * sizeof(unsigned short) + 16);
         }
         // Tensor maps of the ping-pong feature buffers (own-row tiles of the
         // layer).  The register-gather layer is the default: on the 2M-vertex

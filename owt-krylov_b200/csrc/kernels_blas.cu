@@ -557,40 +557,44 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
 }
 
 // q = r / d (FP32) with ||r|| and ||q|| in the same pass: the learned
-// preconditioner's input scaling.  Same per-thread order, CTA merge and fixed
-// combine order as k_norm over each array, so both norms equal k_norm's.
+// preconditioner's input scaling.  Plain FP64 sums of squares (the inputs
+// are residuals; the network needs the norms to FP32 accuracy only), summed
+// per thread, per CTA and over CTAs in a fixed order: deterministic.
 template<class T>
-__global__ void __launch_bounds__(kThreads) k_prepare_norms(std::size_t n, const T* __restrict__ r,
-                                                            const float* __restrict__ dinv, float* __restrict__ q,
-                                                            double* partials, unsigned* ticket, double* norms)
+__global__ void __launch_bounds__(256) k_prepare_norms(std::size_t n, const T* __restrict__ r,
+                                                       const float* __restrict__ dinv, float* __restrict__ q,
+                                                       double* partials, unsigned* ticket, double* norms)
 {
-    ScaledSum a{0.0, 0.0, 0}, b{0.0, 0.0, 0};
-    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
-    constexpr int kU = 8;
-    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += kU * stride) {
-        double va[kU], vb[kU];
+    constexpr int kU = 4;
+    double a = 0.0, b = 0.0;
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * 256;
+    for (std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * 256 + threadIdx.x; i0 < n; i0 += kU * stride) {
+        T rv[kU];
+        float dv[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
-            const std::size_t idx = i + u * stride;
-            va[u] = 0.0;
-            vb[u] = 0.0;
-            if (idx < n) {
-                const T rv = r[idx];
-                const float qv = static_cast<float>(rv) * dinv[idx];
-                q[idx] = qv;
-                va[u] = static_cast<double>(rv);
-                vb[u] = static_cast<double>(qv);
+            const std::size_t i = i0 + u * stride;
+            rv[u] = i < n ? r[i] : T(0);
+            dv[u] = i < n ? dinv[i] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const std::size_t i = i0 + u * stride;
+            if (i < n) {
+                const float qv = static_cast<float>(rv[u]) * dv[u];
+                q[i] = qv;
+                const double rd = static_cast<double>(rv[u]), qd = static_cast<double>(qv);
+                a = fma(rd, rd, a);
+                b = fma(qd, qd, b);
             }
         }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            norm_push(a, va[u]);
-            norm_push(b, vb[u]);
-        }
     }
-    a = norm_warp(a);
-    b = norm_warp(b);
-    __shared__ ScaledSum red[2][kThreads / 32];
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, m);
+        b += __shfl_xor_sync(0xffffffffu, b, m);
+    }
+    __shared__ double red[2][8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         red[0][warp] = a;
@@ -598,47 +602,40 @@ __global__ void __launch_bounds__(kThreads) k_prepare_norms(std::size_t n, const
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        ScaledSum s0 = red[0][0], s1 = red[1][0];
-        for (int w = 1; w < kThreads / 32; ++w) {
-            s0 = norm_merge(s0, red[0][w]);
-            s1 = norm_merge(s1, red[1][w]);
+        double sa = 0.0, sb = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            sa += red[0][w];
+            sb += red[1][w];
         }
-        double* p = partials + 6 * blockIdx.x;
-        p[0] = s0.scale;
-        p[1] = s0.ssq;
-        p[2] = s0.nan;
-        p[3] = s1.scale;
-        p[4] = s1.ssq;
-        p[5] = s1.nan;
+        partials[2 * blockIdx.x] = sa;
+        partials[2 * blockIdx.x + 1] = sb;
     }
     if (last_block(ticket)) {
         __threadfence();
-        ScaledSum t0{0.0, 0.0, 0}, t1{0.0, 0.0, 0};
-        for (unsigned k = threadIdx.x; k < gridDim.x; k += kThreads) {
-            const double* p = partials + 6 * k;
-            t0 = norm_merge(t0, ScaledSum{__ldcg(p), __ldcg(p + 1), __ldcg(p + 2) != 0.0});
-            t1 = norm_merge(t1, ScaledSum{__ldcg(p + 3), __ldcg(p + 4), __ldcg(p + 5) != 0.0});
+        double ta = 0.0, tb = 0.0;
+        for (unsigned k = threadIdx.x; k < gridDim.x; k += 256) {
+            ta += __ldcg(partials + 2 * k);
+            tb += __ldcg(partials + 2 * k + 1);
         }
-        t0 = norm_warp(t0);
-        t1 = norm_warp(t1);
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) {
+            ta += __shfl_xor_sync(0xffffffffu, ta, m);
+            tb += __shfl_xor_sync(0xffffffffu, tb, m);
+        }
         __syncthreads();
         if (lane == 0) {
-            red[0][warp] = t0;
-            red[1][warp] = t1;
+            red[0][warp] = ta;
+            red[1][warp] = tb;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                ScaledSum s = red[j][0];
-                for (int w = 1; w < kThreads / 32; ++w) s = norm_merge(s, red[j][w]);
-                double v;
-                if (s.nan) v = __longlong_as_double(0x7ff8000000000000LL);
-                else if (s.scale == 0.0 || isinf(s.scale)) v = s.scale;
-                else v = s.scale * sqrt(s.ssq);
-                norms[2 * j] = v;
-                norms[2 * j + 1] = v;
+            double sa = 0.0, sb = 0.0;
+            for (int w = 0; w < 8; ++w) {
+                sa += red[0][w];
+                sb += red[1][w];
             }
+            norms[0] = norms[1] = sqrt(sa);
+            norms[2] = norms[3] = sqrt(sb);
             *ticket = 0;
         }
     }
@@ -836,8 +833,10 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
 template<class T>
 void prepare_norms(Context& c, std::size_t n, const T* r, const float* dinv, float* q, double* norms)
 {
-    const unsigned blocks = reduce_blocks(c, n);
-    k_prepare_norms<T><<<blocks, kThreads, 0, c.stream>>>(n, r, dinv, q, partials_of(c), ticket_of(c), norms);
+    const std::size_t want = (n + 256 * 4 - 1) / (256 * 4);
+    const unsigned blocks = static_cast<unsigned>(std::min<std::size_t>(std::max<std::size_t>(want, 1),
+                                                                       std::min(c.sm_count * 8, kReduceBlocks)));
+    k_prepare_norms<T><<<blocks, 256, 0, c.stream>>>(n, r, dinv, q, partials_of(c), ticket_of(c), norms);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }

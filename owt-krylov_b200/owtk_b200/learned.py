@@ -50,9 +50,11 @@ def make_pairs(ctx, matrix, rhs: np.ndarray, pairs: int, rng=None):
 
 
 def train(ctx, net, systems, epochs: int = 4, learning_rate: float = 1e-3, pairs_per_system: int = 4,
-          seed: int = 0):
+          seed: int = 0, final_learning_rate=None):
     """Adam over all pairs of all systems for `epochs` passes; returns the
-    mean loss of each epoch (the first is the untrained loss)."""
+    mean loss of each epoch (the first is the untrained loss).  With
+    `final_learning_rate` the rate decays geometrically from `learning_rate`
+    to it over the epochs."""
     rng = np.random.default_rng(seed)
     data = []
     for s in systems:
@@ -60,6 +62,9 @@ def train(ctx, net, systems, epochs: int = 4, learning_rate: float = 1e-3, pairs
         data.append((m, make_pairs(ctx, m, s.rhs, pairs_per_system)))
     history = []
     for ep in range(epochs + 1):
+        lr = learning_rate
+        if final_learning_rate is not None and epochs > 1 and ep > 0:
+            lr = learning_rate * (final_learning_rate / learning_rate) ** ((ep - 1) / (epochs - 1))
         losses = []
         order = rng.permutation(len(data))
         for i in order:
@@ -71,7 +76,7 @@ def train(ctx, net, systems, epochs: int = 4, learning_rate: float = 1e-3, pairs
                     raise FloatingPointError(f"training loss is {loss} (epoch {ep})")
                 losses.append(loss)
                 if ep > 0:
-                    net.adam_step(learning_rate)
+                    net.adam_step(lr)
         history.append(float(np.mean(losses)))
     return history
 

@@ -83,9 +83,12 @@ def test_forward_matches_restatement(native, ctx):
     np.testing.assert_allclose(y.download(), jac, rtol=2e-7)
 
 
-def test_tma_and_register_gather_agree_bitwise(native, ctx, monkeypatch):
+def test_tma_and_register_gather_agree(native, ctx, monkeypatch):
     # Both layer kernels aggregate neighbours in edge order with the same FP32
-    # operations, so forward outputs and gradients are identical.
+    # operations (BF16 edge weights), so the training forward pass (separate
+    # FP32 decoder) and the gradients are identical.  An inference pass of the
+    # register path decodes on the tensor cores (BF16 decoder weights), so its
+    # output agrees to BF16 level with the TMA path's FP32 decoder.
     c, m, net, g = setup(native, ctx, side=40, seed=37)
     n, bs = c["owned"], c["bs"]
     assert not net.uses_tma
@@ -102,7 +105,8 @@ def test_tma_and_register_gather_agree_bitwise(native, ctx, monkeypatch):
     y1, y2 = native.Vector(ctx, n, 0, bs), native.Vector(ctx, n, 0, bs)
     net.apply(r, y1)
     net2.apply(r, y2)
-    assert_bitwise(y1.download(), y2.download(), "network output")
+    a, b = y1.download(), y2.download()
+    assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b), np.linalg.norm(a - b) / np.linalg.norm(b)
     l1, g1 = net.loss_grad(r, e, want_grads=True)
     l2, g2 = net2.loss_grad(r, e, want_grads=True)
     assert l1 == l2 and np.array_equal(g1, g2)
