@@ -316,6 +316,32 @@ __global__ void __launch_bounds__(kThreads) k_cgs_update(std::size_t n, int k, P
     }
 }
 
+// The last Gram-Schmidt pass fused with the normalisation: out = (w - V h) * s,
+// with the sum of k_cgs_update and the product of k_scaled_copy in the same
+// order, so the bits equal those two launches; w itself is left as it was.
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_cgs_update_scale(std::size_t n, int k, PtrPack basis,
+                                                               const double* __restrict__ h,
+                                                               const T* __restrict__ w, T s, T* __restrict__ out)
+{
+    __shared__ const T* sp[kMaxBatch];
+    __shared__ T sh[kMaxBatch];
+    for (int j = threadIdx.x; j < k; j += kThreads) {
+        sp[j] = static_cast<const T*>(basis.p[j]);
+        sh[j] = -static_cast<T>(h[j]);
+    }
+    __syncthreads();
+    EW_PROLOGUE
+#pragma unroll
+    for (int u = 0; u < kIlp; ++u) {
+        const std::size_t i = i0 + static_cast<std::size_t>(u) * kThreads;
+        if (i >= n) continue;
+        T wv = w[i];
+        for (int j = 0; j < k; ++j) wv = add_rn(wv, mul_rn(sh[j], sp[j][i]));
+        out[i] = mul_rn(wv, s);
+    }
+}
+
 // Neumaier-compensated correction sum (krylov_solvers.hpp:24-40).
 template<class T>
 __global__ void __launch_bounds__(kThreads) k_gmres_update(std::size_t n, int k, PtrPack dirs,
@@ -778,6 +804,11 @@ template<class T> void cgs_update(Context& c, std::size_t n, int k, const T* con
 {
     LAUNCH_EW(k_cgs_update<T>, n, k, pack(reinterpret_cast<const void* const*>(basis), k), h, w);
 }
+template<class T> void cgs_update_scale(Context& c, std::size_t n, int k, const T* const* basis, const double* h,
+                                        const T* w, T s, T* out)
+{
+    LAUNCH_EW(k_cgs_update_scale<T>, n, k, pack(reinterpret_cast<const void* const*>(basis), k), h, w, s, out);
+}
 template<class T> void gmres_update(Context& c, std::size_t n, int k, const T* const* dirs,
                                     const double* coef, const T* base, T* out)
 {
@@ -878,6 +909,7 @@ template void convert<__nv_bfloat16, double>(Context&, std::size_t, const double
     template void scaled_copy<T>(Context&, std::size_t, const T*, T, T*);                          \
     template void reciprocal_checked<T>(Context&, std::size_t, const T*, T, T*);                   \
     template void cgs_update<T>(Context&, std::size_t, int, const T* const*, const double*, T*);   \
+    template void cgs_update_scale<T>(Context&, std::size_t, int, const T* const*, const double*, const T*, T, T*); \
     template void gmres_update<T>(Context&, std::size_t, int, const T* const*, const double*, const T*, T*); \
     template void multidot<T>(Context&, std::size_t, int, const T* const*, const T* const*, double*, double*); \
     template void cgs_update_dot<T>(Context&, std::size_t, int, const T* const*, const double*, T*, double*, double*); \

@@ -257,6 +257,10 @@ template<class T> void ch_rw(Context& c, std::size_t n, T alpha, T omega, const 
 // GMRES: w -= sum_i h_i V_i in reference order (h on device, negated inside).
 template<class T> void cgs_update(Context& c, std::size_t n, int k, const T* const* basis,
                                   const double* h, T* w);
+// GMRES: out = (w - sum_i h_i V_i) * s (the last pass and the normalisation
+// in one; w is not written).
+template<class T> void cgs_update_scale(Context& c, std::size_t n, int k, const T* const* basis,
+                                        const double* h, const T* w, T s, T* out);
 // GMRES fused: w -= sum_i h_i V_i, then dots of the new w with V_i and w.w.
 template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T* const* basis,
                                       const double* h, T* w, double* out_dev, double* out_host);

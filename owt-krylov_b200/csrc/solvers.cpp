@@ -591,10 +591,17 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
                     pb[k] = e.p(w);
                     kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(kSlotB), e.hslot(kSlotB));
                 }
-                kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotB), e.p(w));
+                // The last pass, w -= V h2, waits for the norm: it is fused
+                // with the normalisation into V[cols + 1] below.
             } else {
                 kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w));
             }
+            bool last_pass_pending = iterated;
+            const auto finish_last_pass = [&] {
+                if (!last_pass_pending) return;
+                kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotB), e.p(w));
+                last_pass_pending = false;
+            };
             e.c.sync();
             const T original = e.scalar(kSlotA + static_cast<int>(k));
             T projected = original;
@@ -629,17 +636,28 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             if (original < std::numeric_limits<T>::min() || !std::isfinite(nsq)
                 || nsq <= std::numeric_limits<T>::epsilon() * original
                 || (nsq > T(0) && nsq < std::numeric_limits<T>::min())) {
+                finish_last_pass();
                 h(cols + 1, cols) = e.norm(w);
                 ++res.arnoldi_norm_verifications;
             } else {
                 h(cols + 1, cols) = std::sqrt(std::max(nsq, T(0)));
             }
-            if (!std::isfinite(h(cols + 1, cols))) { e.breakdown(kNonFinite); return; }
+            if (!std::isfinite(h(cols + 1, cols))) {
+                finish_last_pass();
+                e.breakdown(kNonFinite);
+                return;
+            }
             T cscale = 0;
             for (std::size_t row = 0; row <= cols + 1; ++row) cscale = std::max(cscale, std::abs(h(row, cols)));
             if (h(cols + 1, cols) > e.btol() * cscale) {
-                kern::scaled_copy<T>(e.c, e.n, e.p(w), T(1) / h(cols + 1, cols), e.p(*V[cols + 1]));
+                if (last_pass_pending)
+                    kern::cgs_update_scale<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotB), e.p(w),
+                                              T(1) / h(cols + 1, cols), e.p(*V[cols + 1]));
+                else
+                    kern::scaled_copy<T>(e.c, e.n, e.p(w), T(1) / h(cols + 1, cols), e.p(*V[cols + 1]));
+                last_pass_pending = false;
             } else {
+                finish_last_pass();
                 arnoldi_breakdown = true;
             }
             for (std::size_t row = 0; row < cols; ++row) {
