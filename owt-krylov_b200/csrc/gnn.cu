@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __
 //  * the tile's own rows h arrive by one 2D TMA load whose 128-byte swizzle
 //    is the MMA's K-major operand layout, issued while the previous tile
 //    finishes (and the tile after next has its index rows prefetched to L2);
-//  * each warp aggregates m_v = sum_u w_vu h_u for 32 rows, four at a time
+//  * each of the 8 warps aggregates m_v = sum_u w_vu h_u for 16 rows, four at a time
 //    (an 8-lane group per row, lane `chunk` owning features 8*chunk..+7), over
 //    the rows' padded 8-slot neighbour lists: lane `chunk` loads slot
 //    `chunk`'s index and BF16 weight two row steps ahead and the group shares
@@ -339,10 +339,19 @@ __global__ void __launch_bounds__(256) k_gnn_decode(GraphArgs g, const float* __
 // the sign mask of Y (one 64-bit word per row) for the backward pass.
 constexpr int kEll = 8;            // padded neighbour slots per row
 #ifndef OWTK_GNN_DEPTH
-#define OWTK_GNN_DEPTH 4
+#define OWTK_GNN_DEPTH 1
 #endif
 constexpr int kGatherDepth = OWTK_GNN_DEPTH;   // quarter steps (2 slots) in flight per warp
-constexpr int kLayerThreads = 128;
+constexpr int kLayerThreads = 128;   // backward kernels
+#ifndef OWTK_GNN_WARPS
+#define OWTK_GNN_WARPS 8
+#endif
+constexpr int kFwdWarps = OWTK_GNN_WARPS;          // forward layer: 4 or 8 warps per tile
+constexpr int kFwdThreads = 32 * kFwdWarps;
+constexpr int kRowsPerWarp = kTile / kFwdWarps;    // gather rows per warp
+constexpr int kRowSteps = kRowsPerWarp / 4;        // row steps of 4 rows
+constexpr int kEpiHalves = 8 / kFwdWarps;          // epilogue column halves per thread
+static_assert(kFwdWarps == 4 || kFwdWarps == 8, "forward layer: 4 or 8 warps");
 constexpr int kLayerSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128;   // A: [h | m], B: Wl
 constexpr int kDecodeRows = 16;                                      // Wd padded to N = 16
 constexpr int kLayerSmemDec = kLayerSmem + kDecodeRows * 128;        // + Wd (BF16, swizzled)
@@ -374,8 +383,11 @@ struct DecodeArgs {
     O* out;
 };
 
+#ifndef OWTK_GNN_DEC_BLOCKS
+#define OWTK_GNN_DEC_BLOCKS 4
+#endif
 template<bool TRAIN, bool DECODE = false, class O = float>
-__global__ void __launch_bounds__(kLayerThreads, 4)
+__global__ void __launch_bounds__(kFwdThreads, DECODE ? OWTK_GNN_DEC_BLOCKS : 4)
     k_gnn_layer(GraphArgs g, const __grid_constant__ CUtensorMap tmap_in, const __grid_constant__ CUtensorMap tmap_out,
                 const bf16* __restrict__ h_in, const bf16* __restrict__ wl, bf16* __restrict__ m_out,
                 unsigned long long* __restrict__ mask_out, DecodeArgs<O> dec, unsigned* status)
@@ -391,7 +403,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     const int ntiles = (g.n + kTile - 1) / kTile;
 
     // Layer weight (64 x 128, row-major = K-major) into the two B blocks.
-    for (int i = threadIdx.x; i < kH * 16; i += kLayerThreads) {
+    for (int i = threadIdx.x; i < kH * 16; i += kFwdThreads) {
         const int r = i >> 4, c16 = i & 15;
         const uint4 v = *reinterpret_cast<const uint4*>(wl + r * 128 + c16 * 8);
         *reinterpret_cast<uint4*>(tile + 2 * kTile * 128 + (c16 >> 3) * kH * 128 + sw128(r, c16 & 7)) = v;
@@ -401,7 +413,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
     const std::uint32_t wdt = b1 + kH * 128;   // decoder weight tile (DECODE)
     if (DECODE) {
         // Wd (bs x 64, FP32) as a 16-row BF16 operand, rows past bs zero.
-        for (int i = threadIdx.x; i < kDecodeRows * 8; i += kLayerThreads) {
+        for (int i = threadIdx.x; i < kDecodeRows * 8; i += kFwdThreads) {
             const int c = i >> 3, c8 = i & 7;
             float f[8];
 #pragma unroll
@@ -452,9 +464,9 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         // Lane `chunk` of a group loads the row's slot `chunk` (index and
         // weight, two row steps ahead of its first gather) and shares it by
         // shuffles.
-        const int first = row0 + 32 * warp + grp;
+        const int first = row0 + kRowsPerWarp * warp + grp;
         const auto ell_at = [&](int s) { return static_cast<long long>(min(first + 4 * s, g.n - 1)) * kEll + chunk; };
-        constexpr int kQuarters = 4 * 8;
+        constexpr int kQuarters = 4 * kRowSteps;
         int ecol[8];
         unsigned ew[8];   // BF16 weight bits
         // A padding slot loads nothing (weight 0): it keeps a chunk gathered
@@ -480,7 +492,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         load_ell(2);
 #pragma unroll
         for (int k = 0; k < kGatherDepth; ++k) {
-            if ((k & 3) == 0 && k > 0 && (k >> 2) + 2 < 8) load_ell((k >> 2) + 2);
+            if ((k & 3) == 0 && k > 0 && (k >> 2) + 2 < kRowSteps) load_ell((k >> 2) + 2);
             issue(k);
         }
         float2 acc[4];
@@ -488,7 +500,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         for (int k = 0; k < kQuarters; ++k) {
             const int kn = k + kGatherDepth;
             if (kn < kQuarters) {
-                if ((kn & 3) == 0 && (kn >> 2) + 2 < 8) load_ell((kn >> 2) + 2);
+                if ((kn & 3) == 0 && (kn >> 2) + 2 < kRowSteps) load_ell((kn >> 2) + 2);
                 issue(kn);
             }
             const int s = k >> 2;
@@ -501,7 +513,7 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
                                    __shfl_sync(0xffffffffu, ew[s & 7], (lane & ~7) + 2 * (k & 3) + j)),
                                ring[k % (kGatherDepth + 1)][j], acc);
             if ((k & 3) == 3) {
-                const int r = 32 * warp + 4 * s + grp, v = row0 + r;
+                const int r = kRowsPerWarp * warp + 4 * s + grp, v = row0 + r;
                 if (overflow && v < g.n) {   // rows with more than 8 neighbours
                     const int e1 = g.nb_ptr[v + 1];
                     for (int e = g.nb_ptr[v] + kEll; e < e1; ++e)
@@ -537,33 +549,34 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
         ok = wait_phase(bar, mma_waits++ & 1);
         tmem_fence_after_sync();
         if (!__syncthreads_and(ok)) break;
-        // ---- epilogue: row = tile row 32*warp + lane
-        const int r = 32 * warp + lane, v = row0 + r;
-        unsigned long long mask = 0;
-        uint4 outv[8];
+        // ---- epilogue: row = tile row 32*(warp % 4) + lane (the warp's TMEM
+        // lane quarter); with 8 warps each thread takes one half of the row.
+        const int quad = warp & 3, r = 32 * quad + lane, v = row0 + r;
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            float y[32];
-            tmem_ld32(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + 32 * half, y);
+        for (int hh = 0; hh < kEpiHalves; ++hh) {
+            const int half = kFwdWarps == 8 ? (warp >> 2) : hh;
+            std::uint32_t mask = 0;
+            float y[16];
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
                 const int c8 = half * 4 + c4;
+                if ((c4 & 1) == 0) tmem_ld16(tmem + (static_cast<std::uint32_t>(32 * quad) << 16) + 8 * c8, y);
+                uint4* cell = reinterpret_cast<uint4*>(tile + sw128(r, c8));
                 float hf[8];
-                bf16x8_to_f32(*reinterpret_cast<const uint4*>(tile + sw128(r, c8)), hf);
+                bf16x8_to_f32(*cell, hf);
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    const float yv = y[c4 * 8 + i];
-                    if (yv > 0.0f) mask |= 1ull << (c8 * 8 + i);
+                    const float yv = y[(c4 & 1) * 8 + i];
+                    if (yv > 0.0f) mask |= 1u << (c4 * 8 + i);
                     hf[i] += fmaxf(yv, 0.0f);
                 }
-                outv[c8] = f32_to_bf16x8(hf);
+                // The new rows replace the old ones in A0 (each thread its own
+                // row and chunks): the operand of the decoder's MMA, or the
+                // source of one TMA store.
+                *cell = f32_to_bf16x8(hf);
             }
+            if (TRAIN && v < g.n) reinterpret_cast<std::uint32_t*>(mask_out + v)[half] = mask;
         }
-        if (TRAIN && v < g.n) mask_out[v] = mask;
-        // The new rows replace the old ones in A0 (each thread its own row):
-        // the operand of the decoder's MMA, or the source of one TMA store.
-#pragma unroll
-        for (int c8 = 0; c8 < 8; ++c8) *reinterpret_cast<uint4*>(tile + sw128(r, c8)) = outv[c8];
         fence_proxy_async_smem();
         if constexpr (DECODE) {
             // out = q + rms(q) (h Wd^T): four K=16 MMAs into TMEM columns 64..79.
@@ -580,8 +593,8 @@ __global__ void __launch_bounds__(kLayerThreads, 4)
             tmem_fence_after_sync();
             if (!__syncthreads_and(ok)) break;
             float y[kDecodeRows];
-            tmem_ld16(tmem + (static_cast<std::uint32_t>(32 * warp) << 16) + kH, y);
-            if (v < g.n) {
+            if (warp < 4) tmem_ld16(tmem + (static_cast<std::uint32_t>(32 * quad) << 16) + kH, y);
+            if (warp < 4 && v < g.n) {
                 const long long o0 = static_cast<long long>(v) * g.bs;
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
@@ -1472,7 +1485,7 @@ void gnn_forward(Gnn& G, const T* r, O* out)
             if constexpr (!TRAIN) {
               if (l == gnn::kLayers - 1) {   // last layer with the decoder fused
                 const gnn::DecodeArgs<O> dec{G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWd, out};
-                gnn::k_gnn_layer<false, true, O><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmemDec, c.stream>>>(
+                gnn::k_gnn_layer<false, true, O><<<G.layer_grid(), gnn::kFwdThreads, gnn::kLayerSmemDec, c.stream>>>(
                     g, tm, tm, hin, wl, nullptr, nullptr, dec, c.status.as<unsigned>());
                 OWTK_CUDA(cudaGetLastError());
                 c.launched();
@@ -1481,7 +1494,7 @@ void gnn_forward(Gnn& G, const T* r, O* out)
               }
             }
             const CUtensorMap& tmo = TRAIN ? G.tmap_h[l + 1] : (l % 2 == 0 ? G.tmap_b : G.tmap_a);
-            gnn::k_gnn_layer<TRAIN><<<G.layer_grid(), gnn::kLayerThreads, gnn::kLayerSmem, c.stream>>>(
+            gnn::k_gnn_layer<TRAIN><<<G.layer_grid(), gnn::kFwdThreads, gnn::kLayerSmem, c.stream>>>(
                 g, tm, tmo, hin, wl, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
                 TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, gnn::DecodeArgs<float>{},
                 c.status.as<unsigned>());
