@@ -668,21 +668,37 @@ __global__ void __launch_bounds__(256) k_prepare_norms(std::size_t n, const T* _
 }
 
 // ||x - w|| and ||x|| in one pass (the learned preconditioner's residual
-// check), same one-pass scaled sums and fixed combine order as k_norm.
-__global__ void __launch_bounds__(kThreads) k_residual_norms(std::size_t n, const double* __restrict__ x,
-                                                              const double* __restrict__ w, double* partials,
-                                                              unsigned* ticket, double* out_dev, double* out_host)
+// check, which only compares the two): plain FP64 sums of squares, loads four
+// deep per thread, summed per thread, per CTA and over CTAs in a fixed order
+// (every thread of the last CTA takes a strided share of the partials).
+__global__ void __launch_bounds__(256) k_residual_norms(std::size_t n, const double* __restrict__ x,
+                                                        const double* __restrict__ w, double* partials,
+                                                        unsigned* ticket, double* out_dev, double* out_host)
 {
-    ScaledSum a{0.0, 0.0, 0}, b{0.0, 0.0, 0};
-    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
-    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
-        const double xv = x[i];
-        norm_push(a, xv - w[i]);
-        norm_push(b, xv);
+    constexpr int kU = 4;
+    double a = 0.0, b = 0.0;
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * 256;
+    for (std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * 256 + threadIdx.x; i0 < n; i0 += kU * stride) {
+        double xv[kU], wv[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const std::size_t i = i0 + u * stride;
+            xv[u] = i < n ? x[i] : 0.0;
+            wv[u] = i < n ? w[i] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const double d = xv[u] - wv[u];
+            a = fma(d, d, a);
+            b = fma(xv[u], xv[u], b);
+        }
     }
-    a = norm_warp(a);
-    b = norm_warp(b);
-    __shared__ ScaledSum red[2][kThreads / 32];
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, m);
+        b += __shfl_xor_sync(0xffffffffu, b, m);
+    }
+    __shared__ double red[2][8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         red[0][warp] = a;
@@ -690,37 +706,40 @@ __global__ void __launch_bounds__(kThreads) k_residual_norms(std::size_t n, cons
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        ScaledSum s0 = red[0][0], s1 = red[1][0];
-        for (int k = 1; k < kThreads / 32; ++k) {
-            s0 = norm_merge(s0, red[0][k]);
-            s1 = norm_merge(s1, red[1][k]);
+        double sa = 0.0, sb = 0.0;
+        for (int k = 0; k < 8; ++k) {
+            sa += red[0][k];
+            sb += red[1][k];
         }
-        double* p = partials + 6 * blockIdx.x;
-        p[0] = s0.scale;
-        p[1] = s0.ssq;
-        p[2] = s0.nan;
-        p[3] = s1.scale;
-        p[4] = s1.ssq;
-        p[5] = s1.nan;
+        partials[2 * blockIdx.x] = sa;
+        partials[2 * blockIdx.x + 1] = sb;
+    }
+    if (last_block(ticket)) {
         __threadfence();
-        if (atomicAdd(ticket, 1u) == gridDim.x - 1) {
-            __threadfence();
-            ScaledSum t0{0.0, 0.0, 0}, t1{0.0, 0.0, 0};
-            for (unsigned k = 0; k < gridDim.x; ++k) {
-                const double* q = partials + 6 * k;
-                t0 = norm_merge(t0, ScaledSum{__ldcg(q), __ldcg(q + 1), __ldcg(q + 2) != 0.0});
-                t1 = norm_merge(t1, ScaledSum{__ldcg(q + 3), __ldcg(q + 4), __ldcg(q + 5) != 0.0});
+        double ta = 0.0, tb = 0.0;
+        for (unsigned k = threadIdx.x; k < gridDim.x; k += 256) {
+            ta += __ldcg(partials + 2 * k);
+            tb += __ldcg(partials + 2 * k + 1);
+        }
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) {
+            ta += __shfl_xor_sync(0xffffffffu, ta, m);
+            tb += __shfl_xor_sync(0xffffffffu, tb, m);
+        }
+        __syncthreads();
+        if (lane == 0) {
+            red[0][warp] = ta;
+            red[1][warp] = tb;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sa = 0.0, sb = 0.0;
+            for (int k = 0; k < 8; ++k) {
+                sa += red[0][k];
+                sb += red[1][k];
             }
-            const ScaledSum ts[2] = {t0, t1};
-            for (int k = 0; k < 2; ++k) {
-                const ScaledSum& t = ts[k];
-                double r;
-                if (t.nan) r = __longlong_as_double(0x7ff8000000000000LL);
-                else if (t.scale == 0.0 || isinf(t.scale)) r = t.scale;
-                else r = t.scale * sqrt(t.ssq);
-                out_dev[k] = r;
-                out_host[k] = r;
-            }
+            out_dev[0] = out_host[0] = sqrt(sa);
+            out_dev[1] = out_host[1] = sqrt(sb);
             *ticket = 0;
         }
     }
@@ -875,8 +894,10 @@ template void prepare_norms<double>(Context&, std::size_t, const double*, const 
 
 void residual_norms(Context& c, std::size_t n, const double* x, const double* w, double* out_dev, double* out_host)
 {
-    const unsigned blocks = reduce_blocks(c, n);
-    k_residual_norms<<<blocks, kThreads, 0, c.stream>>>(n, x, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    const std::size_t want = (n + 256 * 4 - 1) / (256 * 4);
+    const unsigned blocks = static_cast<unsigned>(std::min<std::size_t>(std::max<std::size_t>(want, 1),
+                                                                       std::min(c.sm_count * 8, kReduceBlocks)));
+    k_residual_norms<<<blocks, 256, 0, c.stream>>>(n, x, w, partials_of(c), ticket_of(c), out_dev, out_host);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }
