@@ -198,69 +198,63 @@ __global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* _
     if (i < count) q[i] = static_cast<float>(r[i]) * dinv[i];
 }
 
-// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...].  An 8-lane
-// group per vertex, lane `c8` computing features 8*c8..8*c8+7 (one coalesced
-// 16-byte store each) as packed f32x2 FMAs over the 2 BS nonzero inputs in
-// ascending order; the zero inputs are skipped, which leaves every sum
-// bit-identical to the full 16-term one (fma(w, 0, s) = s, s never -0).  Each
-// thread takes 4 vertices per pass (their inputs loaded first) and reads each
-// weight pair once for all 4; the transposed weights are laid out so that the
-// 8 lanes of a group read 8 distinct bank quads.
+// Encoder: h0 = x We^T with x = [r / rms(r), q / rms(q), 0...].  A warp
+// takes 32 vertices per round: lane j loads vertex j's 2 BS inputs (coalesced;
+// the next round's inputs are loaded before this round's arithmetic), then in
+// 8 passes of 4 vertices an 8-lane group per vertex computes it, lane `c8`
+// features 8*c8..8*c8+7 from its own weights held in registers, the inputs
+// shared by shuffles; one coalesced 16-byte store per lane.  The sums are
+// packed f32x2 FMAs over the 2 BS nonzero inputs in ascending order; the zero
+// inputs are skipped, which leaves every sum bit-identical to the full
+// 16-term one (fma(w, 0, s) = s, s never -0).
 template<class T, int BS>
 __global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
                                                     const double* norms, const float* __restrict__ we,
                                                     bf16* __restrict__ h0)
 {
-    constexpr int NF = 2 * BS, U = 4;
-    // wt[f * 64 + half * 32 + c8 * 4 + i] = We[8 * c8 + 4 * half + i][f]
-    __shared__ __align__(16) float wt[NF * kH];
-    for (int j = threadIdx.x; j < NF * kH; j += blockDim.x) {
-        const int f = j / kH, k = j % kH, half = k / 32, c8 = (k % 32) / 4, i = k % 4;
-        wt[j] = we[(8 * c8 + 4 * half + i) * kF + f];
-    }
-    __syncthreads();
+    constexpr int NF = 2 * BS;
+    const int lane = threadIdx.x & 31, grp = lane >> 3, c8 = lane & 7;
+    float2 w[NF][4];   // w[f][k] = (We[8 c8 + 2k][f], We[8 c8 + 2k + 1][f])
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            w[f][k] = make_float2(we[(8 * c8 + 2 * k) * kF + f], we[(8 * c8 + 2 * k + 1) * kF + f]);
     const double root = sqrt(static_cast<double>(g.n) * g.bs), nr = norms[0], nq = norms[2];
     const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
     const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
-    const int c8 = threadIdx.x & 7;
-    const float4* w4 = reinterpret_cast<const float4*>(wt);
-    const long long total = 8ll * g.n, stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long t0 = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; t0 < total; t0 += U * stride) {
-        float x[U][NF];
+    const long long n = g.n;
+    const long long step = static_cast<long long>(gridDim.x) * (blockDim.x / 32) * 32;
+    const auto load = [&](long long v0, float (&x)[NF]) {
+        const long long v = min(v0 + lane, n - 1);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long t = min(t0 + u * stride, total - 1);
-            const long long vb = (t >> 3) * BS;
+        for (int c = 0; c < BS; ++c) {
+            x[c] = static_cast<float>(r[v * BS + c]) * inv_r;
+            x[BS + c] = q[v * BS + c] * inv_q;
+        }
+    };
+    long long v0 = (static_cast<long long>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5)) * 32;
+    float x[NF], xn[NF];
+    if (v0 < n) load(v0, x);
+    for (; v0 < n; v0 += step) {
+        if (v0 + step < n) load(v0 + step, xn);
 #pragma unroll
-            for (int c = 0; c < BS; ++c) {
-                x[u][c] = static_cast<float>(r[vb + c]) * inv_r;
-                x[u][BS + c] = q[vb + c] * inv_q;
+        for (int p = 0; p < 8; ++p) {
+            const int src = 4 * p + grp;
+            float2 acc[4] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f),
+                             make_float2(0.0f, 0.0f)};
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const float xf = __shfl_sync(0xffffffffu, x[f], src);
+                const float2 xx = make_float2(xf, xf);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[k] = __ffma2_rn(w[f][k], xx, acc[k]);
             }
-        }
-        float2 acc[U][4];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[u][i] = make_float2(0.0f, 0.0f);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const float4 wa = w4[f * 16 + c8], wb = w4[f * 16 + 8 + c8];
-            const float2 w0 = make_float2(wa.x, wa.y), w1 = make_float2(wa.z, wa.w), w2 = make_float2(wb.x, wb.y),
-                         w3 = make_float2(wb.z, wb.w);
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const float2 xx = make_float2(x[u][f], x[u][f]);
-                acc[u][0] = __ffma2_rn(w0, xx, acc[u][0]);
-                acc[u][1] = __ffma2_rn(w1, xx, acc[u][1]);
-                acc[u][2] = __ffma2_rn(w2, xx, acc[u][2]);
-                acc[u][3] = __ffma2_rn(w3, xx, acc[u][3]);
-            }
+            const long long v = v0 + src;
+            if (v < n) reinterpret_cast<uint4*>(h0 + v * kH)[c8] = pack_bf16x8(acc);
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long t = t0 + u * stride;
-            if (t < total) reinterpret_cast<uint4*>(h0 + (t >> 3) * kH)[c8] = pack_bf16x8(acc[u]);
-        }
+        for (int f = 0; f < NF; ++f) x[f] = xn[f];
     }
 }
 
@@ -1462,7 +1456,7 @@ void gnn_forward(Gnn& G, const T* r, O* out)
     double* norms = G.norm_r.as<double>();
     kern::prepare_norms<T>(c, static_cast<std::size_t>(nb), r, G.dinv.as<float>(), G.qbuf.as<float>(), norms);
     gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
-    gnn::launch_encode<T>(std::min(G.blocks(8ll * G.n), static_cast<unsigned>(c.sm_count * 8)), c.stream, g, r,
+    gnn::launch_encode<T>(std::min(G.blocks(G.n), static_cast<unsigned>(c.sm_count * 8)), c.stream, g, r,
                           G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
