@@ -485,6 +485,52 @@ __global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, Ptr
     }
 }
 
+// Dots of x with every V_j (j < k) and x.x in one pass: x and each V_j are
+// read once per element.  The products and the per-thread, per-CTA and
+// over-CTA sums are those of k_multidot on the pairs (x, V_j) and (x, x), so
+// the results are the same bits.
+template<class T, int G>
+__global__ void __launch_bounds__(kThreads) k_basis_dots(std::size_t n, int k, PtrPack basis,
+                                                         const T* __restrict__ x, double* partials, unsigned* ticket,
+                                                         double* out_dev, double* out_host)
+{
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    double acc[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) acc[j] = 0;
+    double self = 0.0;
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+        const T xv = x[i];
+        const T* const* bp = reinterpret_cast<const T* const*>(basis.p);
+#pragma unroll
+        for (int j = 0; j < G - 1; ++j)
+            if (j < k) acc[j] += static_cast<double>(xv) * static_cast<double>(bp[j][i]);
+        self += static_cast<double>(xv) * static_cast<double>(xv);
+    }
+    {
+        // block_partials<G>, written out so that acc stays in registers.
+        __shared__ double red[G][kThreads / 32];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const double v = warp_sum(j == k ? self : acc[j]);
+            if (lane == 0) red[j][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x <= k) {
+            double t = 0;
+#pragma unroll
+            for (int w = 0; w < kThreads / 32; ++w) t += red[threadIdx.x][w];
+            partials[static_cast<std::size_t>(threadIdx.x) * gridDim.x + blockIdx.x] = t;
+        }
+        __syncthreads();
+    }
+    if (last_block(ticket)) {
+        combine(k + 1, partials, out_dev, out_host);
+        if (threadIdx.x == 0) *ticket = 0;
+    }
+}
+
 // w -= V h (reference axpy order), then dots of the updated w with every V_j
 // and w.w, in one pass over V (second Gram-Schmidt pass, krylov_solvers.hpp:310-322).
 template<class T, int G>
@@ -494,27 +540,48 @@ __global__ void __launch_bounds__(kThreads) k_cgs_update_dot(std::size_t n, int 
                                                              double* out_dev, double* out_host)
 {
     const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    const T* const* bp = reinterpret_cast<const T* const*>(basis.p);
     double acc[G];
 #pragma unroll
     for (int j = 0; j < G; ++j) acc[j] = 0;
+    double self = 0.0;
     for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
         T wv = w[i];
+        T vj[G - 1];   // each basis value is read once, for the update and for its dot
 #pragma unroll
-        for (int j = 0; j < G; ++j) {
+        for (int j = 0; j < G - 1; ++j) vj[j] = j < k ? bp[j][i] : T(0);
+#pragma unroll
+        for (int j = 0; j < G - 1; ++j) {
             if (j < k) {
                 const T coef = -static_cast<T>(h[j]);
-                wv = add_rn(wv, mul_rn(coef, static_cast<const T*>(basis.p[j])[i]));
+                wv = add_rn(wv, mul_rn(coef, vj[j]));
             }
         }
         w[i] = wv;
         const double wd = static_cast<double>(wv);
 #pragma unroll
-        for (int j = 0; j < G; ++j) {
-            if (j < k) acc[j] += wd * static_cast<double>(static_cast<const T*>(basis.p[j])[i]);
-            else if (j == k) acc[j] += wd * wd;
-        }
+        for (int j = 0; j < G - 1; ++j)
+            if (j < k) acc[j] += wd * static_cast<double>(vj[j]);
+        self += wd * wd;
     }
-    block_partials<G>(acc, k + 1, partials, 0);
+    {
+        // The CTA's partials (block_partials written out: acc stays in registers).
+        __shared__ double red[G][kThreads / 32];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const double v = warp_sum(j == k ? self : acc[j]);
+            if (lane == 0) red[j][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x <= k) {
+            double t = 0;
+#pragma unroll
+            for (int wi = 0; wi < kThreads / 32; ++wi) t += red[threadIdx.x][wi];
+            partials[static_cast<std::size_t>(threadIdx.x) * gridDim.x + blockIdx.x] = t;
+        }
+        __syncthreads();
+    }
     if (last_block(ticket)) {
         combine(k + 1, partials, out_dev, out_host);
         if (threadIdx.x == 0) *ticket = 0;
@@ -856,6 +923,22 @@ template<class T> void multidot(Context& c, std::size_t n, int k, const T* const
     c.launched();
 }
 
+template<class T> void basis_dots(Context& c, std::size_t n, int k, const T* const* basis, const T* x,
+                                  double* out_dev, double* out_host)
+{
+    if (k + 1 > 32) fail(OWTK_ERR_INVALID_ARGUMENT, "basis dots take at most 31 basis vectors");
+    const unsigned blocks = reduce_blocks(c, n);
+    const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
+    if (k + 1 <= 8)
+        k_basis_dots<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 16)
+        k_basis_dots<T, 16><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    else
+        k_basis_dots<T, 32><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
 template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T* const* basis,
                                       const double* h, T* w, double* out_dev, double* out_host)
 {
@@ -931,6 +1014,7 @@ template void convert<__nv_bfloat16, double>(Context&, std::size_t, const double
     template void reciprocal_checked<T>(Context&, std::size_t, const T*, T, T*);                   \
     template void cgs_update<T>(Context&, std::size_t, int, const T* const*, const double*, T*);   \
     template void cgs_update_scale<T>(Context&, std::size_t, int, const T* const*, const double*, const T*, T, T*); \
+    template void basis_dots<T>(Context&, std::size_t, int, const T* const*, const T*, double*, double*); \
     template void gmres_update<T>(Context&, std::size_t, int, const T* const*, const double*, const T*, T*); \
     template void multidot<T>(Context&, std::size_t, int, const T* const*, const T* const*, double*, double*); \
     template void cgs_update_dot<T>(Context&, std::size_t, int, const T* const*, const double*, T*, double*, double*); \

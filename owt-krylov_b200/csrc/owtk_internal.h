@@ -261,6 +261,10 @@ template<class T> void cgs_update(Context& c, std::size_t n, int k, const T* con
 // in one; w is not written).
 template<class T> void cgs_update_scale(Context& c, std::size_t n, int k, const T* const* basis,
                                         const double* h, const T* w, T s, T* out);
+// GMRES: dots of x with V_i (i < k) and x.x, each vector read once (the same
+// values as multidot on those pairs); k + 1 <= 32.
+template<class T> void basis_dots(Context& c, std::size_t n, int k, const T* const* basis, const T* x,
+                                  double* out_dev, double* out_host);
 // GMRES fused: w -= sum_i h_i V_i, then dots of the new w with V_i and w.w.
 template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T* const* basis,
                                       const double* h, T* w, double* out_dev, double* out_host);

@@ -567,8 +567,10 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             for (std::size_t j = 0; j < k; ++j) vb[j] = vptr[j];
             ++res.global_reductions;
             const bool iterated = o.gmres_orthogonalization == 0;
-            {
-                // First projection batch: w.V_j (j < k) and w.w.
+            if (k + 1 <= 32) {
+                // First projection batch: w.V_j (j < k) and w.w, w read once.
+                kern::basis_dots<T>(e.c, e.n, static_cast<int>(k), vb, e.p(w), e.dslot(kSlotA), e.hslot(kSlotA));
+            } else {
                 const T* pa[kMaxBatch];
                 const T* pb[kMaxBatch];
                 for (std::size_t j = 0; j < k; ++j) { pa[j] = e.p(w); pb[j] = vptr[j]; }
