@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--bs", default="3", help="block sizes of the kernel sweep, comma separated")
     p.add_argument("--orders", default="rcm", help="vertex orders of the kernel sweep: rcm,hilbert")
     p.add_argument("--only", default="", help="kernel sweep: comma-separated subset of "
-                   "spmv,split,spmv32,ilu,ssor,dot,norm,axpy,gnn")
+                   "spmv,split,spmv32,ilu,ssor,dot,norm,axpy,gnn (default) and fgmres_learned")
     p.add_argument("--reps", type=int, default=20, help="kernel sweep: timed launches per kernel")
     p.add_argument("--form", choices=["plain", "mixed", "batching", "learned"], default="plain",
                    help="plain: the FP64 GMRES(30)+ILU(0) headline; mixed / batching / learned: the three "
@@ -447,6 +447,23 @@ def run_kernels(args):
                 us = timed(lambda: net.apply(x, y), max(2, args.reps // 2))
                 emit("gnn", us, per_vertex * n, tensor_tflops=round(flops / (us * 1e-6) / 1e12, 2),
                      note="one learned-preconditioner application (65 kFLOP on the tensor cores vs ~1.3 kB per vertex)")
+            if "fgmres_learned" in only and bs <= 8:
+                # One FGMRES solve with the (untrained) network and the ILU(0)
+                # fallback, 14 iterations fixed: the per-iteration mix of
+                # network, SpMV, residual check and Gram-Schmidt kernels.
+                ilu = native.Preconditioner(m, native.PC_ILU, 0)
+                pcl = native.LearnedPreconditioner(native.Learned(m, seed=1), ilu)
+                xs = native.Vector(ctx, n, 0, bs)
+                ws = native.Workspace(ctx)
+                opts = native.default_options(relative_tolerance=0.0, maximum_iterations=14, restart=30)
+
+                def solve():
+                    xs.fill(0.0)
+                    native.solve(native.FGMRES, m, pcl, x, xs, opts, ws)
+
+                us = timed(solve, 1)
+                emit("fgmres_learned", us, 0, iterations=14, fallbacks=pcl.counts()[1],
+                     note="one learned-preconditioned FGMRES solve, 14 iterations")
             ctx.synchronize()
     return 0
 

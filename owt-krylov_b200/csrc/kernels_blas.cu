@@ -499,13 +499,27 @@ __global__ void __launch_bounds__(kThreads) k_basis_dots(std::size_t n, int k, P
 #pragma unroll
     for (int j = 0; j < G; ++j) acc[j] = 0;
     double self = 0.0;
-    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
-        const T xv = x[i];
-        const T* const* bp = reinterpret_cast<const T* const*>(basis.p);
+    const T* const* bp = reinterpret_cast<const T* const*>(basis.p);
+    // U elements per pass, all loads first (the basis is read-only here).
+    constexpr int U = G <= 16 ? 2 : 1;
+    for (std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i0 < n; i0 += U * stride) {
+        T xv[U], vj[U][G - 1];
 #pragma unroll
-        for (int j = 0; j < G - 1; ++j)
-            if (j < k) acc[j] += static_cast<double>(xv) * static_cast<double>(bp[j][i]);
-        self += static_cast<double>(xv) * static_cast<double>(xv);
+        for (int u = 0; u < U; ++u) {
+            const std::size_t i = i0 + u * stride;
+            const bool in = i < n;
+            xv[u] = in ? x[i] : T(0);
+#pragma unroll
+            for (int j = 0; j < G - 1; ++j) vj[u][j] = (in && j < k) ? __ldg(bp[j] + i) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (i0 + u * stride >= n) break;
+#pragma unroll
+            for (int j = 0; j < G - 1; ++j)
+                if (j < k) acc[j] += static_cast<double>(xv[u]) * static_cast<double>(vj[u][j]);
+            self += static_cast<double>(xv[u]) * static_cast<double>(xv[u]);
+        }
     }
     {
         // block_partials<G>, written out so that acc stays in registers.
@@ -545,24 +559,37 @@ __global__ void __launch_bounds__(kThreads) k_cgs_update_dot(std::size_t n, int 
 #pragma unroll
     for (int j = 0; j < G; ++j) acc[j] = 0;
     double self = 0.0;
-    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
-        T wv = w[i];
-        T vj[G - 1];   // each basis value is read once, for the update and for its dot
+    T coef[G - 1];
 #pragma unroll
-        for (int j = 0; j < G - 1; ++j) vj[j] = j < k ? bp[j][i] : T(0);
+    for (int j = 0; j < G - 1; ++j) coef[j] = j < k ? -static_cast<T>(h[j]) : T(0);
+    // U elements per pass, all loads first; each basis value is read once
+    // (read-only path), for the update and for its dot.
+    constexpr int U = G <= 16 ? 2 : 1;
+    for (std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i0 < n; i0 += U * stride) {
+        T wv[U], vj[U][G - 1];
 #pragma unroll
-        for (int j = 0; j < G - 1; ++j) {
-            if (j < k) {
-                const T coef = -static_cast<T>(h[j]);
-                wv = add_rn(wv, mul_rn(coef, vj[j]));
-            }
+        for (int u = 0; u < U; ++u) {
+            const std::size_t i = i0 + u * stride;
+            const bool in = i < n;
+            wv[u] = in ? w[i] : T(0);
+#pragma unroll
+            for (int j = 0; j < G - 1; ++j) vj[u][j] = (in && j < k) ? __ldg(bp[j] + i) : T(0);
         }
-        w[i] = wv;
-        const double wd = static_cast<double>(wv);
 #pragma unroll
-        for (int j = 0; j < G - 1; ++j)
-            if (j < k) acc[j] += wd * static_cast<double>(vj[j]);
-        self += wd * wd;
+        for (int u = 0; u < U; ++u) {
+            const std::size_t i = i0 + u * stride;
+            if (i >= n) break;
+            T v = wv[u];
+#pragma unroll
+            for (int j = 0; j < G - 1; ++j)
+                if (j < k) v = add_rn(v, mul_rn(coef[j], vj[u][j]));
+            w[i] = v;
+            const double wd = static_cast<double>(v);
+#pragma unroll
+            for (int j = 0; j < G - 1; ++j)
+                if (j < k) acc[j] += wd * static_cast<double>(vj[u][j]);
+            self += wd * wd;
+        }
     }
     {
         // The CTA's partials (block_partials written out: acc stays in registers).
