@@ -174,6 +174,28 @@ def test_fallback_takes_every_failed_step(native, ctx):
     assert_bitwise(x1.download(), x2.download(), "fallback solution")
 
 
+def test_fgmres_reuses_the_check_product(native, ctx):
+    # FGMRES takes the network's residual-check product A z as its Arnoldi
+    # vector when the network is bound to the solver's own operator.  The
+    # same solve against a second Matrix holding the same values (no reuse:
+    # FGMRES applies the operator itself) must give the same bits, the same
+    # iterations and the same counted operator applications.
+    c, m, net, g = setup(native, ctx, side=20, seed=31)
+    n, bs = c["owned"], c["bs"]
+    net.set_parameters(bf16_weights(bs, 9))
+    m2 = native.Matrix(ctx, "bsr", n, 0, bs, c["rowptr"], c["cols"], c["vals"])
+    ilu = native.Preconditioner(m, native.PC_ILU, 0)
+    pc = native.LearnedPreconditioner(net, ilu)
+    b = native.Vector(ctx, n, 0, bs).upload(c["rhs"][: n * bs])
+    x1, x2 = native.Vector(ctx, n, 0, bs), native.Vector(ctx, n, 0, bs)
+    r1 = native.solve(native.FGMRES, m, pc, b, x1)
+    r2 = native.solve(native.FGMRES, m2, pc, b, x2)
+    assert r1.status == 0 and r1.iterations == r2.iterations
+    assert r1.operator_applications == r2.operator_applications
+    assert r1.preconditioner_applications == r2.preconditioner_applications
+    assert_bitwise(x1.download(), x2.download(), "solution with and without the reused product")
+
+
 def test_trained_network_beats_untrained(native, ctx):
     # Train on residual/error pairs of ILU(0)-GMRES solves over a few
     # coefficient draws of an anisotropic mesh, then compare FGMRES
