@@ -16,7 +16,12 @@
 // L2 round trip.  For block sizes up to 32 a lane publishes its (row,
 // component) from inside its polling loop, so a row waits for its own
 // dependencies only, not for those of the other rows of its warp's task
-// (2M-vertex mesh, bs 3: ILU(0) apply 5.75 -> 5.02 ms, SSOR 8.44 -> 6.00 ms).
+// (2M-vertex mesh, bs 3: ILU(0) apply 5.75 -> 5.02 ms, SSOR 8.44 -> 6.00 ms);
+// the dense-block sweeps publish a block row, or in the backward sweep a row
+// once all of its block rows are final (FP64 dense-block ILU(0)-FGMRES on
+// that mesh 150.6 -> 92.3 ms).  A second poll round in flight, half a round
+// trip behind the first, was slower (5.0 -> 9.6 ms): the polls and the spin
+// that staggers them cost more issue and L2 traffic than they save.
 // The numeric factorisation, which updates factor entries in
 // place, publishes per-row epoch flags instead (fence + release / relaxed
 // loads + fence).  Every wait is bounded (kSpinLimit polls): a wait that gives
@@ -361,6 +366,11 @@ constexpr bool is_scalar_apply(int mode)
     return mode == kIluForward || mode == kIluBackward || mode == kSsorForward || mode == kSsorBackward;
 }
 
+constexpr bool is_lane_apply(int mode)
+{
+    return is_scalar_apply(mode) || mode == kBlockForward || mode == kBlockBackward;
+}
+
 // Dense-block rows: acc -= sum_k (sum_j B_k[i][j] dep[col_k][j]) over k in
 // [b, e), each block-row product summed from +0 over j (the dense SpMV's
 // order); dependency values are polled until published.
@@ -423,6 +433,135 @@ __device__ __forceinline__ T block_eliminate(T acc, const SweepArgs<T, F>& a, co
         }
     }
     return acc;
+}
+
+// Dense-block apply of block row i of `row` with early publication (the
+// counterpart of eliminate_publish): the forward sweep publishes each block
+// row as soon as its own dependencies have arrived; the backward sweep forms
+// w = y - sum U x per block row, and a row publishes x = Dinv w (shuffles
+// over its bs lanes, the same sum order as the warp path) once all of its
+// lanes hold their w.  Warp-uniform loop; row < 0 for lanes without a row.
+template<class T, class F, bool BACK>
+__device__ __forceinline__ void block_apply_lane(const SweepArgs<T, F>& a, int row, int i, int rl)
+{
+    using U = typename Bits<T>::U;
+    const int bs = a.bs;
+    const bool valid = row >= 0;
+    const std::size_t rb = valid ? static_cast<std::size_t>(row) * bs : 0;
+    const T* dep = BACK ? a.out : a.work;
+    int b = 0, e = 0;
+    T acc = 0, dinv[kMaxBlock];
+#pragma unroll
+    for (int j = 0; j < kMaxBlock; ++j) dinv[j] = 0;
+    if (valid) {
+        if (BACK) {
+            b = a.diagpos[row] + 1;
+            e = a.rowptr[row + 1];
+            acc = a.work[rb + i];
+#pragma unroll
+            for (int j = 0; j < kMaxBlock; ++j)
+                if (j < bs) dinv[j] = cvt<T>(a.inv[static_cast<std::size_t>(row) * bs * bs + i * bs + j]);
+        } else {
+            b = a.rowptr[row];
+            e = a.diagpos[row];
+            acc = a.in[rb + i];
+        }
+    }
+    constexpr int kQ = 4;   // block entries per round
+    T co[kQ][kMaxBlock];
+    U xb[kQ][kMaxBlock];
+    const T* src[kQ];
+    bool on[kQ];
+    int k0 = b, it = 0;
+    bool loaded = false, ready = !valid, done = !valid;
+    const int base = (rl * bs) & 31;
+    const unsigned rowmask = (bs < 32 ? ((1u << bs) - 1u) : 0xffffffffu) << base;
+    for (;;) {
+        if (!ready) {
+            if (!loaded && k0 >= e) {
+                ready = true;
+            } else {
+                if (!loaded) {
+#pragma unroll
+                    for (int q = 0; q < kQ; ++q) {
+                        const int k = k0 + q;
+                        on[q] = k < e;
+                        src[q] = dep + static_cast<std::size_t>(on[q] ? a.cols[k] : 0) * bs;
+#pragma unroll
+                        for (int j = 0; j < kMaxBlock; ++j) {
+                            if (on[q] && j < bs) {
+                                co[q][j] = cvt<T>(a.vals[(static_cast<std::size_t>(k) * bs + i) * bs + j]);
+                                xb[q][j] = ld_relaxed_bits(src[q] + j);
+                            }
+                        }
+                    }
+                    loaded = true;
+                }
+                bool pending = false;
+#pragma unroll
+                for (int q = 0; q < kQ; ++q)
+#pragma unroll
+                    for (int j = 0; j < kMaxBlock; ++j)
+                        pending |= on[q] && j < bs && xb[q][j] == Bits<T>::kSentinel;
+                if (pending) {
+                    if (it >= kSpinLimit) {
+                        atomicOr(a.status, kErrTimeout);
+                        pending = false;
+                    } else if ((it & 1023) == 1023
+                               && (*reinterpret_cast<volatile unsigned*>(a.status) & kErrTimeout)) {
+                        pending = false;
+                    }
+                }
+                if (!pending) {
+#pragma unroll
+                    for (int q = 0; q < kQ; ++q) {
+                        if (!on[q]) continue;
+                        T sum = 0;
+#pragma unroll
+                        for (int j = 0; j < kMaxBlock; ++j)
+                            if (j < bs) sum = add_rn(sum, mul_rn(co[q][j], from_bits(xb[q][j])));
+                        acc = sub_rn(acc, sum);
+                    }
+                    k0 += kQ;
+                    loaded = false;
+                    if (k0 >= e) ready = true;
+                } else {
+                    if (it >= 256) __nanosleep(32);
+                    ++it;
+#pragma unroll
+                    for (int q = 0; q < kQ; ++q)
+#pragma unroll
+                        for (int j = 0; j < kMaxBlock; ++j)
+                            if (on[q] && j < bs && xb[q][j] == Bits<T>::kSentinel)
+                                xb[q][j] = ld_relaxed_bits(src[q] + j);
+                }
+            }
+        }
+        if constexpr (!BACK) {
+            if (ready && !done) {
+                publish(a.work + rb + i, acc);
+                done = true;
+            }
+        } else {
+            const unsigned rdy = __ballot_sync(0xffffffffu, ready);
+            const bool row_ready = (rdy & rowmask) == rowmask;
+            if (__any_sync(0xffffffffu, row_ready && !done)) {
+                T x = 0;
+#pragma unroll
+                for (int j = 0; j < kMaxBlock; ++j) {
+                    if (j < bs) {
+                        const T wj = __shfl_sync(0xffffffffu, acc, (base + j) & 31);
+                        x = add_rn(x, mul_rn(dinv[j], wj));
+                    }
+                }
+                if (row_ready && !done) {
+                    publish(a.out + rb + i, x);
+                    done = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, !done)) break;
+    }
 }
 
 // In-place Gauss-Jordan inverse of a bs x bs block with partial pivoting
@@ -552,8 +691,8 @@ __device__ __forceinline__ T row_body(const SweepArgs<T, F>& a, int row, int c0,
     return T(0);
 }
 
-// LANE: scalar applies with block size <= 32 through apply_lane (early
-// publication); otherwise row_body.
+// LANE: applies with block size <= 32 through apply_lane / block_apply_lane
+// (early publication); otherwise row_body.
 template<class T, class F, int MODE, bool LANE = false>
 __global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T, F> a)
 {
@@ -580,9 +719,11 @@ __global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T, F> a)
         const int s = a.task_start[t], nrows = a.task_start[t + 1] - s;
         const int row = rl < nrows ? a.order[s + rl] : -1;
         T w = 0;
-        if constexpr (LANE) apply_lane<T, F, MODE>(a, row, c0);
+        if constexpr (LANE && (MODE == kBlockForward || MODE == kBlockBackward))
+            block_apply_lane<T, F, MODE == kBlockBackward>(a, row, c0, rl);
+        else if constexpr (LANE) apply_lane<T, F, MODE>(a, row, c0);
         else if (row >= 0) w = row_body<T, F, MODE>(a, row, c0, cstep);
-        if constexpr (MODE == kBlockBackward) {
+        if constexpr (MODE == kBlockBackward && !LANE) {
             // x_r[i] = sum_j Dinv_r[i][j] w_j: the row's w_j live in the
             // lanes rl*bs + j of this warp.
             __syncwarp();
@@ -654,10 +795,14 @@ void launch(Context& c, Preconditioner& p, Sweep& s, SweepArgs<T, F>& a)
     a.status = c.status.as<unsigned>();
     a.owned = static_cast<int>(p.owned);
     a.bs = static_cast<int>(p.bs);
-    if (is_scalar_apply(MODE) && p.bs <= 32)
-        k_sweep<T, F, MODE, true><<<blocks, kThreads, 0, c.stream>>>(a);
-    else
-        k_sweep<T, F, MODE><<<blocks, kThreads, 0, c.stream>>>(a);
+    bool lane = false;
+    if constexpr (is_lane_apply(MODE)) {
+        if (p.bs <= 32) {
+            k_sweep<T, F, MODE, true><<<blocks, kThreads, 0, c.stream>>>(a);
+            lane = true;
+        }
+    }
+    if (!lane) k_sweep<T, F, MODE><<<blocks, kThreads, 0, c.stream>>>(a);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
     p.ticket_base += static_cast<unsigned long long>(s.tasks)
