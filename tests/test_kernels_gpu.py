@@ -258,6 +258,31 @@ def test_ilu_bitwise(native, ctx, golden, name, level):
     ctx.synchronize()
 
 
+@pytest.mark.parametrize("side,bs", [(200, 3), (160, 1), (120, 4)])
+def test_sweeps_bitwise_many_levels(native, ctx, restatement, side, bs):
+    # Hundreds of levels and thousands of warp tasks: every lane publishes its
+    # row from inside its polling loop while other lanes of its warp still
+    # wait, and rows of later levels poll rows published by other warps.
+    c = cases.lattice_case(side=side, bs=bs, seed=side + bs)
+    n = c["owned"]
+    m = bsr(native, ctx, c)
+    x = dvec(native, ctx, c, c["x"])
+    y = dvec(native, ctx, c, fill=77.0)
+    p = native.Preconditioner(m, native.PC_ILU, 0)
+    lo, up, dl, du = p.levels()
+    assert dl > 100 and du > 100
+    ref = restatement.ilu(n, bs, c["rowptr"], c["cols"], c["vals"], 0)
+    for rep in range(2):
+        p.apply(x, y)
+        assert_bitwise(y.download()[: n * bs], ref.apply(c["x"]), f"ilu(0) apply {rep}")
+    for om in (1.0, 1.3):
+        code, expect = restatement.ssor_apply(n, bs, c["rowptr"], c["cols"], c["vals"], om, c["x"])
+        assert code == 0
+        native.Preconditioner(m, native.PC_SSOR, om).apply(x, y)
+        assert_bitwise(y.download()[: n * bs], expect, f"ssor {om}")
+    ctx.synchronize()
+
+
 def test_ilu_levels_match_oracle(native, ctx, restatement):
     c = cases.build("lattice8_bs3")
     m = bsr(native, ctx, c)

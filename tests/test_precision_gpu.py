@@ -44,6 +44,26 @@ def test_block_ilu_bitwise(native, ctx, restatement, kw):
     ctx.synchronize()
 
 
+@pytest.mark.parametrize("side,bs", [(120, 3), (90, 4)])
+def test_block_ilu_bitwise_many_levels(native, ctx, restatement, side, bs):
+    # Hundreds of levels: block rows publish as soon as their own
+    # dependencies arrive, and a row of the backward sweep publishes once all
+    # of its block rows are final.
+    c = cases.dense_case(side=side, bs=bs, seed=side)
+    n = c["owned"]
+    m = dense_matrix(native, ctx, c)
+    p = native.Preconditioner(m, native.PC_BLOCK_ILU)
+    ref = restatement.block_ilu(n, bs, c["rowptr"], c["cols"], c["vals"])
+    assert ref.status == 0
+    x = native.Vector(ctx, n, 0, bs).upload(c["x"])
+    y = native.Vector(ctx, n, 0, bs)
+    expect = ref.apply(c["x"])
+    for rep in range(2):
+        p.apply(x, y)
+        assert_bitwise(y.download(), expect, f"block apply {rep}")
+    ctx.synchronize()
+
+
 def test_block_ilu_update_values(native, ctx, restatement):
     c = cases.dense_case(side=5, bs=3, seed=18)
     n, bs = c["owned"], c["bs"]
