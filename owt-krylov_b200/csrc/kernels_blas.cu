@@ -486,9 +486,10 @@ __global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, Ptr
 }
 
 // Dots of x with every V_j (j < k) and x.x in one pass: x and each V_j are
-// read once per element.  The products and the per-thread, per-CTA and
-// over-CTA sums are those of k_multidot on the pairs (x, V_j) and (x, x), so
-// the results are the same bits.
+// read once per element.  The grid, the per-thread element order and the CTA
+// and over-CTA sums follow k_multidot on the pairs (x, V_j) and (x, x); the
+// results agree with it to FP64 rounding (a few ulps, measured), not always
+// bit for bit, so a caller keeps to one of the two kernels for a given dot.
 template<class T, int G>
 __global__ void __launch_bounds__(kThreads) k_basis_dots(std::size_t n, int k, PtrPack basis,
                                                          const T* __restrict__ x, double* partials, unsigned* ticket,
