@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--bs", default="3", help="block sizes of the kernel sweep, comma separated")
     p.add_argument("--orders", default="rcm", help="vertex orders of the kernel sweep: rcm,hilbert")
     p.add_argument("--only", default="", help="kernel sweep: comma-separated subset of "
-                   "spmv,split,spmv32,ilu,ssor,dot,norm,axpy,gnn (default) and fgmres_learned")
+                   "spmv,split,spmv32,dense,dense32,ilu,ssor,dot,norm,axpy,gnn (default) and fgmres_learned")
     p.add_argument("--reps", type=int, default=20, help="kernel sweep: timed launches per kernel")
     p.add_argument("--form", choices=["plain", "mixed", "batching", "learned"], default="plain",
                    help="plain: the FP64 GMRES(30)+ILU(0) headline; mixed / batching / learned: the three "
@@ -331,6 +331,8 @@ def kernel_bytes(kind: str, n: int, bs: int, nnz: int, sv: int = 8, factor_entri
     vec = n * bs * sv
     if kind in ("spmv", "spmv32"):
         return nnz * (bs * sv + 4) + (n + 1) * 4 + 2 * vec
+    if kind in ("dense", "dense32"):
+        return nnz * (bs * bs * sv + 4) + (n + 1) * 4 + 2 * vec
     if kind == "split":
         return vec + off_entries * (bs * sv + 4) + (n + 1) * 4 + 2 * vec
     if kind == "ilu":
@@ -362,8 +364,8 @@ def run_kernels(args):
     from owtk_b200 import native, problems
 
     peak, peak_kind = measured_peaks()
-    only = set(filter(None, args.only.split(","))) or {"spmv", "split", "spmv32", "ilu", "ssor", "dot", "norm", "axpy",
-                                                        "gnn"}
+    only = set(filter(None, args.only.split(","))) or {"spmv", "split", "spmv32", "dense", "dense32", "ilu", "ssor",
+                                                        "dot", "norm", "axpy", "gnn"}
     t = time.time()
     xy, edges = problems.disk_mesh(args.vertices, args.seed)
     gen_s = time.time() - t
@@ -414,6 +416,22 @@ def run_kernels(args):
                 x32 = native.Vector(ctx, n, 0, bs, dtype=np.float32).upload(s.rhs)
                 y32 = native.Vector(ctx, n, 0, bs, dtype=np.float32)
                 emit("spmv32", timed(lambda: m32.apply(x32, y32), args.reps), kernel_bytes("spmv32", n, bs, nnz, sv=4))
+            if ("dense" in only or "dense32" in only) and bs <= 4:
+                # Dense bs x bs blocks on the same mesh (the precision form's
+                # matrix): FP64, and FP32 as its inner SpMV.
+                sd = problems.dense_block_system(xy, edges, bs, np.random.default_rng(args.seed), order=order)
+                if "dense" in only:
+                    md = native.Matrix(ctx, "dense", n, 0, bs, sd.rowptr, sd.cols, sd.vals)
+                    xd = native.Vector(ctx, n, 0, bs).upload(sd.rhs)
+                    emit("dense", timed(lambda: md.apply(xd, y), args.reps), kernel_bytes("dense", n, bs, sd.nnz))
+                    del md
+                if "dense32" in only:
+                    md32 = native.Matrix(ctx, "dense", n, 0, bs, sd.rowptr, sd.cols, sd.vals, dtype=np.float32)
+                    xd32 = native.Vector(ctx, n, 0, bs, dtype=np.float32).upload(sd.rhs)
+                    yd32 = native.Vector(ctx, n, 0, bs, dtype=np.float32)
+                    emit("dense32", timed(lambda: md32.apply(xd32, yd32), args.reps),
+                         kernel_bytes("dense32", n, bs, sd.nnz, sv=4))
+                    del md32
             if "ilu" in only:
                 pc = native.Preconditioner(m, native.PC_ILU, 0)
                 fe = int(pc.ilu_factors()[1].size)

@@ -53,9 +53,12 @@ __device__ __forceinline__ int div_bs(int k, unsigned long long magic)
     return static_cast<int>((static_cast<unsigned long long>(k) * magic) >> 32);
 }
 
-// KIND 0: component-diagonal BSR, 1: split view, 2: dense BSR.
-template<class T, int KIND>
-__global__ void __launch_bounds__(kThreads, 4) k_spmv_tiles(SpmvArgs<T> a)
+// KIND 0: component-diagonal BSR, 1: split view, 2: dense BSR.  BS: dense
+// block size known at compile time (0: any); those instances load every
+// operand of a thread's units before the first product and keep two CTAs
+// per SM for the registers that takes.
+template<class T, int KIND, int BS = 0>
+__global__ void __launch_bounds__(kThreads, (KIND == 2 && BS > 0) ? 2 : 4) k_spmv_tiles(SpmvArgs<T> a)
 {
     constexpr int kPer = kStage / kThreads;   // staged units per thread
     __shared__ T prod[kStage];
@@ -103,7 +106,36 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmv_tiles(SpmvArgs<T> a)
         }
     }
 
-    if (KIND == 2) {
+    if (KIND == 2 && BS > 0) {
+        // Contribution of entry e to block row br: sum_bc B[e][br][bc] x[col][bc]
+        // (summed from +0 over bc), with all of this thread's block-row
+        // values, columns and x blocks requested before the arithmetic.
+        T bv[kPer][BS > 0 ? BS : 1], xv[kPer][BS > 0 ? BS : 1];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            if (k < units) {
+                const int e = div_bs(k, a.magic);
+                const T* blk = a.vals + (static_cast<std::size_t>(e0) * BS + k) * BS;
+                const T* xs = a.x + static_cast<std::size_t>(__ldg(a.cols + e0 + e)) * BS;
+#pragma unroll
+                for (int bc = 0; bc < BS; ++bc) {
+                    bv[j][bc] = __ldcs(blk + bc);
+                    xv[j][bc] = __ldg(xs + bc);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            const int k = threadIdx.x + j * kThreads;
+            if (k < units) {
+                T contribution = 0;
+#pragma unroll
+                for (int bc = 0; bc < BS; ++bc) contribution = add_rn(contribution, mul_rn(bv[j][bc], xv[j][bc]));
+                prod[k] = contribution;
+            }
+        }
+    } else if (KIND == 2) {
         // Contribution of entry e to block row br: sum_bc B[e][br][bc] x[col][bc].
         for (int k = threadIdx.x; k < units; k += kThreads) {
             const int e = div_bs(k, a.magic);
@@ -608,6 +640,12 @@ template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
         k_spmv_tiles<T, 0><<<grid, kThreads, 0, c.stream>>>(a);
     } else if (m.kind == 1) {
         k_spmv_tiles<T, 1><<<grid, kThreads, 0, c.stream>>>(a);
+    } else if (m.bs == 2) {
+        k_spmv_tiles<T, 2, 2><<<grid, kThreads, 0, c.stream>>>(a);
+    } else if (m.bs == 3) {
+        k_spmv_tiles<T, 2, 3><<<grid, kThreads, 0, c.stream>>>(a);
+    } else if (m.bs == 4) {
+        k_spmv_tiles<T, 2, 4><<<grid, kThreads, 0, c.stream>>>(a);
     } else {
         k_spmv_tiles<T, 2><<<grid, kThreads, 0, c.stream>>>(a);
     }
