@@ -1,7 +1,7 @@
 """Device-resident solves through the C ABI against the reference's solves.
 
 The device reductions sum in a different order than the reference's 8-lane
-serial reduction, so the bar is the north-star one: same status, the same
+serial reduction, so the bar is: same status, the same
 true-residual tolerance reached, iteration counts within +-2 (and identical
 work counters whenever the iteration counts agree), and solutions equal to
 the reference's to the solver tolerance.
