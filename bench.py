@@ -34,7 +34,7 @@ METRIC = "time-to-rtol 1e-8 on B200, learned/mixed vs plain FP64 ILU-GMRES; SpMV
 # ncu capture on the 1M-vertex disk mesh (profiles/ilu0_sweeps_fp64_1m_vertices.md,
 # profiles/spmv_bulk_bsr3_fp64_1m_vertices.md); traffic grows with the vertex
 # count, so the benchmark's per-launch traffic is this times its vertices.
-PROFILED_TRAFFIC_PER_VERTEX = {"ilu0 sweep pair": (255.98e6 + 20.89e6 + 279.87e6 + 21.80e6) / 999_573,
+PROFILED_TRAFFIC_PER_VERTEX = {"ilu0 sweep pair": (255.98e6 + 20.01e6 + 279.70e6 + 21.33e6) / 999_573,
                                "spmv": (224.46e6 + 5.60e6) / 999_573}
 WORKLOAD = "plain-fp64-gmres30-ilu0"
 
