@@ -1,14 +1,23 @@
-"""Benchmark: time to true-residual rtol 1e-8 of plain FP64 GMRES(30) + block-Jacobi
-ILU(0) on the 2M-vertex Poisson-disk/Delaunay disk mesh (RCM-ordered, bs 3),
-plus the SpMV / ILU-apply kernels' achieved HBM bandwidth.
+"""Benchmark: time to true-residual rtol 1e-8 on one B200 of the learned-
+preconditioned FGMRES(30) against plain FP64 ILU(0)-GMRES(30), on the
+8M-vertex anisotropic Poisson-disk/Delaunay unit-square mesh (RCM, bs 3).
 
-One step = one complete solve from x0 = 0 with the matrix and the ILU(0)
-factors resident in HBM (setup timed separately).  N GPUs run N independent
+One step = one complete solve from x0 = 0 with the matrix, the ILU(0)
+factors and the trained network resident in HBM (setup timed separately).
+`value` is the learned solve; the plain FP64 ILU(0)-GMRES(30) solve of the
+same system on the same GPU, their ratio, the network's layer roofline and
+the 2M-vertex plain workload are extra keys.  N GPUs run N independent
 replicas (the path has no exchange step on one rank's system): every rank
 solves its own copy, steps are timed with CUDA events on the library's stream
 between barriers, and the slowest rank's time is reported.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form learned|plain|mixed|batching] [--kernels]
+
+--impl reference times the reference's own CPU GMRES(30) + ILU(0)
+(oracle/_ref, built from the unmodified reference headers) on the same
+system, which that process builds with the reference's own RCM ordering and
+without loading this project's library.
 """
 from __future__ import annotations
 
@@ -29,25 +38,26 @@ for _p in (REPO, PKG):
 import numpy as np  # noqa: E402
 
 METRIC = "time-to-rtol 1e-8 on B200, learned/mixed vs plain FP64 ILU-GMRES; SpMV HBM GB/s"
-
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per vertex from one
-# ncu capture on the 1M-vertex disk mesh (profiles/ilu0_sweeps_fp64_1m_vertices.md,
-# profiles/spmv_bulk_bsr3_fp64_1m_vertices.md); traffic grows with the vertex
-# count, so the benchmark's per-launch traffic is this times its vertices.
-PROFILED_TRAFFIC_PER_VERTEX = {"ilu0 sweep pair": (255.98e6 + 20.01e6 + 279.70e6 + 21.33e6) / 999_573,
-                               "spmv": (224.46e6 + 5.60e6) / 999_573}
-WORKLOAD = "plain-fp64-gmres30-ilu0"
+WEIGHTS = os.path.join(PKG, "weights", "learned_anisotropic_bs3.owtkgnn")
+TRAFFIC_FILE = os.path.join(REPO, "profiles", "dram_traffic_per_vertex.txt")
+MESH_CACHE = os.path.join(REPO, ".bench_cache")
+WORKLOADS = {"learned": "learned-fgmres30-vs-ilu0-gmres30-anisotropic-8m",
+             "plain": "plain-fp64-gmres30-ilu0"}
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--vertices", type=int, default=2_000_000)
-    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--vertices", type=int, default=None,
+                   help="mesh size (default: 8M for the learned form, 2M otherwise)")
+    p.add_argument("--seed", type=int, default=None, help="mesh seed (default: 4 learned, 1 otherwise)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain-2m", action="store_true", help="learned form: skip the 2M-vertex plain keys")
+    p.add_argument("--ref-budget", type=float, default=900.0,
+                   help="reference arm: seconds of timed full solves at most (the first solve is the warm-up)")
     p.add_argument("--kernels", action="store_true",
                    help="standalone kernel throughput sweep (one JSON line per kernel) instead of the solve")
     p.add_argument("--bs", default="3", help="block sizes of the kernel sweep, comma separated")
@@ -55,14 +65,17 @@ def parse():
     p.add_argument("--only", default="", help="kernel sweep: comma-separated subset of "
                    "spmv,split,spmv32,dense,dense32,ilu,ssor,dot,norm,axpy,gnn (default) and fgmres_learned")
     p.add_argument("--reps", type=int, default=20, help="kernel sweep: timed launches per kernel")
-    p.add_argument("--form", choices=["plain", "mixed", "batching", "learned"], default="plain",
-                   help="plain: the FP64 GMRES(30)+ILU(0) headline; mixed / batching / learned: the three "
-                        "other forms, one JSON line each")
+    p.add_argument("--form", choices=["learned", "plain", "mixed", "batching"], default="learned",
+                   help="learned: the headline (8M anisotropic, learned FGMRES vs plain FP64 ILU(0)-GMRES); "
+                        "plain: FP64 GMRES(30)+ILU(0) on the 2M disk mesh; mixed / batching: the other forms")
     p.add_argument("--systems", type=int, default=256, help="batching: number of systems")
-    p.add_argument("--draws", type=int, default=32, help="learned: coefficient draws of the training mesh")
-    p.add_argument("--train-vertices", type=int, default=200_000, help="learned: training mesh size")
-    p.add_argument("--epochs", type=int, default=20, help="learned: passes over the training pairs (rate 3e-3 decaying to 3e-4)")
-    return p.parse_args()
+    p.add_argument("--weights", default=WEIGHTS, help="learned: checkpoint of the trained network")
+    a = p.parse_args(argv)
+    if a.vertices is None:
+        a.vertices = 8_000_000 if a.form == "learned" else 2_000_000
+    if a.seed is None:
+        a.seed = 4 if a.form == "learned" else 1
+    return a
 
 
 def dist_env():
@@ -75,6 +88,29 @@ def measured_peaks():
         d = json.load(open(path))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_tensor_peak():
+    """Dense BF16 TFLOP/s sustained (a kernel timed inside a long solve)."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        if "bf16_tflops_sustained" in d:
+            return float(d["bf16_tflops_sustained"]), "measured sustained"
+    return 1400.0, "fallback sustained"
+
+
+def profiled_traffic():
+    """DRAM bytes per vertex of each kernel from ncu captures, kept as
+    "name: bytes_per_vertex" lines in the profiles' traffic table."""
+    out = {}
+    if os.path.exists(TRAFFIC_FILE):
+        for line in open(TRAFFIC_FILE):
+            line = line.split("#", 1)[0].strip()
+            if ":" in line:
+                k, v = line.rsplit(":", 1)
+                out[k.strip()] = float(v)
+    return out
 
 
 class Clocks:
@@ -121,12 +157,59 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_system(n_vertices: int, seed: int):
+# ---------------------------------------------------------------- systems
+def cached_mesh(n_target: int, seed: int, domain: str):
+    """Poisson-disk points and Delaunay edges, kept in .bench_cache/ so the
+    second arm run on the same host reuses the first one's mesh."""
+    from owtk_b200 import problems
+
+    os.makedirs(MESH_CACHE, exist_ok=True)
+    stem = os.path.join(MESH_CACHE, f"{domain}-{n_target}-{seed}")
+    try:
+        meta = json.load(open(stem + ".json"))
+        xy = np.load(stem + "-xy.npy")
+        edges = np.load(stem + "-edges.npy")
+        if xy.shape == (meta["points"], 2) and edges.shape == (meta["edges"], 2):
+            return xy, edges
+    except (OSError, ValueError, KeyError):
+        pass
+    xy, edges = problems.disk_mesh(n_target, seed, domain=domain)
+    np.save(stem + "-xy.npy", xy)
+    np.save(stem + "-edges.npy", edges)
+    json.dump({"points": int(xy.shape[0]), "edges": int(edges.shape[0])}, open(stem + ".json", "w"))
+    return xy, edges
+
+
+def build_system(form: str, n_vertices: int, seed: int, rcm=None):
+    """The workload's system; `rcm` computes the RCM order (default: this
+    library's; the reference arm passes the reference's own)."""
     from owtk_b200 import problems
 
     t = time.time()
-    s = problems.config1(n_vertices, seed=seed)
+    if form == "learned":
+        xy, edges = cached_mesh(n_vertices, seed, "square")
+        rng = np.random.default_rng([seed, 0])
+        s = problems.anisotropic_system(xy, edges, 3, rng, order="rcm", rcm=rcm)
+    else:
+        xy, edges = cached_mesh(n_vertices, seed, "disk")
+        rng = np.random.default_rng(seed)
+        s = problems.component_diagonal_system(xy, edges, 3, rng, order="rcm", rcm=rcm)
     return s, time.time() - t
+
+
+def workload_config(form: str, s, world: int) -> dict:
+    """The `config` both arms print for one workload (same keys and values)."""
+    if form == "learned":
+        return {"workload": WORKLOADS["learned"], "vertices": s.owned, "entries": s.nnz, "block_size": s.bs,
+                "mesh": "poisson-disk unit square, delaunay, anisotropic w=1+1e4(e.d)^2, skew U(-0.3,0.3)",
+                "solver": "ours: fgmres(30) + learned network (ilu(0) fallback), fp64 outer; "
+                          "reference: gmres(30) + ilu(0) fp64",
+                "rtol": 1e-8, "ordering": "rcm", "parallelism": f"replicas{world}",
+                "l2": "inputs larger than L2 (matrix 1.3 GB, Krylov basis 11.5 GB)"}
+    return {"workload": WORKLOADS["plain"], "vertices": s.owned, "entries": s.nnz, "block_size": s.bs,
+            "mesh": "poisson-disk unit disk, delaunay, component-diagonal", "solver": "gmres(30)+ilu(0)",
+            "rtol": 1e-8, "ordering": "rcm", "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (matrix 336 MB, Krylov basis 2.9 GB)"}
 
 
 def algorithmic_bytes(s, ilu_entries: int):
@@ -134,60 +217,142 @@ def algorithmic_bytes(s, ilu_entries: int):
     return kernel_bytes("spmv", n, bs, nnz), kernel_bytes("ilu", n, bs, nnz, factor_entries=ilu_entries)
 
 
-def cpu_reference_solve(s, reps: int, native_build: bool = False):
-    """The reference's own CPU GMRES(30)+ILU(0) (oracle/_ref), one host thread."""
+def gnn_layer_bytes(n: int) -> int:
+    """One fused message-passing layer (layers 1-3): each vertex's BF16 row of
+    64 features read once and its new row written once (128 B each), and its
+    padded 8-slot neighbour list (32-bit column + BF16 weight per slot, 48 B)."""
+    return n * (2 * 128 + 48)
+
+
+def gnn_layer_flops(n: int) -> int:
+    """[h | m] (n x 128) times Wl^T (128 x 64) on the tensor cores."""
+    return 2 * n * 128 * 64
+
+
+# ---------------------------------------------------------------- CPU reference
+def cpu_reference_solve(s, reps: int, native_build: bool = False, restart: int = 30):
+    """The reference's own CPU GMRES(restart)+ILU(0) (oracle/_ref), one host
+    thread; returns None when that build is absent."""
     import oracle
 
     try:
         ref = oracle.Reference(native=native_build)
-        kind = "reference"
     except FileNotFoundError:
         return None
     m = ref.matrix("bsr", s.owned, 0, s.bs, s.rowptr, s.cols, s.vals)
     t = time.time()
     pc = ref.pc("ilu", m, 0)
     setup = time.time() - t
-    opts = oracle.default_options(restart=30)
+    opts = oracle.default_options(restart=restart)
     times, last = [], None
     for _ in range(reps):
         t = time.time()
         r, x = ref.solve("gmres", m, pc, opts, s.rhs, np.zeros(s.owned * s.bs))
         times.append(time.time() - t)
         last = r
-    return {"kind": kind, "seconds": times, "setup_seconds": setup, "iterations": int(last.iterations),
-            "status": int(last.status), "true_residual": float(last.true_residual_norm)}
+    return {"kind": "reference", "isa": ref.isa or "as shipped (no -march)", "seconds": times,
+            "setup_seconds": setup, "iterations": int(last.iterations), "status": int(last.status),
+            "true_residual": float(last.true_residual_norm)}
 
 
 def run_reference(args):
+    """The reference's CPU GMRES(30)+ILU(0) on the workload's system, built in
+    this process with the reference's own RCM (oracle/_ref); this project's
+    library is not loaded.  One step = one full solve from x0 = 0.  The first
+    full solve is the warm-up; timed solves stop at --steps or when
+    --ref-budget seconds of them are spent, whichever comes first."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    s, gen = build_system(args.vertices, args.seed)
-    res = cpu_reference_solve(s, args.warmup + args.steps)
-    if res is None:
+    import oracle
+
+    try:
+        ref = oracle.Reference()
+    except FileNotFoundError:
         print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
         return 0
-    timed = res["seconds"][args.warmup:]
+    form = "learned" if args.form == "learned" else "plain"
+    s, gen_s = build_system(form, args.vertices, args.seed, rcm=ref.rcm)
+    m = ref.matrix("bsr", s.owned, 0, s.bs, s.rowptr, s.cols, s.vals)
+    t = time.time()
+    pc = ref.pc("ilu", m, 0)
+    setup_s = time.time() - t
+    opts = oracle.default_options(restart=30)
+    x0 = np.zeros(s.owned * s.bs)
+    warm, timed, last = [], [], None
+    for _ in range(max(1, min(args.warmup, 1))):
+        t = time.time()
+        last, _x = ref.solve("gmres", m, pc, opts, s.rhs, x0)
+        warm.append(time.time() - t)
+    spent = 0.0
+    while len(timed) < args.steps and (not timed or spent + timed[-1] <= args.ref_budget):
+        t = time.time()
+        last, _x = ref.solve("gmres", m, pc, opts, s.rhs, x0)
+        timed.append(time.time() - t)
+        spent += timed[-1]
     v = statistics.mean(timed)
+    cpu = oracle.host_cpu()
     line = {
-        "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": len(timed),
+        "warmup": len(warm), "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "vertices": s.owned, "entries": s.nnz, "block_size": s.bs,
-                   "solver": "gmres(30)+ilu(0)", "rtol": 1e-8, "ordering": "rcm"},
+        "config": workload_config(form, s, world),
         "impl": "reference",
-        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": res["kind"],
-                         "sample": f"full solve of the {s.owned}-vertex system, {res['iterations']} iterations, "
-                                   "one thread (the reference is single-threaded)"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
+                         "sample": f"{len(timed)} full reference GMRES(30)+ILU(0) solves of the "
+                                   f"{s.owned}-vertex system ({int(last.iterations)} iterations each), one thread "
+                                   f"(the reference is single-threaded); steps requested {args.steps}, "
+                                   f"timed solves capped at {args.ref_budget:.0f} s",
+                         "cpu": cpu},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_iterations": res["iterations"], "reference_setup_s": res["setup_seconds"],
+        "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "reference_iterations": int(last.iterations), "reference_status": int(last.status),
+        "reference_true_relative_residual": float(last.true_residual_norm / np.linalg.norm(s.rhs)),
+        "reference_setup_s": setup_s, "system_build_s": gen_s, "warmup_seconds": warm,
+        "ordering_by": "reference reverse_cuthill_mckee_order",
     }
     print(json.dumps(line))
     return 0
 
 
-def run_ours(args):
+# ---------------------------------------------------------------- our arm
+def _events(stream, fn, steps):
     import torch
+
+    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    c.record(stream)
+    c.synchronize()
+    return a.elapsed_time(c) / steps
+
+
+def _max_over_ranks(ms, world, local):
+    if world > 1:
+        import torch
+
+        tt = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        return float(tt.item())
+    return ms
+
+
+def _checked(r, rhs_norm, rtol=1e-8, what="solve"):
+    """A timed step counts only if it converged with the true residual at
+    rtol (x0 = 0: the initial residual is the right-hand side)."""
+    if r.status != 0 or not (r.true_residual_norm <= rtol * rhs_norm * (1 + 1e-12)):
+        raise RuntimeError(f"{what} did not reach rtol {rtol}: {r.as_dict()}")
+    return r
+
+
+def run_learned(args):
+    """The headline: learned-preconditioned FGMRES(30) vs plain FP64
+    ILU(0)-GMRES(30) on the 8M-vertex anisotropic mesh, both to true-residual
+    rtol 1e-8 from x0 = 0.  The network's weights come from the committed
+    checkpoint (trained on 500 coefficient draws of a 200k-vertex mesh)."""
+    import torch
+    from owtk_b200 import checkpoint, native
 
     rank, world, local = dist_env()
     if world > 1:
@@ -195,16 +360,18 @@ def run_ours(args):
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    from owtk_b200 import native
-
-    s, gen_s = build_system(args.vertices, args.seed + 0)   # replicas share the system
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    s, gen_s = build_system("learned", args.vertices, args.seed)
     n, bs = s.owned, s.bs
+    bnorm = float(np.linalg.norm(s.rhs))
     ctx = native.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     t = time.time()
     m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
-    pc = native.Preconditioner(m, native.PC_ILU, 0)
+    ilu = native.Preconditioner(m, native.PC_ILU, 0)
+    net = native.Learned(m, seed=1)
+    ck = checkpoint.load_network(args.weights, net, with_optimizer=False)
+    pcl = native.LearnedPreconditioner(net, ilu)
     ctx.synchronize()
     setup_s = time.time() - t
     opts = native.default_options(restart=30, relative_tolerance=1e-8)
@@ -218,106 +385,281 @@ def run_ours(args):
         torch.cuda.synchronize(local)
         ctx.synchronize()
 
-    def step():
+    last = {}
+
+    def step(pc, name):
         x.fill(0.0)
-        r = native.solve(native.FGMRES, m, pc, b, x, opts, ws)
-        if r.status != 0:
-            raise RuntimeError(f"solve did not converge: {r.as_dict()}")
-        return r
+        last[name] = _checked(native.solve(native.FGMRES, m, pc, b, x, opts, ws), bnorm, what=name)
 
     for _ in range(args.warmup):
-        last = step()
+        step(pcl, "learned")
     barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    apps0, falls0 = pcl.counts()
     launches0 = ctx.kernel_launches
     with Clocks(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            last = step()
-        e1.record(stream)
-        e1.synchronize()
+        ms = _events(stream, lambda: step(pcl, "learned"), args.steps)
     barrier()
     launches = ctx.kernel_launches - launches0
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        tt = torch.tensor([ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
+    apps1, falls1 = pcl.counts()
+    ms = _max_over_ranks(ms, world, local)
+    learned_x = x.download()
+
+    # Plain FP64 ILU(0)-GMRES(30) on the same system and GPU.
+    for _ in range(max(1, args.warmup // 2)):
+        step(ilu, "plain")
+    barrier()
+    plain_ms = _max_over_ranks(_events(stream, lambda: step(ilu, "plain"), args.steps), world, local)
 
     # End to end through the reference-facing host-buffer call: pinned rhs/x
     # copied in, solved, x copied back, every step.
     hb = torch.from_numpy(s.rhs.astype(np.float64)).pin_memory()
     hx = torch.zeros(n * bs, dtype=torch.float64).pin_memory()
-    for _ in range(1):
-        hx.zero_()
-        native.solve_host(native.FGMRES, m, pc, hb.data_ptr(), hx.data_ptr(), opts, ws)
-    barrier()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        hx.zero_()
-        r = native.solve_host(native.FGMRES, m, pc, hb.data_ptr(), hx.data_ptr(), opts, ws)
-        assert r.status == 0
-    e3.record(stream)
-    e3.synchronize()
-    e2e_ms = e2.elapsed_time(e3) / args.steps
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
 
-    # Kernel rooflines, live: average launch time of the dominant kernel (the
-    # ILU(0) forward+backward sweep pair) and of the SpMV, CUDA events on the
-    # library's stream.  The matrix (336 MB) exceeds L2, so each launch streams
-    # it from HBM.
+    def host_step():
+        hx.zero_()
+        _checked(native.solve_host(native.FGMRES, m, pcl, hb.data_ptr(), hx.data_ptr(), opts, ws), bnorm,
+                 what="learned (host buffers)")
+
+    host_step()
+    barrier()
+    e2e_ms = _max_over_ranks(_events(stream, host_step, args.steps), world, local)
+
+    # Roofline of the dominant kernel, live: the fused message-passing layer
+    # (k_gnn_layer, layers 1-3) timed per launch with CUDA events on the
+    # library's stream over a network application on the right-hand side.
+    y = native.Vector(ctx, n, 0, bs)
+    st = net.stage_times(b, y, 20)
+    peak, peak_kind = measured_peaks()
+    tpeak, tpeak_kind = measured_tensor_peak()
+    lb, lf = gnn_layer_bytes(n), gnn_layer_flops(n)
+    layer_s = st["layer"] * 1e-3
+    traffic = profiled_traffic()
+    per_solve_apps = (apps1 - apps0) / args.steps
+    clocks = clk.summary()
+    cpu = plain2m = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        cpu = cpu_reference_solve(s, 1)
+        vec = cpu_reference_solve(s, 1, native_build=True) if cpu else None
+    if not args.no_plain_2m:
+        plain2m = plain_2m_keys(ctx, stream, world, local)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+bf16", "data": "synthetic",
+            "config": workload_config("learned", s, world),
+            "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * n * bs * 8,
+                    "d2h_bytes_per_step": n * bs * 8},
+            "roofline": {"bound": "hbm", "kernel": "k_gnn_layer (fused message-passing layer, layers 1-3)",
+                         "achieved": lb / layer_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": lb / layer_s / 1e9 / peak,
+                         "traffic": traffic["k_gnn_layer"] * n if "k_gnn_layer" in traffic else None,
+                         "traffic_source": "ncu DRAM bytes per vertex of one captured launch, scaled to this mesh",
+                         "bytes_per_launch": lb, "ms_per_launch": st["layer"], "peak_source": peak_kind,
+                         "tensor": {"achieved": lf / layer_s / 1e12, "peak": tpeak, "unit": "TFLOP/s",
+                                    "frac": lf / layer_s / 1e12 / tpeak, "flops_per_launch": lf,
+                                    "peak_source": tpeak_kind},
+                         "network_stages_ms": st,
+                         "network_share_of_solve": per_solve_apps * st["application"] / ms},
+            "learned": {"iterations": int(last["learned"].iterations),
+                        "true_relative_residual": float(last["learned"].true_residual_norm / bnorm),
+                        "network_applications_per_solve": per_solve_apps,
+                        "fallbacks_per_solve": (falls1 - falls0) / args.steps,
+                        "weights": os.path.relpath(args.weights, REPO),
+                        "training": {k: ck["metadata"].get(k) for k in ("draws", "train_vertices", "epochs",
+                                                                        "pairs_per_draw", "command")}},
+            "plain_fp64_ilu0_gmres30": {"ms": plain_ms, "iterations": int(last["plain"].iterations),
+                                        "true_relative_residual": float(last["plain"].true_residual_norm / bnorm)},
+            "speedup_vs_plain_fp64_ilu_gmres": plain_ms / ms,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "setup_s": setup_s, "system_build_s": gen_s,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {
+                "value": cpu["seconds"][0], "unit": "s", "cores": 1, "kind": "reference",
+                "sample": f"one full reference GMRES(30)+ILU(0) solve of the same system "
+                          f"({cpu['iterations']} iterations, ILU setup {cpu['setup_seconds']:.1f} s excluded), "
+                          "reference built as shipped (-O3, no -march)",
+                "cpu": oracle.host_cpu(),
+                "vector_build": None if vec is None else {
+                    "value": vec["seconds"][0], "isa": vec["isa"], "iterations": vec["iterations"]}}
+            line["parity"] = {"plain_iterations": int(last["plain"].iterations),
+                              "reference_iterations": cpu["iterations"],
+                              "within_2": abs(int(last["plain"].iterations) - cpu["iterations"]) <= 2,
+                              "reference_true_relative_residual": cpu["true_residual"] / bnorm}
+        if plain2m is not None:
+            line["plain_2m"] = plain2m
+        print(json.dumps(line))
+    del learned_x
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def plain_2m_keys(ctx, stream, world, local, steps: int = 5):
+    """The 2M-vertex disk workload (FP64 GMRES(30)+ILU(0)): solve time, e2e,
+    and the live rooflines of the ILU(0) sweep pair and the SpMV."""
+    import torch
+    from owtk_b200 import native
+
+    s, gen_s = build_system("plain", 2_000_000, 1)
+    n, bs = s.owned, s.bs
+    bnorm = float(np.linalg.norm(s.rhs))
+    m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
+    pc = native.Preconditioner(m, native.PC_ILU, 0)
+    opts = native.default_options(restart=30, relative_tolerance=1e-8)
+    ws = native.Workspace(ctx)
+    b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
+    x = native.Vector(ctx, n, 0, bs)
+    res = {}
+
+    def step():
+        x.fill(0.0)
+        res["r"] = _checked(native.solve(native.FGMRES, m, pc, b, x, opts, ws), bnorm, what="plain 2M")
+
+    for _ in range(2):
+        step()
+    ctx.synchronize()
+    ms = _max_over_ranks(_events(stream, step, steps), world, local)
+    hb = torch.from_numpy(s.rhs.astype(np.float64)).pin_memory()
+    hx = torch.zeros(n * bs, dtype=torch.float64).pin_memory()
+
+    def host_step():
+        hx.zero_()
+        _checked(native.solve_host(native.FGMRES, m, pc, hb.data_ptr(), hx.data_ptr(), opts, ws), bnorm)
+
+    host_step()
+    e2e_ms = _max_over_ranks(_events(stream, host_step, steps), world, local)
     ilu_entries = int(pc.ilu_factors()[1].size)
     spmv_bytes, ilu_bytes = algorithmic_bytes(s, ilu_entries)
     y = native.Vector(ctx, n, 0, bs)
+    m.apply(b, y)
+    pc.apply(b, y)
+    ctx.synchronize()
+    spmv_ms = _events(stream, lambda: m.apply(b, y), 50)
+    ilu_ms = _events(stream, lambda: pc.apply(b, y), 10)
+    peak, _ = measured_peaks()
+    traffic = profiled_traffic()
+    return {"config": workload_config("plain", s, world), "ms": ms, "iterations": int(res["r"].iterations),
+            "true_relative_residual": float(res["r"].true_residual_norm / bnorm),
+            "e2e_ms": e2e_ms, "system_build_s": gen_s,
+            "ilu0_sweep_pair": {"ms_per_launch": ilu_ms, "bytes_per_launch": ilu_bytes,
+                                "achieved": ilu_bytes / (ilu_ms * 1e-3) / 1e9,
+                                "frac": ilu_bytes / (ilu_ms * 1e-3) / 1e9 / peak,
+                                "traffic": traffic["ilu0 sweep pair"] * n if "ilu0 sweep pair" in traffic else None},
+            "spmv": {"us_per_launch": spmv_ms * 1e3, "bytes_per_launch": spmv_bytes,
+                     "achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9,
+                     "frac": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak,
+                     "traffic": traffic["spmv"] * n if "spmv" in traffic else None}}
 
-    def time_op(fn, reps):
-        fn()
+
+def run_plain(args):
+    """FP64 GMRES(30)+ILU(0) on the 2M-vertex disk mesh (the plain drop-in at
+    scale) with the sweep-pair and SpMV rooflines."""
+    import torch
+    from owtk_b200 import native
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    s, gen_s = build_system("plain", args.vertices, args.seed)
+    n, bs = s.owned, s.bs
+    bnorm = float(np.linalg.norm(s.rhs))
+    ctx = native.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    t = time.time()
+    m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
+    pc = native.Preconditioner(m, native.PC_ILU, 0)
+    ctx.synchronize()
+    setup_s = time.time() - t
+    opts = native.default_options(restart=30, relative_tolerance=1e-8)
+    ws = native.Workspace(ctx)
+    b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
+    x = native.Vector(ctx, n, 0, bs)
+    last = {}
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(local)
         ctx.synchronize()
-        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            fn()
-        c.record(stream)
-        c.synchronize()
-        return a.elapsed_time(c) / reps
 
-    spmv_ms = time_op(lambda: m.apply(b, y), 50)
-    ilu_ms = time_op(lambda: pc.apply(b, y), 10)
+    def step():
+        x.fill(0.0)
+        last["r"] = _checked(native.solve(native.FGMRES, m, pc, b, x, opts, ws), bnorm)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    launches0 = ctx.kernel_launches
+    with Clocks(local) as clk:
+        ms = _events(stream, step, args.steps)
+    barrier()
+    launches = ctx.kernel_launches - launches0
+    ms = _max_over_ranks(ms, world, local)
+    hb = torch.from_numpy(s.rhs.astype(np.float64)).pin_memory()
+    hx = torch.zeros(n * bs, dtype=torch.float64).pin_memory()
+
+    def host_step():
+        hx.zero_()
+        _checked(native.solve_host(native.FGMRES, m, pc, hb.data_ptr(), hx.data_ptr(), opts, ws), bnorm)
+
+    host_step()
+    barrier()
+    e2e_ms = _max_over_ranks(_events(stream, host_step, args.steps), world, local)
+    ilu_entries = int(pc.ilu_factors()[1].size)
+    spmv_bytes, ilu_bytes = algorithmic_bytes(s, ilu_entries)
+    y = native.Vector(ctx, n, 0, bs)
+    m.apply(b, y)
+    pc.apply(b, y)
+    ctx.synchronize()
+    spmv_ms = _events(stream, lambda: m.apply(b, y), 50)
+    ilu_ms = _events(stream, lambda: pc.apply(b, y), 10)
     peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic()
     clocks = clk.summary()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
         cpu = cpu_reference_solve(s, 1)
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "vertices": n, "entries": s.nnz, "block_size": bs,
-                       "solver": "gmres(30)+ilu(0)", "rtol": 1e-8, "ordering": "rcm", "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (matrix 336 MB, Krylov basis 2.9 GB)",
-                       "iterations": int(last.iterations), "setup_s": setup_s, "mesh_gen_s": gen_s},
+            "config": workload_config("plain", s, world),
             "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * n * bs * 8,
                     "d2h_bytes_per_step": n * bs * 8},
-            "roofline": {"bound": "hbm", "kernel": "ilu0 forward+backward sweep", "achieved": ilu_bytes / (ilu_ms * 1e-3) / 1e9,
-                         "peak": peak, "unit": "GB/s", "frac": ilu_bytes / (ilu_ms * 1e-3) / 1e9 / peak,
-                         "traffic": PROFILED_TRAFFIC_PER_VERTEX["ilu0 sweep pair"] * n,
-                         "traffic_source": "ncu DRAM bytes per vertex on the 1M-vertex mesh, scaled to this mesh",
+            "roofline": {"bound": "hbm", "kernel": "ilu0 forward+backward sweep",
+                         "achieved": ilu_bytes / (ilu_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": ilu_bytes / (ilu_ms * 1e-3) / 1e9 / peak,
+                         "traffic": traffic["ilu0 sweep pair"] * n if "ilu0 sweep pair" in traffic else None,
+                         "traffic_source": "ncu DRAM bytes per vertex of one captured launch, scaled to this mesh",
                          "bytes_per_launch": ilu_bytes, "ms_per_launch": ilu_ms, "peak_source": peak_kind},
             "spmv": {"achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "unit": "GB/s",
                      "frac": spmv_bytes / (spmv_ms * 1e-3) / 1e9 / peak, "us_per_launch": spmv_ms * 1e3,
-                     "bytes_per_launch": spmv_bytes, "traffic": PROFILED_TRAFFIC_PER_VERTEX["spmv"] * n},
+                     "bytes_per_launch": spmv_bytes,
+                     "traffic": traffic["spmv"] * n if "spmv" in traffic else None},
+            "iterations": int(last["r"].iterations), "setup_s": setup_s, "system_build_s": gen_s,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["seconds"][0], "unit": "s", "cores": 1, "kind": cpu["kind"],
                                     "sample": f"one full reference solve of the same system "
-                                              f"({cpu['iterations']} iterations, ILU setup {cpu['setup_seconds']:.2f} s excluded)"}
+                                              f"({cpu['iterations']} iterations, ILU setup "
+                                              f"{cpu['setup_seconds']:.2f} s excluded)",
+                                    "cpu": oracle.host_cpu()}
+            line["parity"] = {"iterations": int(last["r"].iterations), "reference_iterations": cpu["iterations"],
+                              "within_2": abs(int(last["r"].iterations) - cpu["iterations"]) <= 2}
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -485,17 +827,10 @@ def run_kernels(args):
             ctx.synchronize()
     return 0
 
+
 # ---------------------------------------------------------------- other forms
 def _event_time(stream, fn, steps):
-    import torch
-
-    a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(steps):
-        fn()
-    c.record(stream)
-    c.synchronize()
-    return a.elapsed_time(c) / steps
+    return _events(stream, fn, steps)
 
 
 def _line(args, workload, value_s, e2e_s, cfg, dtype, extra):
@@ -617,11 +952,33 @@ def _cpu_batch_sample(systems, its, budget_s: float = 20.0):
                       f"scaled by unknowns x iterations to the whole batch"}
 
 
+def reference_dense_solution(s, rtol: float = 1e-13, budget_s: float = 300.0):
+    """FP64 solution of a dense-block system by the reference's own GMRES(30)
+    on its DenseBlockCsrMatrix (the reference has no preconditioner for dense
+    blocks, so none is used), one host thread; None when oracle/_ref is absent."""
+    import oracle
+
+    try:
+        ref = oracle.Reference()
+    except FileNotFoundError:
+        return None, None
+    m = ref.matrix("dense", s.owned, 0, s.bs, s.rowptr, s.cols, s.vals)
+    pc = ref.pc("identity", m, 0.0)
+    t = time.time()
+    r, x = ref.solve("gmres", m, pc, oracle.default_options(relative_tolerance=rtol, maximum_iterations=5000,
+                                                            restart=30), s.rhs, np.zeros(s.owned * s.bs))
+    info = {"solver": "reference gmres(30), no preconditioner", "rtol": rtol, "iterations": int(r.iterations),
+            "status": int(r.status), "true_relative_residual": float(r.true_residual_norm / np.linalg.norm(s.rhs)),
+            "seconds": time.time() - t}
+    return (x if r.status == 0 else None), info
+
+
 def run_mixed(args):
     """Dense 3x3 blocks on the 2M-vertex disk mesh: FP64 FGMRES(30) outer
     refinement to rtol 1e-10 around block-ILU(0) factors stored in FP32 and in
-    BF16 with an FP32 inner solve, against the plain FP64 block-ILU(0) FGMRES;
-    errors against the FP64 solution."""
+    BF16 with an FP32 inner solve of 0, 1, 2 or 4 GMRES steps, against the
+    plain FP64 block-ILU(0) FGMRES; each solution's error is taken against
+    the reference's own FP64 solution of the same system (rtol 1e-13)."""
     import torch
     from owtk_b200 import native, problems
 
@@ -629,115 +986,59 @@ def run_mixed(args):
     s = problems.config2(args.vertices)
     gen_s = time.time() - t
     n, bs = s.owned, s.bs
+    bnorm = float(np.linalg.norm(s.rhs))
     ctx = native.Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
     m = native.Matrix(ctx, "dense", n, 0, bs, s.rowptr, s.cols, s.vals)
     b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
     opts = native.default_options(relative_tolerance=1e-10, restart=30)
+    xref, ref_info = (None, None) if args.no_cpu_baseline else reference_dense_solution(s)
     out = {}
-    xref = None
-    for name, storage, inner in (("fp64", native.F64, None), ("fp32", native.F32, 4), ("bf16", native.BF16, 4)):
+    runs = [("fp64", native.F64, None)]
+    for storage_name, storage in (("fp32", native.F32), ("bf16", native.BF16)):
+        for inner in (0, 1, 2, 4):
+            runs.append((f"{storage_name}_inner{inner}", storage, inner))
+    xs64 = None
+    for name, storage, inner in runs:
         t = time.time()
         pc = native.Preconditioner(m, native.PC_BLOCK_ILU, 0, storage=storage, mixed_inner=inner)
         ctx.synchronize()
         setup_s = time.time() - t
         x = native.Vector(ctx, n, 0, bs)
         ws = native.Workspace(ctx)
-        res = None
+        res = {}
 
         def step():
-            nonlocal res
             x.fill(0.0)
-            res = native.solve(native.FGMRES, m, pc, b, x, opts, ws)
+            res["r"] = _checked(native.solve(native.FGMRES, m, pc, b, x, opts, ws), bnorm, rtol=1e-10, what=name)
 
         for _ in range(args.warmup):
             step()
         ms = _event_time(stream, step, args.steps)
         xs = x.download()
-        if xref is None:
-            xref = xs
-        out[name] = {"ms": ms, "iterations": int(res.iterations), "status": int(res.status),
-                     "true_relative_residual": float(res.true_residual_norm / np.linalg.norm(s.rhs)),
-                     "error_vs_fp64": float(np.linalg.norm(xs - xref) / np.linalg.norm(xref)), "setup_s": setup_s}
-    best = min(out["fp32"]["ms"], out["bf16"]["ms"])
-    extra = {"mixed": out, "speedup_vs_fp64": out["fp64"]["ms"] / best}
-    print(json.dumps(_line(args, "mixed-dense3x3-fgmres-blockilu0", best / 1e3, None,
+        if xs64 is None:
+            xs64 = xs
+        out[name] = {"ms": ms, "iterations": int(res["r"].iterations),
+                     "preconditioner_applications": int(res["r"].preconditioner_applications),
+                     "true_relative_residual": float(res["r"].true_residual_norm / bnorm),
+                     "error_vs_gpu_fp64": float(np.linalg.norm(xs - xs64) / np.linalg.norm(xs64)),
+                     "setup_s": setup_s}
+        if xref is not None:
+            out[name]["error_vs_reference_fp64"] = float(np.linalg.norm(xs - xref) / np.linalg.norm(xref))
+        del pc, ws, x
+    mixed = {k: v for k, v in out.items() if k != "fp64"}
+    best = min(mixed, key=lambda k: mixed[k]["ms"])
+    extra = {"mixed": out, "best_mixed": best, "speedup_vs_fp64": out["fp64"]["ms"] / mixed[best]["ms"],
+             "reference_solution": ref_info}
+    print(json.dumps(_line(args, "mixed-dense3x3-fgmres-blockilu0", mixed[best]["ms"] / 1e3, None,
                            {"vertices": n, "entries": s.nnz, "block_size": bs, "rtol": 1e-10,
                             "solver": "fgmres(30) fp64 outer, block-ilu(0) fp32/bf16 factors, fp32 inner",
                             "mesh_gen_s": gen_s}, "f64+f32", extra)))
     return 0
 
 
-def run_learned(args):
-    """Anisotropic unit-square mesh (--vertices, default 8M): the network is
-    trained on the GPU on ILU(0)-GMRES residual/error pairs of --draws
-    coefficient draws of a --train-vertices mesh, then FGMRES(30) with the
-    network (ILU(0) fallback; FP64 outer, BF16/FP32 network) is timed against
-    plain FP64 ILU(0)-GMRES(30) on the same system, both to rtol 1e-8."""
-    import torch
-    from owtk_b200 import learned, native, problems
-
-    ctx = native.Context(0)
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
-    # Training.
-    t = time.time()
-    train = [sys_ for _, sys_ in problems.anisotropic_draws(args.train_vertices, 41, range(args.draws))]
-    gen_train_s = time.time() - t
-    m0 = native.Matrix(ctx, "bsr", train[0].owned, 0, 3, train[0].rowptr, train[0].cols, train[0].vals)
-    net = native.Learned(m0, seed=1)
-    t = time.time()
-    hist = learned.train(ctx, net, train, epochs=args.epochs, learning_rate=3e-3, pairs_per_system=6,
-                         final_learning_rate=3e-4)
-    train_s = time.time() - t
-    weights = net.parameters()
-    # The large system.
-    t = time.time()
-    s = problems.config4(args.vertices)
-    gen_s = time.time() - t
-    n, bs = s.owned, s.bs
-    m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
-    t = time.time()
-    ilu = native.Preconditioner(m, native.PC_ILU, 0)
-    ctx.synchronize()
-    ilu_setup_s = time.time() - t
-    netL = native.Learned(m, seed=1)
-    netL.set_parameters(weights)
-    pcl = native.LearnedPreconditioner(netL, ilu)
-    b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
-    x = native.Vector(ctx, n, 0, bs)
-    ws = native.Workspace(ctx)
-    opts = native.default_options(relative_tolerance=1e-8, restart=30)
-    results = {}
-    for name, pc in (("ilu0_gmres_fp64", ilu), ("learned_fgmres", pcl)):
-        res = None
-
-        def step():
-            nonlocal res
-            x.fill(0.0)
-            res = native.solve(native.FGMRES, m, pc, b, x, opts, ws)
-
-        step()
-        ms = _event_time(stream, step, max(1, args.steps))
-        results[name] = {"ms": ms, "iterations": int(res.iterations), "status": int(res.status),
-                         "true_relative_residual": float(res.true_residual_norm / np.linalg.norm(s.rhs))}
-    apps, falls = pcl.counts()
-    results["learned_fgmres"]["network_applications"] = apps
-    results["learned_fgmres"]["fallbacks"] = falls
-    speed = results["ilu0_gmres_fp64"]["ms"] / results["learned_fgmres"]["ms"]
-    extra = {"learned": results, "speedup_vs_plain_fp64_ilu_gmres": speed,
-             "training": {"draws": args.draws, "vertices": train[0].owned, "epochs": args.epochs,
-                          "loss_history": hist, "train_s": train_s, "generate_s": gen_train_s},
-             "setup": {"mesh_gen_s": gen_s, "ilu_setup_s": ilu_setup_s}}
-    print(json.dumps(_line(args, "learned-anisotropic-fgmres", results["learned_fgmres"]["ms"] / 1e3, None,
-                           {"vertices": n, "entries": s.nnz, "block_size": bs, "rtol": 1e-8,
-                            "solver": "fgmres(30) + learned network (ilu(0) fallback) vs gmres(30)+ilu(0)"},
-                           "f64+bf16", extra)))
-    return 0
-
-
-
-def main():
-    args = parse()
+def main(argv=None):
+    args = parse(argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.kernels:
@@ -746,9 +1047,9 @@ def main():
         return run_batching(args)
     if args.form == "mixed":
         return run_mixed(args)
-    if args.form == "learned":
-        return run_learned(args)
-    return run_ours(args)
+    if args.form == "plain":
+        return run_plain(args)
+    return run_learned(args)
 
 
 if __name__ == "__main__":

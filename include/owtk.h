@@ -356,8 +356,22 @@ int owtk_learned_uses_tma(const owtk_learned* net);
 size_t owtk_learned_parameter_count(void);
 owtk_status owtk_learned_get_parameters(owtk_learned* net, float* host, size_t count);
 owtk_status owtk_learned_set_parameters(owtk_learned* net, const float* host, size_t count);
+/* Adam optimiser state (first and second moments, count = parameter count,
+ * and the step number of the bias correction), so training can be saved to
+ * a checkpoint and resumed. */
+owtk_status owtk_learned_get_adam_state(owtk_learned* net, float* first_moment, float* second_moment, size_t count,
+                                        uint64_t* step);
+owtk_status owtk_learned_set_adam_state(owtk_learned* net, const float* first_moment, const float* second_moment,
+                                        size_t count, uint64_t step);
 /* out = M(in), FP64 vectors of the matrix layout. */
 owtk_status owtk_learned_apply(owtk_learned* net, owtk_vector* in, owtk_vector* out);
+/* Profiling: `repetitions` applications out = M(in), each stage bracketed by
+ * CUDA events on the context's stream.  milliseconds[4] receives the mean
+ * time of (0) the norms and the encoder, (1) one of the first three fused
+ * message-passing layers (k_gnn_layer), (2) the last layer with the decoder
+ * fused, (3) the whole application. */
+owtk_status owtk_learned_stage_times(owtk_learned* net, owtk_vector* in, owtk_vector* out, uint32_t repetitions,
+                                     double* milliseconds);
 /* Forward + backward of one training pair: the loss (weights below) and
  * its gradient, kept on the device for owtk_learned_adam_step (and copied
  * to host_grads when it is not NULL). */

@@ -20,7 +20,41 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_SO = os.path.join(HERE, "_build", "libowtk_oracle.so")
 REFERENCE_SO = os.path.join(HERE, "_ref", "libowtk_ref.so")
-REFERENCE_NATIVE_SO = os.path.join(HERE, "_ref", "libowtk_ref_native.so")
+REFERENCE_VECTOR_SO = {"avx512": os.path.join(HERE, "_ref", "libowtk_ref_avx512.so"),
+                       "avx2": os.path.join(HERE, "_ref", "libowtk_ref_avx2.so")}
+
+
+def host_vector_isa() -> str | None:
+    """Highest x86-64 ISA level of the running CPU that a vector build of the
+    reference targets: "avx512" (x86-64-v4), "avx2" (x86-64-v3) or None."""
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+    except OSError:
+        return None
+    if {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl", "avx2", "fma"} <= flags:
+        return "avx512"
+    if {"avx2", "fma", "bmi1", "bmi2", "movbe"} <= flags:
+        return "avx2"
+    return None
+
+
+def host_cpu() -> dict:
+    """CPU model name and logical CPU count of this host."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count(), "usable_cpus": len(os.sched_getaffinity(0))}
 
 
 class Options(ctypes.Structure):
@@ -54,12 +88,21 @@ def default_options(**kw) -> Options:
     return o
 
 
+def reference_root() -> str | None:
+    """The reference checkout the harness compiles against: $OWTK_REFERENCE_ROOT,
+    else baseline/_ref beside the repository; None when neither holds it."""
+    for root in (os.environ.get("OWTK_REFERENCE_ROOT"), os.path.join(os.path.dirname(HERE), "baseline", "_ref")):
+        if root and os.path.exists(os.path.join(root, "include", "owt", "krylov", "core.hpp")):
+            return root
+    return None
+
+
 def build(reference: bool = True) -> None:
     """Compile the checkers (gcc/g++ only; the reference leg needs its sources)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    ref_root = os.environ.get("OWTK_REFERENCE_ROOT", "/root/reference")
-    if reference and os.path.exists(os.path.join(ref_root, "include", "owt", "krylov", "core.hpp")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
+    root = reference_root()
+    if reference and root is not None:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={root}"], check=True)
 
 
 def _p(a):
@@ -323,7 +366,17 @@ class Reference:
               "comm_hiding_bicgstab": 3, "idrs": 4}
 
     def __init__(self, native: bool = False):
-        path = REFERENCE_NATIVE_SO if native else REFERENCE_SO
+        """native=False: the build as the reference ships (no -march).  native=True:
+        the vector build for the running CPU's ISA level (AVX-512 or AVX2 paths
+        of the reference's simd.hpp); FileNotFoundError when there is none."""
+        self.isa = None
+        if native:
+            self.isa = host_vector_isa()
+            if self.isa is None:
+                raise FileNotFoundError("no AVX2 or AVX-512 on this CPU for a vector build of the reference")
+            path = REFERENCE_VECTOR_SO[self.isa]
+        else:
+            path = REFERENCE_SO
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         L = ctypes.CDLL(path)

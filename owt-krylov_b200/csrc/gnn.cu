@@ -1343,6 +1343,10 @@ struct Gnn {
     int adam_t = 0;
     bool train_ready = false;
     std::uint64_t applications = 0;
+    // When set (owtk_learned_stage_times), gnn_forward records one event
+    // before the first launch and one after each stage: [0] start,
+    // [1] norms + encoder, [2..5] layers 1-4 (the last with the decoder).
+    cudaEvent_t* stage_events = nullptr;
 
     gnn::GraphArgs graph() const
     {
@@ -1454,12 +1458,17 @@ void gnn_forward(Gnn& G, const T* r, O* out)
     const gnn::GraphArgs g = G.graph();
     const long long nb = static_cast<long long>(G.n) * G.bs;
     double* norms = G.norm_r.as<double>();
+    auto mark = [&](int k) {
+        if (G.stage_events) OWTK_CUDA(cudaEventRecord(G.stage_events[k], c.stream));
+    };
+    mark(0);
     kern::prepare_norms<T>(c, static_cast<std::size_t>(nb), r, G.dinv.as<float>(), G.qbuf.as<float>(), norms);
     gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
     gnn::launch_encode<T>(std::min(G.blocks(G.n), static_cast<unsigned>(c.sm_count * 8)), c.stream, g, r,
                           G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
+    mark(1);
     const gnn::bf16* hin = h0;
     for (int l = 0; l < gnn::kLayers; ++l) {
         gnn::bf16* hout = TRAIN ? G.h[l + 1].as<gnn::bf16>() : (l % 2 == 0 ? G.hb : G.ha).as<gnn::bf16>();
@@ -1483,6 +1492,7 @@ void gnn_forward(Gnn& G, const T* r, O* out)
                     g, tm, tm, hin, wl, nullptr, nullptr, dec, c.status.as<unsigned>());
                 OWTK_CUDA(cudaGetLastError());
                 c.launched();
+                mark(2 + l);
                 ++G.applications;
                 return;
               }
@@ -1495,12 +1505,14 @@ void gnn_forward(Gnn& G, const T* r, O* out)
         }
         OWTK_CUDA(cudaGetLastError());
         c.launched();
+        if (l < gnn::kLayers - 1) mark(2 + l);
         hin = hout;
     }
     gnn::k_gnn_decode<O><<<G.blocks(8ll * G.n), 256, 0, c.stream>>>(g, G.qbuf.as<float>(), norms,
                                                                G.params.as<float>() + Gnn::kOffWd, hin, out);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
+    mark(2 + gnn::kLayers - 1);
     ++G.applications;
 }
 
@@ -1933,6 +1945,83 @@ owtk_status owtk_learned_set_parameters(owtk_learned* net, const float* host, si
                                   net->ctx->stream));
         owtk::gnn_pack(*net);
         net->ctx->sync();
+    });
+}
+
+owtk_status owtk_learned_stage_times(owtk_learned* net, owtk_vector* in, owtk_vector* out, uint32_t repetitions,
+                                     double* milliseconds)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && in != nullptr && out != nullptr && milliseconds != nullptr
+                          && repetitions > 0,
+                      "null argument or zero repetitions");
+        if (in->dtype != OWTK_F64 || out->dtype != OWTK_F64 || static_cast<int>(in->owned) != net->n
+            || static_cast<int>(in->bs) != net->bs || !in->same_layout(*out) || in->data == out->data)
+            owtk::fail(OWTK_ERR_INVALID_ARGUMENT, "learned preconditioner vector layout mismatch");
+        constexpr int kMarks = 2 + owtk::gnn::kLayers;
+        cudaEvent_t ev[kMarks] = {};
+        for (auto& e : ev) OWTK_CUDA(cudaEventCreate(&e));
+        double acc[kMarks - 1] = {};
+        std::exception_ptr failure;
+        net->stage_events = ev;
+        try {
+            for (uint32_t rep = 0; rep < repetitions; ++rep) {
+                owtk::gnn_forward<double, double, false>(*net, static_cast<const double*>(in->data),
+                                                         static_cast<double*>(out->data));
+                OWTK_CUDA(cudaEventSynchronize(ev[kMarks - 1]));
+                for (int k = 1; k < kMarks; ++k) {
+                    float ms = 0.f;
+                    OWTK_CUDA(cudaEventElapsedTime(&ms, ev[k - 1], ev[k]));
+                    acc[k - 1] += ms;
+                }
+            }
+        } catch (...) {
+            failure = std::current_exception();
+        }
+        net->stage_events = nullptr;
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (failure) std::rethrow_exception(failure);
+        net->ctx->check_device_status();
+        const double r = static_cast<double>(repetitions);
+        double layers = 0.0, total = 0.0;
+        for (int k = 0; k < kMarks - 1; ++k) total += acc[k];
+        for (int l = 0; l < owtk::gnn::kLayers - 1; ++l) layers += acc[1 + l];
+        milliseconds[0] = acc[0] / r;
+        milliseconds[1] = layers / r / (owtk::gnn::kLayers - 1);
+        milliseconds[2] = acc[kMarks - 2] / r;
+        milliseconds[3] = total / r;
+    });
+}
+
+owtk_status owtk_learned_get_adam_state(owtk_learned* net, float* first_moment, float* second_moment, size_t count,
+                                        uint64_t* step)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && first_moment != nullptr && second_moment != nullptr && step != nullptr
+                          && count == owtk::Gnn::kParams,
+                      "adam state count");
+        OWTK_CUDA(cudaMemcpyAsync(first_moment, net->adam_m.ptr, count * sizeof(float), cudaMemcpyDeviceToHost,
+                                  net->ctx->stream));
+        OWTK_CUDA(cudaMemcpyAsync(second_moment, net->adam_v.ptr, count * sizeof(float), cudaMemcpyDeviceToHost,
+                                  net->ctx->stream));
+        net->ctx->sync();
+        *step = static_cast<uint64_t>(net->adam_t);
+    });
+}
+
+owtk_status owtk_learned_set_adam_state(owtk_learned* net, const float* first_moment, const float* second_moment,
+                                        size_t count, uint64_t step)
+{
+    return owtk::guarded([&] {
+        owtk::require(net != nullptr && first_moment != nullptr && second_moment != nullptr
+                          && count == owtk::Gnn::kParams && step < (1ull << 31),
+                      "adam state count");
+        OWTK_CUDA(cudaMemcpyAsync(net->adam_m.ptr, first_moment, count * sizeof(float), cudaMemcpyHostToDevice,
+                                  net->ctx->stream));
+        OWTK_CUDA(cudaMemcpyAsync(net->adam_v.ptr, second_moment, count * sizeof(float), cudaMemcpyHostToDevice,
+                                  net->ctx->stream));
+        net->ctx->sync();
+        net->adam_t = static_cast<int>(step);
     });
 }
 

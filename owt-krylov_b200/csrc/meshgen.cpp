@@ -4,9 +4,20 @@
 // disk (radius 1, centred at the origin) or the unit square [0,1]^2.  The RNG is
 // a counter-free xoshiro256** seeded through splitmix64, so a seed reproduces
 // the same point set on any machine.  Host-only; no CUDA.
+//
+// Built as a stand-alone program (lib/owtk_meshgen), not a library, so a
+// process that only reads its output maps none of this project's code:
+//
+//     owtk_meshgen <radius> <domain 0|1> <seed> <max_points> <output file>
+//
+// writes the points as raw little-endian float64 (x, y) pairs and exits 0,
+// or exits 2 when more than max_points would be needed, 1 on a usage or I/O
+// error.
 
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 namespace {
@@ -110,3 +121,27 @@ long long owtk_poisson_disk(double radius, int domain, unsigned long long seed,
 }
 
 }  // extern "C"
+
+int main(int argc, char** argv)
+{
+    if (argc != 6) {
+        std::fprintf(stderr, "usage: %s radius domain(0 square, 1 disk) seed max_points output\n", argv[0]);
+        return 1;
+    }
+    const double radius = std::strtod(argv[1], nullptr);
+    const int domain = std::atoi(argv[2]);
+    const unsigned long long seed = std::strtoull(argv[3], nullptr, 10);
+    const long long max_points = std::strtoll(argv[4], nullptr, 10);
+    if (!(radius > 0.0) || (domain != 0 && domain != 1) || max_points <= 0) {
+        std::fprintf(stderr, "owtk_meshgen: invalid arguments\n");
+        return 1;
+    }
+    std::vector<double> xy(static_cast<std::size_t>(2 * max_points));
+    const long long count = owtk_poisson_disk(radius, domain, seed, max_points, xy.data());
+    if (count < 0) return 2;
+    std::FILE* f = std::fopen(argv[5], "wb");
+    if (f == nullptr) return 1;
+    const std::size_t want = static_cast<std::size_t>(2 * count);
+    const bool ok = std::fwrite(xy.data(), sizeof(double), want, f) == want;
+    return (std::fclose(f) == 0 && ok) ? 0 : 1;
+}

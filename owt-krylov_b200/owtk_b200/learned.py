@@ -50,16 +50,18 @@ def make_pairs(ctx, matrix, rhs: np.ndarray, pairs: int, rng=None):
 
 
 def train(ctx, net, systems, epochs: int = 4, learning_rate: float = 1e-3, pairs_per_system: int = 4,
-          seed: int = 0, final_learning_rate=None):
+          seed: int = 0, final_learning_rate=None, log=None):
     """Adam over all pairs of all systems for `epochs` passes; returns the
     mean loss of each epoch (the first is the untrained loss).  With
     `final_learning_rate` the rate decays geometrically from `learning_rate`
-    to it over the epochs."""
+    to it over the epochs.  `systems` may be a generator: only the device
+    copies (matrix and pairs) of each system are kept."""
     rng = np.random.default_rng(seed)
     data = []
     for s in systems:
         m = native.Matrix(ctx, "bsr", s.owned, 0, s.bs, s.rowptr, s.cols, s.vals)
         data.append((m, make_pairs(ctx, m, s.rhs, pairs_per_system)))
+        del s
     history = []
     for ep in range(epochs + 1):
         lr = learning_rate
@@ -78,6 +80,8 @@ def train(ctx, net, systems, epochs: int = 4, learning_rate: float = 1e-3, pairs
                 if ep > 0:
                     net.adam_step(lr)
         history.append(float(np.mean(losses)))
+        if log is not None:
+            log(f"epoch {ep}/{epochs}: rate {lr:.2e} mean loss {history[-1]:.5f}")
     return history
 
 

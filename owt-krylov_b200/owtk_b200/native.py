@@ -144,7 +144,10 @@ def lib():
             "owtk_learned_uses_tma": (c_int, [vp]),
             "owtk_learned_get_parameters": (c_int, [vp, vp, sz]),
             "owtk_learned_set_parameters": (c_int, [vp, vp, sz]),
+            "owtk_learned_get_adam_state": (c_int, [vp, vp, vp, sz, u64p]),
+            "owtk_learned_set_adam_state": (c_int, [vp, vp, vp, sz, c_uint64]),
             "owtk_learned_apply": (c_int, [vp, vp, vp]),
+            "owtk_learned_stage_times": (c_int, [vp, vp, vp, ctypes.c_uint32, POINTER(c_double)]),
             "owtk_learned_loss_grad": (c_int, [vp, vp, vp, POINTER(c_double), vp]),
             "owtk_learned_adam_step": (c_int, [vp, c_double]),
             "owtk_learned_set_loss_weights": (c_int, [vp, c_double, c_double]),
@@ -514,8 +517,27 @@ class Learned:
         p = np.ascontiguousarray(p, dtype=np.float32)
         check(lib().owtk_learned_set_parameters(self.h, _ptr(p), p.size))
 
+    def adam_state(self):
+        """(first moment, second moment, step) of the Adam optimiser."""
+        m = np.empty(self.parameter_count(), dtype=np.float32)
+        v = np.empty_like(m)
+        t = c_uint64()
+        check(lib().owtk_learned_get_adam_state(self.h, _ptr(m), _ptr(v), m.size, ctypes.byref(t)))
+        return m, v, int(t.value)
+
+    def set_adam_state(self, m, v, step: int):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        check(lib().owtk_learned_set_adam_state(self.h, _ptr(m), _ptr(v), m.size, int(step)))
+
     def apply(self, x: Vector, y: Vector):
         check(lib().owtk_learned_apply(self.h, x.h, y.h))
+
+    def stage_times(self, x: Vector, y: Vector, repetitions: int = 10) -> dict:
+        """Mean milliseconds per stage of y = M(x) (CUDA events on the stream)."""
+        ms = (c_double * 4)()
+        check(lib().owtk_learned_stage_times(self.h, x.h, y.h, repetitions, ms))
+        return {"norms_encoder": ms[0], "layer": ms[1], "last_layer_decoder": ms[2], "application": ms[3]}
 
     def loss_grad(self, r: Vector, e: Vector, want_grads: bool = False):
         loss = c_double()

@@ -11,14 +11,23 @@ component ``c`` and undirected edge ``(i, j)`` as
 with rows stored in ascending column order, the diagonal included.  RNG
 streams are numpy PCG64 generators drawn in a fixed order (points, w, s,
 diagonal noise, right-hand side), so a seed pins the system on any machine.
-Point sets: jittered triangulated lattices, or Poisson-disk samples triangulated
+Point sets: jittered triangulated lattices, or Poisson-disk samples (the
+stand-alone program lib/owtk_meshgen, run as a child process) triangulated
 with Delaunay (scipy's Qhull).
+
+Orderings: "rcm" relabels by reverse Cuthill-McKee, "hilbert" by the Hilbert
+curve.  The builders take an optional ``rcm`` callable ``(n, rowptr, cols) ->
+new_to_old`` that computes the RCM permutation; by default it is this
+library's ``owtk_rcm_order``.  The reference's own ordering can be passed
+instead, so a process that must not load this library (the CPU reference
+timing) builds the same system.
 """
 from __future__ import annotations
 
-import ctypes
 import math
 import os
+import subprocess
+import tempfile
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -61,25 +70,26 @@ class BlockSystem:
         return off_rowptr, off_cols, diag, off
 
 
-def _meshgen():
-    lib = ctypes.CDLL(os.path.join(_LIB_DIR, "libowtk_meshgen.so"))
-    lib.owtk_poisson_disk.restype = ctypes.c_longlong
-    lib.owtk_poisson_disk.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
-                                      ctypes.c_longlong, ctypes.c_void_p]
-    return lib
+MESHGEN = os.path.join(_LIB_DIR, "owtk_meshgen")
 
 
 def poisson_disk(target: int, domain: str, seed: int) -> np.ndarray:
-    """About ``target`` Poisson-disk points in the unit disk or the unit square."""
+    """About ``target`` Poisson-disk points in the unit disk or the unit square
+    (Bridson sampling by the program lib/owtk_meshgen in a child process)."""
+    if not os.path.exists(MESHGEN):
+        raise FileNotFoundError(f"mesh point generator not built: {MESHGEN} (run `make -C owt-krylov_b200`)")
     area = math.pi if domain == "disk" else 1.0
     radius = math.sqrt(0.616 * area / target)
     cap = int(target * 1.5) + 1024
-    buf = np.empty((cap, 2), dtype=np.float64)
-    count = _meshgen().owtk_poisson_disk(radius, 1 if domain == "disk" else 0, seed, cap,
-                                         buf.ctypes.data)
-    if count < 0:
-        raise RuntimeError("Poisson-disk buffer overflow")
-    return buf[:count].copy()
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "points.f64")
+        rc = subprocess.run([MESHGEN, repr(radius), "1" if domain == "disk" else "0", str(int(seed)), str(cap), out],
+                            check=False).returncode
+        if rc == 2:
+            raise RuntimeError("Poisson-disk point buffer overflow")
+        if rc != 0:
+            raise RuntimeError(f"owtk_meshgen failed with exit code {rc}")
+        return np.fromfile(out, dtype="<f8").reshape(-1, 2)
 
 
 def delaunay_edges(xy: np.ndarray) -> np.ndarray:
@@ -148,26 +158,40 @@ def _relabel(edges: np.ndarray, new_to_old: np.ndarray):
     return e
 
 
-def component_diagonal_system(xy, edges, bs, rng, order: str = "natural") -> BlockSystem:
-    """Coefficients as documented above; optional RCM or Hilbert relabelling."""
+def component_diagonal_system(xy, edges, bs, rng, order="natural", rcm=None) -> BlockSystem:
+    """Coefficients as documented above; optional RCM or Hilbert relabelling
+    (``order`` may also be a precomputed new_to_old permutation)."""
     n = xy.shape[0]
     a_fwd, a_bwd, diag = _coefficients(n, edges, bs, rng)
     rhs = rng.uniform(-1.0, 1.0, size=n * bs)
-    return _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order)
+    return _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order, rcm)
 
 
-def _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order) -> BlockSystem:
+def ordering(xy, edges, order: str, rcm=None) -> np.ndarray | None:
+    """new_to_old of the named vertex order of a mesh (None for "natural")."""
     n = xy.shape[0]
-    meta = {"order": order}
-    if order != "natural":
+    if order == "natural":
+        return None
+    if order == "rcm":
+        rp, cp = pattern(n, edges)
+        if rcm is None:
+            from . import native
+            rcm = native.rcm_order
+        return np.asarray(rcm(n, rp, cp), dtype=np.int64)
+    if order == "hilbert":
         from . import native
-        if order == "rcm":
-            rp, cp = pattern(n, edges)
-            new_to_old = native.rcm_order(n, rp, cp)
-        elif order == "hilbert":
-            new_to_old = native.hilbert_order(xy)
-        else:
-            raise ValueError(order)
+        return np.asarray(native.hilbert_order(xy), dtype=np.int64)
+    raise ValueError(order)
+
+
+def _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order, rcm=None) -> BlockSystem:
+    n = xy.shape[0]
+    if isinstance(order, np.ndarray):
+        new_to_old, name = order, "given"
+    else:
+        new_to_old, name = ordering(xy, edges, order, rcm), order
+    meta = {"order": name}
+    if new_to_old is not None:
         edges = _relabel(edges, new_to_old)
         flip = edges[:, 0] > edges[:, 1]
         a_fwd, a_bwd = np.where(flip[:, None], a_bwd, a_fwd), np.where(flip[:, None], a_fwd, a_bwd)
@@ -192,7 +216,7 @@ def angle_field(xy: np.ndarray, rng, modes: int = 6) -> np.ndarray:
     return np.pi * theta
 
 
-def anisotropic_system(xy, edges, bs, rng, strength: float = 1e4, order: str = "rcm") -> BlockSystem:
+def anisotropic_system(xy, edges, bs, rng, strength: float = 1e4, order="rcm", rcm=None) -> BlockSystem:
     """w_ij = 1 + strength (e_ij . d(x_ij))^2 per edge, with e_ij the unit edge
     vector and d the unit direction rotated by the smooth angle field at the
     edge midpoint; per component a skew s ~ U(-0.3, 0.3) (s_ji = -s_ij),
@@ -214,17 +238,17 @@ def anisotropic_system(xy, edges, bs, rng, strength: float = 1e4, order: str = "
                        + np.bincount(j, weights=np.abs(a_bwd[:, c]), minlength=n))
     diag = 1.05 * absum + rng.uniform(0.0, 0.1, size=(n, bs))
     rhs = rng.uniform(-1.0, 1.0, size=n * bs)
-    return _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order)
+    return _ordered_system(xy, edges, bs, a_fwd, a_bwd, diag, rhs, order, rcm)
 
 
 def config4(n_target: int = 8_000_000, seed: int = 4, bs: int = 3, draw: int = 0,
-            order: str = "rcm") -> BlockSystem:
+            order: str = "rcm", rcm=None) -> BlockSystem:
     """Poisson-disk points in the unit square, Delaunay, anisotropic
     coefficients (draw `draw` of the coefficient stream), RCM-ordered, bs 3."""
     def build():
         xy, edges = disk_mesh(n_target, seed, domain="square")
         rng = np.random.default_rng([seed, draw])
-        return anisotropic_system(xy, edges, bs, rng, order=order)
+        return anisotropic_system(xy, edges, bs, rng, order=order, rcm=rcm)
 
     sysm = _cached(f"square-{n_target}-{seed}-{bs}-{draw}-{order}", build)
     sysm.meta.update(config=f"poisson-square-{sysm.owned}-delaunay-anisotropic-{order}-bs{bs}", seed=seed, draw=draw)
@@ -287,24 +311,24 @@ def _cached(key: str, build):
     return s
 
 
-def config1(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm") -> BlockSystem:
+def config1(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm", rcm=None) -> BlockSystem:
     """Poisson-disk points in the unit disk, Delaunay, RCM-ordered, bs 3."""
     def build():
         xy, edges = disk_mesh(n_target, seed)
         rng = np.random.default_rng(seed)
-        return component_diagonal_system(xy, edges, bs, rng, order=order)
+        return component_diagonal_system(xy, edges, bs, rng, order=order, rcm=rcm)
 
     sysm = _cached(f"disk-{n_target}-{seed}-{bs}-{order}", build)
     sysm.meta.update(config=f"poisson-disk-{sysm.owned}-delaunay-{order}-bs{bs}", seed=seed)
     return sysm
 
 
-def config2(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm") -> BlockSystem:
+def config2(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = "rcm", rcm=None) -> BlockSystem:
     """The config-1 disk mesh with dense bs x bs blocks (see dense_block_system)."""
     def build():
         xy, edges = disk_mesh(n_target, seed)
         rng = np.random.default_rng([seed, 2])
-        return dense_block_system(xy, edges, bs, rng, order=order)
+        return dense_block_system(xy, edges, bs, rng, order=order, rcm=rcm)
 
     sysm = _cached(f"disk-dense-{n_target}-{seed}-{bs}-{order}", build)
     sysm.kind = "dense"
@@ -312,25 +336,24 @@ def config2(n_target: int = 2_000_000, seed: int = 1, bs: int = 3, order: str = 
     return sysm
 
 
-def anisotropic_draws(n_target: int, seed: int, draws, bs: int = 3, order: str = "rcm"):
+def anisotropic_draws(n_target: int, seed: int, draws, bs: int = 3, order: str = "rcm", rcm=None):
     """Coefficient draws of one anisotropic unit-square mesh (mesh and
     ordering built once); yields (draw, BlockSystem)."""
     xy, edges = disk_mesh(n_target, seed, domain="square")
+    perm = ordering(xy, edges, order, rcm)
     for d in draws:
         rng = np.random.default_rng([seed, d])
-        s = anisotropic_system(xy, edges, bs, rng, order=order)
-        s.meta.update(draw=d)
+        s = anisotropic_system(xy, edges, bs, rng, order=perm if perm is not None else "natural")
+        s.meta.update(draw=d, order=order)
         yield d, s
 
 
-def dense_block_system(xy, edges, bs: int, rng, order: str = "natural") -> BlockSystem:
+def dense_block_system(xy, edges, bs: int, rng, order: str = "natural", rcm=None) -> BlockSystem:
     """Dense bs x bs blocks: off-diagonal -w_ij (I + 0.3 R_ij), R ~ N(0,1)/3 drawn
     per direction; diagonal 1.1 * sum ||off||_1 * I + 0.05 N(0,1)."""
     n = xy.shape[0]
-    if order == "rcm":
-        from . import native
-        rp, cp = pattern(n, edges)
-        new_to_old = native.rcm_order(n, rp, cp)
+    new_to_old = ordering(xy, edges, order, rcm)
+    if new_to_old is not None:
         edges = np.sort(_relabel(edges, new_to_old), axis=1)
         xy = xy[new_to_old]
     e = edges.shape[0]

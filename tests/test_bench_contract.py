@@ -73,12 +73,55 @@ def test_peak_is_the_measured_copy_bandwidth(bench):
 
 
 def test_timing_defaults(bench):
-    sys_argv = sys.argv
-    sys.argv = ["bench.py"]
-    try:
-        args = bench.parse()
-    finally:
-        sys.argv = sys_argv
-    assert args.gpus == 1 and args.impl == "ours" and args.form == "plain"
+    args = bench.parse([])
+    # The headline: the 8M-vertex anisotropic learned-vs-plain workload.
+    assert args.gpus == 1 and args.impl == "ours" and args.form == "learned"
     assert args.warmup >= 3 and args.steps >= 1
-    assert args.vertices == 2_000_000
+    assert args.vertices == 8_000_000 and args.seed == 4
+    plain = bench.parse(["--form", "plain"])
+    assert plain.vertices == 2_000_000 and plain.seed == 1
+
+
+def test_gnn_layer_counts(bench):
+    # One fused layer per vertex: own row 128 B read, new row 128 B written,
+    # 8-slot list of 32-bit columns and BF16 weights; [h|m] (128) x Wl^T (64).
+    assert bench.gnn_layer_bytes(1000) == 1000 * 304
+    assert bench.gnn_layer_flops(1000) == 1000 * 2 * 128 * 64
+
+
+class _System:
+    owned, nnz, bs = 7_991_199, 55_938_393, 3
+
+
+def test_both_arms_print_one_config(bench):
+    # The driver compares the two arms' config objects key for key.
+    a = bench.workload_config("learned", _System(), 1)
+    b = bench.workload_config("learned", _System(), 1)
+    assert a == b and a["workload"] == bench.WORKLOADS["learned"]
+    assert {"workload", "vertices", "entries", "block_size", "rtol", "l2", "parallelism"} <= set(a)
+    assert "iterations" not in a and "setup_s" not in a
+
+
+def test_reference_arm_loads_no_project_library(tmp_path):
+    """The reference arm's process (bench.py --impl reference) must map only
+    the reference build: check which modules its imports pull in by running
+    its system-building helpers on a tiny mesh in a child process."""
+    code = r"""
+import sys, os, json
+sys.argv = ["bench.py"]
+import importlib.util
+spec = importlib.util.spec_from_file_location("b", os.path.join(%r, "bench.py"))
+b = importlib.util.module_from_spec(spec); spec.loader.exec_module(b)
+b.MESH_CACHE = %r
+import oracle
+ref = oracle.Reference()
+s, _ = b.build_system("learned", 3000, 4, rcm=ref.rcm)
+maps = open("/proc/self/maps").read()
+print(json.dumps({"n": s.owned, "owtk_b200_so": "libowtk_b200" in maps, "meshgen_so": "meshgen.so" in maps,
+                  "native_imported": "owtk_b200.native" in sys.modules}))
+""" % (REPO, str(tmp_path))
+    import subprocess
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout
+    got = json.loads(out.strip().splitlines()[-1])
+    assert got["n"] > 2000
+    assert not got["owtk_b200_so"] and not got["meshgen_so"] and not got["native_imported"], got
