@@ -114,7 +114,7 @@ owtk_status owtk_dense_bsr_create(owtk_context* ctx, owtk_dtype dtype, size_t ow
                                   const uint64_t* row_offsets, const uint64_t* column_indices,
                                   const void* values, owtk_matrix** out);
 owtk_status owtk_matrix_destroy(owtk_matrix* m);
-/* kind: 0 component-diagonal BSR, 1 split view, 2 dense BSR. */
+/* kind: 0 component-diagonal BSR, 1 split view, 2 dense BSR, 3 host callback. */
 owtk_status owtk_matrix_info(owtk_matrix* m, int* kind, size_t* owned_nodes,
                              size_t* ghost_nodes, size_t* block_size, size_t* entries);
 /* Matrix::apply (block_csr.hpp:192-215, split_block_csr.hpp:89-119,
@@ -136,7 +136,9 @@ typedef enum owtk_pc_kind {
     /* Created only by owtk_pc_create_mixed. */
     OWTK_PC_MIXED = 6,
     /* Created only by owtk_pc_create_learned. */
-    OWTK_PC_LEARNED = 7
+    OWTK_PC_LEARNED = 7,
+    /* Created only by owtk_pc_create_callback. */
+    OWTK_PC_CALLBACK = 8
 } owtk_pc_kind;
 
 owtk_status owtk_pc_create(owtk_matrix* m, owtk_pc_kind kind, double parameter,
@@ -238,17 +240,6 @@ uint64_t owtk_workspace_allocation_epochs(owtk_workspace* ws);
 /* Workspace vector `index` (same slot order as the reference solver), or NULL. */
 owtk_vector* owtk_workspace_vector(owtk_workspace* ws, size_t index);
 
-/* solve_specwave_native (specwave_compat.hpp:99-249) for the legacy SpecWave
- * solver IDs: 3, 4, 10, 22 communication-hiding BiCGSTAB + SSOR (4: residual
- * replacement 50 when unset); 5, 8, 11 BiCGSTAB + SSOR; 7 GMRES + SSOR;
- * 9, 13 BiCGSTAB + ILU(0); 12, 15 pipelined BiCGSTAB + SSOR; 14 IDR(s) + SSOR;
- * 21 pipelined BiCGSTAB + ILU(0); SSOR with omega = options->relaxation.  ID 6
- * (PETSc) returns the default result (invalid_input); the stationary and
- * multigrid IDs are rejected with OWTK_ERR_INVALID_ARGUMENT. */
-owtk_status owtk_solve_specwave(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
-                                const owtk_solver_options* options, owtk_workspace* workspace,
-                                owtk_solver_result* result);
-
 /* Device-resident solve: rhs and x are device vectors with the matrix layout.
  * pc may be NULL (identity); workspace may be NULL (a temporary is used). */
 owtk_status owtk_solve(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,
@@ -260,6 +251,108 @@ owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_precondi
                             const void* host_rhs, void* host_x,
                             const owtk_solver_options* options, owtk_workspace* workspace,
                             owtk_solver_result* result);
+
+/* ---- reductions, application convergence tests, Arnoldi snapshots ---------
+ * The reference's solvers take a Reduction, an optional
+ * SolverOptions::convergence_test callback and (FGMRES) an optional
+ * ArnoldiSnapshot; owtk_solve_ex / owtk_solve_host_ex take them as extras. */
+typedef enum owtk_reduction_kind {
+    OWTK_REDUCTION_SERIAL = 0,          /* SerialReduction (reduction.hpp:103-168) */
+    /* CompensatedSerialReduction (reduction.hpp:175-226): Neumaier-compensated
+     * sums of the rounded products, partial pairs merged exactly. */
+    OWTK_REDUCTION_COMPENSATED = 1,
+    /* MixedPrecisionSerialReduction (reduction.hpp:228-299): products split
+     * exactly by FMA and summed in doubled precision (Dot2 of Ogita, Rump and
+     * Oishi), at least as accurate as the reference's long double sums; the
+     * 2-norm in doubled precision too. */
+    OWTK_REDUCTION_MIXED_PRECISION = 2
+} owtk_reduction_kind;
+
+/* dot / norm with a chosen reduction.  `low` (may be NULL) receives the low
+ * part of the compensated result: result + low is the exact sum of the
+ * device's (sum, correction) pair, the analogue of the reference's
+ * long double local_dot. */
+owtk_status owtk_dot_ex(owtk_vector* lhs, owtk_vector* rhs, owtk_reduction_kind reduction, double* result,
+                        double* low);
+owtk_status owtk_norm_ex(owtk_vector* v, owtk_reduction_kind reduction, double* result);
+
+/* SolverOptions::convergence_test (core.hpp:102-108, called as in
+ * krylov_solvers.hpp:122-143): called at iteration zero and after each
+ * complete iterate with the iteration count and a HOST copy of the candidate
+ * solution ((owned + ghost) * bs values in the solve's dtype).  Return 1 to
+ * stop (the solver then measures the true residual and reports
+ * converged_by_application), 0 to continue, a negative value to abort the
+ * solve with OWTK_ERR_RUNTIME.  While a test is set, the residual tolerance
+ * is replaced by it, as in the reference. */
+typedef int (*owtk_convergence_test_fn)(void* user, uint64_t iteration, const void* candidate, size_t count);
+
+/* ArnoldiSnapshot<T> (core.hpp:462-534): the last unrotated Arnoldi relation
+ * FGMRES produced — the Hessenberg entries h(row, column) of the last cycle
+ * and its preconditioned basis vectors (device vectors owned by the snapshot). */
+typedef struct owtk_arnoldi_snapshot owtk_arnoldi_snapshot;
+owtk_status owtk_arnoldi_snapshot_create(owtk_context* ctx, owtk_arnoldi_snapshot** out);
+owtk_status owtk_arnoldi_snapshot_destroy(owtk_arnoldi_snapshot* snapshot);
+owtk_status owtk_arnoldi_snapshot_clear(owtk_arnoldi_snapshot* snapshot);
+size_t owtk_arnoldi_snapshot_columns(const owtk_arnoldi_snapshot* snapshot);
+/* OWTK_ERR_OUT_OF_RANGE unless column < columns and row <= columns. */
+owtk_status owtk_arnoldi_snapshot_h(const owtk_arnoldi_snapshot* snapshot, size_t row, size_t column,
+                                    double* value);
+/* Borrowed handle of preconditioned basis vector `column` (< columns). */
+owtk_status owtk_arnoldi_snapshot_basis(owtk_arnoldi_snapshot* snapshot, size_t column, owtk_vector** out);
+
+typedef struct owtk_solve_extras {
+    int32_t reduction;                          /* owtk_reduction_kind */
+    int32_t reserved;                           /* 0 */
+    owtk_convergence_test_fn convergence_test;  /* NULL: none */
+    void* convergence_user;
+    owtk_arnoldi_snapshot* arnoldi_snapshot;    /* FGMRES only; NULL: none */
+} owtk_solve_extras;
+
+/* owtk_solve / owtk_solve_host with extras (NULL extras: the plain call). */
+owtk_status owtk_solve_ex(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc, owtk_vector* rhs,
+                          owtk_vector* x, const owtk_solver_options* options, owtk_workspace* workspace,
+                          const owtk_solve_extras* extras, owtk_solver_result* result);
+owtk_status owtk_solve_host_ex(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,
+                               const void* host_rhs, void* host_x, const owtk_solver_options* options,
+                               owtk_workspace* workspace, const owtk_solve_extras* extras,
+                               owtk_solver_result* result);
+
+/* solve_specwave_native (specwave_compat.hpp:99-249) for the legacy SpecWave
+ * solver IDs: 3, 4, 10, 22 communication-hiding BiCGSTAB + SSOR (4: residual
+ * replacement 50 when unset); 5, 8, 11 BiCGSTAB + SSOR; 7 GMRES + SSOR;
+ * 9, 13 BiCGSTAB + ILU(0); 12, 15 pipelined BiCGSTAB + SSOR; 14 IDR(s) + SSOR;
+ * 21 pipelined BiCGSTAB + ILU(0); SSOR with omega = options->relaxation.  ID 10
+ * uses the mixed-precision reduction and ID 22 the compensated one, as in the
+ * reference; the other IDs use `reduction` (serial for owtk_solve_specwave).
+ * ID 6 (PETSc) returns the default result (invalid_input); the stationary and
+ * multigrid IDs are rejected with OWTK_ERR_INVALID_ARGUMENT. */
+owtk_status owtk_solve_specwave(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
+                                const owtk_solver_options* options, owtk_workspace* workspace,
+                                owtk_solver_result* result);
+owtk_status owtk_solve_specwave_ex(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
+                                   const owtk_solver_options* options, owtk_workspace* workspace,
+                                   owtk_reduction_kind reduction, owtk_solver_result* result);
+
+/* ---- host-callback operators and preconditioners ----------------------------
+ * The reference's solvers are templates over duck-typed operators and
+ * preconditioners (docs/MANUAL.tex:676-712): any type with apply(in, out).
+ * These wrap such an application-supplied host function so the device
+ * solvers can use it: each application copies `in` ((owned + ghost) * bs
+ * values) and the current `out` to host buffers, calls apply(user, in, out,
+ * count) and copies out's owned values (and in's ghost values, which a halo
+ * exchange may write) back.  apply returns 0 on success; anything else fails
+ * the call with OWTK_ERR_RUNTIME.  Every application synchronises the
+ * stream, so these suit matrix-free operators and prototypes, not speed. */
+typedef int (*owtk_host_apply_fn)(void* user, void* in, void* out, size_t count);
+/* A matrix of kind 3 usable wherever an operator is (owtk_spmv, solves);
+ * preconditioners that need coefficients (Jacobi, SSOR, ILU) reject it. */
+owtk_status owtk_callback_operator_create(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes,
+                                          size_t ghost_nodes, size_t block_size, owtk_host_apply_fn apply,
+                                          void* user, owtk_matrix** out);
+/* A preconditioner of kind OWTK_PC_CALLBACK (8) for vectors of this layout. */
+owtk_status owtk_pc_create_callback(owtk_context* ctx, owtk_dtype dtype, size_t owned_nodes, size_t ghost_nodes,
+                                    size_t block_size, owtk_host_apply_fn apply, void* user,
+                                    owtk_preconditioner** out);
 
 /* ---- allocation-free variant (no counterpart in the reference) ----------
  * The batched dot product of owtk_dot_batch for callers that cannot allocate

@@ -405,6 +405,11 @@ class Reference:
             ("ref_solve", c_int, [c_int, c_int, vp, vp, POINTER(Options), vp, vp, vp, POINTER(Result)]),
             ("ref_dot", c_double, [sz, sz, sz, vp, vp]),
             ("ref_norm", c_double, [sz, sz, sz, vp]),
+            ("ref_solve_ex", c_int, [c_int, c_int, vp, vp, POINTER(Options), vp, vp, c_uint64, vp, vp, vp,
+                                     POINTER(Result)]),
+            ("ref_solve_specwave", c_int, [c_int, vp, POINTER(Options), vp, vp, POINTER(Result)]),
+            ("ref_dot_kind", c_double, [c_int, sz, sz, sz, vp, vp, vp]),
+            ("ref_norm_kind", c_double, [c_int, sz, sz, sz, vp]),
             ("ref_rcm", c_int, [sz, sz, vp, vp, vp]),
             ("ref_hilbert", c_int, [sz, vp, vp]),
             ("ref_inverse_permutation", c_int, [sz, vp, vp]),
@@ -431,6 +436,50 @@ class Reference:
         self.check(self.L.ref_solve(self.SOLVER[solver], reduction, matrix.h, pc.h, ctypes.byref(options), _p(b),
                                     _p(x), workspace, ctypes.byref(r)))
         return r, x
+
+    REDUCTION = {"serial": 0, "compensated": 1, "mixed": 2}
+
+    def solve_ex(self, solver, matrix, pc, options, rhs, x0, reduction="serial", stop_at=0, snapshot=False):
+        """ref_solve_ex: optional convergence test stopping at iteration
+        `stop_at` and (FGMRES) the Arnoldi snapshot: returns (result, x,
+        snapshot dict or None)."""
+        x = np.array(x0, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(rhs, np.float64)
+        r = Result()
+        cols = ctypes.c_uint64(0)
+        R = int(options.restart)
+        n = b.size
+        h = np.zeros((R + 1) * max(R, 1)) if snapshot else None
+        z = np.zeros(max(R, 1) * n) if snapshot else None
+        self.check(self.L.ref_solve_ex(self.SOLVER[solver], self.REDUCTION[reduction], matrix.h, pc.h,
+                                       ctypes.byref(options), _p(b), _p(x), int(stop_at),
+                                       ctypes.byref(cols) if snapshot else None, _p(h) if snapshot else None,
+                                       _p(z) if snapshot else None, ctypes.byref(r)))
+        snap = None
+        if snapshot:
+            c = int(cols.value)
+            snap = {"columns": c, "h": h.reshape(max(R, 1), R + 1)[:c, : c + 1].T.copy(),
+                    "basis": z[: c * n].reshape(c, n).copy()}
+        return r, x, snap
+
+    def solve_specwave(self, solver_id, matrix, options, rhs, x0):
+        x = np.array(x0, dtype=np.float64, copy=True)
+        b = np.ascontiguousarray(rhs, np.float64)
+        r = Result()
+        self.check(self.L.ref_solve_specwave(int(solver_id), matrix.h, ctypes.byref(options), _p(b), _p(x),
+                                             ctypes.byref(r)))
+        return r, x
+
+    def dot_kind(self, reduction, owned, ghost, bs, a, b):
+        """(hi, lo) of the reference dot with the named reduction."""
+        a, b = np.ascontiguousarray(a, np.float64), np.ascontiguousarray(b, np.float64)
+        lo = ctypes.c_double(0)
+        hi = self.L.ref_dot_kind(self.REDUCTION[reduction], owned, ghost, bs, _p(a), _p(b), ctypes.byref(lo))
+        return hi, lo.value
+
+    def norm_kind(self, reduction, owned, ghost, bs, a):
+        a = np.ascontiguousarray(a, np.float64)
+        return self.L.ref_norm_kind(self.REDUCTION[reduction], owned, ghost, bs, _p(a))
 
     def dot(self, owned, ghost, bs, a, b):
         a, b = np.ascontiguousarray(a, np.float64), np.ascontiguousarray(b, np.float64)

@@ -18,6 +18,7 @@
 #include <owt/krylov/pipelined_bicgstab.hpp>
 #include <owt/krylov/preconditioner.hpp>
 #include <owt/krylov/reduction.hpp>
+#include <owt/krylov/specwave_compat.hpp>
 #include <owt/krylov/split_block_csr.hpp>
 
 #include <cstdint>
@@ -452,6 +453,136 @@ int ref_solve(int solver, int reduction, void* matrix, void* pc_handle,
         out->converged_by_application = r.converged_by_application ? 1 : 0;
         out->solve_seconds = r.solve_seconds();
     });
+}
+
+namespace {
+ok::SolverOptions<double> options_of(const ref_options* o)
+{
+    ok::SolverOptions<double> opt;
+    opt.relative_tolerance = o->relative_tolerance;
+    opt.absolute_tolerance = o->absolute_tolerance;
+    opt.breakdown_tolerance = o->breakdown_tolerance;
+    opt.maximum_iterations = o->maximum_iterations;
+    opt.convergence_check_interval = o->convergence_check_interval;
+    opt.restart = o->restart;
+    opt.residual_replacement_interval = o->residual_replacement_interval;
+    opt.idr_shadow_space = o->idr_shadow_space;
+    opt.relaxation = o->relaxation;
+    opt.verify_true_residual = o->verify_true_residual != 0;
+    opt.collect_timings = true;
+    opt.gmres_orthogonalization = static_cast<ok::GmresOrthogonalization>(o->gmres_orthogonalization);
+    return opt;
+}
+
+void result_of(const ok::SolverResult<double>& r, ref_result* out)
+{
+    out->status = static_cast<std::int32_t>(r.status);
+    out->breakdown_reason = static_cast<std::int32_t>(r.breakdown_reason);
+    out->iterations = r.iterations;
+    out->operator_applications = r.operator_applications;
+    out->preconditioner_applications = r.preconditioner_applications;
+    out->global_reductions = r.global_reductions;
+    out->reorthogonalizations = r.reorthogonalizations;
+    out->arnoldi_norm_verifications = r.arnoldi_norm_verifications;
+    out->initial_residual_norm = r.initial_residual_norm;
+    out->recursive_residual_norm = r.recursive_residual_norm;
+    out->true_residual_norm = r.true_residual_norm;
+    out->relative_residual_norm = r.relative_residual_norm;
+    out->converged_by_application = r.converged_by_application ? 1 : 0;
+    out->solve_seconds = r.solve_seconds();
+}
+}  // namespace
+
+// ref_solve with the two optional inputs of the reference's solvers: an
+// application convergence test that stops at iteration `stop_at` (0: none;
+// core.hpp:102-108) and, for FGMRES, an ArnoldiSnapshot (core.hpp:462-534)
+// whose columns, Hessenberg entries h(row, col) (column-major, restart + 1
+// rows) and owned preconditioned-basis values are copied out.
+int ref_solve_ex(int solver, int reduction, void* matrix, void* pc_handle, const ref_options* o,
+                 const double* rhs, double* x, std::uint64_t stop_at, std::uint64_t* snapshot_columns,
+                 double* snapshot_h, double* snapshot_basis, ref_result* out)
+{
+    return guarded([&] {
+        auto* m = static_cast<Matrix*>(matrix);
+        const Pc* pc = static_cast<Pc*>(pc_handle);
+        ok::SolverOptions<double> opt = options_of(o);
+        if (stop_at > 0)
+            opt.convergence_test = [stop_at](std::size_t it, const ok::BlockVector<double>&) { return it >= stop_at; };
+        auto vb = view(m, rhs);
+        auto vx = view(m, x);
+        Op op{m};
+        ok::ArnoldiSnapshot<double> snap;
+        ok::SolverResult<double> r;
+        auto run = [&](auto red) {
+            switch (solver) {
+            case 0: r = ok::fgmres(op, vb, vx, opt, PcRef{pc}, red, static_cast<ok::SolverWorkspace<double>*>(nullptr), snapshot_columns ? &snap : nullptr); break;
+            case 1: r = ok::bicgstab(op, vb, vx, opt, PcRef{pc}, red); break;
+            case 2: r = ok::pipelined_bicgstab(op, vb, vx, opt, PcRef{pc}, red); break;
+            case 3: r = ok::communication_hiding_bicgstab(op, vb, vx, opt, PcRef{pc}, red); break;
+            case 4: r = ok::idrs(op, vb, vx, opt, PcRef{pc}, red); break;
+            default: throw std::invalid_argument("unknown solver");
+            }
+        };
+        if (reduction == 1) run(ok::CompensatedSerialReduction<double>{});
+        else if (reduction == 2) run(ok::MixedPrecisionSerialReduction<double>{});
+        else run(ok::SerialReduction<double>{});
+        result_of(r, out);
+        if (snapshot_columns) {
+            const std::size_t cols = snap.columns(), R = o->restart, n = m->owned * m->bs;
+            *snapshot_columns = cols;
+            for (std::size_t c = 0; c < cols; ++c) {
+                for (std::size_t row = 0; row <= cols; ++row) snapshot_h[c * (R + 1) + row] = snap.h(row, c);
+                const auto& z = snap.preconditioned_basis(c);
+                std::copy(z.owned().begin(), z.owned().end(), snapshot_basis + c * n);
+            }
+        }
+    });
+}
+
+// solve_specwave_native (specwave_compat.hpp:99-249) on a component-diagonal
+// BSR handle with its operator and no halo.
+int ref_solve_specwave(int solver_id, void* matrix, const ref_options* o, const double* rhs, double* x,
+                       ref_result* out)
+{
+    return guarded([&] {
+        auto* m = static_cast<Matrix*>(matrix);
+        if (m->kind != 0) throw std::invalid_argument("SpecWave dispatch needs a component-diagonal BSR");
+        auto vb = view(m, rhs);
+        auto vx = view(m, x);
+        ok::DistributedBlockOperator<Bsr&> op(*m->bsr);
+        ok::NoHaloExchange halo;
+        const auto r = ok::solve_specwave_native(static_cast<ok::SpecWaveSolver>(solver_id), *m->bsr, op, halo, vb,
+                                                 vx, options_of(o));
+        result_of(r, out);
+    });
+}
+
+// dot and norm with a chosen reduction (0 serial, 1 compensated, 2 mixed
+// precision); the mixed local_dot's long double is returned as hi + lo.
+double ref_dot_kind(int kind, std::size_t owned, std::size_t ghost, std::size_t bs, const double* a,
+                    const double* b, double* low)
+{
+    const std::size_t n = (owned + ghost) * bs;
+    auto va = ok::BlockVector<double>::view(owned, ghost, bs, std::span<double>(const_cast<double*>(a), n));
+    auto vb = ok::BlockVector<double>::view(owned, ghost, bs, std::span<double>(const_cast<double*>(b), n));
+    if (low) *low = 0.0;
+    if (kind == 1) return ok::CompensatedSerialReduction<double>{}.dot(va, vb);
+    if (kind == 2) {
+        const long double w = ok::MixedPrecisionSerialReduction<double>{}.local_dot(va, vb);
+        const double hi = static_cast<double>(w);
+        if (low) *low = static_cast<double>(w - static_cast<long double>(hi));
+        return hi;
+    }
+    return ok::SerialReduction<double>{}.dot(va, vb);
+}
+
+double ref_norm_kind(int kind, std::size_t owned, std::size_t ghost, std::size_t bs, const double* a)
+{
+    const std::size_t n = (owned + ghost) * bs;
+    auto va = ok::BlockVector<double>::view(owned, ghost, bs, std::span<double>(const_cast<double*>(a), n));
+    if (kind == 1) return ok::CompensatedSerialReduction<double>{}.norm(va);
+    if (kind == 2) return ok::MixedPrecisionSerialReduction<double>{}.norm(va);
+    return ok::SerialReduction<double>{}.norm(va);
 }
 
 double ref_dot(std::size_t owned, std::size_t ghost, std::size_t bs,

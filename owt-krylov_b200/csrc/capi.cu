@@ -377,9 +377,97 @@ void numeric_update(Preconditioner& p, Matrix& m)
 
 }  // namespace
 
+// ------------------------------------------------------------ host callbacks
+namespace {
+// One application of a host function: in and the current out copied to host
+// buffers, the function called, out's owned values and in's ghost values
+// (which a halo exchange of the application may write) copied back.
+void host_apply_call(Context& c, owtk_host_apply_fn fn, void* user, std::vector<unsigned char>& hin,
+                     std::vector<unsigned char>& hout, Vector& in, Vector& out)
+{
+    const std::size_t count = in.local_size(), es = in.elem(), bytes = count * es;
+    hin.resize(bytes);
+    hout.resize(bytes);
+    OWTK_CUDA(cudaMemcpyAsync(hin.data(), in.data, bytes, cudaMemcpyDeviceToHost, c.stream));
+    OWTK_CUDA(cudaMemcpyAsync(hout.data(), out.data, bytes, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    if (fn(user, hin.data(), hout.data(), count) != 0) fail(OWTK_ERR_RUNTIME, "host apply callback failed");
+    const std::size_t owned_bytes = in.owned_size() * es;
+    OWTK_CUDA(cudaMemcpyAsync(out.data, hout.data(), owned_bytes, cudaMemcpyHostToDevice, c.stream));
+    if (in.ghost > 0 && in.data != out.data)
+        OWTK_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(in.data) + owned_bytes, hin.data() + owned_bytes,
+                                  bytes - owned_bytes, cudaMemcpyHostToDevice, c.stream));
+    c.sync();
+}
+}  // namespace
+
+std::unique_ptr<Vector> make_vector_like(const Vector& like)
+{
+    auto v = std::make_unique<owtk_vector>();
+    v->ctx = like.ctx;
+    v->dtype = like.dtype;
+    v->owned = like.owned;
+    v->ghost = like.ghost;
+    v->bs = like.bs;
+    v->storage.allocate(like.local_size() * like.elem() + 16);
+    v->data = v->storage.ptr;
+    OWTK_CUDA(cudaMemsetAsync(v->data, 0, like.local_size() * like.elem(), like.ctx->stream));
+    return v;
+}
+
+// ------------------------------------------------------------ Arnoldi snapshot
+// core.hpp:462-534.
+void ArnoldiSnapshot::begin_cycle(const Vector& layout, std::size_t maximum_columns)
+{
+    max_columns = maximum_columns;
+    columns = 0;
+    h.assign((maximum_columns + 1) * maximum_columns, 0.0);
+    if (basis.size() < maximum_columns
+        || (!basis.empty() && (!basis.front()->same_layout(layout) || basis.front()->dtype != layout.dtype))) {
+        basis.clear();
+        basis.reserve(maximum_columns);
+        for (std::size_t i = 0; i < maximum_columns; ++i) basis.push_back(make_vector_like(layout));
+    }
+}
+
+void ArnoldiSnapshot::record_column(std::size_t column, const double* values, std::size_t count)
+{
+    if (column >= max_columns || count != column + 2)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "invalid Arnoldi snapshot column");
+    for (std::size_t row = 0; row < count; ++row) h[column * (max_columns + 1) + row] = values[row];
+}
+
+void ArnoldiSnapshot::finish_cycle(const std::vector<Vector*>& preconditioned, std::size_t count)
+{
+    if (count > max_columns || preconditioned.size() < count)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "invalid Arnoldi snapshot basis");
+    columns = count;
+    for (std::size_t col = 0; col < count; ++col) {
+        const Vector& z = *preconditioned[col];
+        OWTK_CUDA(cudaMemcpyAsync(basis[col]->data, z.data, z.owned_size() * z.elem(), cudaMemcpyDeviceToDevice,
+                                  z.ctx->stream));
+    }
+}
+
+void ArnoldiSnapshot::clear()
+{
+    columns = 0;
+    max_columns = 0;
+    h.clear();
+    basis.clear();
+}
+
 // ------------------------------------------------------------ shared ops
 void apply_operator(Matrix& m, Vector& in, Vector& out)
 {
+    if (m.kind == 3) {
+        if (!in.same_layout(out) || in.owned != m.owned || in.ghost != m.ghost || in.bs != m.bs)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "operator vector layout mismatch");
+        if (in.dtype != m.dtype || out.dtype != m.dtype)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "vector dtype differs from operator dtype");
+        host_apply_call(*m.ctx, m.host_apply, m.host_user, m.host_in, m.host_out, in, out);
+        return;
+    }
     if (m.dtype == OWTK_F64) {
         matrix_layout_check<double>(m, in, out);
         kern::spmv<double>(*m.ctx, m, static_cast<const double*>(in.data), static_cast<double*>(out.data));
@@ -433,6 +521,14 @@ void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out)
             kern::ilu_apply_lp<__nv_bfloat16>(c, *p, static_cast<const float*>(in.data), static_cast<float*>(out.data));
         else
             kern::block_ilu_apply(c, *p, static_cast<const double*>(in.data), static_cast<double*>(out.data));
+        return;
+    }
+    if (p != nullptr && p->kind == OWTK_PC_CALLBACK) {
+        if (in.owned != p->owned || in.ghost != p->ghost || in.bs != p->bs)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner layout mismatch");
+        if (in.dtype != p->dtype || out.dtype != p->dtype)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "vector dtype differs from preconditioner dtype");
+        host_apply_call(c, p->host_apply, p->host_user, p->host_in, p->host_out, in, out);
         return;
     }
     if (p == nullptr || p->kind == OWTK_PC_IDENTITY) {
@@ -724,6 +820,7 @@ owtk_status owtk_bsr_update_values(owtk_matrix* m, const void* values)
     return guarded([&] {
         require(m != nullptr && values != nullptr, "null handle");
         require(m->kind != 1, "split views borrow their coefficients; write the device arrays directly");
+        require(m->kind != 3, "a callback operator has no stored values");
         const std::size_t per = m->kind == 2 ? m->bs * m->bs : m->bs;
         OWTK_CUDA(cudaMemcpyAsync(m->values.ptr, values, m->entries * per * dsize(m->dtype),
                                   cudaMemcpyHostToDevice, m->ctx->stream));
@@ -811,6 +908,7 @@ owtk_status owtk_matrix_diagonal(owtk_matrix* m, void* host_out)
         const std::size_t n = m->owned * m->bs;
         Context& c = *m->ctx;
         if (m->kind == 2) fail(OWTK_ERR_INVALID_ARGUMENT, "dense-block CSR has no diagonal()");
+        if (m->kind == 3) fail(OWTK_ERR_INVALID_ARGUMENT, "a callback operator has no diagonal()");
         if (m->kind == 1) {
             OWTK_CUDA(cudaMemcpyAsync(host_out, m->diag, n * dsize(m->dtype), cudaMemcpyDeviceToHost, c.stream));
             c.sync();
@@ -853,7 +951,7 @@ std::unique_ptr<owtk_preconditioner> make_pc(owtk_matrix* m, owtk_pc_kind kind, 
     switch (kind) {
     case OWTK_PC_IDENTITY: break;
     case OWTK_PC_JACOBI:
-        if (m->kind == 2) fail(OWTK_ERR_INVALID_ARGUMENT, "Jacobi needs a matrix with diagonal()");
+        if (m->kind == 2 || m->kind == 3) fail(OWTK_ERR_INVALID_ARGUMENT, "Jacobi needs a matrix with diagonal()");
         p->inv_diag.allocate(n * es + 16);
         break;
     case OWTK_PC_SSOR:
@@ -919,7 +1017,8 @@ std::unique_ptr<owtk_preconditioner> make_pc(owtk_matrix* m, owtk_pc_kind kind, 
 // converted on the device by the mixed preconditioner's numeric update).
 std::unique_ptr<Matrix> f32_copy(const Matrix& m)
 {
-    if (m.kind == 1) fail(OWTK_ERR_INVALID_ARGUMENT, "mixed precision needs an owning matrix, not a split view");
+    if (m.kind == 1 || m.kind == 3)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "mixed precision needs an owning matrix, not a split view or callback");
     auto c = std::make_unique<owtk_matrix>();
     c->ctx = m.ctx;
     c->kind = m.kind;
@@ -1047,6 +1146,8 @@ owtk_status owtk_pc_update_values(owtk_preconditioner* pc, owtk_matrix* m)
         require(pc != nullptr && m != nullptr, "null handle");
         if (m->owned != pc->owned || m->ghost != pc->ghost || m->bs != pc->bs || m->dtype != pc->dtype)
             fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner matrix layout mismatch");
+        if (pc->kind == OWTK_PC_CALLBACK)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "a callback preconditioner has no numeric values to update");
         if (pc->kind == OWTK_PC_ILU || pc->kind == OWTK_PC_BLOCK_ILU) ilu_pattern_check(*pc, *m);
         if (pc->kind == OWTK_PC_MIXED) {
             if (m->kind != pc->m32->kind) fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner matrix kind mismatch");
@@ -1189,6 +1290,188 @@ owtk_status owtk_workspace_destroy(owtk_workspace* ws)
 
 uint64_t owtk_workspace_allocation_epochs(owtk_workspace* ws) { return ws ? ws->epochs : 0; }
 
+// ------------------------------------------------------------ extras
+owtk_status owtk_dot_ex(owtk_vector* a, owtk_vector* b, owtk_reduction_kind reduction, double* result, double* low)
+{
+    return guarded([&] {
+        same_layout_or_throw(a, b);
+        require(result != nullptr, "null output");
+        if (reduction < OWTK_REDUCTION_SERIAL || reduction > OWTK_REDUCTION_MIXED_PRECISION)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "unknown reduction kind");
+        Context& c = *a->ctx;
+        const void* pa[1] = {a->data};
+        const void* pb[1] = {b->data};
+        double* lo_slot = c.dev_scalars + 1;   // host view of scalar slot 1
+        if (reduction == OWTK_REDUCTION_SERIAL) {
+            if (a->dtype == OWTK_F64)
+                kern::multidot<double>(c, a->owned_size(), 1, reinterpret_cast<const double* const*>(pa),
+                                       reinterpret_cast<const double* const*>(pb), c.dev_scalar_copy.as<double>(),
+                                       c.dev_scalars);
+            else
+                kern::multidot<float>(c, a->owned_size(), 1, reinterpret_cast<const float* const*>(pa),
+                                      reinterpret_cast<const float* const*>(pb), c.dev_scalar_copy.as<double>(),
+                                      c.dev_scalars);
+            c.host_scalars[1] = 0.0;
+        } else if (a->dtype == OWTK_F64) {
+            kern::multidot_accurate<double>(c, a->owned_size(), 1, reduction, reinterpret_cast<const double* const*>(pa),
+                                            reinterpret_cast<const double* const*>(pb), c.dev_scalar_copy.as<double>(),
+                                            c.dev_scalars, lo_slot);
+        } else {
+            kern::multidot_accurate<float>(c, a->owned_size(), 1, reduction, reinterpret_cast<const float* const*>(pa),
+                                           reinterpret_cast<const float* const*>(pb), c.dev_scalar_copy.as<double>(),
+                                           c.dev_scalars, lo_slot);
+        }
+        c.sync();
+        const double hi = c.host_scalars[0];
+        *result = a->dtype == OWTK_F64 ? hi : static_cast<double>(static_cast<float>(hi));
+        if (low != nullptr) *low = a->dtype == OWTK_F64 ? c.host_scalars[1] : 0.0;
+    });
+}
+
+owtk_status owtk_norm_ex(owtk_vector* a, owtk_reduction_kind reduction, double* result)
+{
+    return guarded([&] {
+        require(a != nullptr && result != nullptr, "null handle");
+        if (reduction < OWTK_REDUCTION_SERIAL || reduction > OWTK_REDUCTION_MIXED_PRECISION)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "unknown reduction kind");
+        if (reduction != OWTK_REDUCTION_MIXED_PRECISION) {   // the compensated norm is the serial one
+            const owtk_status st = owtk_norm(a, result);
+            if (st != OWTK_OK) fail(st, owtk_last_error());
+            return;
+        }
+        Context& c = *a->ctx;
+        double* scratch = c.dev_scalar_copy.as<double>() + 8;
+        if (a->dtype == OWTK_F64)
+            kern::norm_accurate<double>(c, a->owned_size(), static_cast<const double*>(a->data), scratch,
+                                        c.dev_scalar_copy.as<double>(), c.dev_scalars);
+        else
+            kern::norm_accurate<float>(c, a->owned_size(), static_cast<const float*>(a->data), scratch,
+                                       c.dev_scalar_copy.as<double>(), c.dev_scalars);
+        c.sync();
+        *result = a->dtype == OWTK_F64 ? c.host_scalars[0] : static_cast<double>(static_cast<float>(c.host_scalars[0]));
+    });
+}
+
+owtk_status owtk_arnoldi_snapshot_create(owtk_context* ctx, owtk_arnoldi_snapshot** out)
+{
+    return guarded([&] {
+        require(ctx != nullptr && out != nullptr, "null handle");
+        auto s = std::make_unique<owtk_arnoldi_snapshot>();
+        s->ctx = ctx;
+        *out = s.release();
+    });
+}
+
+owtk_status owtk_arnoldi_snapshot_destroy(owtk_arnoldi_snapshot* snapshot)
+{
+    return guarded([&] { delete snapshot; });
+}
+
+owtk_status owtk_arnoldi_snapshot_clear(owtk_arnoldi_snapshot* snapshot)
+{
+    return guarded([&] {
+        require(snapshot != nullptr, "null handle");
+        snapshot->clear();
+    });
+}
+
+size_t owtk_arnoldi_snapshot_columns(const owtk_arnoldi_snapshot* snapshot)
+{
+    return snapshot ? snapshot->columns : 0;
+}
+
+owtk_status owtk_arnoldi_snapshot_h(const owtk_arnoldi_snapshot* snapshot, size_t row, size_t column, double* value)
+{
+    return guarded([&] {
+        require(snapshot != nullptr && value != nullptr, "null handle");
+        if (column >= snapshot->columns || row > snapshot->columns) fail(OWTK_ERR_OUT_OF_RANGE, "Arnoldi snapshot entry");
+        *value = snapshot->h[column * (snapshot->max_columns + 1) + row];
+    });
+}
+
+owtk_status owtk_arnoldi_snapshot_basis(owtk_arnoldi_snapshot* snapshot, size_t column, owtk_vector** out)
+{
+    return guarded([&] {
+        require(snapshot != nullptr && out != nullptr, "null handle");
+        if (column >= snapshot->columns) fail(OWTK_ERR_OUT_OF_RANGE, "Arnoldi snapshot basis");
+        snapshot->ctx->sync();
+        *out = static_cast<owtk_vector*>(snapshot->basis[column].get());
+    });
+}
+
+owtk_status owtk_callback_operator_create(owtk_context* ctx, owtk_dtype dtype, size_t owned, size_t ghost, size_t bs,
+                                          owtk_host_apply_fn apply, void* user, owtk_matrix** out)
+{
+    return guarded([&] {
+        require(ctx != nullptr && out != nullptr && apply != nullptr, "null handle");
+        if (owned == 0 || bs == 0) fail(OWTK_ERR_INVALID_ARGUMENT, "invalid operator layout");
+        if (dtype != OWTK_F64 && dtype != OWTK_F32) fail(OWTK_ERR_INVALID_ARGUMENT, "operator dtype must be F64 or F32");
+        auto m = std::make_unique<owtk_matrix>();
+        m->ctx = ctx;
+        m->kind = 3;
+        m->dtype = dtype;
+        m->owned = owned;
+        m->ghost = ghost;
+        m->bs = bs;
+        m->host_apply = apply;
+        m->host_user = user;
+        *out = m.release();
+    });
+}
+
+owtk_status owtk_pc_create_callback(owtk_context* ctx, owtk_dtype dtype, size_t owned, size_t ghost, size_t bs,
+                                    owtk_host_apply_fn apply, void* user, owtk_preconditioner** out)
+{
+    return guarded([&] {
+        require(ctx != nullptr && out != nullptr && apply != nullptr, "null handle");
+        if (owned == 0 || bs == 0) fail(OWTK_ERR_INVALID_ARGUMENT, "invalid preconditioner layout");
+        if (dtype != OWTK_F64 && dtype != OWTK_F32)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "preconditioner dtype must be F64 or F32");
+        auto p = std::make_unique<owtk_preconditioner>();
+        p->ctx = ctx;
+        p->kind = OWTK_PC_CALLBACK;
+        p->dtype = dtype;
+        p->owned = owned;
+        p->ghost = ghost;
+        p->bs = bs;
+        p->host_apply = apply;
+        p->host_user = user;
+        *out = p.release();
+    });
+}
+
+namespace {
+SolveExtras extras_of(owtk_solver_kind kind, const owtk_solve_extras* e)
+{
+    SolveExtras x;
+    if (e == nullptr) return x;
+    if (e->reduction < OWTK_REDUCTION_SERIAL || e->reduction > OWTK_REDUCTION_MIXED_PRECISION || e->reserved != 0)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "unknown reduction kind");
+    if (e->arnoldi_snapshot != nullptr && kind != OWTK_SOLVER_FGMRES)
+        fail(OWTK_ERR_INVALID_ARGUMENT, "Arnoldi snapshots are recorded by FGMRES only");
+    x.reduction = e->reduction;
+    x.test = e->convergence_test;
+    x.user = e->convergence_user;
+    x.snapshot = e->arnoldi_snapshot;
+    return x;
+}
+}  // namespace
+
+owtk_status owtk_solve_ex(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc, owtk_vector* rhs,
+                          owtk_vector* x, const owtk_solver_options* options, owtk_workspace* workspace,
+                          const owtk_solve_extras* extras, owtk_solver_result* result)
+{
+    return guarded([&] {
+        require(m != nullptr && rhs != nullptr && x != nullptr && options != nullptr && result != nullptr,
+                "null handle");
+        const SolveExtras ex = extras_of(kind, extras);
+        owtk_workspace local;
+        local.ctx = m->ctx;
+        Workspace& ws = workspace ? static_cast<Workspace&>(*workspace) : static_cast<Workspace&>(local);
+        solve(kind, *m, pc, *rhs, *x, *options, ws, *result, &ex);
+    });
+}
+
 // ------------------------------------------------------------ solves
 owtk_status owtk_solve(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc, owtk_vector* rhs,
                        owtk_vector* x, const owtk_solver_options* options, owtk_workspace* workspace,
@@ -1206,14 +1489,27 @@ owtk_status owtk_solve(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditione
 
 // solve_specwave_native (specwave_compat.hpp:99-249): the legacy SpecWave
 // solver IDs mapped onto the device solvers and preconditioners exactly as the
-// reference maps them.  IDs 10 and 22 select the reference's mixed-precision
-// and compensated serial reductions; on the device every reduction is the
-// two-stage FP64 reduction.  Stationary and multigrid IDs are not on this path.
+// reference maps them.  ID 10 takes the mixed-precision reduction and ID 22
+// the compensated one whatever the caller passes (specwave_compat.hpp:157-176,
+// :223-243); the others take the caller's.  Stationary and multigrid IDs are
+// not on this path.
 owtk_status owtk_solve_specwave(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
                                 const owtk_solver_options* options, owtk_workspace* workspace,
                                 owtk_solver_result* result)
 {
+    return owtk_solve_specwave_ex(solver_id, m, rhs, x, options, workspace, OWTK_REDUCTION_SERIAL, result);
+}
+
+owtk_status owtk_solve_specwave_ex(int solver_id, owtk_matrix* m, owtk_vector* rhs, owtk_vector* x,
+                                   const owtk_solver_options* options, owtk_workspace* workspace,
+                                   owtk_reduction_kind reduction, owtk_solver_result* result)
+{
     return guarded([&] {
+        if (reduction < OWTK_REDUCTION_SERIAL || reduction > OWTK_REDUCTION_MIXED_PRECISION)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "unknown reduction kind");
+        SolveExtras ex;
+        ex.reduction = solver_id == 10 ? OWTK_REDUCTION_MIXED_PRECISION
+                     : solver_id == 22 ? OWTK_REDUCTION_COMPENSATED : reduction;
         require(m != nullptr && rhs != nullptr && x != nullptr && options != nullptr && result != nullptr,
                 "null handle");
         owtk_solver_options o = *options;
@@ -1247,7 +1543,7 @@ owtk_status owtk_solve_specwave(int solver_id, owtk_matrix* m, owtk_vector* rhs,
         owtk_workspace local;
         local.ctx = m->ctx;
         Workspace& ws = workspace ? static_cast<Workspace&>(*workspace) : static_cast<Workspace&>(local);
-        solve(kind, *m, pc.get(), *rhs, *x, o, ws, *result);
+        solve(kind, *m, pc.get(), *rhs, *x, o, ws, *result, &ex);
     });
 }
 
@@ -1255,10 +1551,19 @@ owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_precondi
                             const void* host_rhs, void* host_x, const owtk_solver_options* options,
                             owtk_workspace* workspace, owtk_solver_result* result)
 {
+    return owtk_solve_host_ex(kind, m, pc, host_rhs, host_x, options, workspace, nullptr, result);
+}
+
+owtk_status owtk_solve_host_ex(owtk_solver_kind kind, owtk_matrix* m, owtk_preconditioner* pc,
+                               const void* host_rhs, void* host_x, const owtk_solver_options* options,
+                               owtk_workspace* workspace, const owtk_solve_extras* extras,
+                               owtk_solver_result* result)
+{
     return guarded([&] {
         require(m != nullptr && host_rhs != nullptr && host_x != nullptr && options != nullptr
                     && result != nullptr,
                 "null handle");
+        const SolveExtras ex = extras_of(kind, extras);
         Context& c = *m->ctx;
         owtk_workspace local;
         local.ctx = m->ctx;
@@ -1291,7 +1596,7 @@ owtk_status owtk_solve_host(owtk_solver_kind kind, owtk_matrix* m, owtk_precondi
         const std::size_t bytes = layout.local_size() * layout.elem();
         OWTK_CUDA(cudaMemcpyAsync(b.data, host_rhs, bytes, cudaMemcpyHostToDevice, c.stream));
         OWTK_CUDA(cudaMemcpyAsync(x.data, host_x, bytes, cudaMemcpyHostToDevice, c.stream));
-        solve(kind, *m, pc, b, x, *options, ws, *result);
+        solve(kind, *m, pc, b, x, *options, ws, *result, &ex);
         OWTK_CUDA(cudaMemcpyAsync(host_x, x.data, bytes, cudaMemcpyDeviceToHost, c.stream));
         c.sync();
     });

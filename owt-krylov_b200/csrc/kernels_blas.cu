@@ -677,6 +677,235 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
     }
 }
 
+// ---------------------------------------------------------- accurate reductions
+// The reference's CompensatedSerialReduction sums the rounded products with
+// Neumaier's compensated summation, and MixedPrecisionSerialReduction sums in
+// long double (reduction.hpp:175-299).  The device forms below keep those
+// accuracy classes with a parallel order:
+//   mode 1 (compensated): rounded products, each thread a Neumaier pair
+//     (sum, correction);
+//   mode 2 (mixed precision): each product split exactly by an FMA
+//     (TwoProduct) and summed with TwoSum into (sum, correction) -- the Dot2
+//     algorithm of Ogita, Rump and Oishi ("Accurate sum and dot product",
+//     SIAM J. Sci. Comput. 26, 2005): as accurate as a computation in twice
+//     the working precision rounded once, and at least as accurate as the
+//     reference's 80-bit long double sum.
+// Pairs from threads, warps and CTAs merge exactly: (s1, c1) + (s2, c2) =
+// (TwoSum(s1, s2).sum, c1 + c2 + TwoSum(s1, s2).error).  Merges run in a
+// fixed order, so results are deterministic.  Float inputs are widened to
+// FP64 first (products of floats are exact in FP64).
+struct CompPair {
+    double s, c;
+};
+
+__device__ __forceinline__ void two_sum(double a, double b, double& sum, double& err)
+{
+    sum = __dadd_rn(a, b);
+    const double bb = __dsub_rn(sum, a);
+    err = __dadd_rn(__dsub_rn(a, __dsub_rn(sum, bb)), __dsub_rn(b, bb));
+}
+
+__device__ __forceinline__ CompPair comp_merge(CompPair x, CompPair y)
+{
+    double s, e;
+    two_sum(x.s, y.s, s, e);
+    return {s, __dadd_rn(__dadd_rn(x.c, y.c), e)};
+}
+
+template<int MODE>
+__device__ __forceinline__ void comp_push(CompPair& a, double x, double y)
+{
+    if constexpr (MODE == 1) {
+        const double p = __dmul_rn(x, y);
+        const double t = __dadd_rn(a.s, p);
+        a.c = __dadd_rn(a.c, fabs(a.s) >= fabs(p) ? __dadd_rn(__dsub_rn(a.s, t), p)
+                                                   : __dadd_rn(__dsub_rn(p, t), a.s));
+        a.s = t;
+    } else {
+        const double h = __dmul_rn(x, y);
+        const double r = __fma_rn(x, y, -h);   // exact: x*y = h + r
+        double s, q;
+        two_sum(a.s, h, s, q);
+        a.s = s;
+        a.c = __dadd_rn(a.c, __dadd_rn(q, r));
+    }
+}
+
+__device__ __forceinline__ CompPair comp_warp(CompPair v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const CompPair o{__shfl_down_sync(0xffffffffu, v.s, off), __shfl_down_sync(0xffffffffu, v.c, off)};
+        v = comp_merge(v, o);
+    }
+    return v;
+}
+
+// k accurate dots a_j . b_j, G per pass.  Partials: two doubles per (dot, CTA).
+template<class T, int MODE, int G>
+__global__ void __launch_bounds__(kThreads) k_multidot_acc(std::size_t n, int k, PtrPack a, PtrPack b,
+                                                           double* partials, unsigned* ticket, double* out_dev,
+                                                           double* out_host, double* out_lo)
+{
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    __shared__ CompPair red[G][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int g0 = 0; g0 < k; g0 += G) {
+        CompPair acc[G];
+        const T* pa[G];
+        const T* pb[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            acc[j] = {0.0, 0.0};
+            pa[j] = g0 + j < k ? static_cast<const T*>(a.p[g0 + j]) : nullptr;
+            pb[j] = g0 + j < k ? static_cast<const T*>(b.p[g0 + j]) : nullptr;
+        }
+        for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+            for (int j = 0; j < G; ++j)
+                if (g0 + j < k)
+                    comp_push<MODE>(acc[j], static_cast<double>(pa[j][i]), static_cast<double>(pb[j][i]));
+        }
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const CompPair v = comp_warp(acc[j]);
+            if (lane == 0) red[j][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < G && g0 + static_cast<int>(threadIdx.x) < k) {
+            CompPair t = red[threadIdx.x][0];
+            for (int w = 1; w < kThreads / 32; ++w) t = comp_merge(t, red[threadIdx.x][w]);
+            const std::size_t d = static_cast<std::size_t>(g0) + threadIdx.x;
+            partials[(2 * d) * gridDim.x + blockIdx.x] = t.s;
+            partials[(2 * d + 1) * gridDim.x + blockIdx.x] = t.c;
+        }
+        __syncthreads();
+    }
+    if (last_block(ticket)) {
+        __threadfence();
+        for (int j = warp; j < k; j += kThreads / 32) {
+            const std::size_t d = static_cast<std::size_t>(j);
+            CompPair t{0.0, 0.0};
+            for (unsigned bb = lane; bb < gridDim.x; bb += 32)
+                t = comp_merge(t, {__ldcg(partials + (2 * d) * gridDim.x + bb),
+                                   __ldcg(partials + (2 * d + 1) * gridDim.x + bb)});
+            t = comp_warp(t);
+            if (lane == 0) {
+                double hi, lo;
+                two_sum(t.s, t.c, hi, lo);   // hi + lo == s + c exactly
+                out_dev[j] = hi;
+                out_host[j] = hi;
+                if (out_lo != nullptr) out_lo[j] = lo;
+            }
+        }
+        if (threadIdx.x == 0) *ticket = 0;
+    }
+}
+
+// Largest magnitude with NaN detection: scratch[0] = max |x|, scratch[1] = 1
+// when a NaN was seen.
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_absmax(std::size_t n, const T* __restrict__ x, double* partials,
+                                                     unsigned* ticket, double* scratch)
+{
+    double m = 0.0, bad = 0.0;
+    const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+        const double v = fabs(static_cast<double>(x[i]));
+        if (isnan(v)) bad = 1.0;
+        else m = fmax(m, v);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+        bad = fmax(bad, __shfl_down_sync(0xffffffffu, bad, off));
+    }
+    __shared__ double rm[kThreads / 32], rb[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        rm[warp] = m;
+        rb[warp] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kThreads / 32; ++w) {
+            m = fmax(m, rm[w]);
+            bad = fmax(bad, rb[w]);
+        }
+        partials[2 * blockIdx.x] = m;
+        partials[2 * blockIdx.x + 1] = bad;
+    }
+    if (last_block(ticket)) {
+        __threadfence();
+        if (threadIdx.x == 0) {
+            double mm = 0.0, bb = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) {
+                mm = fmax(mm, __ldcg(partials + 2 * b));
+                bb = fmax(bb, __ldcg(partials + 2 * b + 1));
+            }
+            scratch[0] = mm;
+            scratch[1] = bb;
+            *ticket = 0;
+        }
+    }
+}
+
+// Doubled-precision 2-norm: entries scaled by the power of two of max |x|
+// (exact), squares split by TwoProduct and summed as in Dot2, the square
+// root of the (sum, correction) pair refined by one Newton step.  NaN gives
+// NaN; an infinite or zero maximum is returned as is.
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_norm_acc(std::size_t n, const T* __restrict__ x,
+                                                       const double* __restrict__ scratch, double* partials,
+                                                       unsigned* ticket, double* out_dev, double* out_host)
+{
+    const double mx = scratch[0];
+    const bool special = scratch[1] != 0.0 || mx == 0.0 || isinf(mx);
+    const int e = special ? 0 : ilogb(mx);
+    CompPair acc{0.0, 0.0};
+    if (!special) {
+        const std::size_t stride = static_cast<std::size_t>(gridDim.x) * kThreads;
+        for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < n; i += stride) {
+            const double y = scalbn(static_cast<double>(x[i]), -e);
+            comp_push<2>(acc, y, y);
+        }
+    }
+    acc = comp_warp(acc);
+    __shared__ CompPair red[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        CompPair t = red[0];
+        for (int w = 1; w < kThreads / 32; ++w) t = comp_merge(t, red[w]);
+        partials[2 * blockIdx.x] = t.s;
+        partials[2 * blockIdx.x + 1] = t.c;
+    }
+    if (last_block(ticket)) {
+        __threadfence();
+        if (threadIdx.x == 0) {
+            CompPair t{0.0, 0.0};
+            for (unsigned b = 0; b < gridDim.x; ++b)
+                t = comp_merge(t, {__ldcg(partials + 2 * b), __ldcg(partials + 2 * b + 1)});
+            double r;
+            if (scratch[1] != 0.0) {
+                r = __longlong_as_double(0x7ff8000000000000LL);
+            } else if (special) {
+                r = mx;
+            } else {
+                double hi, lo;
+                two_sum(t.s, t.c, hi, lo);
+                const double r0 = sqrt(hi);
+                const double resid = __dadd_rn(__fma_rn(-r0, r0, hi), lo);   // (hi + lo) - r0^2
+                r = scalbn(__dadd_rn(r0, __ddiv_rn(resid, __dmul_rn(2.0, r0))), e);
+            }
+            *out_dev = r;
+            *out_host = r;
+            *ticket = 0;
+        }
+    }
+}
+
 // q = r / d (FP32) with ||r|| and ||q|| in the same pass: the learned
 // preconditioner's input scaling.  Plain FP64 sums of squares (the inputs
 // are residuals; the network needs the norms to FP32 accuracy only), summed
@@ -991,6 +1220,36 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
     c.launched();
 }
 
+template<class T> void multidot_accurate(Context& c, std::size_t n, int k, int mode, const T* const* a,
+                                         const T* const* b, double* out_dev, double* out_host, double* out_lo)
+{
+    if (k <= 0) return;
+    if (k > kMaxBatch) fail(OWTK_ERR_INVALID_ARGUMENT, "dot batch too large");
+    if (mode != 1 && mode != 2) fail(OWTK_ERR_INVALID_ARGUMENT, "unknown reduction mode");
+    const unsigned blocks = reduce_blocks(c, n);
+    const PtrPack pa = pack(reinterpret_cast<const void* const*>(a), k);
+    const PtrPack pb = pack(reinterpret_cast<const void* const*>(b), k);
+    if (mode == 1)
+        k_multidot_acc<T, 1, 4><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, partials_of(c), ticket_of(c),
+                                                                    out_dev, out_host, out_lo);
+    else
+        k_multidot_acc<T, 2, 4><<<blocks, kThreads, 0, c.stream>>>(n, k, pa, pb, partials_of(c), ticket_of(c),
+                                                                    out_dev, out_host, out_lo);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+template<class T> void norm_accurate(Context& c, std::size_t n, const T* x, double* scratch, double* out_dev,
+                                     double* out_host)
+{
+    const unsigned blocks = reduce_blocks(c, n);
+    k_absmax<T><<<blocks, kThreads, 0, c.stream>>>(n, x, partials_of(c), ticket_of(c), scratch);
+    k_norm_acc<T><<<blocks, kThreads, 0, c.stream>>>(n, x, scratch, partials_of(c), ticket_of(c), out_dev,
+                                                     out_host);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched(2);
+}
+
 template<class T>
 void prepare_norms(Context& c, std::size_t n, const T* r, const float* dinv, float* q, double* norms)
 {
@@ -1046,7 +1305,10 @@ template void convert<__nv_bfloat16, double>(Context&, std::size_t, const double
     template void gmres_update<T>(Context&, std::size_t, int, const T* const*, const double*, const T*, T*); \
     template void multidot<T>(Context&, std::size_t, int, const T* const*, const T* const*, double*, double*); \
     template void cgs_update_dot<T>(Context&, std::size_t, int, const T* const*, const double*, T*, double*, double*); \
-    template void norm<T>(Context&, std::size_t, const T*, double*, double*);
+    template void norm<T>(Context&, std::size_t, const T*, double*, double*);                       \
+    template void multidot_accurate<T>(Context&, std::size_t, int, int, const T* const*, const T* const*,  \
+                                       double*, double*, double*);                                 \
+    template void norm_accurate<T>(Context&, std::size_t, const T*, double*, double*, double*);
 
 INSTANTIATE(double)
 INSTANTIATE(float)

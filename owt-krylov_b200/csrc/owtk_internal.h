@@ -141,6 +141,11 @@ struct Matrix {
     const void* diag = nullptr;      // split view: borrowed device diagonal
     const void* off = nullptr;       // split view: borrowed device off-diagonal
     TilePlan plan;
+    // Kind 3 (owtk_callback_operator_create): an application function applied
+    // on host copies of the vectors.
+    owtk_host_apply_fn host_apply = nullptr;
+    void* host_user = nullptr;
+    std::vector<unsigned char> host_in, host_out;
     const void* value_ptr() const { return kind == 1 ? off : values.ptr; }
     std::size_t local_size() const { return (owned + ghost) * bs; }
 };
@@ -211,6 +216,10 @@ struct Preconditioner {
     Preconditioner* fallback = nullptr;
     std::uint64_t learned_applications = 0, learned_fallbacks = 0;
     DeviceBuffer check_work, alias_copy;
+    // OWTK_PC_CALLBACK: an application function applied on host copies.
+    owtk_host_apply_fn host_apply = nullptr;
+    void* host_user = nullptr;
+    std::vector<unsigned char> host_in, host_out;
 };
 // gnn.cu.  With `product` non-null, returns true when it also holds A z for
 // the network's own matrix (no fallback was taken).
@@ -275,6 +284,14 @@ template<class T> void gmres_update(Context& c, std::size_t n, int k, const T* c
 template<class T> void multidot(Context& c, std::size_t n, int k, const T* const* a,
                                 const T* const* b, double* out_dev, double* out_host);
 template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_dev, double* out_host);
+// Accurate reductions: mode 1 compensated (Neumaier over rounded products),
+// mode 2 doubled precision (TwoProduct + TwoSum, the Dot2 algorithm).  out_lo
+// (host, may be null) receives the low part: out + out_lo is the pair's exact sum.
+template<class T> void multidot_accurate(Context& c, std::size_t n, int k, int mode, const T* const* a,
+                                         const T* const* b, double* out_dev, double* out_host, double* out_lo);
+// Doubled-precision 2-norm; scratch: two device doubles.
+template<class T> void norm_accurate(Context& c, std::size_t n, const T* x, double* scratch, double* out_dev,
+                                     double* out_host);
 // ||x - w|| and ||x|| (two results) in one pass.
 void residual_norms(Context& c, std::size_t n, const double* x, const double* w, double* out_dev, double* out_host);
 // q = r / d (FP32 q, FP32 1/d) with norms[0] = norms[1] = ||r||, norms[2] = norms[3] = ||q||.
@@ -306,9 +323,37 @@ void apply_preconditioner(Preconditioner* p, Vector& in, Vector& out);
 bool apply_preconditioner_product(Preconditioner* p, Vector& in, Vector& out, double* product);
 void matrix_layout_check_f64(Matrix& m, Vector& in, Vector& out);
 
+// Last unrotated Arnoldi relation of FGMRES (core.hpp:462-534): the
+// Hessenberg columns as recorded before the Givens rotations (column-major,
+// (max_columns + 1) rows) and device copies of the preconditioned basis.
+struct ArnoldiSnapshot {
+    Context* ctx = nullptr;
+    std::size_t max_columns = 0, columns = 0;
+    std::vector<double> h;
+    std::vector<std::unique_ptr<Vector>> basis;
+    void begin_cycle(const Vector& layout, std::size_t maximum_columns);
+    void record_column(std::size_t column, const double* values, std::size_t count);
+    void finish_cycle(const std::vector<Vector*>& preconditioned, std::size_t count);
+    void clear();
+};
+
+// Optional parts of a solve (owtk_solve_ex): the reduction (0 serial,
+// 1 compensated, 2 mixed precision), the application convergence test
+// (SolverOptions::convergence_test, core.hpp:102-108) and the FGMRES snapshot.
+struct SolveExtras {
+    int reduction = 0;
+    owtk_convergence_test_fn test = nullptr;
+    void* user = nullptr;
+    ArnoldiSnapshot* snapshot = nullptr;
+};
+
+// A device vector with its own storage and the layout and dtype of `like`.
+std::unique_ptr<Vector> make_vector_like(const Vector& like);
+
 // Solver recurrences (solvers.cpp).
 void solve(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& rhs, Vector& x,
-           const owtk_solver_options& options, Workspace& ws, owtk_solver_result& result);
+           const owtk_solver_options& options, Workspace& ws, owtk_solver_result& result,
+           const SolveExtras* extras = nullptr);
 
 }  // namespace owtk
 
@@ -318,3 +363,4 @@ struct owtk_vector : owtk::Vector {};
 struct owtk_matrix : owtk::Matrix {};
 struct owtk_preconditioner : owtk::Preconditioner {};
 struct owtk_workspace : owtk::Workspace {};
+struct owtk_arnoldi_snapshot : owtk::ArnoldiSnapshot {};

@@ -31,6 +31,7 @@ enum Reason {
 constexpr int kSlotA = 0;      // first reduction batch
 constexpr int kSlotB = 128;    // second Gram-Schmidt batch
 constexpr int kSlotCoef = 256; // coefficients uploaded for update kernels
+constexpr int kSlotScratch = 508;   // two device doubles for the accurate norm
 
 template<class T>
 struct Engine {
@@ -40,6 +41,12 @@ struct Engine {
     std::size_t n;                 // owned values
     owtk_solver_result& res;
     const owtk_solver_options& o;
+    const SolveExtras* ex = nullptr;
+    std::vector<unsigned char> candidate_host;          // host copy for the convergence test
+    std::unique_ptr<Vector> app_residual, app_work;     // its true-residual vectors
+
+    int mode() const { return ex ? ex->reduction : 0; }
+    bool has_test() const { return ex != nullptr && ex->test != nullptr; }
 
     T* p(Vector& v) const { return static_cast<T*>(v.data); }
     const T* p(const Vector& v) const { return static_cast<const T*>(v.data); }
@@ -75,7 +82,8 @@ struct Engine {
         const T* pa[kMaxBatch];
         const T* pb[kMaxBatch];
         for (int j = 0; j < k; ++j) { pa[j] = p(*a[j]); pb[j] = p(*b[j]); }
-        kern::multidot<T>(c, n, k, pa, pb, dslot(slot), hslot(slot));
+        if (mode() != 0) kern::multidot_accurate<T>(c, n, k, mode(), pa, pb, dslot(slot), hslot(slot), nullptr);
+        else kern::multidot<T>(c, n, k, pa, pb, dslot(slot), hslot(slot));
         c.sync();
     }
     T dot(Vector& a, Vector& b)
@@ -88,7 +96,10 @@ struct Engine {
     }
     T norm_nocount(Vector& v)
     {
-        kern::norm<T>(c, n, p(v), dslot(kSlotA), hslot(kSlotA));
+        // The compensated reduction keeps the serial scaled norm
+        // (reduction.hpp:217-220); the mixed-precision one widens it (:283-286).
+        if (mode() == 2) kern::norm_accurate<T>(c, n, p(v), dslot(kSlotScratch), dslot(kSlotA), hslot(kSlotA));
+        else kern::norm<T>(c, n, p(v), dslot(kSlotA), hslot(kSlotA));
         c.sync();
         return scalar(kSlotA);
     }
@@ -126,12 +137,43 @@ struct Engine {
         res.true_residual_norm = true_norm;
         res.relative_residual_norm = static_cast<double>(true_norm / (rhs_norm > T(0) ? rhs_norm : T(1)));
     }
-    // core.hpp:549-560 (no application convergence test through the C ABI)
+    // core.hpp:549-560: an application convergence test replaces the tolerance.
     T threshold(T rhs_norm) const
     {
         const T rel = static_cast<T>(o.relative_tolerance) * (rhs_norm > T(0) ? rhs_norm : T(1));
         if (!std::isfinite(rhs_norm) || !std::isfinite(rel)) return std::numeric_limits<T>::quiet_NaN();
+        if (has_test()) return T(0);
         return std::max(static_cast<T>(o.absolute_tolerance), rel);
+    }
+    // krylov_solvers.hpp:122-143: ask the application whether `candidate`
+    // solves the problem; if so, measure its true residual (one operator
+    // application, two norms) and finish as converged by the application.
+    bool app_converged(Vector& b, Vector& candidate)
+    {
+        if (!has_test()) return false;
+        const std::size_t count = candidate.local_size();
+        candidate_host.resize(count * candidate.elem());
+        OWTK_CUDA(cudaMemcpyAsync(candidate_host.data(), candidate.data, candidate_host.size(),
+                                  cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        const int verdict = ex->test(ex->user, res.iterations, candidate_host.data(), count);
+        if (verdict < 0) fail(OWTK_ERR_RUNTIME, "application convergence test failed");
+        if (verdict == 0) return false;
+        if (!app_residual) {
+            app_residual = make_vector_like(candidate);
+            app_work = make_vector_like(candidate);
+        }
+        true_residual(b, candidate, *app_residual, *app_work);
+        const T rhs_norm = norm(b);
+        const T true_norm = norm(*app_residual);
+        set_residuals(static_cast<T>(res.recursive_residual_norm), true_norm, rhs_norm);
+        if (!std::isfinite(true_norm) || !std::isfinite(rhs_norm)) {
+            breakdown(kNonFinite);
+        } else {
+            res.status = kConverged;
+            res.converged_by_application = 1;
+        }
+        return true;
     }
     T tiny() const { return T(1024) * std::numeric_limits<T>::min(); }
     T btol() const { return static_cast<T>(o.breakdown_tolerance); }
@@ -164,6 +206,7 @@ void bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
     Vector& omid = *ws.vectors[7];
     Vector& work = *ws.vectors[8];
 
+    if (e.app_converged(b, x)) return;
     e.true_residual(b, x, r, work);
     e.copy(r, shadow);
     const T bnorm = e.norm(b);
@@ -211,6 +254,7 @@ void bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         const T mnorm = e.norm(mid);
         if (mnorm <= thr) {
             e.axpy(alpha, psearch, x);
+            if (e.app_converged(b, x)) return;
             e.true_residual(b, x, r, work);
             const T tn = e.norm(r);
             e.set_residuals(mnorm, tn, bnorm);
@@ -236,8 +280,9 @@ void bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             return;
         }
         kern::bicg_xr<T>(e.c, e.n, alpha, e.p(psearch), omega, e.p(pmid), e.p(mid), e.p(omid), e.p(x), e.p(r));
+        if (e.app_converged(b, x)) return;
         const bool replace = o.residual_replacement_interval > 0 && it % o.residual_replacement_interval == 0;
-        const bool check = it % o.convergence_check_interval == 0;
+        const bool check = !e.has_test() && it % o.convergence_check_interval == 0;
         if (replace || check) {
             const T rn = e.norm(r);
             if (replace || rn <= thr) {
@@ -277,6 +322,7 @@ void pipelined_bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
     Vector& pmid = *ws.vectors[7];
     Vector& work = *ws.vectors[8];
 
+    if (e.app_converged(b, x)) return;
     e.true_residual(b, x, r, work);
     e.copy(r, shadow);
     e.copy(r, search);
@@ -324,6 +370,7 @@ void pipelined_bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         if (mnorm <= thr || !std::isfinite(g1) || std::abs(g1) <= tiny) {
             if (mnorm <= thr) {
                 e.axpy(alpha, psearch, x);
+                if (e.app_converged(b, x)) return;
                 e.true_residual(b, x, r, work);
                 const T tn = e.norm(r);
                 e.set_residuals(mnorm, tn, bnorm);
@@ -347,6 +394,7 @@ void pipelined_bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         const T rsq2 = e.scalar(kSlotA + 1);
         rnorm = e.norm_from_squared(r, rsq2);
         res.recursive_residual_norm = rnorm;
+        if (e.app_converged(b, x)) return;
         if (rnorm <= thr) {
             e.true_residual(b, x, r, work);
             const T tn = e.norm(r);
@@ -395,6 +443,7 @@ void comm_hiding_bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
     Vector& y = *ws.vectors[14];
     Vector& work = *ws.vectors[15];
 
+    if (e.app_converged(b, x)) return;
     e.true_residual(b, x, r, work);
     e.copy(r, rp);
     {
@@ -457,6 +506,7 @@ void comm_hiding_bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         if (mnorm <= thr || !std::isfinite(f1) || std::abs(f1) <= tiny) {
             if (mnorm <= thr) {
                 e.axpy(alpha, p2, x);
+                if (e.app_converged(b, x)) return;
                 e.true_residual(b, x, r, work);
                 const T tn = e.norm(r);
                 e.set_residuals(mnorm, tn, bnorm);
@@ -487,6 +537,7 @@ void comm_hiding_bicgstab(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         rnorm = e.norm_from_squared(r, g0);
         rho = g1;
         res.recursive_residual_norm = rnorm;
+        if (e.app_converged(b, x)) return;
         if (rnorm <= thr) {
             e.true_residual(b, x, r, work);
             const T tn = e.norm(r);
@@ -540,7 +591,12 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
     std::vector<const T*> vptr(R + 1), zptr(R);
     for (std::size_t j = 0; j <= R; ++j) vptr[j] = e.p(*V[j]);
     for (std::size_t j = 0; j < R; ++j) zptr[j] = e.p(*Z[j]);
+    ArnoldiSnapshot* snap = e.ex ? e.ex->snapshot : nullptr;
 
+    if (e.app_converged(b, x)) {
+        if (snap) snap->clear();
+        return;
+    }
     e.true_residual(b, x, r, w);
     const T bnorm = e.norm(b);
     const T r0 = e.norm(r);
@@ -548,11 +604,22 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
     res.initial_residual_norm = r0;
     e.set_residuals(r0, r0, bnorm);
     if (!std::isfinite(r0) || !std::isfinite(thr)) { e.breakdown(kNonFinite); return; }
-    if (r0 <= thr) { res.status = kConverged; return; }
+    if (r0 <= thr) {
+        if (snap) snap->clear();
+        res.status = kConverged;
+        return;
+    }
 
-    std::vector<T> H((R + 1) * R), cs(R), sn(R), g(R + 1), coef(R);
+    // krylov_solvers.hpp:232: the candidate iterate of the convergence test.
+    std::unique_ptr<Vector> candidate = e.has_test() ? make_vector_like(b) : nullptr;
+    std::vector<T> H((R + 1) * R), cs(R), sn(R), g(R + 1), coef(R + 1);
+    std::vector<double> column(R + 2);
     auto h = [&](std::size_t row, std::size_t col) -> T& { return H[col * (R + 1) + row]; };
+    // The fused Gram-Schmidt kernels sum in the serial reduction's order; the
+    // accurate reductions take the general path (pair dots, then updates).
+    const bool fusable = e.mode() == 0;
     while (res.iterations < o.maximum_iterations) {
+        if (snap) snap->begin_cycle(b, R);
         const T beta = e.norm(r);
         kern::divide<T>(e.c, e.n, e.p(r), beta, e.p(*V[0]));
         std::fill(H.begin(), H.end(), T(0));
@@ -567,31 +634,34 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             for (std::size_t j = 0; j < k; ++j) vb[j] = vptr[j];
             ++res.global_reductions;
             const bool iterated = o.gmres_orthogonalization == 0;
-            if (k + 1 <= 32) {
-                // First projection batch: w.V_j (j < k) and w.w, w read once.
-                kern::basis_dots<T>(e.c, e.n, static_cast<int>(k), vb, e.p(w), e.dslot(kSlotA), e.hslot(kSlotA));
-            } else {
+            // w.V_j (j < k) and w.w as one batch of pair dots into `slot`.
+            const auto pair_dots = [&](int slot) {
                 const T* pa[kMaxBatch];
                 const T* pb[kMaxBatch];
                 for (std::size_t j = 0; j < k; ++j) { pa[j] = e.p(w); pb[j] = vptr[j]; }
                 pa[k] = e.p(w);
                 pb[k] = e.p(w);
-                kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(kSlotA), e.hslot(kSlotA));
+                if (e.mode() != 0)
+                    kern::multidot_accurate<T>(e.c, e.n, static_cast<int>(k + 1), e.mode(), pa, pb, e.dslot(slot),
+                                               e.hslot(slot), nullptr);
+                else
+                    kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(slot), e.hslot(slot));
+            };
+            if (fusable && k + 1 <= 32) {
+                // First projection batch: w.V_j (j < k) and w.w, w read once.
+                kern::basis_dots<T>(e.c, e.n, static_cast<int>(k), vb, e.p(w), e.dslot(kSlotA), e.hslot(kSlotA));
+            } else {
+                pair_dots(kSlotA);
             }
             if (iterated) {
                 // w -= V h1, fused with the second batch (one pass over V while
                 // the batch fits the fused kernel); then w -= V h2.
-                if (k + 1 <= 32) {
+                if (fusable && k + 1 <= 32) {
                     kern::cgs_update_dot<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w),
                                             e.dslot(kSlotB), e.hslot(kSlotB));
                 } else {
                     kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotA), e.p(w));
-                    const T* pa[kMaxBatch];
-                    const T* pb[kMaxBatch];
-                    for (std::size_t j = 0; j < k; ++j) { pa[j] = e.p(w); pb[j] = vptr[j]; }
-                    pa[k] = e.p(w);
-                    pb[k] = e.p(w);
-                    kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(kSlotB), e.hslot(kSlotB));
+                    pair_dots(kSlotB);
                 }
                 // The last pass, w -= V h2, waits for the norm: it is fused
                 // with the normalisation into V[cols + 1] below.
@@ -617,12 +687,7 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             T nsq = nonneg;
             if (iterated || adaptive) {
                 if (adaptive) {
-                    const T* pa[kMaxBatch];
-                    const T* pb[kMaxBatch];
-                    for (std::size_t j = 0; j < k; ++j) { pa[j] = e.p(w); pb[j] = vptr[j]; }
-                    pa[k] = e.p(w);
-                    pb[k] = e.p(w);
-                    kern::multidot<T>(e.c, e.n, static_cast<int>(k + 1), pa, pb, e.dslot(kSlotB), e.hslot(kSlotB));
+                    pair_dots(kSlotB);
                     kern::cgs_update<T>(e.c, e.n, static_cast<int>(k), vb, e.dslot(kSlotB), e.p(w));
                     e.c.sync();
                 }
@@ -662,6 +727,10 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
                 finish_last_pass();
                 arnoldi_breakdown = true;
             }
+            if (snap) {
+                for (std::size_t row = 0; row <= cols + 1; ++row) column[row] = static_cast<double>(h(row, cols));
+                snap->record_column(cols, column.data(), cols + 2);
+            }
             for (std::size_t row = 0; row < cols; ++row) {
                 const T first = cs[row] * h(row, cols) + sn[row] * h(row + 1, cols);
                 h(row + 1, cols) = -sn[row] * h(row, cols) + cs[row] * h(row + 1, cols);
@@ -683,12 +752,42 @@ void fgmres(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             g[cols] *= cs[cols];
             const T est = std::abs(g[cols + 1]);
             res.recursive_residual_norm = est;
+            if (candidate) {
+                // krylov_solvers.hpp:399-425: x_k = x + Z c without ending the
+                // cycle, c from the rotated system so far; offered to the test.
+                bool nonsingular = true;
+                for (std::size_t row = cols + 1; row-- > 0;) {
+                    T value = g[row];
+                    for (std::size_t j = row + 1; j <= cols; ++j) value -= h(row, j) * coef[j];
+                    if (h(row, row) == T(0)) {
+                        nonsingular = false;
+                        break;
+                    }
+                    coef[row] = value / h(row, row);
+                }
+                if (nonsingular) {
+                    for (std::size_t j = 0; j <= cols; ++j) e.c.host_scalars[kSlotCoef + j] = static_cast<double>(coef[j]);
+                    OWTK_CUDA(cudaMemcpyAsync(e.dslot(kSlotCoef), e.c.host_scalars + kSlotCoef,
+                                              (cols + 1) * sizeof(double), cudaMemcpyHostToDevice, e.c.stream));
+                    kern::gmres_update<T>(e.c, e.n, static_cast<int>(cols + 1), zptr.data(), e.dslot(kSlotCoef),
+                                          e.p(x), e.p(*candidate));
+                    ++res.iterations;
+                    if (e.app_converged(b, *candidate)) {
+                        if (snap) snap->finish_cycle(Z, cols + 1);
+                        e.copy(*candidate, x);
+                        e.c.sync();
+                        return;
+                    }
+                    --res.iterations;
+                }
+            }
             if (est <= thr || arnoldi_breakdown) {
                 ++cols;
                 ++res.iterations;
                 break;
             }
         }
+        if (snap) snap->finish_cycle(Z, cols);
         std::fill(coef.begin(), coef.end(), T(0));
         for (std::size_t rv = cols; rv-- > 0;) {
             T val = g[rv];
@@ -760,6 +859,7 @@ void idrs(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         U[k] = ws.vectors[4 + s + k].get();
         P[k] = ws.vectors[4 + 2 * s + k].get();
     }
+    if (e.app_converged(b, x)) return;
     e.true_residual(b, x, r, work);
     const T bnorm = e.norm(b);
     T rnorm = e.norm(r);
@@ -881,6 +981,7 @@ void idrs(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
             f[k] = 0;
             ++res.iterations;
             restarts = 0;
+            if (e.app_converged(b, x)) return;
             rnorm = e.norm(r);
             res.recursive_residual_norm = rnorm;
             if (!std::isfinite(rnorm)) { e.breakdown(kNonFinite); return; }
@@ -927,6 +1028,7 @@ void idrs(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
         e.axpy(-omega, work, r);
         ++res.iterations;
         restarts = 0;
+        if (e.app_converged(b, x)) return;
         rnorm = e.norm(r);
         res.recursive_residual_norm = rnorm;
         if (!std::isfinite(rnorm)) { e.breakdown(kNonFinite); return; }
@@ -957,12 +1059,16 @@ void idrs(Engine<T>& e, Vector& b, Vector& x, Workspace& ws)
 
 template<class T>
 void run(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& b, Vector& x,
-         const owtk_solver_options& o, Workspace& ws, owtk_solver_result& res)
+         const owtk_solver_options& o, Workspace& ws, owtk_solver_result& res, const SolveExtras* ex)
 {
     Engine<T> e{*m.ctx, m, pc, b.owned_size(), res, o};
+    e.ex = ex;
     switch (kind) {
     case OWTK_SOLVER_FGMRES:
-        if (o.restart == 0) return;
+        if (o.restart == 0) {
+            if (ex && ex->snapshot) ex->snapshot->clear();
+            return;
+        }
         fgmres<T>(e, b, x, ws);
         break;
     case OWTK_SOLVER_BICGSTAB: bicgstab<T>(e, b, x, ws); break;
@@ -985,8 +1091,9 @@ void run(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& b, Vector
 }  // namespace
 
 void solve(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& b, Vector& x,
-           const owtk_solver_options& o, Workspace& ws, owtk_solver_result& res)
+           const owtk_solver_options& o, Workspace& ws, owtk_solver_result& res, const SolveExtras* ex)
 {
+    if (ex && (ex->reduction < 0 || ex->reduction > 2)) fail(OWTK_ERR_INVALID_ARGUMENT, "unknown reduction kind");
     std::memset(&res, 0, sizeof(res));
     res.status = kInvalid;
     res.breakdown_reason = kNone;
@@ -997,8 +1104,10 @@ void solve(owtk_solver_kind kind, Matrix& m, Preconditioner* pc, Vector& b, Vect
     const bool bad = !b.same_layout(x) || b.dtype != x.dtype
         || (m.dtype == OWTK_F64 ? !valid_options<double>(o) : !valid_options<float>(o));
     if (!bad) {
-        if (m.dtype == OWTK_F64) run<double>(kind, m, pc, b, x, o, ws, res);
-        else run<float>(kind, m, pc, b, x, o, ws, res);
+        if (m.dtype == OWTK_F64) run<double>(kind, m, pc, b, x, o, ws, res, ex);
+        else run<float>(kind, m, pc, b, x, o, ws, res, ex);
+    } else if (kind == OWTK_SOLVER_FGMRES && ex && ex->snapshot) {
+        ex->snapshot->clear();   // krylov_solvers.hpp:177-182
     }
     m.ctx->check_device_status();
     res.solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

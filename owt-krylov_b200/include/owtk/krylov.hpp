@@ -15,10 +15,14 @@
 //     used; after writing coefficients in place, call sync_values() on the
 //     matrix (preconditioner update_values(matrix) does it too).  The
 //     reference reads host arrays at every apply instead.
-//   * SolverOptions::convergence_test (an application callback) is rejected:
-//     it would need a host round trip per iterate.
-//   * Reductions always run on the device; the Reduction template argument of
-//     the solvers is accepted for source compatibility and otherwise unused.
+//   * SolverOptions::convergence_test is called with a host copy of each
+//     candidate iterate (one device-to-host copy per call).
+//   * Reductions run on the device: SerialReduction, CompensatedSerialReduction
+//     and MixedPrecisionSerialReduction select the matching device reduction;
+//     any other Reduction type reduces like SerialReduction.
+//   * Operators and preconditioners that are not this header's types (any
+//     type with apply(in, out)) are called on host copies of the vectors once
+//     per application.
 // Link with -lowtk_b200 and add the repository's include/ directory.
 #pragma once
 
@@ -791,36 +795,175 @@ public:
 };
 
 // ------------------------------------------------------------------ reductions
-// Device reductions of host vectors (reduction.hpp:103-168); solvers always
-// reduce on the device, whichever Reduction type they are given.
+// Device reductions of host vectors (reduction.hpp:103-299).  Solvers given
+// one of these three types run their reductions on the device with the same
+// accuracy class: serial (two-stage FP64 sums), compensated (Neumaier pairs)
+// or mixed precision (doubled-precision Dot2 sums and norm).  Any other
+// Reduction type is accepted for source compatibility and reduces serially.
+namespace detail {
+
 template<std::floating_point T>
-class SerialReduction {
+std::pair<double, double> device_dot(const BlockVector<T>& a, const BlockVector<T>& b, owtk_reduction_kind kind)
+{
+    if (!a.same_layout(b)) throw std::invalid_argument("dot layout mismatch");
+    auto [da, db] = cuda::Runtime::instance().scratch(cuda::dtype_of<T>(), a.owned_nodes(), a.ghost_nodes(),
+                                                      a.block_size());
+    cuda::check(owtk_vector_upload(da, a.data(), a.owned_size()));
+    cuda::check(owtk_vector_upload(db, b.data(), b.owned_size()));
+    double hi = 0, lo = 0;
+    cuda::check(owtk_dot_ex(da, db, kind, &hi, &lo));
+    return {hi, lo};
+}
+
+template<std::floating_point T>
+T device_norm(const BlockVector<T>& a, owtk_reduction_kind kind)
+{
+    auto [da, db] = cuda::Runtime::instance().scratch(cuda::dtype_of<T>(), a.owned_nodes(), a.ghost_nodes(),
+                                                      a.block_size());
+    (void)db;
+    cuda::check(owtk_vector_upload(da, a.data(), a.owned_size()));
+    double r = 0;
+    cuda::check(owtk_norm_ex(da, kind, &r));
+    return static_cast<T>(r);
+}
+
+template<std::floating_point T, owtk_reduction_kind Kind>
+class DeviceReduction {
 public:
-    [[nodiscard]] T dot(const BlockVector<T>& a, const BlockVector<T>& b) const
+    struct Request {};
+    static constexpr owtk_reduction_kind device_kind = Kind;
+
+    [[nodiscard]] T dot(const BlockVector<T>& lhs, const BlockVector<T>& rhs) const
     {
-        if (!a.same_layout(b)) throw std::invalid_argument("dot layout mismatch");
-        auto [da, db] = cuda::Runtime::instance().scratch(cuda::dtype_of<T>(), a.owned_nodes(), a.ghost_nodes(),
-                                                          a.block_size());
-        cuda::check(owtk_vector_upload(da, a.data(), a.owned_size()));
-        cuda::check(owtk_vector_upload(db, b.data(), b.owned_size()));
-        double r = 0;
-        cuda::check(owtk_dot(da, db, &r));
-        return static_cast<T>(r);
+        return static_cast<T>(device_dot(lhs, rhs, Kind).first);
     }
-    [[nodiscard]] T local_dot(const BlockVector<T>& a, const BlockVector<T>& b) const { return dot(a, b); }
-    [[nodiscard]] T norm(const BlockVector<T>& a) const
+    [[nodiscard]] T local_dot(const BlockVector<T>& lhs, const BlockVector<T>& rhs) const { return dot(lhs, rhs); }
+    [[nodiscard]] T norm(const BlockVector<T>& vector) const { return device_norm(vector, Kind); }
+    void sum(std::span<const T> local, std::span<T> global) const
     {
-        auto [da, db] = cuda::Runtime::instance().scratch(cuda::dtype_of<T>(), a.owned_nodes(), a.ghost_nodes(),
-                                                          a.block_size());
-        (void)db;
-        cuda::check(owtk_vector_upload(da, a.data(), a.owned_size()));
-        double r = 0;
-        cuda::check(owtk_norm(da, &r));
-        return static_cast<T>(r);
+        if (local.size() != global.size()) throw std::invalid_argument("reduction batch size mismatch");
+        std::copy(local.begin(), local.end(), global.begin());
     }
+    [[nodiscard]] Request begin_sum(std::span<const T> local, std::span<T> global) const
+    {
+        sum(local, global);
+        return {};
+    }
+    void end(Request&) const noexcept {}
 };
-template<std::floating_point T> using CompensatedSerialReduction = SerialReduction<T>;
-template<std::floating_point T> using MixedPrecisionSerialReduction = SerialReduction<T>;
+
+template<class R>
+constexpr owtk_reduction_kind reduction_kind_of()
+{
+    if constexpr (requires { R::device_kind; }) return R::device_kind;
+    else return OWTK_REDUCTION_SERIAL;
+}
+
+}  // namespace detail
+
+template<std::floating_point T>
+class SerialReduction : public detail::DeviceReduction<T, OWTK_REDUCTION_SERIAL> {};
+
+// Neumaier-compensated reduction (reduction.hpp:175-226).
+template<std::floating_point T>
+class CompensatedSerialReduction : public detail::DeviceReduction<T, OWTK_REDUCTION_COMPENSATED> {};
+
+// Wide local products (reduction.hpp:228-299): local_dot returns long double,
+// here the device's doubled-precision (sum, correction) pair added in long double.
+template<std::floating_point T>
+class MixedPrecisionSerialReduction {
+public:
+    struct Request {};
+    static constexpr owtk_reduction_kind device_kind = OWTK_REDUCTION_MIXED_PRECISION;
+
+    [[nodiscard]] T dot(const BlockVector<T>& lhs, const BlockVector<T>& rhs) const
+    {
+        return static_cast<T>(local_dot(lhs, rhs));
+    }
+    [[nodiscard]] long double local_dot(const BlockVector<T>& lhs, const BlockVector<T>& rhs) const
+    {
+        const auto [hi, lo] = detail::device_dot(lhs, rhs, device_kind);
+        return static_cast<long double>(hi) + static_cast<long double>(lo);
+    }
+    [[nodiscard]] T norm(const BlockVector<T>& vector) const { return detail::device_norm(vector, device_kind); }
+    void sum(std::span<const long double> local, std::span<T> global) const
+        requires(!std::same_as<T, long double>)
+    {
+        if (local.size() != global.size()) throw std::invalid_argument("reduction batch size mismatch");
+        std::transform(local.begin(), local.end(), global.begin(), [](long double v) { return static_cast<T>(v); });
+    }
+    [[nodiscard]] Request begin_sum(std::span<const long double> local, std::span<T> global) const
+        requires(!std::same_as<T, long double>)
+    {
+        sum(local, global);
+        return {};
+    }
+    void sum(std::span<const T> local, std::span<T> global) const
+    {
+        if (local.size() != global.size()) throw std::invalid_argument("reduction batch size mismatch");
+        std::copy(local.begin(), local.end(), global.begin());
+    }
+    [[nodiscard]] Request begin_sum(std::span<const T> local, std::span<T> global) const
+    {
+        sum(local, global);
+        return {};
+    }
+    void end(Request&) const noexcept {}
+};
+
+// ------------------------------------------------------------------ Arnoldi snapshot
+// The last unrotated Arnoldi relation produced by FGMRES (core.hpp:462-534),
+// recorded on the device; preconditioned_basis() copies a vector to the host
+// on first access after a solve.
+template<std::floating_point T>
+class ArnoldiSnapshot {
+public:
+    void clear() noexcept
+    {
+        if (s_) owtk_arnoldi_snapshot_clear(s_.get());
+        cache_.clear();
+    }
+    [[nodiscard]] std::size_t columns() const noexcept { return s_ ? owtk_arnoldi_snapshot_columns(s_.get()) : 0; }
+    [[nodiscard]] T h(std::size_t row, std::size_t column) const
+    {
+        if (!s_) throw std::out_of_range("Arnoldi snapshot entry");
+        double v = 0;
+        cuda::check(owtk_arnoldi_snapshot_h(s_.get(), row, column, &v));
+        return static_cast<T>(v);
+    }
+    [[nodiscard]] const BlockVector<T>& preconditioned_basis(std::size_t column) const
+    {
+        if (!s_ || column >= columns()) throw std::out_of_range("Arnoldi snapshot basis");
+        if (cache_.size() != columns()) cache_.assign(columns(), BlockVector<T>());
+        if (cache_[column].owned_nodes() == 0) {
+            owtk_vector* v = nullptr;
+            cuda::check(owtk_arnoldi_snapshot_basis(s_.get(), column, &v));
+            BlockVector<T> host(owned_, ghost_, bs_);
+            cuda::check(owtk_vector_download(v, host.data(), host.owned_size()));
+            cache_[column] = std::move(host);
+        }
+        return cache_[column];
+    }
+    // The device snapshot a solve records into (created on first use).
+    owtk_arnoldi_snapshot* device_for(std::size_t owned, std::size_t ghost, std::size_t bs)
+    {
+        if (!s_) {
+            owtk_arnoldi_snapshot* p = nullptr;
+            cuda::check(owtk_arnoldi_snapshot_create(cuda::Runtime::instance().context(), &p));
+            s_ = cuda::own(p, [](owtk_arnoldi_snapshot* q) { owtk_arnoldi_snapshot_destroy(q); });
+        }
+        owned_ = owned;
+        ghost_ = ghost;
+        bs_ = bs;
+        cache_.clear();
+        return s_.get();
+    }
+
+private:
+    std::shared_ptr<owtk_arnoldi_snapshot> s_;
+    std::size_t owned_ = 0, ghost_ = 0, bs_ = 0;
+    mutable std::vector<BlockVector<T>> cache_;
+};
 
 // ------------------------------------------------------------------ solvers
 namespace detail {
@@ -828,31 +971,64 @@ namespace detail {
 template<class Op>
 concept DeviceOperator = requires(Op& op) { op.matrix().device(); };
 
-template<class P>
-owtk_preconditioner* pc_handle(const P& pc)
-{
-    if constexpr (requires { pc.device(); }) {
-        return pc.device();
-    } else {
-        static_assert(sizeof(P) == 0, "device solves take the preconditioners of owtk/krylov.hpp");
-        return nullptr;
-    }
-}
+// An application operator or preconditioner (any type with apply(in, out),
+// docs/MANUAL.tex:676-712) behind a C callback; errors it throws are kept and
+// rethrown by the solver call.
+template<std::floating_point T>
+struct HostCallbacks {
+    std::size_t owned = 0, ghost = 0, bs = 0;
+    std::function<void(BlockVector<T>&, BlockVector<T>&)> op, pc;
+    const std::function<bool(std::size_t, const BlockVector<T>&)>* test = nullptr;
+    std::exception_ptr error;
 
-template<std::floating_point T, class Op, class P>
+    BlockVector<T> view(void* p, std::size_t count) const
+    {
+        return BlockVector<T>::view(owned, ghost, bs, std::span<T>(static_cast<T*>(p), count));
+    }
+    static int apply_op(void* user, void* in, void* out, size_t count)
+    {
+        auto* h = static_cast<HostCallbacks*>(user);
+        try {
+            auto vi = h->view(in, count), vo = h->view(out, count);
+            h->op(vi, vo);
+            return 0;
+        } catch (...) {
+            h->error = std::current_exception();
+            return 1;
+        }
+    }
+    static int apply_pc(void* user, void* in, void* out, size_t count)
+    {
+        auto* h = static_cast<HostCallbacks*>(user);
+        try {
+            auto vi = h->view(in, count), vo = h->view(out, count);
+            h->pc(vi, vo);
+            return 0;
+        } catch (...) {
+            h->error = std::current_exception();
+            return 1;
+        }
+    }
+    static int convergence(void* user, uint64_t iteration, const void* candidate, size_t count)
+    {
+        auto* h = static_cast<HostCallbacks*>(user);
+        try {
+            const auto v = h->view(const_cast<void*>(candidate), count);
+            return (*h->test)(static_cast<std::size_t>(iteration), v) ? 1 : 0;
+        } catch (...) {
+            h->error = std::current_exception();
+            return -1;
+        }
+    }
+};
+
+template<std::floating_point T, class Op, class P, class Reduction>
 SolverResult<T> device_solve(owtk_solver_kind kind, Op& op, const BlockVector<T>& rhs, BlockVector<T>& x,
-                             const SolverOptions<T>& o, const P& pc, SolverWorkspace<T>* workspace)
+                             const SolverOptions<T>& o, P& pc, SolverWorkspace<T>* workspace,
+                             ArnoldiSnapshot<T>* snapshot = nullptr)
 {
-    static_assert(DeviceOperator<Op>, "solve through PolicyBlockOperator or DistributedBlockOperator");
     SolverResult<T> result;
     const auto t0 = std::chrono::steady_clock::now();
-    if (o.convergence_test)
-        throw std::invalid_argument("application convergence tests are not supported by the device solver");
-    const auto& m = op.matrix();
-    if (rhs.same_layout(x)
-        && (rhs.owned_nodes() != m.owned_nodes() || rhs.ghost_nodes() != m.ghost_nodes()
-            || rhs.block_size() != m.block_size()))
-        throw std::invalid_argument("BlockCsrMatrix vector layout mismatch");
     owtk_solver_options co;
     owtk_default_options(&co);
     co.relative_tolerance = static_cast<double>(o.relative_tolerance);
@@ -866,11 +1042,57 @@ SolverResult<T> device_solve(owtk_solver_kind kind, Op& op, const BlockVector<T>
     co.relaxation = static_cast<double>(o.relaxation);
     co.verify_true_residual = o.verify_true_residual ? 1 : 0;
     co.gmres_orthogonalization = static_cast<std::int32_t>(o.gmres_orthogonalization);
-    if (!rhs.same_layout(x)) return result;
+    if (!rhs.same_layout(x)) {
+        if (snapshot) snapshot->clear();
+        return result;
+    }
+    HostCallbacks<T> cb;
+    cb.owned = rhs.owned_nodes();
+    cb.ghost = rhs.ghost_nodes();
+    cb.bs = rhs.block_size();
+    auto* ctx = cuda::Runtime::instance().context();
+    owtk_matrix* mh = nullptr;
+    std::shared_ptr<owtk_matrix> temp_op;
+    if constexpr (DeviceOperator<Op>) {
+        const auto& m = op.matrix();
+        if (rhs.owned_nodes() != m.owned_nodes() || rhs.ghost_nodes() != m.ghost_nodes()
+            || rhs.block_size() != m.block_size())
+            throw std::invalid_argument("BlockCsrMatrix vector layout mismatch");
+        mh = m.device();
+    } else {
+        cb.op = [&op](BlockVector<T>& in, BlockVector<T>& out) { op.apply(in, out); };
+        owtk_matrix* p = nullptr;
+        cuda::check(owtk_callback_operator_create(ctx, cuda::dtype_of<T>(), cb.owned, cb.ghost, cb.bs,
+                                                  &HostCallbacks<T>::apply_op, &cb, &p));
+        temp_op = cuda::own(p, [](owtk_matrix* q) { owtk_matrix_destroy(q); });
+        mh = p;
+    }
+    owtk_preconditioner* ph = nullptr;
+    std::shared_ptr<owtk_preconditioner> temp_pc;
+    if constexpr (requires { pc.device(); }) {
+        ph = pc.device();
+    } else {
+        cb.pc = [&pc](BlockVector<T>& in, BlockVector<T>& out) { pc.apply(static_cast<const BlockVector<T>&>(in), out); };
+        owtk_preconditioner* p = nullptr;
+        cuda::check(owtk_pc_create_callback(ctx, cuda::dtype_of<T>(), cb.owned, cb.ghost, cb.bs,
+                                            &HostCallbacks<T>::apply_pc, &cb, &p));
+        temp_pc = cuda::own(p, [](owtk_preconditioner* q) { owtk_pc_destroy(q); });
+        ph = p;
+    }
+    owtk_solve_extras ex{};
+    ex.reduction = reduction_kind_of<Reduction>();
+    if (o.convergence_test) {
+        cb.test = &o.convergence_test;
+        ex.convergence_test = &HostCallbacks<T>::convergence;
+        ex.convergence_user = &cb;
+    }
+    if (snapshot) ex.arnoldi_snapshot = snapshot->device_for(cb.owned, cb.ghost, cb.bs);
     SolverWorkspace<T> local;
     SolverWorkspace<T>& ws = workspace ? *workspace : local;
     owtk_solver_result r{};
-    cuda::check(owtk_solve_host(kind, m.device(), pc_handle(pc), rhs.data(), x.data(), &co, ws.handle(), &r));
+    const owtk_status st = owtk_solve_host_ex(kind, mh, ph, rhs.data(), x.data(), &co, ws.handle(), &ex, &r);
+    if (cb.error) std::rethrow_exception(cb.error);
+    cuda::check(st);
     result.status = static_cast<SolverStatus>(r.status);
     result.breakdown_reason = static_cast<BreakdownReason>(r.breakdown_reason);
     result.iterations = r.iterations;
@@ -883,6 +1105,7 @@ SolverResult<T> device_solve(owtk_solver_kind kind, Op& op, const BlockVector<T>
     result.recursive_residual_norm = static_cast<T>(r.recursive_residual_norm);
     result.true_residual_norm = static_cast<T>(r.true_residual_norm);
     result.relative_residual_norm = static_cast<T>(r.relative_residual_norm);
+    result.converged_by_application = r.converged_by_application != 0;
     if (o.collect_timings) {
         result.timings = std::make_shared<SolverTimings<T>>();
         result.timings->solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -892,6 +1115,19 @@ SolverResult<T> device_solve(owtk_solver_kind kind, Op& op, const BlockVector<T>
 
 }  // namespace detail
 
+// fgmres / gmres (krylov_solvers.hpp:159-540): fgmres alone records an Arnoldi snapshot.
+template<std::floating_point T, class Operator, class Preconditioner = IdentityPreconditioner,
+         class Reduction = SerialReduction<T>>
+[[nodiscard]] SolverResult<T> fgmres(Operator& op, const BlockVector<T>& rhs, BlockVector<T>& solution,
+                                     const SolverOptions<T>& options = {},
+                                     Preconditioner&& preconditioner = Preconditioner{}, Reduction = {},
+                                     SolverWorkspace<T>* workspace = nullptr,
+                                     ArnoldiSnapshot<T>* arnoldi_snapshot = nullptr)
+{
+    return detail::device_solve<T, Operator, std::remove_reference_t<Preconditioner>, Reduction>(
+        OWTK_SOLVER_FGMRES, op, rhs, solution, options, preconditioner, workspace, arnoldi_snapshot);
+}
+
 #define OWTK_SOLVER(NAME, KIND)                                                                               \
     template<std::floating_point T, class Operator, class Preconditioner = IdentityPreconditioner,             \
              class Reduction = SerialReduction<T>>                                                             \
@@ -900,8 +1136,17 @@ SolverResult<T> device_solve(owtk_solver_kind kind, Op& op, const BlockVector<T>
                                        Preconditioner&& preconditioner = Preconditioner{}, Reduction = {},     \
                                        SolverWorkspace<T>* workspace = nullptr)                                \
     {                                                                                                          \
-        return detail::device_solve<T>(KIND, op, rhs, solution, options, preconditioner, workspace);           \
-    }                                                                                                          \
+        return detail::device_solve<T, Operator, std::remove_reference_t<Preconditioner>, Reduction>(         \
+            KIND, op, rhs, solution, options, preconditioner, workspace);                                      \
+    }
+
+OWTK_SOLVER(gmres, OWTK_SOLVER_FGMRES)
+OWTK_SOLVER(bicgstab, OWTK_SOLVER_BICGSTAB)
+OWTK_SOLVER(pipelined_bicgstab, OWTK_SOLVER_PIPELINED_BICGSTAB)
+OWTK_SOLVER(communication_hiding_bicgstab, OWTK_SOLVER_COMM_HIDING_BICGSTAB)
+#undef OWTK_SOLVER
+
+#define OWTK_SOLVER_WITH_WORKSPACE(NAME, KIND)                                                                \
     template<std::floating_point T, class Operator, class Preconditioner = IdentityPreconditioner,             \
              class Reduction = SerialReduction<T>>                                                             \
     [[nodiscard]] SolverResult<T> NAME##_with_workspace(Operator& op, const BlockVector<T>& rhs,               \
@@ -910,15 +1155,16 @@ SolverResult<T> device_solve(owtk_solver_kind kind, Op& op, const BlockVector<T>
                                                         Preconditioner&& preconditioner = Preconditioner{},    \
                                                         Reduction = {})                                        \
     {                                                                                                          \
-        return detail::device_solve<T>(KIND, op, rhs, solution, options, preconditioner, &workspace);          \
+        return detail::device_solve<T, Operator, std::remove_reference_t<Preconditioner>, Reduction>(         \
+            KIND, op, rhs, solution, options, preconditioner, &workspace);                                     \
     }
 
-OWTK_SOLVER(fgmres, OWTK_SOLVER_FGMRES)
-OWTK_SOLVER(gmres, OWTK_SOLVER_FGMRES)
-OWTK_SOLVER(bicgstab, OWTK_SOLVER_BICGSTAB)
-OWTK_SOLVER(pipelined_bicgstab, OWTK_SOLVER_PIPELINED_BICGSTAB)
-OWTK_SOLVER(communication_hiding_bicgstab, OWTK_SOLVER_COMM_HIDING_BICGSTAB)
-#undef OWTK_SOLVER
+OWTK_SOLVER_WITH_WORKSPACE(fgmres, OWTK_SOLVER_FGMRES)
+OWTK_SOLVER_WITH_WORKSPACE(gmres, OWTK_SOLVER_FGMRES)
+OWTK_SOLVER_WITH_WORKSPACE(bicgstab, OWTK_SOLVER_BICGSTAB)
+OWTK_SOLVER_WITH_WORKSPACE(pipelined_bicgstab, OWTK_SOLVER_PIPELINED_BICGSTAB)
+OWTK_SOLVER_WITH_WORKSPACE(communication_hiding_bicgstab, OWTK_SOLVER_COMM_HIDING_BICGSTAB)
+#undef OWTK_SOLVER_WITH_WORKSPACE
 
 // idrs has no workspace parameter (idrs.hpp:128-138).
 template<std::floating_point T, class Operator, class Preconditioner = IdentityPreconditioner,
@@ -927,8 +1173,99 @@ template<std::floating_point T, class Operator, class Preconditioner = IdentityP
                                    const SolverOptions<T>& options = {},
                                    Preconditioner&& preconditioner = Preconditioner{}, Reduction = {})
 {
-    return detail::device_solve<T>(OWTK_SOLVER_IDRS, op, rhs, solution, options, preconditioner,
-                                   static_cast<SolverWorkspace<T>*>(nullptr));
+    return detail::device_solve<T, Operator, std::remove_reference_t<Preconditioner>, Reduction>(
+        OWTK_SOLVER_IDRS, op, rhs, solution, options, preconditioner, static_cast<SolverWorkspace<T>*>(nullptr));
+}
+
+// The stability variants (krylov_solvers.hpp:766-809, pipelined_bicgstab.hpp:275-313, :620-661):
+// the same solvers with the reference's option and reduction choices.
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> bicgstab_stable(Operator& op, const BlockVector<T>& rhs, BlockVector<T>& solution,
+                                              SolverOptions<T> options, Preconditioner&& preconditioner)
+{
+    options.verify_true_residual = true;
+    return bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                    MixedPrecisionSerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner = IdentityPreconditioner,
+         class Reduction = SerialReduction<T>>
+[[nodiscard]] SolverResult<T> bicgstab_residual_replacement(Operator& op, const BlockVector<T>& rhs,
+                                                            BlockVector<T>& solution, SolverOptions<T> options,
+                                                            std::size_t replacement_interval,
+                                                            Preconditioner&& preconditioner = Preconditioner{},
+                                                            Reduction reduction = {})
+{
+    options.residual_replacement_interval = replacement_interval;
+    return bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner), std::move(reduction));
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> bicgstab_mixed_precision(Operator& op, const BlockVector<T>& rhs,
+                                                       BlockVector<T>& solution, SolverOptions<T> options,
+                                                       Preconditioner&& preconditioner)
+{
+    return bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                    MixedPrecisionSerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> pipelined_bicgstab_stable(Operator& op, const BlockVector<T>& rhs,
+                                                        BlockVector<T>& solution, SolverOptions<T> options,
+                                                        Preconditioner&& preconditioner)
+{
+    return pipelined_bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                              MixedPrecisionSerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> pipelined_bicgstab_residual_replacement(Operator& op, const BlockVector<T>& rhs,
+                                                                      BlockVector<T>& solution,
+                                                                      SolverOptions<T> options,
+                                                                      std::size_t replacement_interval,
+                                                                      Preconditioner&& preconditioner)
+{
+    options.residual_replacement_interval = replacement_interval;
+    return pipelined_bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                              SerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> pipelined_bicgstab_mixed_precision(Operator& op, const BlockVector<T>& rhs,
+                                                                 BlockVector<T>& solution, SolverOptions<T> options,
+                                                                 Preconditioner&& preconditioner)
+{
+    return pipelined_bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                              MixedPrecisionSerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> communication_hiding_bicgstab_stable(Operator& op, const BlockVector<T>& rhs,
+                                                                   BlockVector<T>& solution, SolverOptions<T> options,
+                                                                   Preconditioner&& preconditioner)
+{
+    return communication_hiding_bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                                         MixedPrecisionSerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> communication_hiding_bicgstab_residual_replacement(
+    Operator& op, const BlockVector<T>& rhs, BlockVector<T>& solution, SolverOptions<T> options,
+    std::size_t replacement_interval, Preconditioner&& preconditioner)
+{
+    options.residual_replacement_interval = replacement_interval;
+    return communication_hiding_bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                                         SerialReduction<T>{});
+}
+
+template<std::floating_point T, class Operator, class Preconditioner>
+[[nodiscard]] SolverResult<T> communication_hiding_bicgstab_mixed_precision(Operator& op, const BlockVector<T>& rhs,
+                                                                            BlockVector<T>& solution,
+                                                                            SolverOptions<T> options,
+                                                                            Preconditioner&& preconditioner)
+{
+    return communication_hiding_bicgstab(op, rhs, solution, options, std::forward<Preconditioner>(preconditioner),
+                                         MixedPrecisionSerialReduction<T>{});
 }
 
 // ------------------------------------------------------------------ SpecWave compatibility
@@ -943,11 +1280,10 @@ enum class SpecWaveSolver : int {
 };
 
 // solve_specwave_native (specwave_compat.hpp:99-249) with the device solvers:
-// the same ID -> solver / preconditioner selection.  IDs 10 and 22 choose the
-// mixed-precision and compensated serial reductions in the reference; device
-// reductions are two-stage FP64 for every ID.  The stationary and multigrid
-// IDs are not on the device path and throw std::invalid_argument; PETSc (6)
-// returns a default SolverResult as the reference does.
+// the same ID -> solver / preconditioner / reduction selection (ID 10 the
+// mixed-precision reduction, ID 22 the compensated one).  The stationary and
+// multigrid IDs are not on the device path and throw std::invalid_argument;
+// PETSc (6) returns a default SolverResult as the reference does.
 template<std::floating_point T, std::integral Index, class Operator, class Halo,
          class Reduction = SerialReduction<T>>
 [[nodiscard]] SolverResult<T> solve_specwave_native(SpecWaveSolver solver, const BlockCsrMatrix<T, Index>& matrix,
@@ -958,10 +1294,16 @@ template<std::floating_point T, std::integral Index, class Operator, class Halo,
     using S = SpecWaveSolver;
     switch (solver) {
     case S::pipelined_stable:
-    case S::pipelined_mixed_precision:
-    case S::async_pipe_stable:
         return communication_hiding_bicgstab(linear_operator, rhs, solution, options,
                                              LocalSsorPreconditioner<T, Index>(matrix, options.relaxation), reduction);
+    case S::pipelined_mixed_precision:
+        return communication_hiding_bicgstab(linear_operator, rhs, solution, options,
+                                             LocalSsorPreconditioner<T, Index>(matrix, options.relaxation),
+                                             MixedPrecisionSerialReduction<T>{});
+    case S::async_pipe_stable:
+        return communication_hiding_bicgstab(linear_operator, rhs, solution, options,
+                                             LocalSsorPreconditioner<T, Index>(matrix, options.relaxation),
+                                             CompensatedSerialReduction<T>{});
     case S::pipelined_residual_replacement:
         if (options.residual_replacement_interval == 0) options.residual_replacement_interval = 50;
         return communication_hiding_bicgstab(linear_operator, rhs, solution, options,
@@ -1024,11 +1366,61 @@ template<std::floating_point T, std::integral Index>
 }
 
 // ------------------------------------------------------------------ vector ops (core.hpp:562-601)
+// Owned entries only; the arithmetic runs on the device with the reference's
+// rounding (no contraction of a*b+c), ghosts are left untouched.
 template<std::floating_point T>
 inline void copy_owned(const BlockVector<T>& s, BlockVector<T>& d)
 {
     if (!s.same_layout(d)) throw std::invalid_argument("BlockVector layout mismatch");
     std::copy(s.owned().begin(), s.owned().end(), d.owned().begin());
+}
+
+namespace detail {
+// Upload x and y (owned parts), run `op` on the device pair, download y.
+template<std::floating_point T, class F>
+void device_pair(const BlockVector<T>& x, BlockVector<T>& y, F&& op)
+{
+    auto [dx, dy] = cuda::Runtime::instance().scratch(cuda::dtype_of<T>(), y.owned_nodes(), y.ghost_nodes(),
+                                                      y.block_size());
+    cuda::check(owtk_vector_upload(dx, x.data(), x.owned_size()));
+    cuda::check(owtk_vector_upload(dy, y.data(), y.owned_size()));
+    op(dx, dy);
+    cuda::check(owtk_context_synchronize(cuda::Runtime::instance().context()));
+    cuda::check(owtk_vector_download(dy, y.data(), y.owned_size()));
+}
+}  // namespace detail
+
+template<std::floating_point T>
+inline void axpy(T alpha, const BlockVector<T>& x, BlockVector<T>& y)
+{
+    if (!x.same_layout(y)) throw std::invalid_argument("BlockVector layout mismatch");
+    detail::device_pair(x, y, [&](owtk_vector* dx, owtk_vector* dy) {
+        cuda::check(owtk_axpy(static_cast<double>(alpha), dx, dy));
+    });
+}
+
+template<std::floating_point T>
+inline void scale(T alpha, BlockVector<T>& x)
+{
+    detail::device_pair(x, x, [&](owtk_vector*, owtk_vector* dy) {
+        cuda::check(owtk_scale(static_cast<double>(alpha), dy));
+    });
+}
+
+template<std::floating_point T>
+inline void assign_linear_combination(BlockVector<T>& out, T alpha, const BlockVector<T>& x, T beta,
+                                      const BlockVector<T>& y)
+{
+    if (!out.same_layout(x) || !out.same_layout(y)) throw std::invalid_argument("BlockVector layout mismatch");
+    auto [dx, dy] = cuda::Runtime::instance().scratch(cuda::dtype_of<T>(), x.owned_nodes(), x.ghost_nodes(),
+                                                      x.block_size());
+    cuda::check(owtk_vector_upload(dx, x.data(), x.owned_size()));
+    cuda::check(owtk_vector_upload(dy, y.data(), y.owned_size()));
+    // The result lands in dx: out = alpha x + beta y, elementwise from the
+    // inputs loaded before the store.
+    cuda::check(owtk_assign_linear_combination(dx, static_cast<double>(alpha), dx, static_cast<double>(beta), dy));
+    cuda::check(owtk_context_synchronize(cuda::Runtime::instance().context()));
+    cuda::check(owtk_vector_download(dx, out.data(), out.owned_size()));
 }
 
 }  // namespace owt::krylov

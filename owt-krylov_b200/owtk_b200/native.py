@@ -59,6 +59,16 @@ class SolverResult(ctypes.Structure):
         return d
 
 
+CONVERGENCE_TEST = ctypes.CFUNCTYPE(c_int, c_void_p, c_uint64, c_void_p, c_size_t)
+HOST_APPLY = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, c_void_p, c_size_t)
+REDUCTION = {"serial": 0, "compensated": 1, "mixed": 2}
+
+
+class SolveExtras(ctypes.Structure):
+    _fields_ = [("reduction", c_int32), ("reserved", c_int32), ("convergence_test", CONVERGENCE_TEST),
+                ("convergence_user", c_void_p), ("arnoldi_snapshot", c_void_p)]
+
+
 class BatchSystem(ctypes.Structure):
     _fields_ = [("owned", c_size_t), ("bs", c_size_t), ("rowptr", c_void_p), ("cols", c_void_p),
                 ("values", c_void_p)]
@@ -137,6 +147,22 @@ def lib():
             "owtk_batch_solve_host": (c_int, [vp, vp, vp, POINTER(SolverOptions), POINTER(SolverResult)]),
             "owtk_bf16_gemm_nt": (c_int, [vp, sz, sz, sz, vp, vp, vp]),
             "owtk_solve_specwave": (c_int, [c_int, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
+            "owtk_dot_ex": (c_int, [vp, vp, c_int, POINTER(c_double), POINTER(c_double)]),
+            "owtk_norm_ex": (c_int, [vp, c_int, POINTER(c_double)]),
+            "owtk_arnoldi_snapshot_create": (c_int, [vp, POINTER(vp)]),
+            "owtk_arnoldi_snapshot_destroy": (c_int, [vp]),
+            "owtk_arnoldi_snapshot_clear": (c_int, [vp]),
+            "owtk_arnoldi_snapshot_columns": (sz, [vp]),
+            "owtk_arnoldi_snapshot_h": (c_int, [vp, sz, sz, POINTER(c_double)]),
+            "owtk_arnoldi_snapshot_basis": (c_int, [vp, sz, POINTER(vp)]),
+            "owtk_solve_ex": (c_int, [c_int, vp, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolveExtras),
+                                      POINTER(SolverResult)]),
+            "owtk_solve_host_ex": (c_int, [c_int, vp, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolveExtras),
+                                           POINTER(SolverResult)]),
+            "owtk_solve_specwave_ex": (c_int, [c_int, vp, vp, vp, POINTER(SolverOptions), vp, c_int,
+                                               POINTER(SolverResult)]),
+            "owtk_callback_operator_create": (c_int, [vp, c_int, sz, sz, sz, HOST_APPLY, vp, POINTER(vp)]),
+            "owtk_pc_create_callback": (c_int, [vp, c_int, sz, sz, sz, HOST_APPLY, vp, POINTER(vp)]),
             "owtk_learned_create": (c_int, [vp, c_uint64, POINTER(vp)]),
             "owtk_learned_destroy": (c_int, [vp]),
             "owtk_learned_update_matrix": (c_int, [vp, vp]),
@@ -458,13 +484,161 @@ def solve(kind: int, matrix: Matrix, pc: Preconditioner | None, rhs: Vector, x: 
 
 
 def solve_specwave(solver_id: int, matrix: Matrix, rhs: Vector, x: Vector, options: SolverOptions | None = None,
-                   workspace: Workspace | None = None) -> SolverResult:
-    """solve_specwave_native: a legacy SpecWave solver id (owtk_solve_specwave)."""
+                   workspace: Workspace | None = None, reduction: str = "serial") -> SolverResult:
+    """solve_specwave_native: a legacy SpecWave solver id (owtk_solve_specwave_ex)."""
     o = options or default_options()
     r = SolverResult()
-    check(lib().owtk_solve_specwave(solver_id, matrix.h, rhs.h, x.h, ctypes.byref(o),
-                                    workspace.h if workspace else None, ctypes.byref(r)))
+    check(lib().owtk_solve_specwave_ex(solver_id, matrix.h, rhs.h, x.h, ctypes.byref(o),
+                                       workspace.h if workspace else None, REDUCTION[reduction], ctypes.byref(r)))
     return r
+
+
+class ArnoldiSnapshot:
+    """owtk_arnoldi_snapshot_*: the last unrotated Arnoldi relation of FGMRES."""
+
+    def __init__(self, ctx: Context):
+        h = c_void_p()
+        check(lib().owtk_arnoldi_snapshot_create(ctx.h, ctypes.byref(h)))
+        self.h, self.ctx = h, ctx
+
+    @property
+    def columns(self) -> int:
+        return int(lib().owtk_arnoldi_snapshot_columns(self.h))
+
+    def h_entry(self, row: int, column: int) -> float:
+        v = c_double()
+        check(lib().owtk_arnoldi_snapshot_h(self.h, row, column, ctypes.byref(v)))
+        return v.value
+
+    def basis(self, column: int, owned: int, ghost: int, bs: int, dtype=np.float64) -> np.ndarray:
+        v = c_void_p()
+        check(lib().owtk_arnoldi_snapshot_basis(self.h, column, ctypes.byref(v)))
+        out = np.empty((owned + ghost) * bs, dtype=dtype)
+        check(lib().owtk_vector_download(v, _ptr(out), out.size))
+        return out
+
+    def clear(self):
+        check(lib().owtk_arnoldi_snapshot_clear(self.h))
+
+    def __del__(self):
+        try:
+            if self.h is not None:
+                lib().owtk_arnoldi_snapshot_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def solve_ex(kind: int, matrix, pc, rhs: Vector, x: Vector, options: SolverOptions | None = None,
+             workspace: Workspace | None = None, reduction: str = "serial", convergence_test=None,
+             snapshot: ArnoldiSnapshot | None = None) -> SolverResult:
+    """owtk_solve_ex.  convergence_test(iteration, candidate ndarray) -> bool."""
+    o = options or default_options()
+    r = SolverResult()
+    ex = SolveExtras()
+    ex.reduction = REDUCTION[reduction]
+    errors = []
+    if convergence_test is not None:
+        dtype = rhs.dtype
+
+        def _test(_user, iteration, candidate, count):
+            try:
+                arr = np.ctypeslib.as_array(ctypes.cast(candidate, POINTER(ctypes.c_double if dtype == np.float64
+                                                                             else ctypes.c_float)), (count,))
+                return 1 if convergence_test(int(iteration), arr.copy()) else 0
+            except Exception as exc:   # kept and re-raised after the call
+                errors.append(exc)
+                return -1
+
+        cb = CONVERGENCE_TEST(_test)
+        ex.convergence_test = cb
+    ex.arnoldi_snapshot = snapshot.h if snapshot is not None else None
+    code = lib().owtk_solve_ex(kind, matrix.h, pc.h if pc else None, rhs.h, x.h, ctypes.byref(o),
+                               workspace.h if workspace else None, ctypes.byref(ex), ctypes.byref(r))
+    if errors:
+        raise errors[0]
+    check(code)
+    return r
+
+
+def dot_ex(a: Vector, b: Vector, reduction: str = "serial"):
+    """(result, low) of owtk_dot_ex."""
+    hi, lo = c_double(), c_double()
+    check(lib().owtk_dot_ex(a.h, b.h, REDUCTION[reduction], ctypes.byref(hi), ctypes.byref(lo)))
+    return hi.value, lo.value
+
+
+def norm_ex(a: Vector, reduction: str = "serial") -> float:
+    r = c_double()
+    check(lib().owtk_norm_ex(a.h, REDUCTION[reduction], ctypes.byref(r)))
+    return r.value
+
+
+class _HostApply:
+    """A Python function fn(in ndarray, out ndarray) behind HOST_APPLY."""
+
+    def __init__(self, fn, dtype):
+        self.fn, self.errors = fn, []
+        ct = ctypes.c_double if np.dtype(dtype) == np.float64 else ctypes.c_float
+
+        def _call(_user, pin, pout, count):
+            try:
+                vin = np.ctypeslib.as_array(ctypes.cast(pin, POINTER(ct)), (count,))
+                vout = np.ctypeslib.as_array(ctypes.cast(pout, POINTER(ct)), (count,))
+                fn(vin, vout)
+                return 0
+            except Exception as exc:
+                self.errors.append(exc)
+                return 1
+
+        self.cb = HOST_APPLY(_call)
+
+
+class CallbackOperator:
+    """owtk_callback_operator_create: an application operator fn(in, out) on
+    host arrays ((owned + ghost) * bs values), usable wherever a Matrix is."""
+
+    def __init__(self, ctx: Context, owned: int, ghost: int, bs: int, fn, dtype=np.float64):
+        self.ctx, self.owned, self.ghost, self.bs, self.dtype = ctx, owned, ghost, bs, np.dtype(dtype)
+        self._apply = _HostApply(fn, dtype)
+        h = c_void_p()
+        check(lib().owtk_callback_operator_create(ctx.h, _dtype_code(dtype), owned, ghost, bs, self._apply.cb, None,
+                                                  ctypes.byref(h)))
+        self.h = h
+
+    def apply(self, x: Vector, y: Vector):
+        check(lib().owtk_spmv(self.h, x.h, y.h))
+
+    def __del__(self):
+        try:
+            if self.h is not None:
+                lib().owtk_matrix_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class CallbackPreconditioner:
+    """owtk_pc_create_callback: an application preconditioner fn(in, out)."""
+
+    def __init__(self, ctx: Context, owned: int, ghost: int, bs: int, fn, dtype=np.float64):
+        self._apply = _HostApply(fn, dtype)
+        h = c_void_p()
+        check(lib().owtk_pc_create_callback(ctx.h, _dtype_code(dtype), owned, ghost, bs, self._apply.cb, None,
+                                            ctypes.byref(h)))
+        self.h = h
+        self.kind = 8
+
+    def apply(self, x: Vector, y: Vector):
+        check(lib().owtk_pc_apply(self.h, x.h, y.h))
+
+    def __del__(self):
+        try:
+            if self.h is not None:
+                lib().owtk_pc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
 
 
 def solve_host(kind: int, matrix: Matrix, pc: Preconditioner | None, rhs_ptr: int, x_ptr: int,

@@ -121,6 +121,116 @@ int main(int argc, char** argv)
         results << "specwave_multigrid invalid_argument\n";
     }
 
+    // The stability variants (krylov_solvers.hpp:766-809,
+    // pipelined_bicgstab.hpp:275-313, :620-661).
+    auto variant = [&](const std::string& name, auto&& solve) {
+        BlockVector<double> xv = rhs.clone_layout();
+        const auto r = solve(xv);
+        report(results, name.c_str(), r);
+        write(dir + "/x_" + name + ".f64", std::vector<double>(xv.owned().begin(), xv.owned().end()));
+    };
+    variant("bicgstab_stable", [&](auto& xv) { return bicgstab_stable(op, rhs, xv, options, ilu); });
+    variant("bicgstab_residual_replacement",
+            [&](auto& xv) { return bicgstab_residual_replacement(op, rhs, xv, options, 7, ilu); });
+    variant("bicgstab_mixed_precision", [&](auto& xv) { return bicgstab_mixed_precision(op, rhs, xv, options, ilu); });
+    variant("pipelined_bicgstab_stable", [&](auto& xv) { return pipelined_bicgstab_stable(op, rhs, xv, options, ilu); });
+    variant("pipelined_bicgstab_residual_replacement",
+            [&](auto& xv) { return pipelined_bicgstab_residual_replacement(op, rhs, xv, options, 7, ilu); });
+    variant("pipelined_bicgstab_mixed_precision",
+            [&](auto& xv) { return pipelined_bicgstab_mixed_precision(op, rhs, xv, options, ilu); });
+    variant("communication_hiding_bicgstab_stable",
+            [&](auto& xv) { return communication_hiding_bicgstab_stable(op, rhs, xv, options, ilu); });
+    variant("communication_hiding_bicgstab_residual_replacement",
+            [&](auto& xv) { return communication_hiding_bicgstab_residual_replacement(op, rhs, xv, options, 7, ilu); });
+    variant("communication_hiding_bicgstab_mixed_precision",
+            [&](auto& xv) { return communication_hiding_bicgstab_mixed_precision(op, rhs, xv, options, ilu); });
+
+    // FGMRES recording its last Arnoldi relation (restart 6: several cycles).
+    ArnoldiSnapshot<double> snapshot;
+    SolverOptions<double> small = options;
+    small.restart = 6;
+    BlockVector<double> x6 = rhs.clone_layout();
+    const auto r6 = fgmres(op, rhs, x6, small, ilu, SerialReduction<double>{}, static_cast<SolverWorkspace<double>*>(nullptr), &snapshot);
+    report(results, "fgmres_snapshot", r6);
+    results << "snapshot_columns " << snapshot.columns() << '\n';
+    {
+        std::vector<double> h, z;
+        for (std::size_t c = 0; c < snapshot.columns(); ++c) {
+            for (std::size_t row = 0; row <= c + 1; ++row) h.push_back(snapshot.h(row, c));
+            const auto& v = snapshot.preconditioned_basis(c);
+            z.insert(z.end(), v.owned().begin(), v.owned().end());
+        }
+        write(dir + "/snapshot_h.f64", h);
+        write(dir + "/snapshot_basis.f64", z);
+        try {
+            (void)snapshot.h(0, snapshot.columns());
+            results << "snapshot_range none\n";
+        } catch (const std::out_of_range&) {
+            results << "snapshot_range out_of_range\n";
+        }
+    }
+
+    // An application convergence test that stops at iteration 5.
+    SolverOptions<double> app = options;
+    std::size_t calls = 0;
+    app.convergence_test = [&calls](std::size_t iteration, const BlockVector<double>&) {
+        ++calls;
+        return iteration >= 5;
+    };
+    BlockVector<double> x7 = rhs.clone_layout();
+    const auto r7 = bicgstab(op, rhs, x7, app, ilu);
+    report(results, "bicgstab_application_test", r7);
+    results << "application " << (r7.converged_by_application ? 1 : 0) << ' ' << calls << '\n';
+
+    // A matrix-free operator and a host preconditioner of the application's
+    // own types (any type with apply), as the reference's templates accept.
+    struct HostSpmv {
+        const BlockCsrMatrix<double>* A;
+        void apply(BlockVector<double>& in, BlockVector<double>& out) const
+        {
+            const std::size_t b = A->block_size();
+            for (std::size_t r = 0; r < A->owned_nodes(); ++r)
+                for (std::size_t c = 0; c < b; ++c) {
+                    double sum = 0;
+                    for (std::size_t e = A->row_offsets()[r]; e < A->row_offsets()[r + 1]; ++e)
+                        sum += A->values()[e * b + c] * in.data()[A->column_indices()[e] * b + c];
+                    out.data()[r * b + c] = sum;
+                }
+        }
+    };
+    struct HostJacobi {
+        std::vector<double> inverse;
+        void apply(const BlockVector<double>& in, BlockVector<double>& out) const
+        {
+            for (std::size_t i = 0; i < inverse.size(); ++i) out.data()[i] = inverse[i] * in.data()[i];
+        }
+    };
+    HostJacobi host_jacobi;
+    for (double d : A.diagonal()) host_jacobi.inverse.push_back(1.0 / d);
+    HostSpmv host_op{&A};
+    BlockVector<double> x8 = rhs.clone_layout();
+    const auto r8 = bicgstab(host_op, rhs, x8, bench, host_jacobi);
+    report(results, "bicgstab_matrix_free", r8);
+    write(dir + "/x_matrix_free.f64", std::vector<double>(x8.owned().begin(), x8.owned().end()));
+
+    // Owned-only vector operations (core.hpp:562-601).
+    BlockVector<double> u = rhs.clone_layout();
+    for (std::size_t i = 0; i < u.owned_size(); ++i) u.data()[i] = 0.25 * static_cast<double>(i % 17) - 1.5;
+    axpy(0.37, rhs, u);
+    scale(-1.7, u);
+    BlockVector<double> w = rhs.clone_layout();
+    assign_linear_combination(w, 0.5, rhs, -1.25, u);
+    write(dir + "/blas_u.f64", std::vector<double>(u.owned().begin(), u.owned().end()));
+    write(dir + "/blas_w.f64", std::vector<double>(w.owned().begin(), w.owned().end()));
+
+    // The three reductions on the same pair.
+    results << std::hexfloat;
+    results << "dot_serial " << SerialReduction<double>{}.dot(rhs, u) << '\n';
+    results << "dot_compensated " << CompensatedSerialReduction<double>{}.dot(rhs, u) << '\n';
+    results << "dot_mixed " << MixedPrecisionSerialReduction<double>{}.dot(rhs, u) << '\n';
+    results << "norm_mixed " << MixedPrecisionSerialReduction<double>{}.norm(u) << '\n';
+    results << std::defaultfloat;
+
     const auto order = reverse_cuthill_mckee_order(A);
     write(dir + "/rcm.u64", order);
     results << "epochs " << workspace.allocation_epochs() << '\n';
