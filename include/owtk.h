@@ -354,6 +354,43 @@ owtk_status owtk_pc_create_callback(owtk_context* ctx, owtk_dtype dtype, size_t 
                                     size_t block_size, owtk_host_apply_fn apply, void* user,
                                     owtk_preconditioner** out);
 
+/* ---- permutations and device ingestion of a split layout -------------------
+ * The orderings above give new_to_old; these apply one on the device.  No
+ * reference counterpart (the reference orders but never permutes; its
+ * inverse_permutation, ordering.hpp:263-277, defines the validation). */
+typedef struct owtk_permutation owtk_permutation;
+/* new_to_old[i] = old index of new node i; every index in [0, n) once. */
+owtk_status owtk_permutation_create(owtk_context* ctx, size_t n, const uint64_t* new_to_old, owtk_permutation** out);
+owtk_status owtk_permutation_destroy(owtk_permutation* p);
+/* Owned nodes of dst from src (same layout, n owned nodes, dst != src):
+ * inverse 0: dst.node(i) = src.node(new_to_old[i]); inverse 1:
+ * dst.node(new_to_old[i]) = src.node(i).  Ghost entries are untouched. */
+owtk_status owtk_vector_permute(owtk_permutation* p, owtk_vector* src, owtk_vector* dst, int inverse);
+/* P A P^T as a component-diagonal BSR matrix, built from an application's
+ * split layout (SplitBlockCsrMatrixView, split_block_csr.hpp:17-28): the
+ * diagonal[node][c] and off_diagonal[edge][c] arrays in DEVICE memory, the
+ * edge structure (off-diagonal row offsets and columns, n owned nodes, no
+ * ghosts) on the host.  Row i of the result is old row new_to_old[i] with
+ * its diagonal and edges relabelled and sorted by new column; the values are
+ * gathered on the device.  owtk_bsr_update_permuted_split re-gathers them
+ * from the same-shaped arrays (a numeric update with no host copy). */
+owtk_status owtk_bsr_create_permuted_split(owtk_permutation* p, owtk_dtype dtype, size_t bs,
+                                           const uint64_t* off_rowptr, const uint64_t* off_cols,
+                                           const void* device_diagonal, const void* device_off_diagonal,
+                                           owtk_matrix** out);
+owtk_status owtk_bsr_update_permuted_split(owtk_matrix* m, const void* device_diagonal,
+                                           const void* device_off_diagonal);
+
+/* ---- bounded device waits (no reference counterpart) ----------------------
+ * Every device-side wait of this library (sweep dependencies, the batched
+ * solver's grid barrier, pipeline stages) gives up after a bounded number of
+ * polls, sets a status bit and lets its launch end; the call then returns
+ * OWTK_ERR_TIMEOUT and the context stays usable.  This hook runs a two-row
+ * ILU forward sweep whose only dependency is never published, with the given
+ * poll limit (1 .. 2^22), so the timeout path can be exercised without any
+ * fault: it returns OWTK_ERR_TIMEOUT. */
+owtk_status owtk_debug_unpublished_dependency(owtk_context* ctx, uint32_t spin_limit);
+
 /* ---- allocation-free variant (no counterpart in the reference) ----------
  * The batched dot product of owtk_dot_batch for callers that cannot allocate
  * device memory (a host framework that owns the device allocator, code where
@@ -366,7 +403,9 @@ owtk_status owtk_pc_create_callback(owtk_context* ctx, owtk_dtype dtype, size_t 
  * k <= 31 (larger batches return OWTK_ERR_INVALID_ARGUMENT); calls that
  * overlap on the GPU race on that array and must be serialised; and the
  * first call on a device looks up the array's address with that device
- * current, so make it before any stream capture. */
+ * current, so make it before any stream capture.  The address is kept for the
+ * life of the process: do not call it again on a device after
+ * cudaDeviceReset, which invalidates that address. */
 owtk_status owtk_dot_batch_f64_noalloc(const double* w, const double* const* basis, size_t k,
                                        size_t n, double* results, void* stream);
 

@@ -495,6 +495,12 @@ class Reference:
         self.check(self.L.ref_rcm(owned, ghost, _p(rp), _p(ci), _p(out)))
         return out.astype(np.int64)
 
+    def inverse_permutation(self, new_to_old):
+        p = _u64(new_to_old)
+        out = np.zeros(p.size, np.uint64)
+        self.check(self.L.ref_inverse_permutation(p.size, _p(p), _p(out)))
+        return out.astype(np.int64)
+
     def hilbert(self, xy):
         xy = np.ascontiguousarray(xy, np.float64)
         out = np.zeros(xy.shape[0], np.uint64)

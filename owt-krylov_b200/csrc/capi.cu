@@ -1290,6 +1290,142 @@ owtk_status owtk_workspace_destroy(owtk_workspace* ws)
 
 uint64_t owtk_workspace_allocation_epochs(owtk_workspace* ws) { return ws ? ws->epochs : 0; }
 
+// ------------------------------------------------------------ permutations
+owtk_status owtk_permutation_create(owtk_context* ctx, size_t n, const uint64_t* new_to_old, owtk_permutation** out)
+{
+    return guarded([&] {
+        require(ctx != nullptr && out != nullptr && new_to_old != nullptr && n > 0, "null handle or empty permutation");
+        auto p = std::make_unique<owtk_permutation>();
+        p->ctx = ctx;
+        p->n = n;
+        p->new_to_old.resize(n);
+        p->old_to_new.assign(n, -1);
+        // ordering.hpp:263-277: every index exactly once.
+        for (std::size_t i = 0; i < n; ++i) {
+            if (new_to_old[i] >= n || p->old_to_new[new_to_old[i]] != -1)
+                fail(OWTK_ERR_INVALID_ARGUMENT, "invalid permutation");
+            p->new_to_old[i] = static_cast<std::int64_t>(new_to_old[i]);
+            p->old_to_new[new_to_old[i]] = static_cast<std::int64_t>(i);
+        }
+        p->d_new_to_old = upload(ctx->stream, p->new_to_old);
+        ctx->sync();
+        *out = p.release();
+    });
+}
+
+owtk_status owtk_permutation_destroy(owtk_permutation* p)
+{
+    return guarded([&] { delete p; });
+}
+
+owtk_status owtk_vector_permute(owtk_permutation* p, owtk_vector* src, owtk_vector* dst, int inverse)
+{
+    return guarded([&] {
+        require(p != nullptr && src != nullptr && dst != nullptr, "null handle");
+        same_layout_or_throw(src, dst);
+        if (src->owned != p->n) fail(OWTK_ERR_INVALID_ARGUMENT, "permutation size differs from owned nodes");
+        if (src->data == dst->data) fail(OWTK_ERR_INVALID_ARGUMENT, "source and destination must differ");
+        Context& c = *src->ctx;
+        if (src->dtype == OWTK_F64)
+            kern::permute_nodes<double>(c, p->n, src->bs, p->d_new_to_old.as<std::int64_t>(),
+                                        static_cast<const double*>(src->data), static_cast<double*>(dst->data), inverse != 0);
+        else
+            kern::permute_nodes<float>(c, p->n, src->bs, p->d_new_to_old.as<std::int64_t>(),
+                                       static_cast<const float*>(src->data), static_cast<float*>(dst->data), inverse != 0);
+        c.sync();
+    });
+}
+
+owtk_status owtk_bsr_create_permuted_split(owtk_permutation* p, owtk_dtype dtype, size_t bs,
+                                           const uint64_t* off_rowptr, const uint64_t* off_cols,
+                                           const void* device_diagonal, const void* device_off_diagonal,
+                                           owtk_matrix** out)
+{
+    return guarded([&] {
+        require(p != nullptr && out != nullptr && off_rowptr != nullptr && device_diagonal != nullptr, "null handle");
+        if (dtype != OWTK_F64 && dtype != OWTK_F32) fail(OWTK_ERR_INVALID_ARGUMENT, "dtype must be F64 or F32");
+        if (bs == 0) fail(OWTK_ERR_INVALID_ARGUMENT, "invalid split CSR storage");
+        const std::size_t n = p->n;
+        const std::uint64_t edges = off_rowptr[n];
+        if (off_rowptr[0] != 0 || (edges > 0 && (off_cols == nullptr || device_off_diagonal == nullptr)))
+            fail(OWTK_ERR_INVALID_ARGUMENT, "invalid split CSR storage");
+        // New row i is old row new_to_old[i]: its diagonal plus its edges with
+        // relabelled columns, sorted by new column.
+        std::vector<std::uint64_t> rowptr(n + 1, 0), cols;
+        std::vector<std::int64_t> map;
+        cols.reserve(n + edges);
+        map.reserve(n + edges);
+        std::vector<std::pair<std::uint64_t, std::int64_t>> row;
+        for (std::size_t i = 0; i < n; ++i) {
+            const std::size_t o = static_cast<std::size_t>(p->new_to_old[i]);
+            if (off_rowptr[o] > off_rowptr[o + 1]) fail(OWTK_ERR_INVALID_ARGUMENT, "nonmonotone split CSR offsets");
+            row.clear();
+            row.emplace_back(i, static_cast<std::int64_t>(o));
+            for (std::uint64_t k = off_rowptr[o]; k < off_rowptr[o + 1]; ++k) {
+                if (off_cols[k] >= n) fail(OWTK_ERR_INVALID_ARGUMENT, "split CSR column outside owned nodes");
+                if (off_cols[k] == o) fail(OWTK_ERR_INVALID_ARGUMENT, "split CSR edge on the diagonal");
+                row.emplace_back(static_cast<std::uint64_t>(p->old_to_new[off_cols[k]]),
+                                 static_cast<std::int64_t>(n + k));
+            }
+            std::sort(row.begin(), row.end());
+            for (const auto& [col, src] : row) {
+                cols.push_back(col);
+                map.push_back(src);
+            }
+            rowptr[i + 1] = cols.size();
+        }
+        auto m = std::make_unique<owtk_matrix>();
+        m->ctx = p->ctx;
+        m->kind = 0;
+        m->dtype = dtype;
+        ingest_structure(*m, n, 0, bs, rowptr.data(), cols.data(), "invalid split CSR storage");
+        m->values.allocate(m->entries * bs * dsize(dtype) + 16);
+        m->split_map = upload(p->ctx->stream, map);
+        m->split_edges = edges;
+        Context& c = *p->ctx;
+        if (dtype == OWTK_F64)
+            kern::gather_split<double>(c, m->entries, bs, n, m->split_map.as<std::int64_t>(),
+                                       static_cast<const double*>(device_diagonal),
+                                       static_cast<const double*>(device_off_diagonal), m->values.as<double>());
+        else
+            kern::gather_split<float>(c, m->entries, bs, n, m->split_map.as<std::int64_t>(),
+                                      static_cast<const float*>(device_diagonal),
+                                      static_cast<const float*>(device_off_diagonal), m->values.as<float>());
+        c.sync();
+        *out = m.release();
+    });
+}
+
+owtk_status owtk_bsr_update_permuted_split(owtk_matrix* m, const void* device_diagonal, const void* device_off_diagonal)
+{
+    return guarded([&] {
+        require(m != nullptr && device_diagonal != nullptr, "null handle");
+        if (m->split_map.ptr == nullptr)
+            fail(OWTK_ERR_INVALID_ARGUMENT, "matrix was not built by owtk_bsr_create_permuted_split");
+        if (m->split_edges > 0 && device_off_diagonal == nullptr) fail(OWTK_ERR_INVALID_ARGUMENT, "null off-diagonal");
+        Context& c = *m->ctx;
+        if (m->dtype == OWTK_F64)
+            kern::gather_split<double>(c, m->entries, m->bs, m->owned, m->split_map.as<std::int64_t>(),
+                                       static_cast<const double*>(device_diagonal),
+                                       static_cast<const double*>(device_off_diagonal), m->values.as<double>());
+        else
+            kern::gather_split<float>(c, m->entries, m->bs, m->owned, m->split_map.as<std::int64_t>(),
+                                      static_cast<const float*>(device_diagonal),
+                                      static_cast<const float*>(device_off_diagonal), m->values.as<float>());
+        c.sync();
+    });
+}
+
+// ------------------------------------------------------------ bounded waits
+owtk_status owtk_debug_unpublished_dependency(owtk_context* ctx, uint32_t spin_limit)
+{
+    return guarded([&] {
+        require(ctx != nullptr && spin_limit > 0 && spin_limit <= (1u << 22), "spin limit out of range");
+        kern::debug_unpublished_dependency(*ctx, static_cast<int>(spin_limit));
+        ctx->check_device_status();
+    });
+}
+
 // ------------------------------------------------------------ extras
 owtk_status owtk_dot_ex(owtk_vector* a, owtk_vector* b, owtk_reduction_kind reduction, double* result, double* low)
 {

@@ -10,7 +10,9 @@
 // Results are deterministic run to run and land both in device memory (for
 // kernels that consume them) and in mapped pinned memory (for the host).
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 
 #include <cuda_bf16.h>
 
@@ -677,6 +679,41 @@ __global__ void __launch_bounds__(kThreads) k_norm(std::size_t n, const T* __res
     }
 }
 
+// ---------------------------------------------------------- permutations
+// Node permutation of a vector (owned nodes, bs values each): forward
+// dst[new] = src[new_to_old[new]], inverse dst[new_to_old[new]] = src[new].
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_permute_nodes(std::size_t n, int bs, const std::int64_t* __restrict__ n2o,
+                                                            const T* __restrict__ src, T* __restrict__ dst,
+                                                            int inverse)
+{
+    const std::size_t total = n * static_cast<std::size_t>(bs);
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < total;
+         i += static_cast<std::size_t>(gridDim.x) * kThreads) {
+        const std::size_t node = i / bs, c = i - node * bs;
+        const std::size_t old = static_cast<std::size_t>(n2o[node]);
+        if (inverse) dst[old * bs + c] = src[i];
+        else dst[i] = src[old * bs + c];
+    }
+}
+
+// Values of a permuted matrix gathered from a split layout: entry e takes
+// node s = map[e] of the diagonal when s < n, else off-diagonal edge s - n.
+template<class T>
+__global__ void __launch_bounds__(kThreads) k_gather_split(std::size_t entries, int bs, std::int64_t n,
+                                                           const std::int64_t* __restrict__ map,
+                                                           const T* __restrict__ diag, const T* __restrict__ off,
+                                                           T* __restrict__ values)
+{
+    const std::size_t total = entries * static_cast<std::size_t>(bs);
+    for (std::size_t i = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i < total;
+         i += static_cast<std::size_t>(gridDim.x) * kThreads) {
+        const std::size_t e = i / bs, c = i - e * bs;
+        const std::int64_t s = map[e];
+        values[i] = s < n ? diag[static_cast<std::size_t>(s) * bs + c] : off[static_cast<std::size_t>(s - n) * bs + c];
+    }
+}
+
 // ---------------------------------------------------------- accurate reductions
 // The reference's CompensatedSerialReduction sums the rounded products with
 // Neumaier's compensated summation, and MixedPrecisionSerialReduction sums in
@@ -1220,6 +1257,31 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
     c.launched();
 }
 
+template<class T> void permute_nodes(Context& c, std::size_t n, std::size_t bs, const std::int64_t* n2o, const T* src,
+                                     T* dst, bool inverse)
+{
+    const std::size_t total = n * bs;
+    if (total == 0) return;
+    const unsigned blocks = static_cast<unsigned>(std::min<std::size_t>((total + kThreads - 1) / kThreads,
+                                                                       static_cast<std::size_t>(c.sm_count) * 16));
+    k_permute_nodes<T><<<blocks, kThreads, 0, c.stream>>>(n, static_cast<int>(bs), n2o, src, dst, inverse ? 1 : 0);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
+template<class T> void gather_split(Context& c, std::size_t entries, std::size_t bs, std::size_t n, const std::int64_t* map,
+                                    const T* diag, const T* off, T* values)
+{
+    const std::size_t total = entries * bs;
+    if (total == 0) return;
+    const unsigned blocks = static_cast<unsigned>(std::min<std::size_t>((total + kThreads - 1) / kThreads,
+                                                                       static_cast<std::size_t>(c.sm_count) * 16));
+    k_gather_split<T><<<blocks, kThreads, 0, c.stream>>>(entries, static_cast<int>(bs), static_cast<std::int64_t>(n),
+                                                         map, diag, off, values);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
 template<class T> void multidot_accurate(Context& c, std::size_t n, int k, int mode, const T* const* a,
                                          const T* const* b, double* out_dev, double* out_host, double* out_lo)
 {
@@ -1308,7 +1370,10 @@ template void convert<__nv_bfloat16, double>(Context&, std::size_t, const double
     template void norm<T>(Context&, std::size_t, const T*, double*, double*);                       \
     template void multidot_accurate<T>(Context&, std::size_t, int, int, const T* const*, const T* const*,  \
                                        double*, double*, double*);                                 \
-    template void norm_accurate<T>(Context&, std::size_t, const T*, double*, double*, double*);
+    template void norm_accurate<T>(Context&, std::size_t, const T*, double*, double*, double*);      \
+    template void permute_nodes<T>(Context&, std::size_t, std::size_t, const std::int64_t*, const T*, T*, bool); \
+    template void gather_split<T>(Context&, std::size_t, std::size_t, std::size_t, const std::int64_t*, const T*, \
+                                  const T*, T*);
 
 INSTANTIATE(double)
 INSTANTIATE(float)

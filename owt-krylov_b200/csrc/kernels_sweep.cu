@@ -83,6 +83,7 @@ struct SweepArgs {
     const int* upd_start;   // factorisation update lists
     const int* upd_target;
     const int* upd_upper;
+    int spin_limit;         // polls before an apply's dependency wait gives up (0: kSpinLimit)
 };
 
 constexpr int kChunk = 8;   // dependency entries handled per unrolled step
@@ -230,7 +231,7 @@ __device__ __forceinline__ T eliminate(T y, const SweepArgs<T, F>& a, const T* d
 #pragma unroll
                 for (int j = 0; j < kChunk; ++j) pending |= on[j] && xb[j] == Bits<T>::kSentinel;
                 if (!pending) break;
-                if (it >= kSpinLimit) {
+                if (it >= a.spin_limit) {
                     atomicOr(a.status, kErrTimeout);
                     break;
                 }
@@ -299,7 +300,7 @@ __device__ __forceinline__ void eliminate_publish(bool valid, T y, const SweepAr
 #pragma unroll
                 for (int j = 0; j < kChunk; ++j) pending |= on[j] && xb[j] == Bits<T>::kSentinel;
                 if (pending) {
-                    if (it >= kSpinLimit) {
+                    if (it >= a.spin_limit) {
                         atomicOr(a.status, kErrTimeout);
                         pending = false;
                     } else if ((it & 1023) == 1023
@@ -406,7 +407,7 @@ __device__ __forceinline__ T block_eliminate(T acc, const SweepArgs<T, F>& a, co
                 for (int j = 0; j < kMaxBlock; ++j)
                     pending |= on[q] && j < bs && xb[q][j] == Bits<T>::kSentinel;
             if (!pending) break;
-            if (it >= kSpinLimit) {
+            if (it >= a.spin_limit) {
                 atomicOr(a.status, kErrTimeout);
                 break;
             }
@@ -504,7 +505,7 @@ __device__ __forceinline__ void block_apply_lane(const SweepArgs<T, F>& a, int r
                     for (int j = 0; j < kMaxBlock; ++j)
                         pending |= on[q] && j < bs && xb[q][j] == Bits<T>::kSentinel;
                 if (pending) {
-                    if (it >= kSpinLimit) {
+                    if (it >= a.spin_limit) {
                         atomicOr(a.status, kErrTimeout);
                         pending = false;
                     } else if ((it & 1023) == 1023
@@ -795,6 +796,7 @@ void launch(Context& c, Preconditioner& p, Sweep& s, SweepArgs<T, F>& a)
     a.status = c.status.as<unsigned>();
     a.owned = static_cast<int>(p.owned);
     a.bs = static_cast<int>(p.bs);
+    if (a.spin_limit <= 0) a.spin_limit = kSpinLimit;
     bool lane = false;
     if constexpr (is_lane_apply(MODE)) {
         if (p.bs <= 32) {
@@ -944,6 +946,43 @@ template void ilu_apply_lp<float>(Context&, Preconditioner&, const float*, float
 template void ilu_apply_lp<__nv_bfloat16>(Context&, Preconditioner&, const float*, float*);
 template void ilu_factorize<double>(Context&, Preconditioner&, const double*);
 template void ilu_factorize<float>(Context&, Preconditioner&, const float*);
+// A two-row ILU forward apply whose schedule holds row 1 only: row 1 waits
+// for row 0, which nothing computes, so its wait runs out after
+// `spin_limit` polls, sets the timeout bit and the launch ends.  Lets a test
+// check the bounded wait and the host's OWTK_ERR_TIMEOUT without any fault.
+void debug_unpublished_dependency(Context& c, int spin_limit)
+{
+    const std::vector<int> rowptr{0, 1, 3}, cols{0, 0, 1}, diagpos{0, 2}, order{1}, task_start{0, 1};
+    const std::vector<double> vals{2.0, -1.0, 2.0}, in{1.0, 1.0}, inv{0.5, 0.5};
+    DeviceBuffer d_rp = upload(c.stream, rowptr), d_ci = upload(c.stream, cols), d_dp = upload(c.stream, diagpos),
+                 d_order = upload(c.stream, order), d_ts = upload(c.stream, task_start),
+                 d_v = upload(c.stream, vals), d_in = upload(c.stream, in), d_inv = upload(c.stream, inv);
+    DeviceBuffer work(2 * sizeof(double) + 16), ticket(sizeof(unsigned long long));
+    OWTK_CUDA(cudaMemsetAsync(ticket.ptr, 0, sizeof(unsigned long long), c.stream));
+    k_fill_sentinel<double><<<1, 32, 0, c.stream>>>(2, work.as<double>());
+    SweepArgs<double> a{};
+    a.order = d_order.as<int>();
+    a.task_start = d_ts.as<int>();
+    a.tasks = 1;
+    a.rowptr = d_rp.as<int>();
+    a.cols = d_ci.as<int>();
+    a.diagpos = d_dp.as<int>();
+    a.vals = d_v.as<double>();
+    a.inv = d_inv.as<double>();
+    a.in = d_in.as<double>();
+    a.out = work.as<double>();
+    a.work = work.as<double>();
+    a.owned = 2;
+    a.bs = 1;
+    a.ticket = ticket.as<unsigned long long>();
+    a.status = c.status.as<unsigned>();
+    a.spin_limit = spin_limit > 0 ? spin_limit : kSpinLimit;
+    k_sweep<double, double, kIluForward, true><<<1, kThreads, 0, c.stream>>>(a);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched(2);
+    c.sync();
+}
+
 template void ilu_apply<double>(Context&, Preconditioner&, const double*, double*);
 template void ilu_apply<float>(Context&, Preconditioner&, const float*, float*);
 template void ssor_apply<double>(Context&, Preconditioner&, const double*, double*);

@@ -18,7 +18,9 @@
 //     zero, is cleared by each call before its kernel runs;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture begins.
+//     before any stream capture begins.  The address is cached for the life
+//     of the process, so the entry point must not be used on a device after
+//     cudaDeviceReset (which recreates the module at a new address).
 
 #include <cuda_runtime.h>
 

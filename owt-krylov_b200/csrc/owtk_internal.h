@@ -146,6 +146,10 @@ struct Matrix {
     owtk_host_apply_fn host_apply = nullptr;
     void* host_user = nullptr;
     std::vector<unsigned char> host_in, host_out;
+    // BSR built from a permuted split layout: per entry its source in the
+    // split arrays (node < owned: diagonal, else owned + edge), for updates.
+    DeviceBuffer split_map;
+    std::size_t split_edges = 0;
     const void* value_ptr() const { return kind == 1 ? off : values.ptr; }
     std::size_t local_size() const { return (owned + ghost) * bs; }
 };
@@ -289,6 +293,12 @@ template<class T> void norm(Context& c, std::size_t n, const T* x, double* out_d
 // (host, may be null) receives the low part: out + out_lo is the pair's exact sum.
 template<class T> void multidot_accurate(Context& c, std::size_t n, int k, int mode, const T* const* a,
                                          const T* const* b, double* out_dev, double* out_host, double* out_lo);
+// Node permutation of owned vector values (forward: dst[new] = src[n2o[new]]).
+template<class T> void permute_nodes(Context& c, std::size_t n, std::size_t bs, const std::int64_t* n2o, const T* src,
+                                     T* dst, bool inverse);
+// values[e] = map[e] < n ? diag[map[e]] : off[map[e] - n] (bs values per entry).
+template<class T> void gather_split(Context& c, std::size_t entries, std::size_t bs, std::size_t n,
+                                    const std::int64_t* map, const T* diag, const T* off, T* values);
 // Doubled-precision 2-norm; scratch: two device doubles.
 template<class T> void norm_accurate(Context& c, std::size_t n, const T* x, double* scratch, double* out_dev,
                                      double* out_host);
@@ -304,6 +314,8 @@ template<class T> void gather_values(Context& c, std::size_t entries, std::size_
 // ILU(0)/SSOR sweeps.
 template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* matrix_values);
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
+// Test hook: a sweep whose only dependency is never published (bounded wait).
+void debug_unpublished_dependency(Context& c, int spin_limit);
 template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T* out);
 template<class T> void reciprocal_checked(Context& c, std::size_t n, const T* d, T minimum, T* inv);
 template<class T> void bsr_diagonal(Context& c, const Matrix& m, T* out);
@@ -364,3 +376,9 @@ struct owtk_matrix : owtk::Matrix {};
 struct owtk_preconditioner : owtk::Preconditioner {};
 struct owtk_workspace : owtk::Workspace {};
 struct owtk_arnoldi_snapshot : owtk::ArnoldiSnapshot {};
+struct owtk_permutation {
+    owtk::Context* ctx = nullptr;
+    std::size_t n = 0;
+    std::vector<std::int64_t> new_to_old, old_to_new;
+    owtk::DeviceBuffer d_new_to_old;
+};

@@ -147,6 +147,12 @@ def lib():
             "owtk_batch_solve_host": (c_int, [vp, vp, vp, POINTER(SolverOptions), POINTER(SolverResult)]),
             "owtk_bf16_gemm_nt": (c_int, [vp, sz, sz, sz, vp, vp, vp]),
             "owtk_solve_specwave": (c_int, [c_int, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
+            "owtk_debug_unpublished_dependency": (c_int, [vp, ctypes.c_uint32]),
+            "owtk_permutation_create": (c_int, [vp, sz, vp, POINTER(vp)]),
+            "owtk_permutation_destroy": (c_int, [vp]),
+            "owtk_vector_permute": (c_int, [vp, vp, vp, c_int]),
+            "owtk_bsr_create_permuted_split": (c_int, [vp, c_int, sz, vp, vp, vp, vp, POINTER(vp)]),
+            "owtk_bsr_update_permuted_split": (c_int, [vp, vp, vp]),
             "owtk_dot_ex": (c_int, [vp, vp, c_int, POINTER(c_double), POINTER(c_double)]),
             "owtk_norm_ex": (c_int, [vp, c_int, POINTER(c_double)]),
             "owtk_arnoldi_snapshot_create": (c_int, [vp, POINTER(vp)]),
@@ -491,6 +497,43 @@ def solve_specwave(solver_id: int, matrix: Matrix, rhs: Vector, x: Vector, optio
     check(lib().owtk_solve_specwave_ex(solver_id, matrix.h, rhs.h, x.h, ctypes.byref(o),
                                        workspace.h if workspace else None, REDUCTION[reduction], ctypes.byref(r)))
     return r
+
+
+class Permutation:
+    """owtk_permutation_*: a node permutation applied on the device."""
+
+    def __init__(self, ctx: Context, new_to_old):
+        p = _u64(new_to_old)
+        h = c_void_p()
+        check(lib().owtk_permutation_create(ctx.h, p.size, _ptr(p), ctypes.byref(h)))
+        self.h, self.ctx, self.n = h, ctx, p.size
+
+    def apply(self, src: Vector, dst: Vector, inverse: bool = False):
+        check(lib().owtk_vector_permute(self.h, src.h, dst.h, 1 if inverse else 0))
+
+    def permuted_split_matrix(self, bs: int, off_rowptr, off_cols, diag: Vector, off: Vector, dtype=np.float64):
+        """P A P^T from a split layout whose coefficient arrays are device vectors."""
+        rp, ci = _u64(off_rowptr), _u64(off_cols)
+        if ci.size == 0:
+            ci = np.zeros(1, dtype=np.uint64)
+        h = c_void_p()
+        check(lib().owtk_bsr_create_permuted_split(self.h, _dtype_code(dtype), bs, _ptr(rp), _ptr(ci),
+                                                   c_void_p(diag.data_ptr), c_void_p(off.data_ptr), ctypes.byref(h)))
+        m = Matrix.__new__(Matrix)
+        m.ctx, m.kind, m.owned, m.ghost, m.bs, m.dtype, m.h = self.ctx, "bsr", self.n, 0, bs, np.dtype(dtype), h
+        return m
+
+    def __del__(self):
+        try:
+            if self.h is not None:
+                lib().owtk_permutation_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def update_permuted_split(matrix: Matrix, diag: Vector, off: Vector):
+    check(lib().owtk_bsr_update_permuted_split(matrix.h, c_void_p(diag.data_ptr), c_void_p(off.data_ptr)))
 
 
 class ArnoldiSnapshot:

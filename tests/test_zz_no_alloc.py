@@ -4,12 +4,15 @@ Callers that cannot allocate device memory (a framework that owns the
 device allocator, or code where cudaMalloc is forbidden) use this entry
 point: it takes caller-owned device inputs and outputs and keeps its
 reduction scratch in a static device array.  This test drives it through
-the C ABI and checks it against owtk_dot_batch, the allocating entry point,
-on two calls in a row (the scratch keeps the previous call's contents, so the
-second call shows nothing stale leaks through).  It builds its own data, so
-it passes alone in a fresh process as well as after the other tests.
+the C ABI and checks it, on two calls in a row (the scratch keeps the
+previous call's contents, so the second call shows nothing stale leaks
+through), against owtk_dot_batch, the allocating entry point, and against an
+independent host answer: the exactly rounded sum (math.fsum) of the same
+products.  It builds its own data, so it passes alone in a fresh process as
+well as after the other tests.
 """
 import ctypes
+import math
 
 import numpy as np
 import pytest
@@ -51,7 +54,10 @@ def test_noalloc_dot_batch_matches_allocating_entry_point(native, ctx):
         wh = w.download()[: owned * bs]
         for j in range(k + 1):
             other = basis[j].download()[: owned * bs] if j < k else wh
-            scale = np.abs(wh * other).sum()
+            products = wh * other
+            scale = np.abs(products).sum()
+            exact = math.fsum(products.tolist())
+            assert abs(got[j] - exact) <= 1e-13 * scale, (call, j, got[j], exact)
             assert abs(got[j] - expect[j]) <= 1e-13 * scale, (call, j, got[j], expect[j])
 
 
