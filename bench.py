@@ -258,9 +258,10 @@ def cpu_reference_solve(s, reps: int, native_build: bool = False, restart: int =
 def run_reference(args):
     """The reference's CPU GMRES(30)+ILU(0) on the workload's system, built in
     this process with the reference's own RCM (oracle/_ref); this project's
-    library is not loaded.  One step = one full solve from x0 = 0.  The first
-    full solve is the warm-up; timed solves stop at --steps or when
-    --ref-budget seconds of them are spent, whichever comes first."""
+    library is not loaded.  One step = one full solve from x0 = 0.  --warmup
+    warm-up solves (fewer if they would exceed a third of --ref-budget, at
+    least one), then timed solves until --steps or until --ref-budget seconds
+    of them are spent, whichever comes first."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
@@ -280,7 +281,9 @@ def run_reference(args):
     opts = oracle.default_options(restart=30)
     x0 = np.zeros(s.owned * s.bs)
     warm, timed, last = [], [], None
-    for _ in range(max(1, min(args.warmup, 1))):
+    # The requested warm-up solves, unless they would take more than a third
+    # of the timed budget (then one).
+    while len(warm) < max(1, args.warmup) and (not warm or sum(warm) + warm[-1] <= args.ref_budget / 3):
         t = time.time()
         last, _x = ref.solve("gmres", m, pc, opts, s.rhs, x0)
         warm.append(time.time() - t)

@@ -173,6 +173,16 @@ owtk_status owtk_ilu_factors(owtk_preconditioner* pc, uint64_t* entries, uint64_
 owtk_status owtk_pc_levels(owtk_preconditioner* pc, int32_t* lower_level, int32_t* upper_level,
                            uint64_t* lower_depth, uint64_t* upper_depth);
 
+/* How an ILU preconditioner's applies are scheduled (no reference
+ * counterpart): cluster_ctas > 0 when they run on one thread-block cluster of
+ * that many CTAs (dependency values through distributed shared memory, epochs
+ * of epoch_levels levels, ring_rows rows of results per CTA), 0 for the
+ * level-scheduled sweep over the whole GPU.  Both give the same bits.  The
+ * environment variable OWTK_CLUSTER_SWEEP=0 at preconditioner creation
+ * selects the level-scheduled sweep. */
+owtk_status owtk_pc_sweep_schedule(owtk_preconditioner* pc, int32_t* cluster_ctas, int32_t* epoch_levels,
+                                   int32_t* ring_rows);
+
 /* ---- host setup (ordering.hpp) -------------------------------------------- */
 /* reverse_cuthill_mckee_order (ordering.hpp:138-180); new_to_old[owned]. */
 owtk_status owtk_rcm_order(size_t owned_nodes, size_t ghost_nodes, const uint64_t* row_offsets,

@@ -248,6 +248,16 @@ void ilu_symbolic(Preconditioner& p, const Matrix& m, std::size_t fill)
     levels_of(n, p.f_rowptr.data(), p.f_cols.data(), lower_level, upper_level);
     build_sweep(*p.ctx, p.lower, n, p.bs, lower_level, false);
     build_sweep(*p.ctx, p.upper, n, p.bs, upper_level, true);
+    if (!p.block) {
+        std::vector<std::uint32_t> loc;
+        build_cluster_sweep(*p.ctx, p.c_lower, n, p.bs, m.dtype, lower_level, p.f_rowptr, p.f_cols, p.f_diagpos,
+                            false, loc);
+        if (p.c_lower.ready)
+            build_cluster_sweep(*p.ctx, p.c_upper, n, p.bs, m.dtype, upper_level, p.f_rowptr, p.f_cols,
+                                p.f_diagpos, true, loc);
+        if (p.c_lower.ready && p.c_upper.ready) p.d_floc = upload(p.ctx->stream, loc);
+        else p.c_lower.ready = p.c_upper.ready = false;
+    }
 }
 
 // preconditioner.hpp:269-311: the new matrix must have the analysed pattern.
@@ -1413,6 +1423,18 @@ owtk_status owtk_bsr_update_permuted_split(owtk_matrix* m, const void* device_di
                                       static_cast<const float*>(device_diagonal),
                                       static_cast<const float*>(device_off_diagonal), m->values.as<float>());
         c.sync();
+    });
+}
+
+owtk_status owtk_pc_sweep_schedule(owtk_preconditioner* pc, int32_t* cluster_ctas, int32_t* epoch_levels,
+                                   int32_t* ring_rows)
+{
+    return guarded([&] {
+        require(pc != nullptr, "null handle");
+        const bool on = pc->c_lower.ready && pc->c_upper.ready;
+        if (cluster_ctas) *cluster_ctas = on ? pc->c_lower.C : 0;
+        if (epoch_levels) *epoch_levels = on ? pc->c_lower.K : 0;
+        if (ring_rows) *ring_rows = on ? std::max(pc->c_lower.R, pc->c_upper.R) : 0;
     });
 }
 

@@ -177,6 +177,15 @@ struct Sweep {
     std::vector<std::int32_t> h_level;
 };
 
+// The same sweep run by one thread-block cluster (kernels_cluster_sweep.cu):
+// tasks dealt round-robin to C CTAs, levels cut into epochs of K levels,
+// a ring of R rows per CTA.
+struct ClusterSweep {
+    bool ready = false;
+    int C = 0, K = 0, E = 0, R = 0, tasks = 0;
+    DeviceBuffer rows, task_ptr, epoch_task, cta_first;
+};
+
 struct Preconditioner {
     Context* ctx = nullptr;
     owtk_pc_kind kind = OWTK_PC_IDENTITY;
@@ -198,6 +207,10 @@ struct Preconditioner {
     DeviceBuffer d_upd_start, d_upd_target, d_upd_upper;
     // SSOR dependency patterns reuse the matrix structure.
     Sweep lower, upper;
+    // Cluster schedules of the ILU applies and, per factor entry, where its
+    // dependency is read (owner CTA and ring slot, or global memory).
+    ClusterSweep c_lower, c_upper;
+    DeviceBuffer d_floc;
     DeviceBuffer flags;        // uint32 per row, epoch-stamped
     DeviceBuffer ticket;       // uint64 monotone task counter
     std::uint32_t epoch = 0;
@@ -237,6 +250,10 @@ void levels_of(std::size_t owned, const std::int32_t* rowptr, const std::int32_t
                std::vector<std::int32_t>& lower, std::vector<std::int32_t>& upper);
 void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
                  const std::vector<std::int32_t>& level, bool descending_rows);
+void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::size_t bs, owtk_dtype dtype,
+                         const std::vector<std::int32_t>& level, const std::vector<std::int32_t>& rowptr,
+                         const std::vector<std::int32_t>& cols, const std::vector<std::int32_t>& diagpos,
+                         bool backward, std::vector<std::uint32_t>& loc);
 void rcm_order(std::size_t owned, const std::int32_t* rowptr, const std::int32_t* cols,
                std::uint64_t* out);
 void hilbert_order(std::size_t n, const double* xy, std::uint64_t* out);
@@ -314,6 +331,7 @@ template<class T> void gather_values(Context& c, std::size_t entries, std::size_
 // ILU(0)/SSOR sweeps.
 template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* matrix_values);
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
+template<class T> bool cluster_ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
 // Test hook: a sweep whose only dependency is never published (bounded wait).
 void debug_unpublished_dependency(Context& c, int spin_limit);
 template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T* out);

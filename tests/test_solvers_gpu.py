@@ -189,7 +189,7 @@ SPECWAVE = {3: ("COMM_HIDING_BICGSTAB", "SSOR"), 4: ("COMM_HIDING_BICGSTAB", "SS
 @pytest.mark.parametrize("solver_id", sorted(SPECWAVE))
 def test_specwave_dispatch_matches_direct_calls(native, ctx, solver_id):
     # specwave_compat.hpp:99-249: each legacy id is the named solver with the
-    # named preconditioner (SSOR omega = options.relaxation, ILU(0)).
+    # named preconditioner (SSOR omega = options.relaxation, ILU(0)) and reduction.
     c = cases.lattice_case(side=20, bs=3, seed=21)
     n, bs = c["owned"], c["bs"]
     m = native.Matrix(ctx, "bsr", n, 0, bs, c["rowptr"], c["cols"], c["vals"])
@@ -200,7 +200,10 @@ def test_specwave_dispatch_matches_direct_calls(native, ctx, solver_id):
     kind, pck = SPECWAVE[solver_id]
     pc = native.Preconditioner(m, getattr(native, "PC_" + pck), 1.2 if pck == "SSOR" else 0)
     direct = native.default_options(relaxation=1.2, residual_replacement_interval=50)
-    r2 = native.solve(getattr(native, kind), m, pc, b, x2, direct)
+    # specwave_compat.hpp:157-176, :223-243: id 10 reduces in mixed precision,
+    # id 22 with compensation.
+    reduction = {10: "mixed", 22: "compensated"}.get(solver_id, "serial")
+    r2 = native.solve_ex(getattr(native, kind), m, pc, b, x2, direct, reduction=reduction)
     d1, d2 = r1.as_dict(), r2.as_dict()
     d1.pop("solve_seconds", None)
     d2.pop("solve_seconds", None)
