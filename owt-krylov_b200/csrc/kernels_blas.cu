@@ -13,6 +13,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include <cuda_bf16.h>
 
@@ -383,6 +386,34 @@ unsigned reduce_blocks(const Context& c, std::size_t n)
     return static_cast<unsigned>(want < 1 ? 1 : (want > cap ? cap : want));
 }
 
+// CTAs of `kernel` that fit on the device at once (one wave), at most `want`:
+// the Gram-Schmidt kernels hold many basis streams in registers, so fewer
+// CTAs fit per SM than the element-wise kernels and a grid sized for those
+// would run in several waves.
+template<class K>
+unsigned resident_blocks(const Context& c, K kernel, unsigned want)
+{
+    static std::mutex mutex;
+    static std::vector<std::pair<const void*, int>> cache;   // kernel -> resident CTAs per SM
+    const void* key = reinterpret_cast<const void*>(kernel);
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lock(mutex);
+        for (const auto& [k, v] : cache)
+            if (k == key) per_sm = v;
+        if (per_sm == 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess
+                || per_sm < 1) {
+                cudaGetLastError();
+                return want;
+            }
+            cache.emplace_back(key, per_sm);
+        }
+    }
+    const unsigned cap = static_cast<unsigned>(per_sm) * static_cast<unsigned>(c.sm_count);
+    return want < cap ? want : cap;
+}
+
 // Reduce G per-thread accumulators across the CTA; thread j < G writes the
 // CTA's partial for accumulator j.
 template<int G>
@@ -493,7 +524,7 @@ __global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, Ptr
 // results agree with it to FP64 rounding (a few ulps, measured), not always
 // bit for bit, so a caller keeps to one of the two kernels for a given dot.
 template<class T, int G>
-__global__ void __launch_bounds__(kThreads) k_basis_dots(std::size_t n, int k, PtrPack basis,
+__global__ void __launch_bounds__(kThreads, 2) k_basis_dots(std::size_t n, int k, PtrPack basis,
                                                          const T* __restrict__ x, double* partials, unsigned* ticket,
                                                          double* out_dev, double* out_host)
 {
@@ -551,7 +582,7 @@ __global__ void __launch_bounds__(kThreads) k_basis_dots(std::size_t n, int k, P
 // w -= V h (reference axpy order), then dots of the updated w with every V_j
 // and w.w, in one pass over V (second Gram-Schmidt pass, krylov_solvers.hpp:310-322).
 template<class T, int G>
-__global__ void __launch_bounds__(kThreads) k_cgs_update_dot(std::size_t n, int k, PtrPack basis,
+__global__ void __launch_bounds__(kThreads, 2) k_cgs_update_dot(std::size_t n, int k, PtrPack basis,
                                                              const double* __restrict__ h, T* __restrict__ w,
                                                              double* partials, unsigned* ticket,
                                                              double* out_dev, double* out_host)
@@ -1221,14 +1252,17 @@ template<class T> void basis_dots(Context& c, std::size_t n, int k, const T* con
                                   double* out_dev, double* out_host)
 {
     if (k + 1 > 32) fail(OWTK_ERR_INVALID_ARGUMENT, "basis dots take at most 31 basis vectors");
-    const unsigned blocks = reduce_blocks(c, n);
+    const unsigned want = reduce_blocks(c, n);
     const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
     if (k + 1 <= 8)
-        k_basis_dots<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_basis_dots<T, 8><<<resident_blocks(c, k_basis_dots<T, 8>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
     else if (k + 1 <= 16)
-        k_basis_dots<T, 16><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_basis_dots<T, 16><<<resident_blocks(c, k_basis_dots<T, 16>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
     else
-        k_basis_dots<T, 32><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_basis_dots<T, 32><<<resident_blocks(c, k_basis_dots<T, 32>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }
@@ -1237,14 +1271,17 @@ template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T*
                                       const double* h, T* w, double* out_dev, double* out_host)
 {
     if (k + 1 > 32) fail(OWTK_ERR_INVALID_ARGUMENT, "fused Gram-Schmidt pass takes at most 31 basis vectors");
-    const unsigned blocks = reduce_blocks(c, n);
+    const unsigned want = reduce_blocks(c, n);
     const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
     if (k + 1 <= 8)
-        k_cgs_update_dot<T, 8><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_cgs_update_dot<T, 8><<<resident_blocks(c, k_cgs_update_dot<T, 8>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     else if (k + 1 <= 16)
-        k_cgs_update_dot<T, 16><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_cgs_update_dot<T, 16><<<resident_blocks(c, k_cgs_update_dot<T, 16>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     else
-        k_cgs_update_dot<T, 32><<<blocks, kThreads, 0, c.stream>>>(n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+        k_cgs_update_dot<T, 32><<<resident_blocks(c, k_cgs_update_dot<T, 32>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
 }

@@ -9,9 +9,12 @@
 // (~0.86 us per level on the 2M-vertex mesh, 2 x 2913 levels per apply).
 // Here one cluster of C CTAs (16 when the device allows it, else 8) runs the
 // whole sweep:
-//   * tasks (rows of one level, <= 32/bs rows, in level order) are dealt
-//     round-robin to the CTAs; every CTA runs its tasks in order with its
-//     warps taking them from a shared-memory ticket;
+//   * tasks (32 rows of one level, one row with all its components per
+//     lane, in level order) are dealt round-robin to the CTAs; every CTA runs
+//     its tasks in order with its warps taking them from a shared-memory
+//     ticket.  Wide tasks keep many levels in flight with the few warps of
+//     one cluster (a task of 32/bs rows, one (row, component) per lane, gave
+//     ~3.7 levels in flight and lost to the sweep over the whole GPU);
 //   * each CTA keeps its results in a shared-memory ring of R rows; a row
 //     whose dependency is recent polls the owner CTA's ring slot over
 //     distributed shared memory (ld.relaxed.cluster.shared::cluster) until the
@@ -54,7 +57,6 @@ namespace {
 using namespace dev;
 
 constexpr int kClusterThreads = 512;
-constexpr int kLocChunk = 8;
 constexpr unsigned kGlobalDep = 0xffffffffu;   // dependency read from global memory
 constexpr int kOwnerShift = 27;                // loc = owner << 27 | ring slot
 constexpr int kSpinDefault = 1 << 22;
@@ -136,50 +138,67 @@ __device__ __forceinline__ unsigned as_bits(float v) { return __float_as_uint(v)
 
 template<class T> __device__ __forceinline__ T ld_global_cg(const T* p) { return __ldcg(p); }
 
-// One (row, component) per lane: y = own - sum_e vals[e] * dep[col_e] over the
-// row's dependency entries [b, e) in entry order (sub_rn(y, mul_rn(v, x)),
-// the reference's rounding), then FIN: 0 y, 1 y * fin.  Recent dependencies
-// are polled in their owner's ring; older ones are read from `dep` in global
-// memory.  The loop is warp-uniform and ends when every lane has published.
-template<class T, int FIN>
-__device__ __forceinline__ void cluster_lane(bool valid, T y, const ClusterArgs<T>& a, const T* dep, int b, int e,
-                                             int c, T fin, T* gdst, unsigned ring_dst, unsigned ring_base)
+// One row per lane, all bs components: y_c = own_c - sum_e vals[e][c] *
+// dep[col_e][c] over the row's dependency entries [b, e) in entry order
+// (sub_rn(y, mul_rn(v, x)), the reference's rounding), then FIN: 0 y,
+// 1 y * fin_c.  Recent dependencies are polled in their owner's ring, older
+// ones read from `dep` in global memory.  A warp-uniform loop that ends when
+// every lane has published its row.
+template<class T, int BS, int FIN>
+__device__ __forceinline__ void cluster_row(bool valid, const T (&own)[BS], const ClusterArgs<T>& a, const T* dep,
+                                            int b, int e, const T (&fin)[BS], T* gdst, unsigned ring_dst,
+                                            unsigned ring_base)
 {
     using U = typename Sent<T>::U;
-    const int bs = a.bs;
-    T fv[kLocChunk];
-    U xb[kLocChunk];
-    unsigned raddr[kLocChunk];
-    bool on[kLocChunk], remote[kLocChunk];
+    constexpr int kC = 4;   // entries per round
+    T y[BS];
+#pragma unroll
+    for (int c = 0; c < BS; ++c) y[c] = own[c];
+    T fv[kC][BS];
+    U xb[kC][BS];
+    unsigned raddr[kC];
+    bool on[kC], remote[kC];
     int k0 = b, it = 0;
     bool loaded = false, done = !valid;
+    auto publish_row = [&]() {
+#pragma unroll
+        for (int c = 0; c < BS; ++c) {
+            T r = FIN == 1 ? mul_rn(y[c], fin[c]) : y[c];
+            if (r != r) r = as_value(Sent<T>::kQuietNan);
+            gdst[c] = r;
+            st_cluster(ring_dst + c * static_cast<unsigned>(sizeof(T)), as_bits(r));
+        }
+    };
     for (;;) {
         if (!done) {
             if (!loaded && k0 >= e) {
-                T r = FIN == 1 ? mul_rn(y, fin) : y;
-                if (r != r) r = as_value(Sent<T>::kQuietNan);
-                *gdst = r;
-                st_cluster(ring_dst, as_bits(r));
+                publish_row();
                 done = true;
             } else {
                 if (!loaded) {
 #pragma unroll
-                    for (int j = 0; j < kLocChunk; ++j) {
+                    for (int j = 0; j < kC; ++j) {
                         const int k = k0 + j;
                         on[j] = k < e;
                         remote[j] = false;
                         if (on[j]) {
                             const int col = a.cols[k];
                             const unsigned l = a.loc[k];
-                            fv[j] = a.vals[static_cast<std::size_t>(k) * bs + c];
+#pragma unroll
+                            for (int c = 0; c < BS; ++c) fv[j][c] = a.vals[static_cast<std::size_t>(k) * BS + c];
                             if (l == kGlobalDep) {
-                                xb[j] = as_bits(ld_global_cg(dep + static_cast<std::size_t>(col) * bs + c));
+#pragma unroll
+                                for (int c = 0; c < BS; ++c)
+                                    xb[j][c] = as_bits(ld_global_cg(dep + static_cast<std::size_t>(col) * BS + c));
                             } else {
                                 remote[j] = true;
                                 const unsigned slot = l & ((1u << kOwnerShift) - 1);
-                                raddr[j] = map_to(ring_base + (slot * bs + c) * static_cast<unsigned>(sizeof(T)),
+                                raddr[j] = map_to(ring_base + slot * BS * static_cast<unsigned>(sizeof(T)),
                                                   l >> kOwnerShift);
-                                xb[j] = ld_cluster(raddr[j], static_cast<T*>(nullptr));
+#pragma unroll
+                                for (int c = 0; c < BS; ++c)
+                                    xb[j][c] = ld_cluster(raddr[j] + c * static_cast<unsigned>(sizeof(T)),
+                                                          static_cast<T*>(nullptr));
                             }
                         }
                     }
@@ -187,7 +206,9 @@ __device__ __forceinline__ void cluster_lane(bool valid, T y, const ClusterArgs<
                 }
                 bool pending = false;
 #pragma unroll
-                for (int j = 0; j < kLocChunk; ++j) pending |= on[j] && remote[j] && xb[j] == Sent<T>::kSentinel;
+                for (int j = 0; j < kC; ++j)
+#pragma unroll
+                    for (int c = 0; c < BS; ++c) pending |= on[j] && remote[j] && xb[j][c] == Sent<T>::kSentinel;
                 if (pending) {
                     if (it >= a.spin_limit) {
                         atomicOr(a.status, kErrTimeout);
@@ -199,23 +220,26 @@ __device__ __forceinline__ void cluster_lane(bool valid, T y, const ClusterArgs<
                 }
                 if (!pending) {
 #pragma unroll
-                    for (int j = 0; j < kLocChunk; ++j)
-                        if (on[j]) y = sub_rn(y, mul_rn(fv[j], as_value(xb[j])));
-                    k0 += kLocChunk;
+                    for (int j = 0; j < kC; ++j)
+                        if (on[j]) {
+#pragma unroll
+                            for (int c = 0; c < BS; ++c) y[c] = sub_rn(y[c], mul_rn(fv[j][c], as_value(xb[j][c])));
+                        }
+                    k0 += kC;
                     loaded = false;
                     if (k0 >= e) {
-                        T r = FIN == 1 ? mul_rn(y, fin) : y;
-                        if (r != r) r = as_value(Sent<T>::kQuietNan);
-                        *gdst = r;
-                        st_cluster(ring_dst, as_bits(r));
+                        publish_row();
                         done = true;
                     }
                 } else {
                     ++it;
 #pragma unroll
-                    for (int j = 0; j < kLocChunk; ++j)
-                        if (on[j] && remote[j] && xb[j] == Sent<T>::kSentinel)
-                            xb[j] = ld_cluster(raddr[j], static_cast<T*>(nullptr));
+                    for (int j = 0; j < kC; ++j)
+#pragma unroll
+                        for (int c = 0; c < BS; ++c)
+                            if (on[j] && remote[j] && xb[j][c] == Sent<T>::kSentinel)
+                                xb[j][c] = ld_cluster(raddr[j] + c * static_cast<unsigned>(sizeof(T)),
+                                                      static_cast<T*>(nullptr));
                 }
             }
         }
@@ -223,7 +247,7 @@ __device__ __forceinline__ void cluster_lane(bool valid, T y, const ClusterArgs<
     }
 }
 
-template<class T, bool BACKWARD>
+template<class T, bool BACKWARD, int BS>
 __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArgs<T> a)
 {
     using U = typename Sent<T>::U;
@@ -231,9 +255,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArg
     U* ring = reinterpret_cast<U*>(smem_raw);
     __shared__ unsigned ticket[2];
     const unsigned k = cluster_rank();
-    const int bs = a.bs;
     const int lane = threadIdx.x & 31;
-    const int rl = lane / bs, c = lane - rl * bs;
     const unsigned ring_base = static_cast<unsigned>(__cvta_generic_to_shared(ring));
     const int first = a.cta_first[k];
     const int* et = a.epoch_task + static_cast<std::size_t>(k) * (a.E + 1);
@@ -241,9 +263,9 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArg
     // are reset one epoch ahead.
     {
         const int p0 = a.task_ptr[et[0]], p1 = a.task_ptr[et[a.E > 0 ? 1 : 0]];
-        for (int i = threadIdx.x; i < (p1 - p0) * bs; i += blockDim.x) {
-            const int p = p0 + i / bs;
-            ring[((p - first) % a.R) * bs + i % bs] = Sent<T>::kSentinel;
+        for (int i = threadIdx.x; i < (p1 - p0) * BS; i += blockDim.x) {
+            const int p = p0 + i / BS;
+            ring[((p - first) % a.R) * BS + i % BS] = Sent<T>::kSentinel;
         }
     }
     if (threadIdx.x < 2) ticket[threadIdx.x] = 0;
@@ -257,28 +279,32 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArg
             const int t = t0 + static_cast<int>(j);
             if (t >= t1) break;
             const int s = a.task_ptr[t], nrows = a.task_ptr[t + 1] - s;
-            const bool valid = rl < nrows;
-            const int p = s + (valid ? rl : 0);
+            const bool valid = lane < nrows;
+            const int p = s + (valid ? lane : 0);
             const int row = valid ? a.rows[p] : 0;
-            const std::size_t o = static_cast<std::size_t>(row) * bs + c;
-            const unsigned ring_dst = ring_base + static_cast<unsigned>((((p - first) % a.R) * bs + c) * sizeof(T));
+            const std::size_t o = static_cast<std::size_t>(row) * BS;
+            const unsigned ring_dst = ring_base + static_cast<unsigned>(((p - first) % a.R) * BS * sizeof(T));
+            T own[BS], fin[BS];
+#pragma unroll
+            for (int c = 0; c < BS; ++c) {
+                own[c] = valid ? a.in[o + c] : T(0);
+                fin[c] = BACKWARD && valid ? a.inv[o + c] : T(1);
+            }
             if constexpr (!BACKWARD) {
                 const int b = valid ? a.rowptr[row] : 0, d = valid ? a.diagpos[row] : 0;
-                const T own = valid ? a.in[o] : T(0);
-                cluster_lane<T, 0>(valid, own, a, a.out, b, d, c, T(1), a.out + o, ring_dst, ring_base);
+                cluster_row<T, BS, 0>(valid, own, a, a.out, b, d, fin, a.out + o, ring_dst, ring_base);
             } else {
                 const int d = valid ? a.diagpos[row] : 0, end = valid ? a.rowptr[row + 1] : 0;
-                const T own = valid ? a.in[o] : T(0), iv = valid ? a.inv[o] : T(1);
-                cluster_lane<T, 1>(valid, own, a, a.out, d + 1, end, c, iv, a.out + o, ring_dst, ring_base);
+                cluster_row<T, BS, 1>(valid, own, a, a.out, d + 1, end, fin, a.out + o, ring_dst, ring_base);
             }
         }
         // Reset the slots of this CTA's next-epoch rows (their previous rows
         // are two epochs old) and the next epoch's ticket.
         if (ep + 1 < a.E) {
             const int p0 = a.task_ptr[et[ep + 1]], p1 = a.task_ptr[et[ep + 2]];
-            for (int i = threadIdx.x; i < (p1 - p0) * bs; i += blockDim.x) {
-                const int pp = p0 + i / bs;
-                st_cluster(ring_base + static_cast<unsigned>((((pp - first) % a.R) * bs + i % bs) * sizeof(T)),
+            for (int i = threadIdx.x; i < (p1 - p0) * BS; i += blockDim.x) {
+                const int pp = p0 + i / BS;
+                st_cluster(ring_base + static_cast<unsigned>((((pp - first) % a.R) * BS + i % BS) * sizeof(T)),
                            Sent<T>::kSentinel);
             }
             if (threadIdx.x == 0) ticket[(ep + 1) & 1] = 0;
@@ -288,9 +314,20 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArg
 }
 
 template<class T, bool BACKWARD>
+auto cluster_kernel(int bs)
+{
+    switch (bs) {
+    case 1: return k_cluster_sweep<T, BACKWARD, 1>;
+    case 2: return k_cluster_sweep<T, BACKWARD, 2>;
+    case 3: return k_cluster_sweep<T, BACKWARD, 3>;
+    default: return k_cluster_sweep<T, BACKWARD, 4>;
+    }
+}
+
+template<class T, bool BACKWARD>
 bool launch_cluster(Context& c, const ClusterSweep& s, ClusterArgs<T> a)
 {
-    auto kernel = k_cluster_sweep<T, BACKWARD>;
+    auto kernel = cluster_kernel<T, BACKWARD>(a.bs);
     const std::size_t smem = static_cast<std::size_t>(s.R) * a.bs * sizeof(T);
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess
         || (s.C > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
@@ -325,9 +362,9 @@ bool launch_cluster(Context& c, const ClusterSweep& s, ClusterArgs<T> a)
 }
 
 template<class T>
-bool cluster_feasible(int C, std::size_t smem)
+bool cluster_feasible(int C, std::size_t smem, int bs)
 {
-    auto kernel = k_cluster_sweep<T, false>;
+    auto kernel = cluster_kernel<T, false>(bs);
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess
         || (C > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
         cudaGetLastError();
@@ -367,14 +404,13 @@ void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::
     const char* env = std::getenv("OWTK_CLUSTER_SWEEP");
     if (env && std::atoi(env) == 0) return;
     const std::size_t n = owned;
-    if (n < 4096 || bs == 0 || bs > 8) return;
+    if (n < 4096 || bs == 0 || bs > 4) return;
     const std::size_t es = dtype == OWTK_F64 ? 8 : 4;
     std::int32_t depth = 0;
     for (const auto l : level) depth = std::max(depth, l + 1);
-    if (depth < 64 || n / static_cast<std::size_t>(depth) < 64) return;   // sequential DAGs: keep the plain sweep
-    // Tasks exactly as build_sweep cuts them: rows by (level, row), at most
-    // 32 / bs rows, never across a level.
-    const int per_task = static_cast<int>(32 / bs);
+    if (depth < 16 || n / static_cast<std::size_t>(depth) < 16) return;   // near-sequential DAGs: keep the plain sweep
+    // Tasks: rows by (level, row), 32 rows (one per lane), never across a level.
+    const int per_task = 32;
     std::vector<std::int32_t> count(static_cast<std::size_t>(depth) + 1, 0);
     for (const auto l : level) ++count[static_cast<std::size_t>(l) + 1];
     for (std::size_t i = 1; i < count.size(); ++i) count[i] += count[i - 1];
@@ -418,7 +454,9 @@ void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::
         }
         if (K == 0) continue;
         const std::size_t smem = static_cast<std::size_t>(R) * bs * es;
-        if (!(dtype == OWTK_F64 ? cluster_feasible<double>(C, smem) : cluster_feasible<float>(C, smem))) continue;
+        if (!(dtype == OWTK_F64 ? cluster_feasible<double>(C, smem, static_cast<int>(bs))
+                                 : cluster_feasible<float>(C, smem, static_cast<int>(bs))))
+            continue;
         const int E = (depth + K - 1) / K;
         // CTA-major processing order; per row its owner and ring slot.
         std::vector<std::vector<std::size_t>> cta_tasks(static_cast<std::size_t>(C));
