@@ -75,6 +75,7 @@ template<> struct Sent<float> {
 
 template<class T>
 struct ClusterArgs {
+    const int4* recs;         // per position: row, first and end dependency entry
     const int* rows;          // processing order, CTA-major
     const int* task_ptr;      // tasks + 1 positions in rows (CTA-major task order)
     const int* epoch_task;    // C * (E + 1): first task of each epoch per CTA
@@ -232,14 +233,27 @@ __device__ __forceinline__ void cluster_row(bool valid, const T (&own)[BS], cons
                         done = true;
                     }
                 } else {
+                    // Re-poll the first pending dependency only (the others are
+                    // older and usually ready by then), backing off while it
+                    // waits: polls of many lanes would otherwise crowd the
+                    // cluster's shared-memory network.
                     ++it;
+                    if (it >= 16) __nanosleep(it >= 256 ? 256 : 32);
+                    bool first_pending = true;
 #pragma unroll
-                    for (int j = 0; j < kC; ++j)
+                    for (int j = 0; j < kC; ++j) {
+                        bool mine = false;
 #pragma unroll
-                        for (int c = 0; c < BS; ++c)
-                            if (on[j] && remote[j] && xb[j][c] == Sent<T>::kSentinel)
-                                xb[j][c] = ld_cluster(raddr[j] + c * static_cast<unsigned>(sizeof(T)),
-                                                      static_cast<T*>(nullptr));
+                        for (int c = 0; c < BS; ++c) mine |= on[j] && remote[j] && xb[j][c] == Sent<T>::kSentinel;
+                        if (mine && first_pending) {
+                            first_pending = false;
+#pragma unroll
+                            for (int c = 0; c < BS; ++c)
+                                if (xb[j][c] == Sent<T>::kSentinel)
+                                    xb[j][c] = ld_cluster(raddr[j] + c * static_cast<unsigned>(sizeof(T)),
+                                                          static_cast<T*>(nullptr));
+                        }
+                    }
                 }
             }
         }
@@ -281,7 +295,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArg
             const int s = a.task_ptr[t], nrows = a.task_ptr[t + 1] - s;
             const bool valid = lane < nrows;
             const int p = s + (valid ? lane : 0);
-            const int row = valid ? a.rows[p] : 0;
+            const int4 rec = a.recs[p];
+            const int row = valid ? rec.x : 0;
             const std::size_t o = static_cast<std::size_t>(row) * BS;
             const unsigned ring_dst = ring_base + static_cast<unsigned>(((p - first) % a.R) * BS * sizeof(T));
             T own[BS], fin[BS];
@@ -290,13 +305,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_cluster_sweep(ClusterArg
                 own[c] = valid ? a.in[o + c] : T(0);
                 fin[c] = BACKWARD && valid ? a.inv[o + c] : T(1);
             }
-            if constexpr (!BACKWARD) {
-                const int b = valid ? a.rowptr[row] : 0, d = valid ? a.diagpos[row] : 0;
-                cluster_row<T, BS, 0>(valid, own, a, a.out, b, d, fin, a.out + o, ring_dst, ring_base);
-            } else {
-                const int d = valid ? a.diagpos[row] : 0, end = valid ? a.rowptr[row + 1] : 0;
-                cluster_row<T, BS, 1>(valid, own, a, a.out, d + 1, end, fin, a.out + o, ring_dst, ring_base);
-            }
+            if constexpr (!BACKWARD)
+                cluster_row<T, BS, 0>(valid, own, a, a.out, rec.y, rec.z, fin, a.out + o, ring_dst, ring_base);
+            else
+                cluster_row<T, BS, 1>(valid, own, a, a.out, rec.y, rec.z, fin, a.out + o, ring_dst, ring_base);
         }
         // Reset the slots of this CTA's next-epoch rows (their previous rows
         // are two epochs old) and the next epoch's ticket.
@@ -335,6 +347,7 @@ bool launch_cluster(Context& c, const ClusterSweep& s, ClusterArgs<T> a)
         return false;
     }
     a.rows = s.rows.as<int>();
+    a.recs = s.recs.as<int4>();
     a.task_ptr = s.task_ptr.as<int>();
     a.epoch_task = s.epoch_task.as<int>();
     a.cta_first = s.cta_first.as<int>();
@@ -502,6 +515,13 @@ void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::
         s.E = E;
         s.R = R;
         s.tasks = static_cast<int>(tasks.size());
+        std::vector<int4> recs(rows.size());
+        for (std::size_t q = 0; q < rows.size(); ++q) {
+            const auto r = static_cast<std::size_t>(rows[q]);
+            recs[q] = backward ? int4{rows[q], diagpos[r] + 1, rowptr[r + 1], 0}
+                               : int4{rows[q], rowptr[r], diagpos[r], 0};
+        }
+        s.recs = upload(ctx.stream, recs);
         s.rows = upload(ctx.stream, rows);
         s.task_ptr = upload(ctx.stream, task_ptr);
         s.epoch_task = upload(ctx.stream, epoch_task);

@@ -183,7 +183,7 @@ struct Sweep {
 struct ClusterSweep {
     bool ready = false;
     int C = 0, K = 0, E = 0, R = 0, tasks = 0;
-    DeviceBuffer rows, task_ptr, epoch_task, cta_first;
+    DeviceBuffer rows, recs, task_ptr, epoch_task, cta_first;
 };
 
 struct Preconditioner {

@@ -135,3 +135,21 @@ def test_bindings_marshal_with_null_handles(native):
             call()
     assert native.Learned.parameter_count() == 64 * 16 + 4 * 64 * 128 + 8 * 64
     b.h = net.h = None
+
+
+def test_mesh_points_program_is_deterministic(problems):
+    """lib/owtk_meshgen (a child process, so a reader maps no project library)
+    gives the same Poisson-disk points for a seed, inside the domain and at
+    least the sampling radius apart."""
+    a = problems.poisson_disk(3000, "square", 11)
+    b = problems.poisson_disk(3000, "square", 11)
+    np.testing.assert_array_equal(a, b)
+    assert 2000 < a.shape[0] < 4000
+    assert np.all((a >= 0) & (a < 1))
+    from scipy.spatial import cKDTree
+    radius = np.sqrt(0.616 / 3000)
+    d, _ = cKDTree(a).query(a, k=2)
+    assert d[:, 1].min() >= radius * (1 - 1e-12)
+    disk = problems.poisson_disk(2000, "disk", 3)
+    assert np.all(np.hypot(disk[:, 0], disk[:, 1]) < 1)
+    assert not np.array_equal(problems.poisson_disk(3000, "square", 12), a)
