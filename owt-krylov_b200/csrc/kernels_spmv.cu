@@ -576,7 +576,9 @@ void launch_bulk_bs(Context& c, const SpmvArgs<T>& a, const Matrix& m)
     case 1: launch_bulk<T, KIND, 1>(c, a, m); break;
     case 2: launch_bulk<T, KIND, 2>(c, a, m); break;
     case 3: launch_bulk<T, KIND, 3>(c, a, m); break;
-    case 4: launch_bulk<T, KIND, 4>(c, a, m); break;
+    // bs 4: entry-major products put a thread's 4 staged values 32 bytes
+    // apart, four threads per bank group (4-way conflicts on every access);
+    // the value-major generic path is conflict-free.
     default: launch_bulk<T, KIND, 0>(c, a, m); break;
     }
 }
