@@ -63,7 +63,7 @@ def parse(argv=None):
     p.add_argument("--bs", default="3", help="block sizes of the kernel sweep, comma separated")
     p.add_argument("--orders", default="rcm", help="vertex orders of the kernel sweep: rcm,hilbert")
     p.add_argument("--only", default="", help="kernel sweep: comma-separated subset of "
-                   "spmv,split,spmv32,dense,dense32,ilu,ssor,dot,norm,axpy,gnn (default) and fgmres_learned")
+                   "spmv,split,spmv32,dense,dense32,ilu,ssor,dot,norm,axpy,gnn (default), fgmres_jacobi and fgmres_learned")
     p.add_argument("--reps", type=int, default=20, help="kernel sweep: timed launches per kernel")
     p.add_argument("--form", choices=["learned", "plain", "mixed", "batching"], default="learned",
                    help="learned: the headline (8M anisotropic, learned FGMRES vs plain FP64 ILU(0)-GMRES); "
@@ -712,7 +712,7 @@ def run_kernels(args):
     only = set(filter(None, args.only.split(","))) or {"spmv", "split", "spmv32", "dense", "dense32", "ilu", "ssor",
                                                         "dot", "norm", "axpy", "gnn"}
     t = time.time()
-    xy, edges = problems.disk_mesh(args.vertices, args.seed)
+    xy, edges = cached_mesh(args.vertices, args.seed, "disk")
     gen_s = time.time() - t
     ctx = native.Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
@@ -810,6 +810,29 @@ def run_kernels(args):
                 us = timed(lambda: net.apply(x, y), max(2, args.reps // 2))
                 emit("gnn", us, per_vertex * n, tensor_tflops=round(flops / (us * 1e-6) / 1e12, 2),
                      note="one learned-preconditioner application (65 kFLOP on the tensor cores vs ~1.3 kB per vertex)")
+            if "fgmres_jacobi" in only:
+                # FGMRES(30) + Jacobi, 14 iterations fixed: the Gram-Schmidt
+                # kernels with one SpMV and one element-wise apply per
+                # iteration.  Algorithmic bytes: per iteration k (1..14) the
+                # basis dots read w and k basis vectors, the fused second pass
+                # reads k + 1 and writes w, the last pass reads k + 1 and
+                # writes V_k (3k + 5 vector passes); the SpMV; Jacobi reads
+                # two vectors and writes one.
+                pj = native.Preconditioner(m, native.PC_JACOBI, 0)
+                xs = native.Vector(ctx, n, 0, bs)
+                ws = native.Workspace(ctx)
+                opts = native.default_options(relative_tolerance=0.0, maximum_iterations=14, restart=30)
+
+                def solve_j():
+                    xs.fill(0.0)
+                    native.solve(native.FGMRES, m, pj, x, xs, opts, ws)
+
+                vec = n * bs * 8
+                gs_bytes = sum((3 * k + 5) * vec for k in range(1, 15))
+                us = timed(solve_j, max(2, args.reps // 4))
+                emit("fgmres_jacobi", us, gs_bytes + 14 * (kernel_bytes("spmv", n, bs, nnz) + 3 * vec),
+                     iterations=14, gram_schmidt_bytes=gs_bytes,
+                     note="FGMRES(30) + Jacobi, 14 iterations: Gram-Schmidt, SpMV and Jacobi bytes over the solve")
             if "fgmres_learned" in only and bs <= 8:
                 # One FGMRES solve with the (untrained) network and the ILU(0)
                 # fallback, 14 iterations fixed: the per-iteration mix of

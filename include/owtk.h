@@ -183,6 +183,15 @@ owtk_status owtk_pc_levels(owtk_preconditioner* pc, int32_t* lower_level, int32_
 owtk_status owtk_pc_sweep_schedule(owtk_preconditioner* pc, int32_t* cluster_ctas, int32_t* epoch_levels,
                                    int32_t* ring_rows);
 
+/* Whether an ILU preconditioner's applies run as the chain sweep (no
+ * reference counterpart): *windows > 0 (the number of row windows) when both
+ * factor DAGs average fewer than 8 rows per level, as on a Hilbert-curve
+ * order, and the applies run one warp per component through windows of up
+ * to 32 consecutive rows; 0 otherwise.  The same bits either way.  The
+ * environment variable OWTK_CHAIN_SWEEP=0 at preconditioner creation turns
+ * it off. */
+owtk_status owtk_pc_chain_schedule(owtk_preconditioner* pc, int32_t* windows);
+
 /* ---- host setup (ordering.hpp) -------------------------------------------- */
 /* reverse_cuthill_mckee_order (ordering.hpp:138-180); new_to_old[owned]. */
 owtk_status owtk_rcm_order(size_t owned_nodes, size_t ghost_nodes, const uint64_t* row_offsets,

@@ -249,6 +249,9 @@ void ilu_symbolic(Preconditioner& p, const Matrix& m, std::size_t fill)
     build_sweep(*p.ctx, p.lower, n, p.bs, lower_level, false);
     build_sweep(*p.ctx, p.upper, n, p.bs, upper_level, true);
     if (!p.block) {
+        build_chain_sweep(*p.ctx, p.chain, n, p.lower.depth, p.upper.depth, p.f_rowptr);
+    }
+    if (!p.block && !p.chain.ready) {
         std::vector<std::uint32_t> loc;
         build_cluster_sweep(*p.ctx, p.c_lower, n, p.bs, m.dtype, lower_level, p.f_rowptr, p.f_cols, p.f_diagpos,
                             false, loc);
@@ -1435,6 +1438,14 @@ owtk_status owtk_pc_sweep_schedule(owtk_preconditioner* pc, int32_t* cluster_cta
         if (cluster_ctas) *cluster_ctas = on ? pc->c_lower.C : 0;
         if (epoch_levels) *epoch_levels = on ? pc->c_lower.K : 0;
         if (ring_rows) *ring_rows = on ? std::max(pc->c_lower.R, pc->c_upper.R) : 0;
+    });
+}
+
+owtk_status owtk_pc_chain_schedule(owtk_preconditioner* pc, int32_t* windows)
+{
+    return guarded([&] {
+        require(pc != nullptr, "null handle");
+        if (windows) *windows = pc->chain.ready ? pc->chain.count : 0;
     });
 }
 

@@ -523,8 +523,14 @@ __global__ void __launch_bounds__(kThreads) k_multidot(std::size_t n, int k, Ptr
 // and over-CTA sums follow k_multidot on the pairs (x, V_j) and (x, x); the
 // results agree with it to FP64 rounding (a few ulps, measured), not always
 // bit for bit, so a caller keeps to one of the two kernels for a given dot.
+#ifndef OWTK_GS_BLOCKS
+#define OWTK_GS_BLOCKS 2
+#endif
+#ifndef OWTK_GS_U
+#define OWTK_GS_U 2
+#endif
 template<class T, int G>
-__global__ void __launch_bounds__(kThreads, 2) k_basis_dots(std::size_t n, int k, PtrPack basis,
+__global__ void __launch_bounds__(kThreads, OWTK_GS_BLOCKS) k_basis_dots(std::size_t n, int k, PtrPack basis,
                                                          const T* __restrict__ x, double* partials, unsigned* ticket,
                                                          double* out_dev, double* out_host)
 {
@@ -535,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_basis_dots(std::size_t n, int k
     double self = 0.0;
     const T* const* bp = reinterpret_cast<const T* const*>(basis.p);
     // U elements per pass, all loads first (the basis is read-only here).
-    constexpr int U = G <= 16 ? 2 : 1;
+    constexpr int U = G <= 16 ? OWTK_GS_U : 1;
     for (std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i0 < n; i0 += U * stride) {
         T xv[U], vj[U][G - 1];
 #pragma unroll
@@ -582,7 +588,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_basis_dots(std::size_t n, int k
 // w -= V h (reference axpy order), then dots of the updated w with every V_j
 // and w.w, in one pass over V (second Gram-Schmidt pass, krylov_solvers.hpp:310-322).
 template<class T, int G>
-__global__ void __launch_bounds__(kThreads, 2) k_cgs_update_dot(std::size_t n, int k, PtrPack basis,
+__global__ void __launch_bounds__(kThreads, OWTK_GS_BLOCKS) k_cgs_update_dot(std::size_t n, int k, PtrPack basis,
                                                              const double* __restrict__ h, T* __restrict__ w,
                                                              double* partials, unsigned* ticket,
                                                              double* out_dev, double* out_host)
@@ -598,7 +604,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_cgs_update_dot(std::size_t n, i
     for (int j = 0; j < G - 1; ++j) coef[j] = j < k ? -static_cast<T>(h[j]) : T(0);
     // U elements per pass, all loads first; each basis value is read once
     // (read-only path), for the update and for its dot.
-    constexpr int U = G <= 16 ? 2 : 1;
+    constexpr int U = G <= 16 ? OWTK_GS_U : 1;
     for (std::size_t i0 = static_cast<std::size_t>(blockIdx.x) * kThreads + threadIdx.x; i0 < n; i0 += U * stride) {
         T wv[U], vj[U][G - 1];
 #pragma unroll

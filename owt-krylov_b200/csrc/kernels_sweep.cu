@@ -843,6 +843,7 @@ template<class T> void fill_sentinel(Context& c, std::size_t n, T* x)
 // vector, so in == out is allowed: `in` is fully read before `out` is reset.
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out)
 {
+    if (chain_ilu_apply<T>(c, p, in, out)) return;
     if (cluster_ilu_apply<T>(c, p, in, out)) return;
     SweepArgs<T> a{};
     a.rowptr = p.d_frowptr.as<int>();

@@ -186,6 +186,16 @@ struct ClusterSweep {
     DeviceBuffer rows, recs, task_ptr, epoch_task, cta_first;
 };
 
+// The ILU applies of a near-sequential DAG by one warp per component
+// (kernels_chain_sweep.cu): windows of up to 32 consecutive rows.
+struct ChainSweep {
+    bool ready = false;
+    int count = 0;
+    DeviceBuffer windows;   // int4 {first row, end row, first entry, end entry}
+};
+// Rows per level (both DAGs) below which the ILU applies take the chain sweep.
+constexpr int kChainRowsPerLevel = 8;
+
 struct Preconditioner {
     Context* ctx = nullptr;
     owtk_pc_kind kind = OWTK_PC_IDENTITY;
@@ -210,6 +220,7 @@ struct Preconditioner {
     // Cluster schedules of the ILU applies and, per factor entry, where its
     // dependency is read (owner CTA and ring slot, or global memory).
     ClusterSweep c_lower, c_upper;
+    ChainSweep chain;
     DeviceBuffer d_floc;
     DeviceBuffer flags;        // uint32 per row, epoch-stamped
     DeviceBuffer ticket;       // uint64 monotone task counter
@@ -250,6 +261,8 @@ void levels_of(std::size_t owned, const std::int32_t* rowptr, const std::int32_t
                std::vector<std::int32_t>& lower, std::vector<std::int32_t>& upper);
 void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
                  const std::vector<std::int32_t>& level, bool descending_rows);
+void build_chain_sweep(Context& ctx, ChainSweep& s, std::size_t owned, int depth_lower, int depth_upper,
+                       const std::vector<std::int32_t>& rowptr);
 void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::size_t bs, owtk_dtype dtype,
                          const std::vector<std::int32_t>& level, const std::vector<std::int32_t>& rowptr,
                          const std::vector<std::int32_t>& cols, const std::vector<std::int32_t>& diagpos,
@@ -332,6 +345,7 @@ template<class T> void gather_values(Context& c, std::size_t entries, std::size_
 template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* matrix_values);
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
 template<class T> bool cluster_ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
+template<class T> bool chain_ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
 // Test hook: a sweep whose only dependency is never published (bounded wait).
 void debug_unpublished_dependency(Context& c, int spin_limit);
 template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T* out);

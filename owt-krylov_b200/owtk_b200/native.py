@@ -149,6 +149,7 @@ def lib():
             "owtk_solve_specwave": (c_int, [c_int, vp, vp, vp, POINTER(SolverOptions), vp, POINTER(SolverResult)]),
             "owtk_debug_unpublished_dependency": (c_int, [vp, ctypes.c_uint32]),
             "owtk_pc_sweep_schedule": (c_int, [vp, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
+            "owtk_pc_chain_schedule": (c_int, [vp, POINTER(c_int32)]),
             "owtk_permutation_create": (c_int, [vp, sz, vp, POINTER(vp)]),
             "owtk_permutation_destroy": (c_int, [vp]),
             "owtk_vector_permute": (c_int, [vp, vp, vp, c_int]),
@@ -436,6 +437,12 @@ class Preconditioner:
         c, k, r = c_int32(), c_int32(), c_int32()
         check(lib().owtk_pc_sweep_schedule(self.h, ctypes.byref(c), ctypes.byref(k), ctypes.byref(r)))
         return c.value, k.value, r.value
+
+    def chain_windows(self):
+        """Row windows of the chain sweep (0: the applies take another sweep)."""
+        w = c_int32()
+        check(lib().owtk_pc_chain_schedule(self.h, ctypes.byref(w)))
+        return w.value
 
     def levels(self):
         m = self.matrix
