@@ -58,9 +58,18 @@ def split_of(case):
     return off_rp, ci[~is_diag].copy(), diag.reshape(-1), v[~is_diag].reshape(-1).copy()
 
 
-def dense_case(side, bs, seed):
+def dense_case(side, bs, seed, hub=0):
+    """Dense bs x bs blocks on a side x side lattice, or with hub > 0 on a
+    star plus a path over `hub` vertices: row 0 couples to every row, so its
+    block row (hub * bs * bs values) is longer than one SpMV tile stages."""
     rng = np.random.default_rng(seed)
-    xy, edges = problems.lattice(side, side, 0.2, rng)
+    if hub:
+        xy = rng.uniform(0.0, 1.0, size=(hub, 2))
+        star = np.stack([np.zeros(hub - 1, np.int64), np.arange(1, hub)], axis=1)
+        path = np.stack([np.arange(1, hub - 1), np.arange(2, hub)], axis=1)
+        edges = np.concatenate([star, path])
+    else:
+        xy, edges = problems.lattice(side, side, 0.2, rng)
     s = problems.dense_block_system(xy, edges, bs, rng)
     x = rng.uniform(-1.0, 1.0, size=s.owned * bs)
     return dict(owned=s.owned, ghost=0, bs=bs, rowptr=s.rowptr, cols=s.cols, vals=s.vals, x=x, rhs=s.rhs)
@@ -77,7 +86,9 @@ SPMV_CASES = {
     "long_rows_bs4": (unsorted_case, dict(n=600, bs=4, seed=17, ghosts=0, extra=1500)),
 }
 ILU_CASES = ["lattice8_bs3", "lattice7_bs1_ghost", "lattice6_bs5_ghost", "unsorted30_bs33"]
-DENSE_CASES = {"dense5_bs3": dict(side=5, bs=3, seed=18), "dense4_bs2": dict(side=4, bs=2, seed=19)}
+DENSE_CASES = {"dense5_bs3": dict(side=5, bs=3, seed=18), "dense4_bs2": dict(side=4, bs=2, seed=19),
+               "dense4_bs4": dict(side=4, bs=4, seed=20), "dense4_bs5": dict(side=4, bs=5, seed=22),
+               "dense_hub300_bs3": dict(side=0, bs=3, seed=23, hub=300)}
 
 
 def build(name):
