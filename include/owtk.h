@@ -178,8 +178,9 @@ owtk_status owtk_pc_levels(owtk_preconditioner* pc, int32_t* lower_level, int32_
  * that many CTAs (dependency values through distributed shared memory, epochs
  * of epoch_levels levels, ring_rows rows of results per CTA), 0 for the
  * level-scheduled sweep over the whole GPU.  Both give the same bits.  The
- * environment variable OWTK_CLUSTER_SWEEP=0 at preconditioner creation
- * selects the level-scheduled sweep. */
+ * cluster schedule is opt-in (environment variable OWTK_CLUSTER_SWEEP=1 at
+ * preconditioner creation): on a 2M-vertex RCM-ordered mesh it measured
+ * slower than the level-scheduled sweep. */
 owtk_status owtk_pc_sweep_schedule(owtk_preconditioner* pc, int32_t* cluster_ctas, int32_t* epoch_levels,
                                    int32_t* ring_rows);
 

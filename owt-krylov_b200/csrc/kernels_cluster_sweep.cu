@@ -40,6 +40,12 @@
 // Per (row, component) the arithmetic is the reference's, term by term in
 // entry order with explicit rounding, so results equal the CPU path bit for
 // bit.
+//
+// Status: opt-in (OWTK_CLUSTER_SWEEP=1 when the preconditioner is created).
+// On the 2M-vertex RCM-ordered disk mesh (bs 3, 2 x 2913 levels) one
+// cluster cannot keep enough rows in flight: an ILU(0) apply took 7.8 ms with
+// tasks of 32/bs rows and 19.7 ms with one row per lane, against 5.0 ms for
+// the level-scheduled sweep over the whole GPU, which stays the default.
 
 #include <cuda.h>
 
@@ -415,7 +421,7 @@ void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::
 {
     s = ClusterSweep{};
     const char* env = std::getenv("OWTK_CLUSTER_SWEEP");
-    if (env && std::atoi(env) == 0) return;
+    if (env == nullptr || std::atoi(env) == 0) return;   // opt-in: slower than the level-scheduled sweep
     const std::size_t n = owned;
     if (n < 4096 || bs == 0 || bs > 4) return;
     const std::size_t es = dtype == OWTK_F64 ? 8 : 4;

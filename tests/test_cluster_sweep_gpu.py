@@ -1,13 +1,24 @@
 """ILU(k) applies on one thread-block cluster (dependency values through
-distributed shared memory, kernels_cluster_sweep.cu) against the oracle and
-against the level-scheduled sweep: the same bits, FP64 and FP32, block sizes
-1-4, fill levels 0 and 1, in place and out of place."""
+distributed shared memory, kernels_cluster_sweep.cu; opt-in with
+OWTK_CLUSTER_SWEEP=1) against the oracle and against the default
+level-scheduled sweep: the same bits, FP64 and FP32, block sizes 1-4, fill
+levels 0 and 1, in place and out of place."""
 import numpy as np
 import pytest
 
 from conftest import assert_bitwise
 
 pytestmark = pytest.mark.gpu
+
+
+def _pair(native, m, fill, monkeypatch):
+    """The cluster sweep is opt-in (OWTK_CLUSTER_SWEEP=1 at creation): one
+    preconditioner on it and one on the default level-scheduled sweep."""
+    monkeypatch.setenv("OWTK_CLUSTER_SWEEP", "1")
+    pc = native.Preconditioner(m, native.PC_ILU, fill)
+    monkeypatch.delenv("OWTK_CLUSTER_SWEEP")
+    plain = native.Preconditioner(m, native.PC_ILU, fill)
+    return pc, plain
 
 
 def _system(problems, side, bs, order, seed):
@@ -22,12 +33,9 @@ def test_cluster_ilu_apply_bitwise(native, ctx, restatement, problems, monkeypat
     s = _system(problems, side, bs, order, 31 + side)
     n = s.owned
     m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
-    pc = native.Preconditioner(m, native.PC_ILU, fill)
+    pc, plain = _pair(native, m, fill, monkeypatch)
     ctas, k, ring = pc.sweep_schedule()
     assert ctas in (8, 16) and k >= 2 and ring > 0, (ctas, k, ring)
-    monkeypatch.setenv("OWTK_CLUSTER_SWEEP", "0")
-    plain = native.Preconditioner(m, native.PC_ILU, fill)
-    monkeypatch.delenv("OWTK_CLUSTER_SWEEP")
     assert plain.sweep_schedule()[0] == 0
     x = np.random.default_rng(side).uniform(-1, 1, n * bs)
     xv = native.Vector(ctx, n, 0, bs).upload(x)
@@ -49,11 +57,8 @@ def test_cluster_ilu_apply_fp32(native, ctx, problems, monkeypatch):
     s = _system(problems, 150, 3, "rcm", 77)
     n, bs = s.owned, s.bs
     m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals, dtype=np.float32)
-    pc = native.Preconditioner(m, native.PC_ILU, 0)
+    pc, plain = _pair(native, m, 0, monkeypatch)
     assert pc.sweep_schedule()[0] in (8, 16)
-    monkeypatch.setenv("OWTK_CLUSTER_SWEEP", "0")
-    plain = native.Preconditioner(m, native.PC_ILU, 0)
-    monkeypatch.delenv("OWTK_CLUSTER_SWEEP")
     x = np.random.default_rng(3).uniform(-1, 1, n * bs).astype(np.float32)
     xv = native.Vector(ctx, n, 0, bs, dtype=np.float32).upload(x)
     y1 = native.Vector(ctx, n, 0, bs, dtype=np.float32)
@@ -68,10 +73,7 @@ def test_cluster_solve_matches_plain_sweep(native, ctx, problems, monkeypatch):
     s = _system(problems, 170, 3, "rcm", 5)
     n, bs = s.owned, s.bs
     m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
-    pc = native.Preconditioner(m, native.PC_ILU, 0)
-    monkeypatch.setenv("OWTK_CLUSTER_SWEEP", "0")
-    plain = native.Preconditioner(m, native.PC_ILU, 0)
-    monkeypatch.delenv("OWTK_CLUSTER_SWEEP")
+    pc, plain = _pair(native, m, 0, monkeypatch)
     b = native.Vector(ctx, n, 0, bs).upload(s.rhs)
     x1, x2 = native.Vector(ctx, n, 0, bs), native.Vector(ctx, n, 0, bs)
     r1 = native.solve(native.FGMRES, m, pc, b, x1)
