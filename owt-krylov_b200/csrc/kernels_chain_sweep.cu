@@ -48,9 +48,10 @@ namespace {
 
 using namespace dev;
 
-constexpr int kRing = 8192;         // results kept in shared memory (rows)
-constexpr int kStageEntries = 1024; // factor entries staged per window
-constexpr int kStages = 3;          // windows in flight: phase A, far values, rows
+constexpr int kRing = 8192;        // results kept in shared memory (rows)
+constexpr int kStageEntries = 512; // factor entries staged per window
+constexpr int kStages = 5;         // windows staged: rows 4 ahead, far values 2 ahead
+constexpr int kRec = 4;            // terms per row held in a record (more: the row's list is walked)
 
 template<class T>
 struct ChainArgs {
@@ -77,14 +78,25 @@ struct Stage {
     T inv[32];
 };
 
+// One row of the window as the sequential phase consumes it.  Forward: `pre`
+// is the input minus the terms before the window, the slots the in-window
+// terms (factor, column - r0).  Backward: `pre` is y, the slots all of the
+// row's terms in column order: in-window (factor, column - r0) or beyond the
+// window (the rounded product, tag -1).  cnt > kRec: walk the row's list.
+template<class T>
+struct Rec {
+    T pre, inv;
+    T v[kRec];
+    int tags;               // kRec signed bytes
+    int cnt;
+};
+
 template<class T>
 struct ChainSmem {
     T ring[kRing];
     Stage<T> stage[kStages];
-    T ftab[32][33];          // [step][lane]: factor of the lane's term on that step's row
-    T ptab[kStageEntries];   // backward: rounded products u * x, by entry
-    short etab[32][32];      // backward: [step][lane] entry of that term
-    int chain_begin[32], chain_count[32], chain_next[32];
+    Rec<T> rec[32];
+    T win[32];              // the window's results, in step order
 };
 
 __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes)
@@ -97,8 +109,10 @@ __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ bool staged(const int4& w) { return w.w - w.z <= kStageEntries; }
+__device__ __forceinline__ int tag_of(int tags, int k) { return static_cast<signed char>((tags >> (8 * k)) & 0xff); }
 
 // Rows, offsets, inputs of window w into stage s (nothing for a window with
 // more entries than a stage holds: it is read from global memory).
@@ -139,38 +153,46 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
     extern __shared__ __align__(16) unsigned char chain_smem_raw[];
     ChainSmem<T>& S = *reinterpret_cast<ChainSmem<T>*>(chain_smem_raw);
     const int c = blockIdx.x, lane = threadIdx.x;
-    const unsigned full = 0xffffffffu;
     const int W = a.count;
     // Window of processing step i (ascending forward, descending backward).
     const auto window = [&](int i) {
         if (i >= W) return make_int4(0, 0, 0, 0);
         return __ldg(a.windows + (BACKWARD ? W - 1 - i : i));
     };
-    int4 w0 = window(0), w1 = window(1), w2 = window(2);
-    stage_rows<T, BACKWARD>(a, S.stage[0], w0, c, lane);
+    // Descriptors of windows i .. i+4 (d[0] is the current one).
+    int4 d0 = window(0), d1 = window(1), d2 = window(2), d3 = window(3), d4 = window(4);
+    // Prologue: rows of windows 0-3, then the far values of windows 0 and 1.
+    stage_rows<T, BACKWARD>(a, S.stage[0], d0, c, lane);
+    if (W > 1) stage_rows<T, BACKWARD>(a, S.stage[1], d1, c, lane);
+    if (W > 2) stage_rows<T, BACKWARD>(a, S.stage[2], d2, c, lane);
+    if (W > 3) stage_rows<T, BACKWARD>(a, S.stage[3], d3, c, lane);
     cp_async_commit();
     cp_async_wait_all();
     __syncwarp();
-    stage_far<T, BACKWARD>(a, S.stage[0], w0, c, lane);
-    if (W > 1) stage_rows<T, BACKWARD>(a, S.stage[1], w1, c, lane);
+    stage_far<T, BACKWARD>(a, S.stage[0], d0, c, lane);
+    if (W > 1) stage_far<T, BACKWARD>(a, S.stage[1], d1, c, lane);
     cp_async_commit();
+    cp_async_wait_all();
+    __syncwarp();
     for (int i = 0; i < W; ++i) {
-        const int4 w3 = window(i + 3);
-        cp_async_wait_all();
+        const int4 d5 = window(i + 5);
+        // Every copy group but the newest has landed: the rows of windows up
+        // to i+3 and the far values up to i+1 (issued two iterations ago).
+        cp_async_wait_one();
         __syncwarp();
-        if (i + 1 < W) stage_far<T, BACKWARD>(a, S.stage[(i + 1) % kStages], w1, c, lane);
-        if (i + 2 < W) stage_rows<T, BACKWARD>(a, S.stage[(i + 2) % kStages], w2, c, lane);
+        if (i + 2 < W) stage_far<T, BACKWARD>(a, S.stage[(i + 2) % kStages], d2, c, lane);
+        if (i + 4 < W) stage_rows<T, BACKWARD>(a, S.stage[(i + 4) % kStages], d4, c, lane);
         cp_async_commit();
 
         Stage<T>& s = S.stage[i % kStages];
-        const int r0 = w0.x, r1 = w0.y, nw = r1 - r0, e0 = w0.z;
+        const int r0 = d0.x, r1 = d0.y, nw = r1 - r0, e0 = d0.z;
         const bool live = lane < nw;
         const int r = r0 + lane;
-        T acc = live ? s.in[lane] : T(0);
-        if (!staged(w0)) {
+        if (!staged(d0)) {
             // A single row with more entries than a stage holds: its whole
             // sum here, from global memory.
             if (lane == 0) {
+                T acc = s.in[0];
                 const int b = BACKWARD ? s.diagpos[0] + 1 : s.rowptr[0];
                 const int e = BACKWARD ? s.rowptr[1] : s.diagpos[0];
                 for (int q = b; q < e; ++q) {
@@ -180,87 +202,100 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
                     acc = sub_rn(acc, mul_rn(a.vals[static_cast<long long>(q) * a.bs + c], v));
                 }
                 if (BACKWARD) acc = mul_rn(acc, s.inv[0]);
-            }
-        } else if (!BACKWARD) {
-            // ---- forward phase A: the terms before the window, in order.
-            unsigned mask = 0;
-            if (live) {
-                const int qe = s.diagpos[lane] - e0;
-                for (int q = s.rowptr[lane] - e0; q < qe; ++q) {
-                    const int col = s.cols[q];
-                    const T f = s.vals[q];
-                    if (col < r0) {
-                        const T v = col >= r0 - kRing ? S.ring[col & (kRing - 1)] : s.far[q];
-                        acc = sub_rn(acc, mul_rn(f, v));
-                    } else {
-                        S.ftab[col - r0][lane] = f;
-                        mask |= 1u << (col - r0);
-                    }
-                }
-            }
-            __syncwarp();
-            // ---- phase B: row t is final at step t.
-#pragma unroll 4
-            for (int t = 0; t < nw; ++t) {
-                const T f = S.ftab[t][lane];
-                const T yt = __shfl_sync(full, acc, t);
-                if ((mask >> t) & 1u) acc = sub_rn(acc, mul_rn(f, yt));
+                S.win[0] = acc;
             }
         } else {
-            // ---- backward phase A: products of the terms after the window;
-            // the in-window terms wait for their steps.
-            unsigned mask = 0;
+            // ---- phase A, one row per lane: the record of its row.
             if (live) {
-                const int qb = s.diagpos[lane] + 1 - e0, qe = s.rowptr[lane + 1] - e0;
+                Rec<T> rc;
+                int n = 0, tags = 0;
+                const int qb = BACKWARD ? s.diagpos[lane] + 1 - e0 : s.rowptr[lane] - e0;
+                const int qe = BACKWARD ? s.rowptr[lane + 1] - e0 : s.diagpos[lane] - e0;
+                T acc = s.in[lane];
                 for (int q = qb; q < qe; ++q) {
                     const int col = s.cols[q];
                     const T f = s.vals[q];
-                    if (col < r1) {
-                        S.ftab[col - r0][lane] = f;
-                        S.etab[col - r0][lane] = static_cast<short>(q);
-                        mask |= 1u << (col - r0);
-                    } else {
-                        const T v = col < r1 + kRing ? S.ring[col & (kRing - 1)] : s.far[q];
-                        S.ptab[q] = mul_rn(f, v);
+                    if (!BACKWARD && col < r0) {   // before the window: final, applied here in order
+                        const T v = col >= r0 - kRing ? S.ring[col & (kRing - 1)] : s.far[q];
+                        acc = sub_rn(acc, mul_rn(f, v));
+                        continue;
                     }
+                    T slot = f;
+                    int tag = col - r0;
+                    if (BACKWARD && col >= r1) {   // after the window: the product, subtracted in turn
+                        const T v = col < r1 + kRing ? S.ring[col & (kRing - 1)] : s.far[q];
+                        slot = mul_rn(f, v);
+                        tag = -1;
+                    }
+                    if (n < kRec) {
+#pragma unroll
+                        for (int k = 0; k < kRec; ++k)
+                            if (k == n) rc.v[k] = slot;
+                        tags |= (tag & 0xff) << (8 * n);
+                    }
+                    ++n;
                 }
-                S.chain_begin[lane] = qb;
-                S.chain_count[lane] = qe - qb;
-                S.chain_next[lane] = qe > qb && s.cols[qb] == r + 1 && r + 1 < r1;
+                rc.pre = acc;
+                rc.inv = BACKWARD ? s.inv[lane] : T(0);
+                rc.tags = tags;
+                rc.cnt = n;
+                S.rec[lane] = rc;
             }
             __syncwarp();
-            // ---- phase B, rows in descending order: step t sums row t's
-            // products in column order; its first, when it is row t+1's
-            // term, comes from a register (formed on the step before).
-            T pnext = T(0);
-            for (int t = nw - 1; t >= 0; --t) {
-                const int qb = S.chain_begin[t], cnt = S.chain_count[t];
-                const bool nxt = S.chain_next[t] != 0;
-                const T inv = s.inv[t];
-                if (lane == t) {
-                    int j = 0;
-                    if (nxt) {
-                        acc = sub_rn(acc, pnext);
-                        j = 1;
+            // ---- phase B: lane 0 finishes the rows in order, each from its
+            // record and the results before it (the last one in a register).
+            if (lane == 0) {
+                T last = T(0);
+                for (int j = 0; j < nw; ++j) {
+                    const int t = BACKWARD ? nw - 1 - j : j;
+                    const Rec<T> rc = S.rec[t];
+                    const int prev = BACKWARD ? t + 1 : t - 1;   // the row finished just before
+                    T acc = rc.pre;
+                    if (rc.cnt <= kRec) {
+#pragma unroll
+                        for (int k = 0; k < kRec; ++k) {
+                            if (k < rc.cnt) {
+                                const int tag = tag_of(rc.tags, k);
+                                if (BACKWARD && tag < 0) {
+                                    acc = sub_rn(acc, rc.v[k]);
+                                } else {
+                                    const T v = tag == prev ? last : S.win[tag & 31];
+                                    acc = sub_rn(acc, mul_rn(rc.v[k], v));
+                                }
+                            }
+                        }
+                    } else {
+                        // More terms than a record holds: the row's list, in order.
+                        const int qb = BACKWARD ? s.diagpos[t] + 1 - e0 : s.rowptr[t] - e0;
+                        const int qe = BACKWARD ? s.rowptr[t + 1] - e0 : s.diagpos[t] - e0;
+                        for (int q = qb; q < qe; ++q) {
+                            const int col = s.cols[q];
+                            if (!BACKWARD && col < r0) continue;   // already in rc.pre
+                            T v;
+                            if (BACKWARD && col >= r1)
+                                v = col < r1 + kRing ? S.ring[col & (kRing - 1)] : s.far[q];
+                            else
+                                v = col - r0 == prev ? last : S.win[col - r0];
+                            acc = sub_rn(acc, mul_rn(s.vals[q], v));
+                        }
                     }
-                    for (; j < cnt; ++j) acc = sub_rn(acc, S.ptab[qb + j]);
-                    acc = mul_rn(acc, inv);
-                }
-                const T xt = __shfl_sync(full, acc, t);
-                if ((mask >> t) & 1u) {
-                    const T p = mul_rn(S.ftab[t][lane], xt);
-                    S.ptab[S.etab[t][lane]] = p;
-                    if (lane == t - 1) pnext = p;
+                    if (BACKWARD) acc = mul_rn(acc, rc.inv);
+                    S.win[t] = acc;
+                    last = acc;
                 }
             }
         }
+        __syncwarp();
         if (live) {
-            S.ring[r & (kRing - 1)] = acc;
-            a.out[static_cast<long long>(r) * a.bs + c] = acc;
+            const T y = S.win[lane];
+            S.ring[r & (kRing - 1)] = y;
+            a.out[static_cast<long long>(r) * a.bs + c] = y;
         }
-        w0 = w1;
-        w1 = w2;
-        w2 = w3;
+        d0 = d1;
+        d1 = d2;
+        d2 = d3;
+        d3 = d4;
+        d4 = d5;
     }
     cp_async_wait_all();
 }
