@@ -44,9 +44,6 @@ constexpr int kTile = 128;         // rows per tensor-core tile
 constexpr int kMmaSpin = 1 << 22;
 
 // ---------------------------------------------------------------- shared pieces
-#ifndef OWTK_GNN_FMA
-#define OWTK_GNN_FMA 0
-#endif
 __device__ __forceinline__ std::uint32_t align1024(std::uint32_t a) { return (a + 1023u) & ~1023u; }
 
 // Bounded wait on an mbarrier phase; false if it gave up.
@@ -88,23 +85,6 @@ __device__ __forceinline__ void accumulate_row(unsigned short w, const uint4& f,
             "fma.rn.f32.bf16 %1, hi, %3, %1;\n\t}"
             : "+f"(acc[k].x), "+f"(acc[k].y)
             : "r"(x[k]), "h"(w));
-}
-
-// acc += w * f for the 8 BF16 features of f, w a BF16 value held as FP32:
-// the features widen exactly (a BF16 is the high half of its FP32) and the
-// sums run as packed FP32 FMAs, lo -> .x, hi -> .y as in accumulate_row, so
-// both give the same bits.
-__device__ __forceinline__ void accumulate_row_f32(float w, const uint4& f, float2 (&acc)[4])
-{
-#if OWTK_GNN_FMA == 1
-    const float2 ww = make_float2(w, w);
-    const std::uint32_t x[4] = {f.x, f.y, f.z, f.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        acc[k] = __ffma2_rn(make_float2(__uint_as_float(x[k] << 16), __uint_as_float(x[k] & 0xffff0000u)), ww, acc[k]);
-#else
-    accumulate_row(static_cast<unsigned short>(__float_as_uint(w) >> 16), f, acc);
-#endif
 }
 
 __device__ __forceinline__ uint4 pack_bf16x8(const float2 (&acc)[4])
@@ -370,9 +350,6 @@ constexpr int kLayerSmem = 1024 + 2 * kTile * 128 + 2 * kH * 128;   // A: [h | m
 constexpr int kDecodeRows = 16;                                      // Wd padded to N = 16
 constexpr int kLayerSmemDec = kLayerSmem + kDecodeRows * 128;        // + Wd (BF16, swizzled)
 
-#ifndef OWTK_GNN_SLOTS
-#define OWTK_GNN_SLOTS 0
-#endif
 #ifndef OWTK_GNN_LDOP
 #define OWTK_GNN_LDOP ".nc"
 #endif
@@ -400,14 +377,11 @@ struct DecodeArgs {
     O* out;
 };
 
-#ifndef OWTK_GNN_BLOCKS
-#define OWTK_GNN_BLOCKS 4
-#endif
 #ifndef OWTK_GNN_DEC_BLOCKS
 #define OWTK_GNN_DEC_BLOCKS 4
 #endif
 template<bool TRAIN, bool DECODE = false, class O = float>
-__global__ void __launch_bounds__(kFwdThreads, DECODE ? OWTK_GNN_DEC_BLOCKS : OWTK_GNN_BLOCKS)
+__global__ void __launch_bounds__(kFwdThreads, DECODE ? OWTK_GNN_DEC_BLOCKS : 4)
     k_gnn_layer(GraphArgs g, const __grid_constant__ CUtensorMap tmap_in, const __grid_constant__ CUtensorMap tmap_out,
                 const bf16* __restrict__ h_in, const bf16* __restrict__ wl, bf16* __restrict__ m_out,
                 unsigned long long* __restrict__ mask_out, DecodeArgs<O> dec, unsigned* status)
@@ -484,7 +458,6 @@ __global__ void __launch_bounds__(kFwdThreads, DECODE ? OWTK_GNN_DEC_BLOCKS : OW
         // Lane `chunk` of a group loads the row's slot `chunk` (index and
         // weight, two row steps ahead of its first gather) and shares it by
         // shuffles.
-#if OWTK_GNN_SLOTS == 0
         const int first = row0 + kRowsPerWarp * warp + grp;
         const auto ell_at = [&](int s) { return static_cast<long long>(min(first + 4 * s, g.n - 1)) * kEll + chunk; };
         constexpr int kQuarters = 4 * kRowSteps;
@@ -551,77 +524,6 @@ __global__ void __launch_bounds__(kFwdThreads, DECODE ? OWTK_GNN_DEC_BLOCKS : OW
                 *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, chunk)) = mv;
             }
         }
-#else
-        const int first = row0 + kRowsPerWarp * warp + grp;
-        constexpr int kQuarters = 4 * kRowSteps;
-        // A padding slot loads nothing (weight 0): it keeps a chunk gathered
-        // earlier in this tile or these zeros.
-        uint4 ring[kGatherDepth + 1][2];
-#pragma unroll
-        for (int i = 0; i <= kGatherDepth; ++i) ring[i][0] = ring[i][1] = make_uint4(0, 0, 0, 0);
-        // Every lane of a group loads its row's whole slot list (8 indices and
-        // 8 BF16 weights, 48 bytes shared by the group's 8 lanes) two row steps
-        // ahead of its first gather, into a ring of two row steps.
-        int4 sc[2][2];
-        uint4 sw[2];
-        const auto load_slots = [&](int s) {
-            const long long v = min(first + 4 * s, g.n - 1);
-            const int4* pc = reinterpret_cast<const int4*>(g.ell_col + v * kEll);
-            sc[s & 1][0] = __ldg(pc);
-            sc[s & 1][1] = __ldg(pc + 1);
-            sw[s & 1] = __ldg(reinterpret_cast<const uint4*>(g.ell_w + v * kEll));
-        };
-        const auto slot_col = [&](int s, int q) {
-            const int4 c = sc[s & 1][q >> 2];
-            return (q & 3) == 0 ? c.x : (q & 3) == 1 ? c.y : (q & 3) == 2 ? c.z : c.w;
-        };
-        const auto slot_w = [&](int s, int q) {   // weight bits in the high half, low half zero
-            const uint4 w = sw[s & 1];
-            const unsigned word = (q >> 1) == 0 ? w.x : (q >> 1) == 1 ? w.y : (q >> 1) == 2 ? w.z : w.w;
-            return (q & 1) ? (word & 0xffff0000u) : (word << 16);
-        };
-        const auto issue = [&](int k) {   // quarter k: slots 2*(k&3), +1 of row step k>>2
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-                load_slot(ring[k % (kGatherDepth + 1)][j], h_in, slot_col(k >> 2, 2 * (k & 3) + j), chunk);
-        };
-        static_assert(kGatherDepth >= 1 && kGatherDepth <= 4, "slot ring holds 2 row steps");
-        load_slots(0);
-        if (kRowSteps > 1) load_slots(1);
-#pragma unroll
-        for (int k = 0; k < kGatherDepth; ++k) issue(k);
-        float2 acc[4];
-#pragma unroll
-        for (int k = 0; k < kQuarters; ++k) {
-            const int kn = k + kGatherDepth;
-            if (kn < kQuarters) issue(kn);
-            const int s = k >> 2;
-            if ((k & 3) == 0)
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i] = make_float2(0.0f, 0.0f);
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-                accumulate_row_f32(__uint_as_float(slot_w(s, 2 * (k & 3) + j)), ring[k % (kGatherDepth + 1)][j], acc);
-            if ((k & 3) == 3) {
-                if (s + 2 < kRowSteps) load_slots(s + 2);   // row step s is done with ring entry s & 1
-                const int r = kRowsPerWarp * warp + 4 * s + grp, v = row0 + r;
-                if (overflow && v < g.n) {   // rows with more than 8 neighbours
-                    const int e1 = g.nb_ptr[v + 1];
-                    for (int e = g.nb_ptr[v] + kEll; e < e1; ++e)
-                        accumulate_row(__bfloat16_as_ushort(__float2bfloat16_rn(g.nb_w[e])),
-                                       __ldg(reinterpret_cast<const uint4*>(
-                                                            h_in + static_cast<long long>(g.nb_col[e]) * kH) + chunk),
-                                       acc);
-                }
-                uint4 mv = make_uint4(0, 0, 0, 0);
-                if (v < g.n) {
-                    mv = pack_bf16x8(acc);
-                    if (TRAIN) *reinterpret_cast<uint4*>(m_out + static_cast<long long>(v) * kH + chunk * 8) = mv;
-                }
-                *reinterpret_cast<uint4*>(tile + kTile * 128 + sw128(r, chunk)) = mv;
-            }
-        }
-#endif
         fence_proxy_async_smem();
         ok = wait_phase(bar_h, iter & 1);
         h_pending = !ok;
@@ -1596,7 +1498,7 @@ void gnn_forward(Gnn& G, const T* r, O* out)
               }
             }
             const CUtensorMap& tmo = TRAIN ? G.tmap_h[l + 1] : (l % 2 == 0 ? G.tmap_b : G.tmap_a);
-            gnn::k_gnn_layer<TRAIN><<<G.layer_grid(OWTK_GNN_BLOCKS), gnn::kFwdThreads, gnn::kLayerSmem, c.stream>>>(
+            gnn::k_gnn_layer<TRAIN><<<G.layer_grid(4), gnn::kFwdThreads, gnn::kLayerSmem, c.stream>>>(
                 g, tm, tmo, hin, wl, TRAIN ? G.m[l].as<gnn::bf16>() : nullptr,
                 TRAIN ? G.mask[l].as<unsigned long long>() : nullptr, gnn::DecodeArgs<float>{},
                 c.status.as<unsigned>());

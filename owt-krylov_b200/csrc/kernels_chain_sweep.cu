@@ -78,17 +78,23 @@ struct Stage {
     T inv[32];
 };
 
-// One row of the window as the sequential phase consumes it.  Forward: `pre`
-// is the input minus the terms before the window, the slots the in-window
-// terms (factor, column - r0).  Backward: `pre` is y, the slots all of the
-// row's terms in column order: in-window (factor, column - r0) or beyond the
-// window (the rounded product, tag -1).  cnt > kRec: walk the row's list.
+// One row of the window as the sequential phase consumes it, built in
+// phase A by the row's lane.  `link` is the factor of the term on the row
+// finished just before (forward: column r-1, the row's last term; backward:
+// column r+1, its first term), 0 when the row has none (`linked` false).  The
+// other terms in the window are slots: forward (factor, column - r0) before
+// the link; backward, after it, (factor, column - r0) in the window or, beyond
+// the window, (rounded product, -1).  Forward `pre` is the input minus the
+// terms before the window, backward the input (y).  cnt > kRec: the row's
+// list is walked instead.
 template<class T>
 struct Rec {
-    T pre, inv;
+    T pre, inv, link;
     T v[kRec];
     int tags;               // kRec signed bytes
-    int cnt;
+    int cnt;                // slots (the link not counted)
+    int linked;
+    int pad;
 };
 
 template<class T>
@@ -208,6 +214,8 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
             // ---- phase A, one row per lane: the record of its row.
             if (live) {
                 Rec<T> rc;
+                rc.link = T(0);
+                rc.linked = 0;
                 int n = 0, tags = 0;
                 const int qb = BACKWARD ? s.diagpos[lane] + 1 - e0 : s.rowptr[lane] - e0;
                 const int qe = BACKWARD ? s.rowptr[lane + 1] - e0 : s.diagpos[lane] - e0;
@@ -218,6 +226,11 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
                     if (!BACKWARD && col < r0) {   // before the window: final, applied here in order
                         const T v = col >= r0 - kRing ? S.ring[col & (kRing - 1)] : s.far[q];
                         acc = sub_rn(acc, mul_rn(f, v));
+                        continue;
+                    }
+                    if (col == (BACKWARD ? r + 1 : r - 1) && (BACKWARD ? col < r1 : col >= r0)) {
+                        rc.link = f;   // forward: always the last term; backward: always the first
+                        rc.linked = 1;
                         continue;
                     }
                     T slot = f;
@@ -242,35 +255,73 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
                 S.rec[lane] = rc;
             }
             __syncwarp();
-            // ---- phase B: lane 0 finishes the rows in order, each from its
-            // record and the results before it (the last one in a register).
+            // ---- phase B: lane 0 finishes the rows in order.  Step j takes
+            // the row finished before (`last`) through the current row's
+            // link; the next row's other terms, which need only older
+            // results, are formed in the same step, off that chain.
             if (lane == 0) {
                 T last = T(0);
-                for (int j = 0; j < nw; ++j) {
-                    const int t = BACKWARD ? nw - 1 - j : j;
-                    const Rec<T> rc = S.rec[t];
-                    const int prev = BACKWARD ? t + 1 : t - 1;   // the row finished just before
-                    T acc = rc.pre;
-                    if (rc.cnt <= kRec) {
+                // The row's terms other than the link, as far as they can be
+                // formed before `last` of its step is known: forward the
+                // partial sum pre - slots (all before the link), backward the
+                // products of the slots (subtracted after the link).
+                T part = T(0);
+                T prod[kRec];
+#pragma unroll
+                for (int k = 0; k < kRec; ++k) prod[k] = T(0);
+                // Terms of record rc at step j (row t), given `last` = result of
+                // the row finished at step j - 1.
+                const auto prepare = [&](const Rec<T>& rc, int t, T prev_result) {
+                    const int prev2 = BACKWARD ? t + 2 : t - 2;   // finished two steps before t
+                    if (!BACKWARD) {
+                        T acc = rc.pre;
 #pragma unroll
                         for (int k = 0; k < kRec; ++k) {
                             if (k < rc.cnt) {
                                 const int tag = tag_of(rc.tags, k);
-                                if (BACKWARD && tag < 0) {
-                                    acc = sub_rn(acc, rc.v[k]);
-                                } else {
-                                    const T v = tag == prev ? last : S.win[tag & 31];
-                                    acc = sub_rn(acc, mul_rn(rc.v[k], v));
-                                }
+                                const T v = tag == prev2 ? prev_result : S.win[tag & 31];
+                                acc = sub_rn(acc, mul_rn(rc.v[k], v));
                             }
+                        }
+                        part = acc;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < kRec; ++k) {
+                            if (k < rc.cnt) {
+                                const int tag = tag_of(rc.tags, k);
+                                const T v = tag == prev2 ? prev_result : S.win[tag & 31];
+                                prod[k] = tag < 0 ? rc.v[k] : mul_rn(rc.v[k], v);
+                            }
+                        }
+                    }
+                };
+                Rec<T> cur = S.rec[BACKWARD ? nw - 1 : 0];
+                if (cur.cnt <= kRec) prepare(cur, BACKWARD ? nw - 1 : 0, T(0));
+                for (int j = 0; j < nw; ++j) {
+                    const int t = BACKWARD ? nw - 1 - j : j;
+                    const int tn = BACKWARD ? t - 1 : t + 1;    // the next row
+                    const bool more = j + 1 < nw;
+                    const Rec<T> nxt = S.rec[more ? tn : t];
+                    T res;
+                    if (cur.cnt <= kRec) {
+                        if (!BACKWARD) {
+                            res = cur.linked ? sub_rn(part, mul_rn(cur.link, last)) : part;
+                        } else {
+                            T acc = cur.linked ? sub_rn(cur.pre, mul_rn(cur.link, last)) : cur.pre;
+#pragma unroll
+                            for (int k = 0; k < kRec; ++k)
+                                if (k < cur.cnt) acc = sub_rn(acc, prod[k]);
+                            res = mul_rn(acc, cur.inv);
                         }
                     } else {
                         // More terms than a record holds: the row's list, in order.
+                        const int prev = BACKWARD ? t + 1 : t - 1;
                         const int qb = BACKWARD ? s.diagpos[t] + 1 - e0 : s.rowptr[t] - e0;
                         const int qe = BACKWARD ? s.rowptr[t + 1] - e0 : s.diagpos[t] - e0;
+                        T acc = cur.pre;
                         for (int q = qb; q < qe; ++q) {
                             const int col = s.cols[q];
-                            if (!BACKWARD && col < r0) continue;   // already in rc.pre
+                            if (!BACKWARD && col < r0) continue;   // already in pre
                             T v;
                             if (BACKWARD && col >= r1)
                                 v = col < r1 + kRing ? S.ring[col & (kRing - 1)] : s.far[q];
@@ -278,10 +329,14 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
                                 v = col - r0 == prev ? last : S.win[col - r0];
                             acc = sub_rn(acc, mul_rn(s.vals[q], v));
                         }
+                        res = BACKWARD ? mul_rn(acc, cur.inv) : acc;
                     }
-                    if (BACKWARD) acc = mul_rn(acc, rc.inv);
-                    S.win[t] = acc;
-                    last = acc;
+                    // The next row's terms: they reach back two rows at most
+                    // to `last` (the row before this one), older ones are in win.
+                    if (more && nxt.cnt <= kRec) prepare(nxt, tn, last);
+                    S.win[t] = res;
+                    last = res;
+                    cur = nxt;
                 }
             }
         }
