@@ -34,6 +34,14 @@
 //
 // There is no wait on another thread's progress anywhere: the only waits are
 // for this warp's own cp.async copies.
+//
+// Measured on the 2M-vertex Hilbert-ordered disk mesh: 724 ms per apply
+// against 1.94 s for the level-scheduled sweep.  A warp alone on its SM
+// issues an instruction about every 5.5 cycles (waits on the previous
+// result, on shared memory and on shuffles), so the cost is the instruction
+// count per row: 29 forward, 102 backward.  Two forms with lane 0 running the
+// rows from per-row records (plain, and software-pipelined) were slower:
+// 1071 and 1113 ms.
 
 #include <algorithm>
 #include <cstdint>
@@ -48,10 +56,10 @@ namespace {
 
 using namespace dev;
 
-constexpr int kRing = 8192;        // results kept in shared memory (rows)
-constexpr int kStageEntries = 512; // factor entries staged per window
-constexpr int kStages = 5;         // windows staged: rows 4 ahead, far values 2 ahead
-constexpr int kRec = 4;            // terms per row held in a record (more: the row's list is walked)
+constexpr int kRing = 8192;         // results kept in shared memory (rows)
+constexpr int kStageEntries = 1024; // factor entries staged per window
+constexpr int kStages = 3;          // windows in flight: phase A, far values, rows
+constexpr int kChain = 5;           // backward: terms of a row held in registers
 
 template<class T>
 struct ChainArgs {
@@ -78,31 +86,14 @@ struct Stage {
     T inv[32];
 };
 
-// One row of the window as the sequential phase consumes it, built in
-// phase A by the row's lane.  `link` is the factor of the term on the row
-// finished just before (forward: column r-1, the row's last term; backward:
-// column r+1, its first term), 0 when the row has none (`linked` false).  The
-// other terms in the window are slots: forward (factor, column - r0) before
-// the link; backward, after it, (factor, column - r0) in the window or, beyond
-// the window, (rounded product, -1).  Forward `pre` is the input minus the
-// terms before the window, backward the input (y).  cnt > kRec: the row's
-// list is walked instead.
-template<class T>
-struct Rec {
-    T pre, inv, link;
-    T v[kRec];
-    int tags;               // kRec signed bytes
-    int cnt;                // slots (the link not counted)
-    int linked;
-    int pad;
-};
-
 template<class T>
 struct ChainSmem {
     T ring[kRing];
     Stage<T> stage[kStages];
-    Rec<T> rec[32];
-    T win[32];              // the window's results, in step order
+    T ftab[32][33];          // [step][lane]: factor of the lane's term on that step's row
+    T ptab[kStageEntries];   // backward: rounded products u * x, by entry
+    short etab[32][32];      // backward: [step][lane] entry of that term
+    int chain_begin[32], chain_count[32];
 };
 
 __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes)
@@ -115,10 +106,8 @@ __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ bool staged(const int4& w) { return w.w - w.z <= kStageEntries; }
-__device__ __forceinline__ int tag_of(int tags, int k) { return static_cast<signed char>((tags >> (8 * k)) & 0xff); }
 
 // Rows, offsets, inputs of window w into stage s (nothing for a window with
 // more entries than a stage holds: it is read from global memory).
@@ -159,46 +148,38 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
     extern __shared__ __align__(16) unsigned char chain_smem_raw[];
     ChainSmem<T>& S = *reinterpret_cast<ChainSmem<T>*>(chain_smem_raw);
     const int c = blockIdx.x, lane = threadIdx.x;
+    const unsigned full = 0xffffffffu;
     const int W = a.count;
     // Window of processing step i (ascending forward, descending backward).
     const auto window = [&](int i) {
         if (i >= W) return make_int4(0, 0, 0, 0);
         return __ldg(a.windows + (BACKWARD ? W - 1 - i : i));
     };
-    // Descriptors of windows i .. i+4 (d[0] is the current one).
-    int4 d0 = window(0), d1 = window(1), d2 = window(2), d3 = window(3), d4 = window(4);
-    // Prologue: rows of windows 0-3, then the far values of windows 0 and 1.
-    stage_rows<T, BACKWARD>(a, S.stage[0], d0, c, lane);
-    if (W > 1) stage_rows<T, BACKWARD>(a, S.stage[1], d1, c, lane);
-    if (W > 2) stage_rows<T, BACKWARD>(a, S.stage[2], d2, c, lane);
-    if (W > 3) stage_rows<T, BACKWARD>(a, S.stage[3], d3, c, lane);
+    int4 w0 = window(0), w1 = window(1), w2 = window(2);
+    stage_rows<T, BACKWARD>(a, S.stage[0], w0, c, lane);
     cp_async_commit();
     cp_async_wait_all();
     __syncwarp();
-    stage_far<T, BACKWARD>(a, S.stage[0], d0, c, lane);
-    if (W > 1) stage_far<T, BACKWARD>(a, S.stage[1], d1, c, lane);
+    stage_far<T, BACKWARD>(a, S.stage[0], w0, c, lane);
+    if (W > 1) stage_rows<T, BACKWARD>(a, S.stage[1], w1, c, lane);
     cp_async_commit();
-    cp_async_wait_all();
-    __syncwarp();
     for (int i = 0; i < W; ++i) {
-        const int4 d5 = window(i + 5);
-        // Every copy group but the newest has landed: the rows of windows up
-        // to i+3 and the far values up to i+1 (issued two iterations ago).
-        cp_async_wait_one();
+        const int4 w3 = window(i + 3);
+        cp_async_wait_all();
         __syncwarp();
-        if (i + 2 < W) stage_far<T, BACKWARD>(a, S.stage[(i + 2) % kStages], d2, c, lane);
-        if (i + 4 < W) stage_rows<T, BACKWARD>(a, S.stage[(i + 4) % kStages], d4, c, lane);
+        if (i + 1 < W) stage_far<T, BACKWARD>(a, S.stage[(i + 1) % kStages], w1, c, lane);
+        if (i + 2 < W) stage_rows<T, BACKWARD>(a, S.stage[(i + 2) % kStages], w2, c, lane);
         cp_async_commit();
 
         Stage<T>& s = S.stage[i % kStages];
-        const int r0 = d0.x, r1 = d0.y, nw = r1 - r0, e0 = d0.z;
+        const int r0 = w0.x, r1 = w0.y, nw = r1 - r0, e0 = w0.z;
         const bool live = lane < nw;
         const int r = r0 + lane;
-        if (!staged(d0)) {
+        T acc = live ? s.in[lane] : T(0);
+        if (!staged(w0)) {
             // A single row with more entries than a stage holds: its whole
             // sum here, from global memory.
             if (lane == 0) {
-                T acc = s.in[0];
                 const int b = BACKWARD ? s.diagpos[0] + 1 : s.rowptr[0];
                 const int e = BACKWARD ? s.rowptr[1] : s.diagpos[0];
                 for (int q = b; q < e; ++q) {
@@ -208,149 +189,111 @@ __global__ void __launch_bounds__(32, 1) k_ilu_chain(ChainArgs<T> a)
                     acc = sub_rn(acc, mul_rn(a.vals[static_cast<long long>(q) * a.bs + c], v));
                 }
                 if (BACKWARD) acc = mul_rn(acc, s.inv[0]);
-                S.win[0] = acc;
+            }
+        } else if (!BACKWARD) {
+            // ---- forward phase A: the terms before the window, in order.
+            unsigned mask = 0;
+            if (live) {
+                const int qe = s.diagpos[lane] - e0;
+                for (int q = s.rowptr[lane] - e0; q < qe; ++q) {
+                    const int col = s.cols[q];
+                    const T f = s.vals[q];
+                    if (col < r0) {
+                        const T v = col >= r0 - kRing ? S.ring[col & (kRing - 1)] : s.far[q];
+                        acc = sub_rn(acc, mul_rn(f, v));
+                    } else {
+                        S.ftab[col - r0][lane] = f;
+                        mask |= 1u << (col - r0);
+                    }
+                }
+            }
+            __syncwarp();
+            // ---- phase B: row t is final at step t.
+#pragma unroll 4
+            for (int t = 0; t < nw; ++t) {
+                const T f = S.ftab[t][lane];
+                const T yt = __shfl_sync(full, acc, t);
+                if ((mask >> t) & 1u) acc = sub_rn(acc, mul_rn(f, yt));
             }
         } else {
-            // ---- phase A, one row per lane: the record of its row.
+            // ---- backward phase A: a row's terms in column order are its
+            // in-window ones (their products formed on the steps that
+            // finish those rows), then the ones after the window (products
+            // formed here).  They are held in a register list of kChain
+            // slots; a row with more takes its products from shared memory.
+            unsigned mask = 0;
+            int m = 0, total = 0;
+            T prods[kChain];
+#pragma unroll
+            for (int k = 0; k < kChain; ++k) prods[k] = T(0);
             if (live) {
-                Rec<T> rc;
-                rc.link = T(0);
-                rc.linked = 0;
-                int n = 0, tags = 0;
-                const int qb = BACKWARD ? s.diagpos[lane] + 1 - e0 : s.rowptr[lane] - e0;
-                const int qe = BACKWARD ? s.rowptr[lane + 1] - e0 : s.diagpos[lane] - e0;
-                T acc = s.in[lane];
+                const int qb = s.diagpos[lane] + 1 - e0, qe = s.rowptr[lane + 1] - e0;
+                total = qe - qb;
                 for (int q = qb; q < qe; ++q) {
                     const int col = s.cols[q];
                     const T f = s.vals[q];
-                    if (!BACKWARD && col < r0) {   // before the window: final, applied here in order
-                        const T v = col >= r0 - kRing ? S.ring[col & (kRing - 1)] : s.far[q];
-                        acc = sub_rn(acc, mul_rn(f, v));
-                        continue;
-                    }
-                    if (col == (BACKWARD ? r + 1 : r - 1) && (BACKWARD ? col < r1 : col >= r0)) {
-                        rc.link = f;   // forward: always the last term; backward: always the first
-                        rc.linked = 1;
-                        continue;
-                    }
-                    T slot = f;
-                    int tag = col - r0;
-                    if (BACKWARD && col >= r1) {   // after the window: the product, subtracted in turn
+                    if (col < r1) {
+                        S.ftab[col - r0][lane] = f;
+                        S.etab[col - r0][lane] = static_cast<short>(total <= kChain ? m : q);
+                        mask |= 1u << (col - r0);
+                        ++m;
+                    } else {
                         const T v = col < r1 + kRing ? S.ring[col & (kRing - 1)] : s.far[q];
-                        slot = mul_rn(f, v);
-                        tag = -1;
-                    }
-                    if (n < kRec) {
+                        const T p = mul_rn(f, v);
+                        const int k = q - qb;
+                        if (total <= kChain) {
 #pragma unroll
-                        for (int k = 0; k < kRec; ++k)
-                            if (k == n) rc.v[k] = slot;
-                        tags |= (tag & 0xff) << (8 * n);
+                            for (int j = 0; j < kChain; ++j)
+                                if (j == k) prods[j] = p;
+                        } else {
+                            S.ptab[q] = p;
+                        }
                     }
-                    ++n;
                 }
-                rc.pre = acc;
-                rc.inv = BACKWARD ? s.inv[lane] : T(0);
-                rc.tags = tags;
-                rc.cnt = n;
-                S.rec[lane] = rc;
+                S.chain_begin[lane] = qb;
+                S.chain_count[lane] = total;
             }
             __syncwarp();
-            // ---- phase B: lane 0 finishes the rows in order.  Step j takes
-            // the row finished before (`last`) through the current row's
-            // link; the next row's other terms, which need only older
-            // results, are formed in the same step, off that chain.
-            if (lane == 0) {
-                T last = T(0);
-                // The row's terms other than the link, as far as they can be
-                // formed before `last` of its step is known: forward the
-                // partial sum pre - slots (all before the link), backward the
-                // products of the slots (subtracted after the link).
-                T part = T(0);
-                T prod[kRec];
+            // ---- phase B, rows in descending order: step t sums row t's
+            // products in column order, scales by the inverse diagonal and
+            // broadcasts the result; the rows with a term on it form that
+            // product at once.
+            for (int t = nw - 1; t >= 0; --t) {
+                const T inv = s.inv[t];
+                const int cnt = S.chain_count[t];
+                if (cnt <= kChain) {
+                    if (lane == t) {
 #pragma unroll
-                for (int k = 0; k < kRec; ++k) prod[k] = T(0);
-                // Terms of record rc at step j (row t), given `last` = result of
-                // the row finished at step j - 1.
-                const auto prepare = [&](const Rec<T>& rc, int t, T prev_result) {
-                    const int prev2 = BACKWARD ? t + 2 : t - 2;   // finished two steps before t
-                    if (!BACKWARD) {
-                        T acc = rc.pre;
-#pragma unroll
-                        for (int k = 0; k < kRec; ++k) {
-                            if (k < rc.cnt) {
-                                const int tag = tag_of(rc.tags, k);
-                                const T v = tag == prev2 ? prev_result : S.win[tag & 31];
-                                acc = sub_rn(acc, mul_rn(rc.v[k], v));
-                            }
-                        }
-                        part = acc;
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < kRec; ++k) {
-                            if (k < rc.cnt) {
-                                const int tag = tag_of(rc.tags, k);
-                                const T v = tag == prev2 ? prev_result : S.win[tag & 31];
-                                prod[k] = tag < 0 ? rc.v[k] : mul_rn(rc.v[k], v);
-                            }
-                        }
+                        for (int k = 0; k < kChain; ++k)
+                            if (k < cnt) acc = sub_rn(acc, prods[k]);
+                        acc = mul_rn(acc, inv);
                     }
-                };
-                Rec<T> cur = S.rec[BACKWARD ? nw - 1 : 0];
-                if (cur.cnt <= kRec) prepare(cur, BACKWARD ? nw - 1 : 0, T(0));
-                for (int j = 0; j < nw; ++j) {
-                    const int t = BACKWARD ? nw - 1 - j : j;
-                    const int tn = BACKWARD ? t - 1 : t + 1;    // the next row
-                    const bool more = j + 1 < nw;
-                    const Rec<T> nxt = S.rec[more ? tn : t];
-                    T res;
-                    if (cur.cnt <= kRec) {
-                        if (!BACKWARD) {
-                            res = cur.linked ? sub_rn(part, mul_rn(cur.link, last)) : part;
-                        } else {
-                            T acc = cur.linked ? sub_rn(cur.pre, mul_rn(cur.link, last)) : cur.pre;
+                } else if (lane == t) {
+                    const int qb = S.chain_begin[t];
+                    for (int j = 0; j < cnt; ++j) acc = sub_rn(acc, S.ptab[qb + j]);
+                    acc = mul_rn(acc, inv);
+                }
+                const T xt = __shfl_sync(full, acc, t);
+                if ((mask >> t) & 1u) {
+                    const T p = mul_rn(S.ftab[t][lane], xt);
+                    const int slot = S.etab[t][lane];
+                    if (total <= kChain) {
 #pragma unroll
-                            for (int k = 0; k < kRec; ++k)
-                                if (k < cur.cnt) acc = sub_rn(acc, prod[k]);
-                            res = mul_rn(acc, cur.inv);
-                        }
+                        for (int j = 0; j < kChain; ++j)
+                            if (j == slot) prods[j] = p;
                     } else {
-                        // More terms than a record holds: the row's list, in order.
-                        const int prev = BACKWARD ? t + 1 : t - 1;
-                        const int qb = BACKWARD ? s.diagpos[t] + 1 - e0 : s.rowptr[t] - e0;
-                        const int qe = BACKWARD ? s.rowptr[t + 1] - e0 : s.diagpos[t] - e0;
-                        T acc = cur.pre;
-                        for (int q = qb; q < qe; ++q) {
-                            const int col = s.cols[q];
-                            if (!BACKWARD && col < r0) continue;   // already in pre
-                            T v;
-                            if (BACKWARD && col >= r1)
-                                v = col < r1 + kRing ? S.ring[col & (kRing - 1)] : s.far[q];
-                            else
-                                v = col - r0 == prev ? last : S.win[col - r0];
-                            acc = sub_rn(acc, mul_rn(s.vals[q], v));
-                        }
-                        res = BACKWARD ? mul_rn(acc, cur.inv) : acc;
+                        S.ptab[slot] = p;
                     }
-                    // The next row's terms: they reach back two rows at most
-                    // to `last` (the row before this one), older ones are in win.
-                    if (more && nxt.cnt <= kRec) prepare(nxt, tn, last);
-                    S.win[t] = res;
-                    last = res;
-                    cur = nxt;
                 }
             }
         }
-        __syncwarp();
         if (live) {
-            const T y = S.win[lane];
-            S.ring[r & (kRing - 1)] = y;
-            a.out[static_cast<long long>(r) * a.bs + c] = y;
+            S.ring[r & (kRing - 1)] = acc;
+            a.out[static_cast<long long>(r) * a.bs + c] = acc;
         }
-        d0 = d1;
-        d1 = d2;
-        d2 = d3;
-        d3 = d4;
-        d4 = d5;
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
     }
     cp_async_wait_all();
 }
