@@ -120,6 +120,14 @@ owtk_status owtk_matrix_info(owtk_matrix* m, int* kind, size_t* owned_nodes,
 /* Matrix::apply (block_csr.hpp:192-215, split_block_csr.hpp:89-119,
  * dense_block_csr.hpp:173-205): owned rows of out are overwritten. */
 owtk_status owtk_spmv(owtk_matrix* m, owtk_vector* in, owtk_vector* out);
+
+/* BlockCsrMatrix / SplitBlockCsrMatrixView / DenseBlockCsrMatrix::apply_rows
+ * (block_csr.hpp:198-215, split_block_csr.hpp:95-119,
+ * dense_block_csr.hpp:179-204): out rows listed in host_rows (count entries,
+ * any order, repeats allowed) computed as apply computes them, bit for bit;
+ * other rows untouched.  A row >= owned gives OWTK_ERR_OUT_OF_RANGE. */
+owtk_status owtk_spmv_rows(owtk_matrix* m, owtk_vector* in, owtk_vector* out, const uint64_t* host_rows,
+                           size_t count);
 /* BlockCsrMatrix::diagonal (block_csr.hpp:217-236), host output. */
 owtk_status owtk_matrix_diagonal(owtk_matrix* m, void* host_out);
 

@@ -914,6 +914,35 @@ owtk_status owtk_spmv(owtk_matrix* m, owtk_vector* in, owtk_vector* out)
     });
 }
 
+owtk_status owtk_spmv_rows(owtk_matrix* m, owtk_vector* in, owtk_vector* out, const uint64_t* host_rows,
+                           size_t count)
+{
+    return guarded([&] {
+        require(m != nullptr && in != nullptr && out != nullptr && (host_rows != nullptr || count == 0),
+                "null handle");
+        if (m->kind == 3) fail(OWTK_ERR_INVALID_ARGUMENT, "a callback operator has no apply_rows()");
+        if (m->dtype == OWTK_F64) matrix_layout_check<double>(*m, *in, *out);
+        else matrix_layout_check<float>(*m, *in, *out);
+        if (count == 0) return;
+        require(count <= static_cast<size_t>(INT32_MAX), "too many rows");
+        std::vector<std::int32_t> rows(count);
+        for (size_t i = 0; i < count; ++i) {
+            if (host_rows[i] >= m->owned) fail(OWTK_ERR_OUT_OF_RANGE, "apply_rows: row out of range");
+            rows[i] = static_cast<std::int32_t>(host_rows[i]);
+        }
+        Context& c = *m->ctx;
+        DeviceBuffer d = upload(c.stream, rows);
+        const int n = static_cast<int>(count);
+        if (m->dtype == OWTK_F64)
+            kern::spmv_rows<double>(c, *m, d.as<int>(), n, static_cast<const double*>(in->data),
+                                    static_cast<double*>(out->data));
+        else
+            kern::spmv_rows<float>(c, *m, d.as<int>(), n, static_cast<const float*>(in->data),
+                                   static_cast<float*>(out->data));
+        c.sync();   // the row list is freed on return
+    });
+}
+
 owtk_status owtk_matrix_diagonal(owtk_matrix* m, void* host_out)
 {
     return guarded([&] {

@@ -611,6 +611,39 @@ __global__ void k_gather_values(std::size_t entries, int bs, const std::int64_t*
     out[k] = s < 0 ? T(0) : values[static_cast<std::size_t>(s) * bs + c];
 }
 
+// Rows of a listed subset (BlockCsrMatrix / SplitBlockCsrMatrixView /
+// DenseBlockCsrMatrix::apply_rows, block_csr.hpp:198-215,
+// split_block_csr.hpp:95-119, dense_block_csr.hpp:179-204): one thread per
+// (listed row, component or block row), the reference's loop for that output
+// term by term (component-diagonal: 0 + v x per entry; split: d x, then + v x;
+// dense: per entry the block row's dot product from 0, then added), so the
+// rows equal those of the whole-matrix apply bit for bit.  Rows not listed
+// are left as they are.
+template<class T>
+__global__ void k_spmv_rows(int kind, int bs, const int* __restrict__ rows, int count, const int* __restrict__ rowptr,
+                            const int* __restrict__ cols, const T* __restrict__ vals, const T* __restrict__ diag,
+                            const T* __restrict__ x, T* __restrict__ y)
+{
+    const long long k = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= static_cast<long long>(count) * bs) return;
+    const int i = static_cast<int>(k / bs), c = static_cast<int>(k - static_cast<long long>(i) * bs);
+    const int row = rows[i];
+    const long long o = static_cast<long long>(row) * bs + c;
+    T acc = kind == 1 ? mul_rn(diag[o], x[o]) : T(0);
+    for (int e = rowptr[row]; e < rowptr[row + 1]; ++e) {
+        const long long xb = static_cast<long long>(cols[e]) * bs;
+        if (kind == 2) {
+            const T* b = vals + static_cast<long long>(e) * bs * bs + static_cast<long long>(c) * bs;
+            T part = T(0);
+            for (int j = 0; j < bs; ++j) part = add_rn(part, mul_rn(b[j], x[xb + j]));
+            acc = add_rn(acc, part);
+        } else {
+            acc = add_rn(acc, mul_rn(vals[static_cast<long long>(e) * bs + c], x[xb + c]));
+        }
+    }
+    y[o] = acc;
+}
+
 }  // namespace
 
 namespace kern {
@@ -655,6 +688,17 @@ template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
     c.launched();
 }
 
+template<class T> void spmv_rows(Context& c, const Matrix& m, const int* rows, int count, const T* x, T* y)
+{
+    if (count == 0) return;
+    const long long total = static_cast<long long>(count) * static_cast<long long>(m.bs);
+    k_spmv_rows<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, c.stream>>>(
+        m.kind, static_cast<int>(m.bs), rows, count, m.rowptr.as<int>(), m.cols.as<int>(),
+        static_cast<const T*>(m.value_ptr()), static_cast<const T*>(m.diag), x, y);
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+}
+
 template<class T> void bsr_diagonal(Context& c, const Matrix& m, T* out)
 {
     const int owned = static_cast<int>(m.owned);
@@ -678,6 +722,8 @@ template<class T> void gather_values(Context& c, std::size_t entries, std::size_
 
 template void spmv<double>(Context&, const Matrix&, const double*, double*);
 template void spmv<float>(Context&, const Matrix&, const float*, float*);
+template void spmv_rows<double>(Context&, const Matrix&, const int*, int, const double*, double*);
+template void spmv_rows<float>(Context&, const Matrix&, const int*, int, const float*, float*);
 template void bsr_diagonal<double>(Context&, const Matrix&, double*);
 template void bsr_diagonal<float>(Context&, const Matrix&, float*);
 template void gather_values<double>(Context&, std::size_t, std::size_t, const std::int64_t*, const double*, double*);

@@ -339,6 +339,7 @@ template<class T>
 void prepare_norms(Context& c, std::size_t n, const T* r, const float* dinv, float* q, double* norms);
 template<class T> void jacobi(Context& c, std::size_t n, const T* inv, const T* in, T* out);
 template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y);
+template<class T> void spmv_rows(Context& c, const Matrix& m, const int* rows, int count, const T* x, T* y);
 template<class T> void gather_values(Context& c, std::size_t entries, std::size_t bs,
                                      const std::int64_t* source, const T* values, T* out);
 // ILU(0)/SSOR sweeps.

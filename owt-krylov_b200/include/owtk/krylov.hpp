@@ -454,6 +454,15 @@ public:
         check_vectors(in, out);
         detail::apply_host(in, out, [&](owtk_vector* a, owtk_vector* b) { cuda::check(owtk_spmv(dev_.get(), a, b)); });
     }
+    // The listed rows only, as apply computes them; other rows untouched.
+    void apply_rows(const BlockVector<T>& in, BlockVector<T>& out, std::span<const std::size_t> rows) const
+    {
+        check_vectors(in, out);
+        const std::vector<std::uint64_t> r(rows.begin(), rows.end());
+        detail::apply_host(in, out, [&](owtk_vector* a, owtk_vector* b) {
+            cuda::check(owtk_spmv_rows(dev_.get(), a, b, r.data(), r.size()));
+        });
+    }
     [[nodiscard]] std::vector<T> diagonal() const
     {
         std::vector<T> d(owned_ * bs_);
@@ -541,6 +550,15 @@ public:
             throw std::invalid_argument("SplitBlockCsrMatrixView vector layout mismatch");
         detail::apply_host(in, out, [&](owtk_vector* a, owtk_vector* b) { cuda::check(owtk_spmv(dev_.get(), a, b)); });
     }
+    // The listed rows only, as apply computes them; other rows untouched.
+    void apply_rows(const BlockVector<T>& in, BlockVector<T>& out, std::span<const std::size_t> rows) const
+    {
+        check_vectors(in, out);
+        const std::vector<std::uint64_t> r(rows.begin(), rows.end());
+        detail::apply_host(in, out, [&](owtk_vector* a, owtk_vector* b) {
+            cuda::check(owtk_spmv_rows(dev_.get(), a, b, r.data(), r.size()));
+        });
+    }
     [[nodiscard]] std::vector<T> diagonal() const { return {diag_.begin(), diag_.end()}; }
 
 private:
@@ -582,6 +600,15 @@ public:
         if (!in.same_layout(out) || in.owned_nodes() != owned_ || in.ghost_nodes() != ghost_ || in.block_size() != bs_)
             throw std::invalid_argument("dense-block CSR vector layout mismatch");
         detail::apply_host(in, out, [&](owtk_vector* a, owtk_vector* b) { cuda::check(owtk_spmv(dev_.get(), a, b)); });
+    }
+    // The listed rows only, as apply computes them; other rows untouched.
+    void apply_rows(const BlockVector<T>& in, BlockVector<T>& out, std::span<const std::size_t> rows) const
+    {
+        check_vectors(in, out);
+        const std::vector<std::uint64_t> r(rows.begin(), rows.end());
+        detail::apply_host(in, out, [&](owtk_vector* a, owtk_vector* b) {
+            cuda::check(owtk_spmv_rows(dev_.get(), a, b, r.data(), r.size()));
+        });
     }
 
 private:

@@ -113,6 +113,7 @@ def lib():
             "owtk_matrix_destroy": (c_int, [vp]),
             "owtk_matrix_info": (c_int, [vp, POINTER(c_int), POINTER(sz), POINTER(sz), POINTER(sz), POINTER(sz)]),
             "owtk_spmv": (c_int, [vp, vp, vp]),
+            "owtk_spmv_rows": (c_int, [vp, vp, vp, vp, sz]),
             "owtk_matrix_diagonal": (c_int, [vp, vp]),
             "owtk_pc_create": (c_int, [vp, c_int, c_double, POINTER(vp)]),
             "owtk_pc_destroy": (c_int, [vp]),
@@ -381,6 +382,11 @@ class Matrix:
 
     def apply(self, x: Vector, y: Vector):
         check(lib().owtk_spmv(self.h, x.h, y.h))
+
+    def apply_rows(self, x: Vector, y: Vector, rows):
+        """The listed rows of y = A x, as apply computes them; other rows untouched."""
+        r = np.ascontiguousarray(rows, dtype=np.uint64)
+        check(lib().owtk_spmv_rows(self.h, x.h, y.h, _ptr(r) if r.size else None, r.size))
 
     def close(self):
         if self.h is not None:

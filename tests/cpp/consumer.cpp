@@ -63,6 +63,17 @@ int main(int argc, char** argv)
     BlockVector<double> y = rhs.clone_layout();
     op.apply(rhs, y);
     write(dir + "/spmv.f64", std::vector<double>(y.owned().begin(), y.owned().end()));
+    // apply_rows (block_csr.hpp:198-215): every third row, last to first;
+    // the other rows keep the 7.0 they start with.
+    {
+        BlockVector<double> z = rhs.clone_layout();
+        std::fill(z.data(), z.data() + z.local_size(), 7.0);
+        std::vector<std::size_t> rows;
+        for (std::size_t r = n; r-- > 0;)
+            if (r % 3 == 0) rows.push_back(r);
+        A.apply_rows(rhs, z, rows);
+        write(dir + "/spmv_rows.f64", std::vector<double>(z.owned().begin(), z.owned().end()));
+    }
 
     Ilu0Preconditioner ilu(A);
     SolverOptions<double> options;

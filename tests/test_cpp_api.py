@@ -58,6 +58,10 @@ def test_consumer_matches_oracle(native, restatement, tmp_path):
     rhs = c["rhs"][: n * bs]
     spmv = np.fromfile(os.path.join(d, "spmv.f64"))
     assert_bitwise(spmv, restatement.bsr_spmv(n, bs, c["rowptr"], c["cols"], c["vals"], rhs), "spmv")
+    rows_out = np.fromfile(os.path.join(d, "spmv_rows.f64")).reshape(n, bs)
+    listed = np.arange(n) % 3 == 0
+    assert_bitwise(rows_out[listed], spmv.reshape(n, bs)[listed], "apply_rows, listed rows")
+    assert (rows_out[~listed] == 7.0).all(), "apply_rows touched a row it was not given"
     mat = restatement.make_matrix("bsr", n, 0, bs, c["rowptr"], c["cols"], c["vals"])
     ilu = restatement.ilu(n, bs, c["rowptr"], c["cols"], c["vals"], 0)
     for key, solver, pck, opts, xfile in [

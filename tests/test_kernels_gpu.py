@@ -61,6 +61,52 @@ def test_spmv_bitwise(native, ctx, golden, name):
     assert_bitwise(y.download()[: n * bs], golden[f"{name}/split_spmv"], "split spmv")
 
 
+@pytest.mark.parametrize("name", list(cases.SPMV_CASES))
+def test_apply_rows_bitwise(native, ctx, golden, name):
+    """apply_rows (block_csr.hpp:198-215, split_block_csr.hpp:95-119): the
+    listed rows (unsorted, one repeated) equal the whole apply's; the others
+    and the ghosts keep what they held; an empty list changes nothing; a row
+    past the owned ones is out of range."""
+    c = cases.build(name)
+    n, bs = c["owned"], c["bs"]
+    rng = np.random.default_rng(n)
+    rows = rng.permutation(n)[: max(1, n // 3)]
+    rows = np.concatenate([rows, rows[:1]])
+    listed = np.zeros(n, bool)
+    listed[rows] = True
+    x = dvec(native, ctx, c, c["x"])
+    keep = []
+    for kind, m, want in [("bsr", bsr(native, ctx, c), golden[f"{name}/spmv"]),
+                          ("split", split_matrix(native, ctx, c, keep)[0], golden[f"{name}/split_spmv"])]:
+        y = dvec(native, ctx, c, fill=77.0)
+        m.apply_rows(x, y, rows)
+        out = y.download()
+        got = out[: n * bs].reshape(n, bs)
+        assert_bitwise(got[listed], want.reshape(n, bs)[listed], f"{kind} apply_rows")
+        assert (got[~listed] == 77.0).all() and (out[n * bs:] == 77.0).all(), f"{kind} apply_rows wrote other rows"
+        m.apply_rows(x, y, np.zeros(0, np.uint64))
+        assert_bitwise(y.download(), out, f"{kind} empty apply_rows")
+        with pytest.raises(native.OwtkError) as err:
+            m.apply_rows(x, y, [n])
+        assert "out of range" in str(err.value)
+
+
+@pytest.mark.parametrize("name", list(cases.DENSE_CASES))
+def test_dense_apply_rows_bitwise(native, ctx, golden, name):
+    c = cases.dense_case(**cases.DENSE_CASES[name])
+    n, bs = c["owned"], c["bs"]
+    m = native.Matrix(ctx, "dense", n, 0, bs, c["rowptr"], c["cols"], c["vals"])
+    rows = np.arange(n)[::-2]
+    listed = np.zeros(n, bool)
+    listed[rows] = True
+    x = dvec(native, ctx, c, c["x"])
+    y = dvec(native, ctx, c, fill=5.0)
+    m.apply_rows(x, y, rows)
+    got = y.download().reshape(n, bs)
+    assert_bitwise(got[listed], golden[f"{name}/spmv"].reshape(n, bs)[listed], "dense apply_rows")
+    assert (got[~listed] == 5.0).all()
+
+
 @pytest.mark.parametrize("side,bs", [(420, 3), (300, 2), (161, 5)])
 def test_spmv_bitwise_many_tiles_per_cta(native, ctx, restatement, side, bs):
     # Thousands of 2048-value tiles: every persistent CTA streams several
