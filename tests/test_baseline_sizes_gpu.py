@@ -5,7 +5,8 @@
   order equals the reference's reverse_cuthill_mckee_order bit for bit
   (ordering.hpp:138-180); the ILU(0) factors computed on the device equal the
   reference's (preconditioner.hpp:439-485) bit for bit; GMRES(30) + ILU(0)
-  reaches true-residual rtol 1e-8 within 2 iterations of the reference;
+  reaches true-residual rtol 1e-8 within 2 iterations of the reference; in
+  the Hilbert order the ILU(0) apply (the chain sweep) equals the reference's;
 * the anisotropic unit-square mesh at 200k vertices (the training size of the
   learned form): plain ILU(0)-GMRES(30) against the reference, and the
   learned FGMRES with the committed trained network reaching the same
@@ -66,6 +67,24 @@ def test_cfg1_rcm_factors_and_gmres_at_2m(native, ctx, reference, problems, disk
     assert r.true_residual_norm <= 1e-8 * bnorm
     xs = x.download()
     assert np.linalg.norm(xs - xr) <= 1e-6 * np.linalg.norm(xr)
+
+
+def test_cfg1_hilbert_chain_sweep_at_2m(native, ctx, reference, problems, disk2m):
+    """The same 2M mesh in the Hilbert order (the sweep over both orderings):
+    the ILU(0) apply takes the chain sweep and equals the reference's apply
+    (preconditioner.hpp:320-363) bit for bit."""
+    xy, edges = disk2m
+    s = problems.component_diagonal_system(xy, edges, 3, np.random.default_rng(1), order="hilbert")
+    n, bs = s.owned, s.bs
+    m = native.Matrix(ctx, "bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
+    pc = native.Preconditioner(m, native.PC_ILU, 0)
+    assert pc.chain_windows() > 0
+    x = native.Vector(ctx, n, 0, bs).upload(s.rhs)
+    y = native.Vector(ctx, n, 0, bs)
+    pc.apply(x, y)
+    rm = reference.matrix("bsr", n, 0, bs, s.rowptr, s.cols, s.vals)
+    want = reference.pc("ilu", rm, 0).apply(s.rhs)
+    np.testing.assert_array_equal(y.download().view(np.uint64), want.view(np.uint64))
 
 
 def test_cfg4_anisotropic_200k_plain_and_learned(native, ctx, reference, problems):
