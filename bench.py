@@ -174,9 +174,16 @@ def cached_mesh(n_target: int, seed: int, domain: str):
     except (OSError, ValueError, KeyError):
         pass
     xy, edges = problems.disk_mesh(n_target, seed, domain=domain)
-    np.save(stem + "-xy.npy", xy)
-    np.save(stem + "-edges.npy", edges)
-    json.dump({"points": int(xy.shape[0]), "edges": int(edges.shape[0])}, open(stem + ".json", "w"))
+    # Written under a private name and renamed into place, so replicas that
+    # build the same mesh at once never leave a torn file for a later reader.
+    tag = f".{os.getpid()}.tmp"
+    for name, arr in (("-xy.npy", xy), ("-edges.npy", edges)):
+        with open(stem + name + tag, "wb") as f:
+            np.save(f, arr)
+        os.replace(stem + name + tag, stem + name)
+    with open(stem + ".json" + tag, "w") as f:
+        json.dump({"points": int(xy.shape[0]), "edges": int(edges.shape[0])}, f)
+    os.replace(stem + ".json" + tag, stem + ".json")
     return xy, edges
 
 
