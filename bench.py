@@ -339,10 +339,13 @@ def _events(stream, fn, steps):
 
 
 def _max_over_ranks(ms, world, local):
+    """The slowest rank's time (all ranks take part; NCCL reduces on the
+    device, gloo on the host)."""
     if world > 1:
         import torch
 
-        tt = torch.tensor([ms], device=f"cuda:{local}")
+        dev = "cpu" if torch.distributed.get_backend() == "gloo" else f"cuda:{local}"
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         return float(tt.item())
     return ms
