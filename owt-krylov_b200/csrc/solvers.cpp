@@ -156,9 +156,9 @@ struct Engine {
         OWTK_CUDA(cudaMemcpyAsync(candidate_host.data(), candidate.data, candidate_host.size(),
                                   cudaMemcpyDeviceToHost, c.stream));
         c.sync();
-        const int verdict = ex->test(ex->user, res.iterations, candidate_host.data(), count);
-        if (verdict < 0) fail(OWTK_ERR_RUNTIME, "application convergence test failed");
-        if (verdict == 0) return false;
+        const int answer = ex->test(ex->user, res.iterations, candidate_host.data(), count);
+        if (answer < 0) fail(OWTK_ERR_RUNTIME, "application convergence test failed");
+        if (answer == 0) return false;
         if (!app_residual) {
             app_residual = make_vector_like(candidate);
             app_work = make_vector_like(candidate);
