@@ -1258,11 +1258,21 @@ template<class T> void basis_dots(Context& c, std::size_t n, int k, const T* con
     if (k + 1 > 32) fail(OWTK_ERR_INVALID_ARGUMENT, "basis dots take at most 31 basis vectors");
     const unsigned want = reduce_blocks(c, n);
     const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
-    if (k + 1 <= 8)
+    // Register tiers of the basis size: fewer registers, more resident CTAs.
+    if (k + 1 <= 4)
+        k_basis_dots<T, 4><<<resident_blocks(c, k_basis_dots<T, 4>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 8)
         k_basis_dots<T, 8><<<resident_blocks(c, k_basis_dots<T, 8>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 12)
+        k_basis_dots<T, 12><<<resident_blocks(c, k_basis_dots<T, 12>, want), kThreads, 0, c.stream>>>(
             n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
     else if (k + 1 <= 16)
         k_basis_dots<T, 16><<<resident_blocks(c, k_basis_dots<T, 16>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 24)
+        k_basis_dots<T, 24><<<resident_blocks(c, k_basis_dots<T, 24>, want), kThreads, 0, c.stream>>>(
             n, k, pb, x, partials_of(c), ticket_of(c), out_dev, out_host);
     else
         k_basis_dots<T, 32><<<resident_blocks(c, k_basis_dots<T, 32>, want), kThreads, 0, c.stream>>>(
@@ -1277,11 +1287,21 @@ template<class T> void cgs_update_dot(Context& c, std::size_t n, int k, const T*
     if (k + 1 > 32) fail(OWTK_ERR_INVALID_ARGUMENT, "fused Gram-Schmidt pass takes at most 31 basis vectors");
     const unsigned want = reduce_blocks(c, n);
     const PtrPack pb = pack(reinterpret_cast<const void* const*>(basis), k);
-    if (k + 1 <= 8)
+    // Register tiers of the basis size: fewer registers, more resident CTAs.
+    if (k + 1 <= 4)
+        k_cgs_update_dot<T, 4><<<resident_blocks(c, k_cgs_update_dot<T, 4>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 8)
         k_cgs_update_dot<T, 8><<<resident_blocks(c, k_cgs_update_dot<T, 8>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 12)
+        k_cgs_update_dot<T, 12><<<resident_blocks(c, k_cgs_update_dot<T, 12>, want), kThreads, 0, c.stream>>>(
             n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     else if (k + 1 <= 16)
         k_cgs_update_dot<T, 16><<<resident_blocks(c, k_cgs_update_dot<T, 16>, want), kThreads, 0, c.stream>>>(
+            n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
+    else if (k + 1 <= 24)
+        k_cgs_update_dot<T, 24><<<resident_blocks(c, k_cgs_update_dot<T, 24>, want), kThreads, 0, c.stream>>>(
             n, k, pb, h, w, partials_of(c), ticket_of(c), out_dev, out_host);
     else
         k_cgs_update_dot<T, 32><<<resident_blocks(c, k_cgs_update_dot<T, 32>, want), kThreads, 0, c.stream>>>(
