@@ -931,15 +931,18 @@ owtk_status owtk_spmv_rows(owtk_matrix* m, owtk_vector* in, owtk_vector* out, co
             rows[i] = static_cast<std::int32_t>(host_rows[i]);
         }
         Context& c = *m->ctx;
-        DeviceBuffer d = upload(c.stream, rows);
+        const std::size_t bytes = count * sizeof(std::int32_t);
+        if (m->row_list.bytes < bytes) m->row_list.allocate(bytes);
+        // The previous call's kernel may still read the list: copy behind it
+        // on the same stream (pageable source: the copy returns once staged).
+        OWTK_CUDA(cudaMemcpyAsync(m->row_list.ptr, rows.data(), bytes, cudaMemcpyHostToDevice, c.stream));
         const int n = static_cast<int>(count);
         if (m->dtype == OWTK_F64)
-            kern::spmv_rows<double>(c, *m, d.as<int>(), n, static_cast<const double*>(in->data),
+            kern::spmv_rows<double>(c, *m, m->row_list.as<int>(), n, static_cast<const double*>(in->data),
                                     static_cast<double*>(out->data));
         else
-            kern::spmv_rows<float>(c, *m, d.as<int>(), n, static_cast<const float*>(in->data),
+            kern::spmv_rows<float>(c, *m, m->row_list.as<int>(), n, static_cast<const float*>(in->data),
                                    static_cast<float*>(out->data));
-        c.sync();   // the row list is freed on return
     });
 }
 

@@ -150,6 +150,8 @@ struct Matrix {
     // split arrays (node < owned: diagonal, else owned + edge), for updates.
     DeviceBuffer split_map;
     std::size_t split_edges = 0;
+    // apply_rows: the last row list's device copy, reused while it fits.
+    DeviceBuffer row_list;
     const void* value_ptr() const { return kind == 1 ? off : values.ptr; }
     std::size_t local_size() const { return (owned + ghost) * bs; }
 };
