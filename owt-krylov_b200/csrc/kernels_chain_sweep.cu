@@ -30,7 +30,8 @@
 // only form the rounded products u * x, and step t subtracts them in column
 // order and multiplies by the inverse diagonal.  Every product and
 // difference is rounded separately (no contraction), as on the CPU, so
-// results equal the reference bit for bit, NaN payloads included.
+// results equal the reference bit for bit (no sentinel is involved, so NaN
+// results are stored as the arithmetic produced them).
 //
 // There is no wait on another thread's progress anywhere: the only waits are
 // for this warp's own cp.async copies.
