@@ -252,6 +252,14 @@ void ilu_symbolic(Preconditioner& p, const Matrix& m, std::size_t fill)
         build_chain_sweep(*p.ctx, p.chain, n, p.lower.depth, p.upper.depth, p.f_rowptr);
     }
     if (!p.block && !p.chain.ready) {
+        build_lockstep_sweep(*p.ctx, p.l_lower, n, p.bs, m.dtype, lower_level, p.f_rowptr, p.f_cols, p.f_diagpos,
+                             false);
+        if (p.l_lower.ready)
+            build_lockstep_sweep(*p.ctx, p.l_upper, n, p.bs, m.dtype, upper_level, p.f_rowptr, p.f_cols,
+                                 p.f_diagpos, true);
+        if (!p.l_lower.ready || !p.l_upper.ready) p.l_lower.ready = p.l_upper.ready = false;
+    }
+    if (!p.block && !p.chain.ready && !p.l_lower.ready) {
         std::vector<std::uint32_t> loc;
         build_cluster_sweep(*p.ctx, p.c_lower, n, p.bs, m.dtype, lower_level, p.f_rowptr, p.f_cols, p.f_diagpos,
                             false, loc);
@@ -1470,6 +1478,18 @@ owtk_status owtk_pc_sweep_schedule(owtk_preconditioner* pc, int32_t* cluster_cta
         if (cluster_ctas) *cluster_ctas = on ? pc->c_lower.C : 0;
         if (epoch_levels) *epoch_levels = on ? pc->c_lower.K : 0;
         if (ring_rows) *ring_rows = on ? std::max(pc->c_lower.R, pc->c_upper.R) : 0;
+    });
+}
+
+owtk_status owtk_pc_lockstep_schedule(owtk_preconditioner* pc, int32_t* cluster_ctas, int32_t* lower_levels,
+                                      int32_t* upper_levels)
+{
+    return guarded([&] {
+        require(pc != nullptr, "null handle");
+        const bool on = pc->l_lower.ready && pc->l_upper.ready;
+        if (cluster_ctas) *cluster_ctas = on ? pc->l_lower.C : 0;
+        if (lower_levels) *lower_levels = on ? pc->l_lower.D : 0;
+        if (upper_levels) *upper_levels = on ? pc->l_upper.D : 0;
     });
 }
 

@@ -844,6 +844,7 @@ template<class T> void fill_sentinel(Context& c, std::size_t n, T* x)
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out)
 {
     if (chain_ilu_apply<T>(c, p, in, out)) return;
+    if (lockstep_ilu_apply<T>(c, p, in, out)) return;
     if (cluster_ilu_apply<T>(c, p, in, out)) return;
     SweepArgs<T> a{};
     a.rowptr = p.d_frowptr.as<int>();

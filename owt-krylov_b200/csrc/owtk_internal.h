@@ -188,6 +188,19 @@ struct ClusterSweep {
     DeviceBuffer rows, recs, task_ptr, epoch_task, cta_first;
 };
 
+// The ILU applies level by level on one thread-block cluster
+// (kernels_lockstep_sweep.cu): per level and CTA a chunk of lane-tasks
+// ((row, component) pairs), per lane-task its entries, per entry where its
+// dependency is read; factor values gathered into entry order after every
+// numeric factorisation.
+struct LockstepSweep {
+    bool ready = false;
+    int C = 0, D = 0;
+    std::size_t entries = 0;
+    std::uint64_t gathered = ~0ull;   // numeric_updates the gathered values belong to
+    DeviceBuffer blk, task_io, task_ent, ent_loc, ent_src, ent_val;
+};
+
 // The ILU applies of a near-sequential DAG by one warp per component
 // (kernels_chain_sweep.cu): windows of up to 32 consecutive rows.
 struct ChainSweep {
@@ -223,6 +236,7 @@ struct Preconditioner {
     // dependency is read (owner CTA and ring slot, or global memory).
     ClusterSweep c_lower, c_upper;
     ChainSweep chain;
+    LockstepSweep l_lower, l_upper;
     DeviceBuffer d_floc;
     DeviceBuffer flags;        // uint32 per row, epoch-stamped
     DeviceBuffer ticket;       // uint64 monotone task counter
@@ -263,6 +277,10 @@ void levels_of(std::size_t owned, const std::int32_t* rowptr, const std::int32_t
                std::vector<std::int32_t>& lower, std::vector<std::int32_t>& upper);
 void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
                  const std::vector<std::int32_t>& level, bool descending_rows);
+void build_lockstep_sweep(Context& ctx, LockstepSweep& s, std::size_t owned, std::size_t bs, owtk_dtype dtype,
+                          const std::vector<std::int32_t>& level, const std::vector<std::int32_t>& rowptr,
+                          const std::vector<std::int32_t>& cols, const std::vector<std::int32_t>& diagpos,
+                          bool backward);
 void build_chain_sweep(Context& ctx, ChainSweep& s, std::size_t owned, int depth_lower, int depth_upper,
                        const std::vector<std::int32_t>& rowptr);
 void build_cluster_sweep(Context& ctx, ClusterSweep& s, std::size_t owned, std::size_t bs, owtk_dtype dtype,
@@ -349,6 +367,7 @@ template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* mat
 template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
 template<class T> bool cluster_ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
 template<class T> bool chain_ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
+template<class T> bool lockstep_ilu_apply(Context& c, Preconditioner& p, const T* in, T* out);
 // Test hook: a sweep whose only dependency is never published (bounded wait).
 void debug_unpublished_dependency(Context& c, int spin_limit);
 template<class T> void ssor_apply(Context& c, Preconditioner& p, const T* in, T* out);

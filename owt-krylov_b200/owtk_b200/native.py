@@ -151,6 +151,7 @@ def lib():
             "owtk_debug_unpublished_dependency": (c_int, [vp, ctypes.c_uint32]),
             "owtk_pc_sweep_schedule": (c_int, [vp, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
             "owtk_pc_chain_schedule": (c_int, [vp, POINTER(c_int32)]),
+            "owtk_pc_lockstep_schedule": (c_int, [vp, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
             "owtk_permutation_create": (c_int, [vp, sz, vp, POINTER(vp)]),
             "owtk_permutation_destroy": (c_int, [vp]),
             "owtk_vector_permute": (c_int, [vp, vp, vp, c_int]),
@@ -443,6 +444,12 @@ class Preconditioner:
         c, k, r = c_int32(), c_int32(), c_int32()
         check(lib().owtk_pc_sweep_schedule(self.h, ctypes.byref(c), ctypes.byref(k), ctypes.byref(r)))
         return c.value, k.value, r.value
+
+    def lockstep_schedule(self):
+        """(cluster CTAs or 0, forward levels, backward levels) of the lockstep sweep."""
+        c, lo, up = c_int32(), c_int32(), c_int32()
+        check(lib().owtk_pc_lockstep_schedule(self.h, ctypes.byref(c), ctypes.byref(lo), ctypes.byref(up)))
+        return c.value, lo.value, up.value
 
     def chain_windows(self):
         """Row windows of the chain sweep (0: the applies take another sweep)."""

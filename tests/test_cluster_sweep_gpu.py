@@ -1,7 +1,7 @@
 """ILU(k) applies on one thread-block cluster (dependency values through
 distributed shared memory, kernels_cluster_sweep.cu; opt-in with
-OWTK_CLUSTER_SWEEP=1) against the oracle and against the default
-level-scheduled sweep: the same bits, FP64 and FP32, block sizes 1-4, fill
+OWTK_CLUSTER_SWEEP=1, with the lockstep schedule off) against the oracle and
+against the level-scheduled sweep: the same bits, FP64 and FP32, block sizes 1-4, fill
 levels 0 and 1, in place and out of place."""
 import numpy as np
 import pytest
@@ -14,10 +14,12 @@ pytestmark = pytest.mark.gpu
 def _pair(native, m, fill, monkeypatch):
     """The cluster sweep is opt-in (OWTK_CLUSTER_SWEEP=1 at creation): one
     preconditioner on it and one on the default level-scheduled sweep."""
+    monkeypatch.setenv("OWTK_LOCKSTEP_SWEEP", "0")
     monkeypatch.setenv("OWTK_CLUSTER_SWEEP", "1")
     pc = native.Preconditioner(m, native.PC_ILU, fill)
     monkeypatch.delenv("OWTK_CLUSTER_SWEEP")
     plain = native.Preconditioner(m, native.PC_ILU, fill)
+    monkeypatch.delenv("OWTK_LOCKSTEP_SWEEP")
     return pc, plain
 
 
