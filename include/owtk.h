@@ -204,10 +204,11 @@ owtk_status owtk_pc_chain_schedule(owtk_preconditioner* pc, int32_t* windows);
 /* Whether an ILU preconditioner's applies run level by level on one
  * thread-block cluster (no reference counterpart): *cluster_ctas > 0 (the
  * cluster's CTAs) with the two sweeps' level counts, 0 otherwise.  The
- * lockstep schedule is taken when every level fits the cluster's lanes (512
- * per CTA, one per row and component) and the DAGs are not near-sequential;
- * the same bits as every other schedule.  The environment variable
- * OWTK_LOCKSTEP_SWEEP=0 at preconditioner creation turns it off. */
+ * lockstep schedule is opt-in (the environment variable OWTK_LOCKSTEP_SWEEP=1
+ * at preconditioner creation; it is slower than the level-scheduled sweep on
+ * the meshes measured) and is taken when every level fits the cluster's lanes
+ * (512 per CTA, one per row and component) and the DAGs are not
+ * near-sequential; the same bits as every other schedule. */
 owtk_status owtk_pc_lockstep_schedule(owtk_preconditioner* pc, int32_t* cluster_ctas, int32_t* lower_levels,
                                       int32_t* upper_levels);
 

@@ -189,16 +189,16 @@ struct ClusterSweep {
 };
 
 // The ILU applies level by level on one thread-block cluster
-// (kernels_lockstep_sweep.cu): per level and CTA a chunk of lane-tasks
-// ((row, component) pairs), per lane-task its entries, per entry where its
-// dependency is read; factor values gathered into entry order after every
-// numeric factorisation.
+// (kernels_lockstep_sweep.cu): per level and CTA a chunk of lanes ((row,
+// component) pairs) with a record each (output index, entries, dependency
+// locations), their factor values (gathered after every numeric
+// factorisation) and the chunk's list of older dependencies.
 struct LockstepSweep {
     bool ready = false;
-    int C = 0, D = 0;
-    std::size_t entries = 0;
+    int C = 0, D = 0, max_lanes = 0, max_far = 0;
+    std::size_t values = 0, ovf_values = 0;
     std::uint64_t gathered = ~0ull;   // numeric_updates the gathered values belong to
-    DeviceBuffer blk, task_io, task_ent, ent_loc, ent_src, ent_val;
+    DeviceBuffer blk, recs, vsrc, vals, far_src, ovf_loc, ovf_src, ovf_val;
 };
 
 // The ILU applies of a near-sequential DAG by one warp per component

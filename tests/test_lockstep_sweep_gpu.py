@@ -1,7 +1,7 @@
 """ILU(k) applies level by level on one thread-block cluster
-(kernels_lockstep_sweep.cu, the default schedule when every level fits the
-cluster's lanes) against the oracle and against the level-scheduled sweep
-(OWTK_LOCKSTEP_SWEEP=0): the same bits.  RCM and natural orders, block
+(kernels_lockstep_sweep.cu, opt-in with OWTK_LOCKSTEP_SWEEP=1, taken when
+every level fits the cluster's lanes) against the oracle and against the
+level-scheduled sweep (the default): the same bits.  RCM and natural orders, block
 sizes 1-4, fill levels 0-2, FP32, in place, repeated applies, numeric
 updates (the factor values are re-gathered), whole solves."""
 import numpy as np
@@ -19,10 +19,10 @@ def _system(problems, side, bs, order, seed):
 
 
 def _pair(native, m, fill, monkeypatch):
+    monkeypatch.setenv("OWTK_LOCKSTEP_SWEEP", "1")
     pc = native.Preconditioner(m, native.PC_ILU, fill)
-    monkeypatch.setenv("OWTK_LOCKSTEP_SWEEP", "0")
-    plain = native.Preconditioner(m, native.PC_ILU, fill)
     monkeypatch.delenv("OWTK_LOCKSTEP_SWEEP")
+    plain = native.Preconditioner(m, native.PC_ILU, fill)
     return pc, plain
 
 
