@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -1032,6 +1033,13 @@ std::unique_ptr<owtk_preconditioner> make_pc(owtk_matrix* m, owtk_pc_kind kind, 
         if (m->kind != 0) fail(OWTK_ERR_INVALID_ARGUMENT, "ILU needs a component-diagonal BSR matrix");
         if (!(parameter >= 0)) fail(OWTK_ERR_INVALID_ARGUMENT, "ILU fill level must be >= 0");
         ilu_symbolic(*p, *m, static_cast<std::size_t>(parameter));
+        if (storage == OWTK_F64 && m->bs <= 32 && !p->chain.ready) {
+            const char* env = std::getenv("OWTK_PACKED_SWEEP");   // 0: applies read the factor in place
+            if (!env || std::atoi(env) != 0) {
+                pack_sweep(*p->ctx, p->lower, m->bs, es, p->f_rowptr, p->f_cols, p->f_diagpos, false);
+                pack_sweep(*p->ctx, p->upper, m->bs, es, p->f_rowptr, p->f_cols, p->f_diagpos, true);
+            }
+        }
         break;
     }
     case OWTK_PC_BLOCK_ILU: {

@@ -66,6 +66,7 @@ struct SweepArgs {
     const int* rowptr;      // dependency pattern (ILU factor pattern or matrix pattern)
     const int* cols;
     const int* diagpos;     // ILU only
+    const int* seg;         // ILU applies on packed segments: entries of order position q in [seg[q], seg[q+1])
     F* vals;                // ILU factor values (written by the factorisation) or matrix/edge values
     const T* diag;          // SSOR diagonal
     F* inv;                 // ILU inverse diagonal (blocks for the dense-block ILU)
@@ -336,20 +337,29 @@ __device__ __forceinline__ void eliminate_publish(bool valid, T y, const SweepAr
 }
 
 // ILU / SSOR apply of (row, component c) with early publication; row < 0:
-// a lane without a row, which only takes part in the warp's votes.
+// a lane without a row, which only takes part in the warp's votes.  q: the
+// row's position in the task order (its packed segment, when a.seg is set).
 template<class T, class F, int MODE>
-__device__ __forceinline__ void apply_lane(const SweepArgs<T, F>& a, int row, int c)
+__device__ __forceinline__ void apply_lane(const SweepArgs<T, F>& a, int row, int q, int c)
 {
     const bool valid = row >= 0;
     const std::size_t o = valid ? static_cast<std::size_t>(row) * a.bs + c : 0;
     if constexpr (MODE == kIluForward) {
-        const int b = valid ? a.rowptr[row] : 0, d = valid ? a.diagpos[row] : 0;
+        int b = 0, d = 0;
+        if (valid) {
+            b = a.seg ? a.seg[q] : a.rowptr[row];
+            d = a.seg ? a.seg[q + 1] : a.diagpos[row];
+        }
         const T own = valid ? a.in[o] : T(0);
         eliminate_publish<T, F, 0, false, 0>(valid, own, a, a.work, b, d, row, c, T(1), a.work + o);
     } else if constexpr (MODE == kIluBackward) {
-        const int d = valid ? a.diagpos[row] : 0, end = valid ? a.rowptr[row + 1] : 0;
+        int b = 0, end = 0;
+        if (valid) {
+            b = a.seg ? a.seg[q] : a.diagpos[row] + 1;
+            end = a.seg ? a.seg[q + 1] : a.rowptr[row + 1];
+        }
         const T own = valid ? a.work[o] : T(0), inv = valid ? cvt<T>(a.inv[o]) : T(1);
-        eliminate_publish<T, F, 0, false, 1>(valid, own, a, a.out, d + 1, end, row, c, inv, a.out + o);
+        eliminate_publish<T, F, 0, false, 1>(valid, own, a, a.out, b, end, row, c, inv, a.out + o);
     } else if constexpr (MODE == kSsorForward) {
         const int b = valid ? a.rowptr[row] : 0, end = valid ? a.rowptr[row + 1] : 0;
         const T own = valid ? a.in[o] : T(0), dg = valid ? a.diag[o] : T(1);
@@ -722,7 +732,7 @@ __global__ void __launch_bounds__(kThreads) k_sweep(SweepArgs<T, F> a)
         T w = 0;
         if constexpr (LANE && (MODE == kBlockForward || MODE == kBlockBackward))
             block_apply_lane<T, F, MODE == kBlockBackward>(a, row, c0, rl);
-        else if constexpr (LANE) apply_lane<T, F, MODE>(a, row, c0);
+        else if constexpr (LANE) apply_lane<T, F, MODE>(a, row, s + rl, c0);
         else if (row >= 0) w = row_body<T, F, MODE>(a, row, c0, cstep);
         if constexpr (MODE == kBlockBackward && !LANE) {
             // x_r[i] = sum_j Dinv_r[i][j] w_j: the row's w_j live in the
@@ -829,6 +839,9 @@ template<class T> void ilu_factorize(Context& c, Preconditioner& p, const T* mat
     a.upd_target = p.d_upd_target.as<int>();
     a.upd_upper = p.d_upd_upper.as<int>();
     launch<T, T, kIluFactor>(c, p, p.lower, a);
+    for (Sweep* s : {&p.lower, &p.upper})
+        if (s->packed)
+            gather_values<T>(c, s->pentries, p.bs, s->psrc.as<std::int64_t>(), p.d_fvalues.as<T>(), s->pvals.as<T>());
 }
 
 template<class T> void fill_sentinel(Context& c, std::size_t n, T* x)
@@ -856,8 +869,19 @@ template<class T> void ilu_apply(Context& c, Preconditioner& p, const T* in, T* 
     a.out = out;
     a.work = p.work.as<T>();
     const std::size_t n = p.owned * p.bs;
+    const bool packed = p.lower.packed && p.upper.packed;
+    if (packed) {
+        a.seg = p.lower.seg.as<int>();
+        a.cols = p.lower.pcols.as<int>();
+        a.vals = p.lower.pvals.as<T>();
+    }
     fill_sentinel<T>(c, n, a.work);
     launch<T, T, kIluForward>(c, p, p.lower, a);
+    if (packed) {
+        a.seg = p.upper.seg.as<int>();
+        a.cols = p.upper.pcols.as<int>();
+        a.vals = p.upper.pvals.as<T>();
+    }
     fill_sentinel<T>(c, n, out);
     launch<T, T, kIluBackward>(c, p, p.upper, a);
 }

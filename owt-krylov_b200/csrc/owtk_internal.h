@@ -177,6 +177,15 @@ struct Sweep {
     int depth = 0;             // number of levels
     int rows_per_task = 1;
     std::vector<std::int32_t> h_level;
+    std::vector<std::int32_t> h_order;
+    // ILU applies: the rows' lower (forward) or upper (backward) factor
+    // entries packed in task order, so a task's columns and values are
+    // contiguous.  seg: int32, rows + 1 (positions in order); psrc: int64
+    // factor entry of each packed entry; pvals refreshed by every numeric
+    // factorisation.
+    bool packed = false;
+    std::size_t pentries = 0;
+    DeviceBuffer seg, pcols, psrc, pvals;
 };
 
 // The same sweep run by one thread-block cluster (kernels_cluster_sweep.cu):
@@ -277,6 +286,9 @@ void levels_of(std::size_t owned, const std::int32_t* rowptr, const std::int32_t
                std::vector<std::int32_t>& lower, std::vector<std::int32_t>& upper);
 void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
                  const std::vector<std::int32_t>& level, bool descending_rows);
+void pack_sweep(Context& ctx, Sweep& s, std::size_t bs, std::size_t element_size,
+                const std::vector<std::int32_t>& rowptr, const std::vector<std::int32_t>& cols,
+                const std::vector<std::int32_t>& diagpos, bool backward);
 void build_lockstep_sweep(Context& ctx, LockstepSweep& s, std::size_t owned, std::size_t bs, owtk_dtype dtype,
                           const std::vector<std::int32_t>& level, const std::vector<std::int32_t>& rowptr,
                           const std::vector<std::int32_t>& cols, const std::vector<std::int32_t>& diagpos,

@@ -71,6 +71,44 @@ void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
     s.tasks = static_cast<int>(tasks.size()) - 1;
     s.order = upload(ctx.stream, order);
     s.task_start = upload(ctx.stream, tasks);
+    s.h_order = std::move(order);
+}
+
+// The factor entries an ILU sweep reads (lower entries for the forward sweep,
+// upper for the backward, in the row's entry order), row after row in task
+// order.  The rows of one level are scattered over the factor, and within a
+// row the lower and upper entries sit side by side, so reading them in place
+// fetches whole sectors for part of a row; packed, a task's entries are one
+// contiguous run.  The values are gathered by every numeric factorisation.
+void pack_sweep(Context& ctx, Sweep& s, std::size_t bs, std::size_t element_size,
+                const std::vector<std::int32_t>& rowptr, const std::vector<std::int32_t>& cols,
+                const std::vector<std::int32_t>& diagpos, bool backward)
+{
+    const std::size_t n = s.h_order.size();
+    std::vector<std::int32_t> seg(n + 1, 0), pcols;
+    std::vector<std::int64_t> psrc;
+    pcols.reserve(cols.size() / 2 + 1);
+    psrc.reserve(cols.size() / 2 + 1);
+    for (std::size_t q = 0; q < n; ++q) {
+        const std::size_t row = static_cast<std::size_t>(s.h_order[q]);
+        const std::int32_t b = backward ? diagpos[row] + 1 : rowptr[row];
+        const std::int32_t e = backward ? rowptr[row + 1] : diagpos[row];
+        for (std::int32_t k = b; k < e; ++k) {
+            pcols.push_back(cols[static_cast<std::size_t>(k)]);
+            psrc.push_back(k);
+        }
+        seg[q + 1] = static_cast<std::int32_t>(pcols.size());
+    }
+    s.pentries = pcols.size();
+    if (pcols.empty()) {
+        pcols.push_back(0);
+        psrc.push_back(0);
+    }
+    s.seg = upload(ctx.stream, seg);
+    s.pcols = upload(ctx.stream, pcols);
+    s.psrc = upload(ctx.stream, psrc);
+    s.pvals.allocate(s.pentries * bs * element_size + 16);
+    s.packed = true;
 }
 
 // ordering.hpp:138-180: BFS from the lowest-degree unvisited node, unvisited
