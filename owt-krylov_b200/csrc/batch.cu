@@ -619,7 +619,11 @@ __device__ void ew_phase(const Args& a, int phase)
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_batch_bicgstab(Args a)
+// MINB: resident CTAs per SM the register budget is cut for (1: the
+// compiler's choice, 80 registers, up to three CTAs; 4: 64 registers, a few
+// spilled).  The autotuner times both.
+template<int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_batch_bicgstab(Args a)
 {
     sp_phase(a, kSp0);
     if (!grid_sync(a)) return;
@@ -712,6 +716,7 @@ struct Batch {
     DeviceBuffer rowptr, xoff, vals, inv, vec, sys, st, tickets, results, ew_first, ew_seg, ew_part, sp_first, sp_seg,
         sp_part, grid, remaining, scratch_b, scratch_x, stage_b, stage_x;
     int blocks_per_sm = 0, max_blocks_per_sm = 0, grid_blocks = 0;
+    int wide_blocks_per_sm = 0;   // resident CTAs of the 80-register instance; more take the 64-register one
     int vpw[batch::kMaxBlockSize + 1] = {};
     std::uint64_t config_version = 1;
     owtk_solver_result* h_results = nullptr;  // pinned
@@ -875,7 +880,10 @@ void enqueue_solve(Batch& B, const batch::Args& a)
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    OWTK_CUDA(cudaLaunchKernelEx(&cfg, batch::k_batch_bicgstab, a));
+    if (B.blocks_per_sm > B.wide_blocks_per_sm)
+        OWTK_CUDA(cudaLaunchKernelEx(&cfg, batch::k_batch_bicgstab<4>, a));
+    else
+        OWTK_CUDA(cudaLaunchKernelEx(&cfg, batch::k_batch_bicgstab<1>, a));
     OWTK_CUDA(cudaMemcpyAsync(B.h_results, a.results, sizeof(owtk_solver_result) * B.nsys, cudaMemcpyDeviceToHost,
                               st));
 }
@@ -1044,10 +1052,14 @@ owtk_status owtk_batch_create(owtk_context* ctx, size_t count, const owtk_batch_
         B->scratch_x.allocate(U * sizeof(double) + 16);
         OWTK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&B->h_results), count * sizeof(owtk_solver_result)));
         for (int bs = 1; bs <= owtk::batch::kMaxBlockSize; ++bs) B->vpw[bs] = owtk::default_vpw(bs);
-        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->max_blocks_per_sm, owtk::batch::k_batch_bicgstab,
+        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->wide_blocks_per_sm,
+                                                                owtk::batch::k_batch_bicgstab<1>, owtk::batch::kBlock, 0));
+        int lean = 0;
+        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lean, owtk::batch::k_batch_bicgstab<4>,
                                                                 owtk::batch::kBlock, 0));
-        if (B->max_blocks_per_sm < 1) fail(OWTK_ERR_CUDA, "batched solver kernel cannot be resident");
-        owtk::set_grid(*B, std::min(B->max_blocks_per_sm, 4));
+        B->max_blocks_per_sm = std::min(std::max(B->wide_blocks_per_sm, lean), 4);
+        if (B->wide_blocks_per_sm < 1) fail(OWTK_ERR_CUDA, "batched solver kernel cannot be resident");
+        owtk::set_grid(*B, B->wide_blocks_per_sm);
         // Jacobi inverse diagonal on the device.
         auto sov = owtk::upload(st, B->sys_of_vertex);
         owtk::batch::k_batch_jacobi<<<static_cast<unsigned>((V + 255) / 256), 256, 0, st>>>(
@@ -1173,7 +1185,7 @@ owtk_status owtk_batch_autotune(owtk_batch* batch, const owtk_solver_options* op
         int pick = B.blocks_per_sm;
         const bool graph = B.use_graph;
         B.use_graph = false;
-        for (int k = 1; k <= B.max_blocks_per_sm; k *= 2) {
+        for (int k = 1; k <= B.max_blocks_per_sm; ++k) {
             owtk::set_grid(B, k);
             float ms = 1e30f;
             for (int rep = 0; rep < 4; ++rep) {   // the first is a warm-up; best of the other three
