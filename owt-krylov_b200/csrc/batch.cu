@@ -619,9 +619,10 @@ __device__ void ew_phase(const Args& a, int phase)
     }
 }
 
-// MINB: resident CTAs per SM the register budget is cut for (1: the
-// compiler's choice, 80 registers, up to three CTAs; 4: 64 registers, a few
-// spilled).  The autotuner times both.
+// MINB: resident CTAs per SM the register budget is cut for (2, 3, 4, 5, 6:
+// 128, 80, 64, 48, 40 registers, the leaner ones with some state spilled).
+// The launch is latency-bound, so more resident warps can outweigh the
+// spills; the autotuner times every count.
 template<int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_batch_bicgstab(Args a)
 {
@@ -716,7 +717,6 @@ struct Batch {
     DeviceBuffer rowptr, xoff, vals, inv, vec, sys, st, tickets, results, ew_first, ew_seg, ew_part, sp_first, sp_seg,
         sp_part, grid, remaining, scratch_b, scratch_x, stage_b, stage_x;
     int blocks_per_sm = 0, max_blocks_per_sm = 0, grid_blocks = 0;
-    int wide_blocks_per_sm = 0;   // resident CTAs of the 80-register instance; more take the 64-register one
     int vpw[batch::kMaxBlockSize + 1] = {};
     std::uint64_t config_version = 1;
     owtk_solver_result* h_results = nullptr;  // pinned
@@ -865,6 +865,23 @@ batch::Args make_args(Batch& B, const double* b, double* x, const batch::Options
     return a;
 }
 
+// The solver instance whose register budget allows k resident CTAs per SM
+// (k = 1 takes the two-CTA budget).
+using SolveKernel = void (*)(batch::Args);
+SolveKernel solve_kernel(int k)
+{
+    switch (k) {
+    case 1:
+    case 2: return batch::k_batch_bicgstab<2>;
+    case 3: return batch::k_batch_bicgstab<3>;
+    case 4: return batch::k_batch_bicgstab<4>;
+    case 5: return batch::k_batch_bicgstab<5>;
+    case 6: return batch::k_batch_bicgstab<6>;
+    case 7: return batch::k_batch_bicgstab<7>;
+    default: return batch::k_batch_bicgstab<8>;
+    }
+}
+
 void enqueue_solve(Batch& B, const batch::Args& a)
 {
     cudaStream_t st = B.ctx->stream;
@@ -880,10 +897,7 @@ void enqueue_solve(Batch& B, const batch::Args& a)
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (B.blocks_per_sm > B.wide_blocks_per_sm)
-        OWTK_CUDA(cudaLaunchKernelEx(&cfg, batch::k_batch_bicgstab<4>, a));
-    else
-        OWTK_CUDA(cudaLaunchKernelEx(&cfg, batch::k_batch_bicgstab<1>, a));
+    OWTK_CUDA(cudaLaunchKernelEx(&cfg, solve_kernel(B.blocks_per_sm), a));
     OWTK_CUDA(cudaMemcpyAsync(B.h_results, a.results, sizeof(owtk_solver_result) * B.nsys, cudaMemcpyDeviceToHost,
                               st));
 }
@@ -1052,14 +1066,17 @@ owtk_status owtk_batch_create(owtk_context* ctx, size_t count, const owtk_batch_
         B->scratch_x.allocate(U * sizeof(double) + 16);
         OWTK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&B->h_results), count * sizeof(owtk_solver_result)));
         for (int bs = 1; bs <= owtk::batch::kMaxBlockSize; ++bs) B->vpw[bs] = owtk::default_vpw(bs);
-        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->wide_blocks_per_sm,
-                                                                owtk::batch::k_batch_bicgstab<1>, owtk::batch::kBlock, 0));
-        int lean = 0;
-        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lean, owtk::batch::k_batch_bicgstab<4>,
-                                                                owtk::batch::kBlock, 0));
-        B->max_blocks_per_sm = std::min(std::max(B->wide_blocks_per_sm, lean), 4);
-        if (B->wide_blocks_per_sm < 1) fail(OWTK_ERR_CUDA, "batched solver kernel cannot be resident");
-        owtk::set_grid(*B, B->wide_blocks_per_sm);
+        // Counts 1..8 whose instance is resident at that count.
+        B->max_blocks_per_sm = 0;
+        for (int k = 1; k <= 8; ++k) {
+            int resident = 0;
+            OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, owtk::solve_kernel(k),
+                                                                    owtk::batch::kBlock, 0));
+            if (resident < k) break;
+            B->max_blocks_per_sm = k;
+        }
+        if (B->max_blocks_per_sm < 1) fail(OWTK_ERR_CUDA, "batched solver kernel cannot be resident");
+        owtk::set_grid(*B, std::min(B->max_blocks_per_sm, 4));
         // Jacobi inverse diagonal on the device.
         auto sov = owtk::upload(st, B->sys_of_vertex);
         owtk::batch::k_batch_jacobi<<<static_cast<unsigned>((V + 255) / 256), 256, 0, st>>>(
