@@ -207,13 +207,8 @@ __global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* _
 // packed f32x2 FMAs over the 2 BS nonzero inputs in ascending order; the zero
 // inputs are skipped, which leaves every sum bit-identical to the full
 // 16-term one (fma(w, 0, s) = s, s never -0).
-#ifdef OWTK_GNN_ENC_BLOCKS
-#define OWTK_GNN_ENC_BOUNDS __launch_bounds__(256, OWTK_GNN_ENC_BLOCKS)
-#else
-#define OWTK_GNN_ENC_BOUNDS __launch_bounds__(256)
-#endif
 template<class T, int BS>
-__global__ void OWTK_GNN_ENC_BOUNDS
+__global__ void __launch_bounds__(256)
     k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
                                                     const double* norms, const float* __restrict__ we,
                                                     bf16* __restrict__ h0)
