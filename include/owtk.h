@@ -475,11 +475,14 @@ owtk_status owtk_batch_layout(const owtk_batch* batch, size_t* unknowns, uint64_
 /* Current launch shape: resident blocks per SM and vertices per warp pass for
  * block sizes 0..32 (33 entries; index = block size). */
 owtk_status owtk_batch_config(const owtk_batch* batch, uint32_t* blocks_per_sm, uint32_t* vertices_per_warp);
-/* Override the shape (0 leaves a field unchanged). */
+/* Override the shape (0 leaves a field unchanged).  Blocks per SM run from 1
+ * to 8 (clamped to what is resident); each count launches the solver build
+ * whose register budget allows it. */
 owtk_status owtk_batch_set_config(owtk_batch* batch, uint32_t blocks_per_sm, size_t bs, uint32_t vertices_per_warp);
 /* Autotuner: times one SpMV pass per vertices-per-warp candidate and block
- * size present, then a few solver iterations per blocks-per-SM candidate, and
- * keeps the fastest; outputs as owtk_batch_config (either may be NULL). */
+ * size present, then a few solver iterations per blocks-per-SM count (every
+ * resident count), and keeps the fastest; outputs as owtk_batch_config (either
+ * may be NULL). */
 owtk_status owtk_batch_autotune(owtk_batch* batch, const owtk_solver_options* options, uint32_t* blocks_per_sm,
                                 uint32_t* vertices_per_warp);
 /* 1 (default): each solve replays a CUDA graph holding the whole launch
