@@ -208,8 +208,7 @@ __global__ void __launch_bounds__(256) k_gnn_prepare(long long count, const T* _
 // inputs are skipped, which leaves every sum bit-identical to the full
 // 16-term one (fma(w, 0, s) = s, s never -0).
 template<class T, int BS>
-__global__ void __launch_bounds__(256)
-    k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
+__global__ void __launch_bounds__(256) k_gnn_encode(GraphArgs g, const T* __restrict__ r, const float* __restrict__ q,
                                                     const double* norms, const float* __restrict__ we,
                                                     bf16* __restrict__ h0)
 {
