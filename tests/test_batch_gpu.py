@@ -158,6 +158,24 @@ def test_batch_autotune(native, ctx, restatement):
     check_against_oracle(restatement, systems, b.offsets, res, x)
 
 
+@pytest.mark.parametrize("blocks_per_sm", [2, 3, 4, 5, 6, 8])
+def test_batch_every_register_budget(native, ctx, restatement, blocks_per_sm):
+    """Each resident-CTA count launches the build whose register budget allows
+    it (2 to 8 CTAs of 256 threads per SM, the leaner ones spilling); every one
+    solves like the reference, and a repeated solve gives the same bits (the
+    reduction order depends on the shape, not on the run)."""
+    systems = small_batch(count=9, seed=31)
+    b = native.Batch(ctx, systems)
+    b.set_config(blocks_per_sm=blocks_per_sm)
+    assert b.config()[0] == blocks_per_sm
+    rhs = np.concatenate([s.rhs for s in systems])
+    res, x = run_batch(native, ctx, b, rhs, np.zeros_like(rhs))
+    check_against_oracle(restatement, systems, b.offsets, res, x)
+    b.set_config(blocks_per_sm=blocks_per_sm)
+    res2, x2 = run_batch(native, ctx, b, rhs, np.zeros_like(rhs))
+    assert np.array_equal(x.view(np.uint64), x2.view(np.uint64))
+
+
 def test_batch_rejections(native, ctx):
     systems = small_batch(count=2, seed=17)
     s = systems[0]
