@@ -373,6 +373,7 @@ void mixed_update(Preconditioner& p, Matrix& m)
 {
     const std::size_t per = m.kind == 2 ? m.bs * m.bs : m.bs;
     kern::convert<float, double>(*p.ctx, m.entries * per, m.values.as<double>(), p.m32->values.as<float>());
+    kern::slices_fill(*p.ctx, *p.m32);
     numeric_update(*p.inner, m);
 }
 
@@ -832,6 +833,7 @@ owtk_status owtk_bsr_create(owtk_context* ctx, owtk_dtype dtype, size_t owned, s
         const std::size_t bytes = m->entries * bs * dsize(dtype);
         m->values.allocate(bytes + 16);
         OWTK_CUDA(cudaMemcpyAsync(m->values.ptr, values, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        kern::slices_fill(*ctx, *m);
         ctx->sync();
         *out = m.release();
     });
@@ -846,6 +848,7 @@ owtk_status owtk_bsr_update_values(owtk_matrix* m, const void* values)
         const std::size_t per = m->kind == 2 ? m->bs * m->bs : m->bs;
         OWTK_CUDA(cudaMemcpyAsync(m->values.ptr, values, m->entries * per * dsize(m->dtype),
                                   cudaMemcpyHostToDevice, m->ctx->stream));
+        kern::slices_fill(*m->ctx, *m);
         m->ctx->sync();
     });
 }
@@ -1182,6 +1185,7 @@ owtk_status owtk_pc_create_mixed(owtk_matrix* m, owtk_pc_kind inner_kind, double
         OWTK_CUDA(cudaMemsetAsync(p->v32.ptr, 0, m->local_size() * sizeof(float), m->ctx->stream));
         const std::size_t per = m->kind == 2 ? m->bs * m->bs : m->bs;
         kern::convert<float, double>(*m->ctx, m->entries * per, m->values.as<double>(), p->m32->values.as<float>());
+        kern::slices_fill(*m->ctx, *p->m32);
         p->numeric_updates = 1;
         m->ctx->sync();
         *out = p.release();
@@ -1452,6 +1456,7 @@ owtk_status owtk_bsr_create_permuted_split(owtk_permutation* p, owtk_dtype dtype
             kern::gather_split<float>(c, m->entries, bs, n, m->split_map.as<std::int64_t>(),
                                       static_cast<const float*>(device_diagonal),
                                       static_cast<const float*>(device_off_diagonal), m->values.as<float>());
+        kern::slices_fill(c, *m);
         c.sync();
         *out = m.release();
     });
@@ -1473,6 +1478,7 @@ owtk_status owtk_bsr_update_permuted_split(owtk_matrix* m, const void* device_di
             kern::gather_split<float>(c, m->entries, m->bs, m->owned, m->split_map.as<std::int64_t>(),
                                       static_cast<const float*>(device_diagonal),
                                       static_cast<const float*>(device_off_diagonal), m->values.as<float>());
+        kern::slices_fill(c, *m);
         c.sync();
     });
 }

@@ -20,6 +20,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <utility>
+#include <vector>
 
 #include "device_common.cuh"
 #include "owtk_internal.h"
@@ -583,6 +586,129 @@ void launch_bulk_bs(Context& c, const SpmvArgs<T>& a, const Matrix& m)
     }
 }
 
+// Row-slice SpMV (component-diagonal BSR, block size BS <= 4): a warp takes a
+// slice of 32 rows, lane j the slice's j-th longest row, and walks the
+// slice's packed steps: at step k the n_k lanes whose row is longer than k
+// load their entry's column (one coalesced run) and BS values (BS coalesced
+// runs of n_k elements), gather x from L2 and add the rounded product to
+// their own sums; a row's products are added from +0 in entry order, the
+// reference's sequence (block_csr.hpp:203-214), so the bits match.  Columns
+// are loaded two steps ahead, values and x one step ahead.  The sums are put
+// back in row order through shared memory and stored as one coalesced run
+// of 32 * BS elements.  Long rows (length 0 here) are written afterwards by
+// the row-list kernel.
+template<class T, int BS>
+__global__ void __launch_bounds__(256) k_spmv_slices(const int* __restrict__ base,
+                                                     const unsigned short* __restrict__ lanes,
+                                                     const int* __restrict__ scols, const T* __restrict__ svals,
+                                                     const T* __restrict__ x, T* __restrict__ y, int slices, int owned)
+{
+    __shared__ T out[8][32 * BS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nw = static_cast<int>(gridDim.x) * 8;
+    for (int s = static_cast<int>(blockIdx.x) * 8 + wib; s < slices; s += nw) {
+        const unsigned meta = lanes[static_cast<long long>(s) * 32 + lane];
+        const int len = static_cast<int>(meta >> 8), pos = static_cast<int>(meta & 255u);
+        const int steps = __shfl_sync(0xffffffffu, len, 0);   // lane 0 holds the longest row
+        int off = base[s];
+        T acc[BS];
+#pragma unroll
+        for (int c = 0; c < BS; ++c) acc[c] = T(0);
+        T v[BS], xv[BS];
+        const auto load_vx = [&](int k, int o, int n, int col, T (&vv)[BS], T (&xx)[BS]) {
+            if (len > k) {
+                const T* vp = svals + static_cast<long long>(o) * BS + lane;
+                const T* xp = x + static_cast<long long>(col) * BS;
+#pragma unroll
+                for (int c = 0; c < BS; ++c) {
+                    vv[c] = __ldcs(vp + c * n);
+                    xx[c] = __ldg(xp + c);
+                }
+            }
+        };
+        // Step 0 (count n0 at `off`), then step 1's column.
+        int n0 = __popc(__ballot_sync(0xffffffffu, len > 0));
+        const int col0 = len > 0 ? __ldcs(scols + off + lane) : 0;
+        load_vx(0, off, n0, col0, v, xv);
+        int off1 = off + n0;
+        int n1 = __popc(__ballot_sync(0xffffffffu, len > 1));
+        int col1 = len > 1 ? __ldcs(scols + off1 + lane) : 0;
+        for (int k = 0; k < steps; ++k) {
+            T vn[BS], xn[BS];
+            load_vx(k + 1, off1, n1, col1, vn, xn);
+            const int off2 = off1 + n1;
+            const int n2 = __popc(__ballot_sync(0xffffffffu, len > k + 2));
+            const int col2 = len > k + 2 ? __ldcs(scols + off2 + lane) : 0;
+            if (len > k)
+#pragma unroll
+                for (int c = 0; c < BS; ++c) acc[c] = add_rn(acc[c], mul_rn(v[c], xv[c]));
+#pragma unroll
+            for (int c = 0; c < BS; ++c) {
+                v[c] = vn[c];
+                xv[c] = xn[c];
+            }
+            off1 = off2;
+            n1 = n2;
+            col1 = col2;
+        }
+        if (pos < 32)
+#pragma unroll
+            for (int c = 0; c < BS; ++c) out[wib][pos * BS + c] = acc[c];
+        __syncwarp();
+        const int rows = min(32, owned - 32 * s);
+        T* ys = y + static_cast<long long>(s) * 32 * BS;
+        for (int i = lane; i < rows * BS; i += 32) ys[i] = out[wib][i];
+        __syncwarp();
+    }
+}
+
+// Fill the row-slice copy from the CSR arrays: a warp per slice walks the
+// same steps as k_spmv_slices and writes each entry where that kernel reads
+// it.
+template<class T>
+__global__ void __launch_bounds__(256) k_slices_fill(const int* __restrict__ base,
+                                                     const unsigned short* __restrict__ lanes,
+                                                     const int* __restrict__ rowptr, const int* __restrict__ cols,
+                                                     const T* __restrict__ vals, int* __restrict__ scols,
+                                                     T* __restrict__ svals, int slices, int bs)
+{
+    const int lane = threadIdx.x & 31;
+    const int s = static_cast<int>(blockIdx.x) * 8 + static_cast<int>(threadIdx.x >> 5);
+    if (s >= slices) return;
+    const unsigned meta = lanes[static_cast<long long>(s) * 32 + lane];
+    const int len = static_cast<int>(meta >> 8), pos = static_cast<int>(meta & 255u);
+    const int steps = __shfl_sync(0xffffffffu, len, 0);
+    const int e0 = len > 0 ? rowptr[32 * s + pos] : 0;
+    int off = base[s];
+    for (int k = 0; k < steps; ++k) {
+        const int n = __popc(__ballot_sync(0xffffffffu, len > k));
+        if (len > k) {
+            const int e = e0 + k;
+            scols[off + lane] = cols[e];
+            for (int c = 0; c < bs; ++c)
+                svals[static_cast<long long>(off) * bs + static_cast<long long>(c) * n + lane] =
+                    vals[static_cast<long long>(e) * bs + c];
+        }
+        off += n;
+    }
+}
+
+template<class T, int BS>
+void launch_slices(Context& c, const Matrix& m, const T* x, T* y)
+{
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_slices<T, BS>, 256, 0));
+        per_sm = std::max(per_sm, 1);
+    }
+    const RowSlices& sl = m.slices;
+    const unsigned grid = static_cast<unsigned>(
+        std::max(1, std::min((sl.slices + 7) / 8, c.sm_count * per_sm)));
+    k_spmv_slices<T, BS><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
+                                                     sl.cols.as<int>(), sl.vals.as<T>(), x, y, sl.slices,
+                                                     static_cast<int>(m.owned));
+}
+
 // First diagonal entry of every row (block_csr.hpp:217-236).
 template<class T>
 __global__ void k_bsr_diagonal(int owned, int bs, const int* rowptr, const int* cols, const T* vals,
@@ -648,9 +774,40 @@ __global__ void k_spmv_rows(int kind, int bs, const int* __restrict__ rows, int 
 
 namespace kern {
 
+// OWTK_SPMV_SLICES=0 sends the component-diagonal BSR back to the bulk-copy
+// pipeline (both give the same bits).
+static bool slices_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("OWTK_SPMV_SLICES");
+        return e == nullptr || e[0] != '0';
+    }();
+    return on;
+}
+
 template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
 {
     if (m.plan.tiles == 0) return;
+    if (m.kind == 0 && m.slices.filled && slices_enabled()) {
+        switch (m.bs) {
+        case 1: launch_slices<T, 1>(c, m, x, y); break;
+        case 2: launch_slices<T, 2>(c, m, x, y); break;
+        case 3: launch_slices<T, 3>(c, m, x, y); break;
+        default: launch_slices<T, 4>(c, m, x, y); break;
+        }
+        OWTK_CUDA(cudaGetLastError());
+        c.launched();
+        const int count = m.slices.long_count;
+        if (count > 0) {
+            const long long total = static_cast<long long>(count) * static_cast<long long>(m.bs);
+            k_spmv_rows<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, c.stream>>>(
+                0, static_cast<int>(m.bs), m.slices.long_rows.as<int>(), count, m.rowptr.as<int>(), m.cols.as<int>(),
+                static_cast<const T*>(m.values.ptr), nullptr, x, y);
+            OWTK_CUDA(cudaGetLastError());
+            c.launched();
+        }
+        return;
+    }
     SpmvArgs<T> a;
     a.tile_rows = m.plan.tile_rows.as<int>();
     a.rowptr = m.rowptr.as<int>();
@@ -697,6 +854,26 @@ template<class T> void spmv_rows(Context& c, const Matrix& m, const int* rows, i
         static_cast<const T*>(m.value_ptr()), static_cast<const T*>(m.diag), x, y);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
+}
+
+void slices_fill(Context& c, Matrix& m)
+{
+    RowSlices& sl = m.slices;
+    if (sl.slices == 0) return;
+    const unsigned grid = static_cast<unsigned>((sl.slices + 7) / 8);
+    if (m.dtype == OWTK_F64)
+        k_slices_fill<double><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
+                                                          m.rowptr.as<int>(), m.cols.as<int>(), m.values.as<double>(),
+                                                          sl.cols.as<int>(), sl.vals.as<double>(), sl.slices,
+                                                          static_cast<int>(m.bs));
+    else
+        k_slices_fill<float><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
+                                                         m.rowptr.as<int>(), m.cols.as<int>(), m.values.as<float>(),
+                                                         sl.cols.as<int>(), sl.vals.as<float>(), sl.slices,
+                                                         static_cast<int>(m.bs));
+    OWTK_CUDA(cudaGetLastError());
+    c.launched();
+    sl.filled = true;
 }
 
 template<class T> void bsr_diagonal(Context& c, const Matrix& m, T* out)
@@ -770,6 +947,50 @@ void build_tile_plan(Matrix& m)
         meta[4 * t + 3] = m.h_rowptr[tiles[t + 1]];
     }
     m.plan.tile_meta = upload(m.ctx->stream, meta);
+    build_row_slices(m);
+}
+
+// Row-slice layout of a component-diagonal BSR with bs <= 4: per slice of 32
+// rows the lanes in order of decreasing row length (ties by row), the first
+// packed entry of each slice, and the long rows; the arrays it fills are
+// allocated here and written by kern::slices_fill.
+void build_row_slices(Matrix& m)
+{
+    RowSlices& sl = m.slices;
+    sl = RowSlices{};
+    if (m.kind != 0 || m.bs > 4 || m.owned == 0 || (m.dtype != OWTK_F64 && m.dtype != OWTK_F32)) return;
+    const int owned = static_cast<int>(m.owned);
+    sl.slices = (owned + 31) / 32;
+    std::vector<std::uint16_t> lanes(static_cast<std::size_t>(sl.slices) * 32, 255);
+    std::vector<std::int32_t> base(static_cast<std::size_t>(sl.slices) + 1, 0), long_rows;
+    std::vector<std::pair<int, int>> order;   // (-length, row in slice)
+    std::size_t packed = 0;
+    for (int s = 0; s < sl.slices; ++s) {
+        order.clear();
+        const int r0 = 32 * s, r1 = std::min(owned, r0 + 32);
+        for (int r = r0; r < r1; ++r) {
+            int len = m.h_rowptr[r + 1] - m.h_rowptr[r];
+            if (len > kSliceMaxRow) {
+                long_rows.push_back(r);
+                len = 0;
+            }
+            order.emplace_back(-len, r - r0);
+        }
+        std::sort(order.begin(), order.end());
+        for (std::size_t j = 0; j < order.size(); ++j) {
+            const int len = -order[j].first;
+            lanes[static_cast<std::size_t>(s) * 32 + j] = static_cast<std::uint16_t>(order[j].second | (len << 8));
+            packed += static_cast<std::size_t>(len);
+        }
+        base[s + 1] = static_cast<std::int32_t>(packed);
+    }
+    sl.packed = packed;
+    sl.base = upload(m.ctx->stream, base);
+    sl.lanes = upload(m.ctx->stream, lanes);
+    sl.cols.allocate(packed * 4 + 16);
+    sl.vals.allocate(packed * m.bs * (m.dtype == OWTK_F64 ? 8 : 4) + 16);
+    sl.long_count = static_cast<int>(long_rows.size());
+    if (!long_rows.empty()) sl.long_rows = upload(m.ctx->stream, long_rows);
 }
 
 }  // namespace owtk

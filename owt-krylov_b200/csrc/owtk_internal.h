@@ -129,6 +129,25 @@ struct TilePlan {
     int tile_values = 0;       // stage capacity used to build the plan
 };
 
+// Row-slice copy of a component-diagonal BSR (bs <= 4), read by its SpMV.
+// Slices of 32 consecutive rows, one warp each; a slice's lanes take its rows
+// longest first.  Step k of a slice holds entry k of the n_k rows longer than
+// k: their columns [lane] and values [component][lane], packed with no
+// padding (step k + 1 starts n_k entries later).  Rows longer than
+// kSliceMaxRow have length 0 in their slice and are listed in long_rows.
+constexpr int kSliceMaxRow = 48;
+struct RowSlices {
+    int slices = 0;
+    std::size_t packed = 0;    // entries held (all but the long rows')
+    DeviceBuffer base;         // int32 per slice + 1: first packed entry
+    DeviceBuffer lanes;        // uint16 per slice lane: row in slice | length << 8 (row 255: none)
+    DeviceBuffer cols;         // int32 per packed entry
+    DeviceBuffer vals;         // element per packed entry and component
+    DeviceBuffer long_rows;    // int32
+    int long_count = 0;
+    bool filled = false;       // cols and vals hold the matrix's current values
+};
+
 struct Matrix {
     Context* ctx = nullptr;
     int kind = 0;              // 0 component-diagonal BSR, 1 split view, 2 dense BSR
@@ -141,6 +160,7 @@ struct Matrix {
     const void* diag = nullptr;      // split view: borrowed device diagonal
     const void* off = nullptr;       // split view: borrowed device off-diagonal
     TilePlan plan;
+    RowSlices slices;
     // Kind 3 (owtk_callback_operator_create): an application function applied
     // on host copies of the vectors.
     owtk_host_apply_fn host_apply = nullptr;
@@ -282,6 +302,7 @@ const Matrix* learned_matrix(const Preconditioner& p);
 
 // ---------------------------------------------------------------- setup (setup.cpp)
 void build_tile_plan(Matrix& m);
+void build_row_slices(Matrix& m);
 void levels_of(std::size_t owned, const std::int32_t* rowptr, const std::int32_t* cols,
                std::vector<std::int32_t>& lower, std::vector<std::int32_t>& upper);
 void build_sweep(Context& ctx, Sweep& s, std::size_t owned, std::size_t bs,
@@ -372,6 +393,9 @@ void prepare_norms(Context& c, std::size_t n, const T* r, const float* dinv, flo
 template<class T> void jacobi(Context& c, std::size_t n, const T* inv, const T* in, T* out);
 template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y);
 template<class T> void spmv_rows(Context& c, const Matrix& m, const int* rows, int count, const T* x, T* y);
+// Copy the matrix's current columns and values into its row-slice layout
+// (a no-op for matrices without one); called after every write of the values.
+void slices_fill(Context& c, Matrix& m);
 template<class T> void gather_values(Context& c, std::size_t entries, std::size_t bs,
                                      const std::int64_t* source, const T* values, T* out);
 // ILU(0)/SSOR sweeps.
