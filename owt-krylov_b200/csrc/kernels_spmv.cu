@@ -593,63 +593,86 @@ void launch_bulk_bs(Context& c, const SpmvArgs<T>& a, const Matrix& m)
 // runs of n_k elements), gather x from L2 and add the rounded product to
 // their own sums; a row's products are added from +0 in entry order, the
 // reference's sequence (block_csr.hpp:203-214), so the bits match.  Columns
-// are loaded two steps ahead, values and x one step ahead.  The sums are put
+// are loaded two steps ahead, x one step ahead, values VD steps ahead, and the
+// next slice's lane word and first entry during this slice.  The sums are put
 // back in row order through shared memory and stored as one coalesced run
 // of 32 * BS elements.  Long rows (length 0 here) are written afterwards by
 // the row-list kernel.
-template<class T, int BS>
-__global__ void __launch_bounds__(256) k_spmv_slices(const int* __restrict__ base,
-                                                     const unsigned short* __restrict__ lanes,
-                                                     const int* __restrict__ scols, const T* __restrict__ svals,
-                                                     const T* __restrict__ x, T* __restrict__ y, int slices, int owned)
+template<class T, int BS, int MINB, int VD>
+__global__ void __launch_bounds__(256, MINB) k_spmv_slices(const int* __restrict__ base,
+                                                           const unsigned short* __restrict__ lanes,
+                                                           const int* __restrict__ scols, const T* __restrict__ svals,
+                                                           const T* __restrict__ x, T* __restrict__ y, int slices,
+                                                           int owned)
 {
     __shared__ T out[8][32 * BS];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nw = static_cast<int>(gridDim.x) * 8;
-    for (int s = static_cast<int>(blockIdx.x) * 8 + wib; s < slices; s += nw) {
-        const unsigned meta = lanes[static_cast<long long>(s) * 32 + lane];
+    int s = static_cast<int>(blockIdx.x) * 8 + wib;
+    // This slice's lane word and first entry, loaded one slice ahead.
+    unsigned meta = s < slices ? lanes[static_cast<long long>(s) * 32 + lane] : 0u;
+    int off = s < slices ? base[s] : 0;
+    for (; s < slices; s += nw) {
         const int len = static_cast<int>(meta >> 8), pos = static_cast<int>(meta & 255u);
         const int steps = __shfl_sync(0xffffffffu, len, 0);   // lane 0 holds the longest row
-        int off = base[s];
+        const int sn = s + nw;
+        meta = sn < slices ? lanes[static_cast<long long>(sn) * 32 + lane] : 0u;
+        const int off_next = sn < slices ? base[sn] : 0;
         T acc[BS];
 #pragma unroll
         for (int c = 0; c < BS; ++c) acc[c] = T(0);
-        T v[BS], xv[BS];
-        const auto load_vx = [&](int k, int o, int n, int col, T (&vv)[BS], T (&xx)[BS]) {
+        const auto count = [&](int k) { return __popc(__ballot_sync(0xffffffffu, len > k)); };
+        const auto load_v = [&](int k, int o, int n, T (&vv)[BS]) {
             if (len > k) {
                 const T* vp = svals + static_cast<long long>(o) * BS + lane;
-                const T* xp = x + static_cast<long long>(col) * BS;
 #pragma unroll
-                for (int c = 0; c < BS; ++c) {
-                    vv[c] = __ldcs(vp + c * n);
-                    xx[c] = __ldg(xp + c);
-                }
+                for (int c = 0; c < BS; ++c) vv[c] = __ldcs(vp + c * n);
             }
         };
-        // Step 0 (count n0 at `off`), then step 1's column.
-        int n0 = __popc(__ballot_sync(0xffffffffu, len > 0));
-        const int col0 = len > 0 ? __ldcs(scols + off + lane) : 0;
-        load_vx(0, off, n0, col0, v, xv);
-        int off1 = off + n0;
-        int n1 = __popc(__ballot_sync(0xffffffffu, len > 1));
-        int col1 = len > 1 ? __ldcs(scols + off1 + lane) : 0;
+        const auto load_x = [&](int k, int col, T (&xx)[BS]) {
+            if (len > k) {
+                const T* xp = x + static_cast<long long>(col) * BS;
+#pragma unroll
+                for (int c = 0; c < BS; ++c) xx[c] = __ldg(xp + c);
+            }
+        };
+        const auto load_col = [&](int k, int o) { return len > k ? __ldcs(scols + o + lane) : 0; };
+        // Values VD steps ahead, x one step ahead, columns two steps ahead.
+        T v[VD + 1][BS], xv[BS];
+        int o[VD + 2], n[VD + 2];
+        o[0] = off;
+        n[0] = count(0);
+#pragma unroll
+        for (int i = 1; i < VD + 2; ++i) {
+            o[i] = o[i - 1] + n[i - 1];
+            n[i] = count(i);
+        }
+#pragma unroll
+        for (int i = 0; i < VD; ++i) load_v(i, o[i], n[i], v[i]);
+        const int col0 = load_col(0, o[0]);
+        int col1 = load_col(1, o[1]);
+        load_x(0, col0, xv);
         for (int k = 0; k < steps; ++k) {
-            T vn[BS], xn[BS];
-            load_vx(k + 1, off1, n1, col1, vn, xn);
-            const int off2 = off1 + n1;
-            const int n2 = __popc(__ballot_sync(0xffffffffu, len > k + 2));
-            const int col2 = len > k + 2 ? __ldcs(scols + off2 + lane) : 0;
+            load_v(k + VD, o[VD], n[VD], v[VD]);
+            T xn[BS];
+            load_x(k + 1, col1, xn);
+            col1 = load_col(k + 2, o[2]);
             if (len > k)
 #pragma unroll
-                for (int c = 0; c < BS; ++c) acc[c] = add_rn(acc[c], mul_rn(v[c], xv[c]));
+                for (int c = 0; c < BS; ++c) acc[c] = add_rn(acc[c], mul_rn(v[0][c], xv[c]));
 #pragma unroll
-            for (int c = 0; c < BS; ++c) {
-                v[c] = vn[c];
-                xv[c] = xn[c];
+            for (int i = 0; i < VD; ++i)
+#pragma unroll
+                for (int c = 0; c < BS; ++c) v[i][c] = v[i + 1][c];
+#pragma unroll
+            for (int c = 0; c < BS; ++c) xv[c] = xn[c];
+#pragma unroll
+            for (int i = 0; i < VD + 1; ++i) {
+                o[i] = o[i + 1];
+                n[i] = n[i + 1];
             }
-            off1 = off2;
-            n1 = n2;
-            col1 = col2;
+            o[VD + 1] = o[VD] + n[VD];
+            n[VD + 1] = count(k + VD + 2);
         }
         if (pos < 32)
 #pragma unroll
@@ -659,6 +682,7 @@ __global__ void __launch_bounds__(256) k_spmv_slices(const int* __restrict__ bas
         T* ys = y + static_cast<long long>(s) * 32 * BS;
         for (int i = lane; i < rows * BS; i += 32) ys[i] = out[wib][i];
         __syncwarp();
+        off = off_next;
     }
 }
 
@@ -693,20 +717,34 @@ __global__ void __launch_bounds__(256) k_slices_fill(const int* __restrict__ bas
     }
 }
 
-template<class T, int BS>
-void launch_slices(Context& c, const Matrix& m, const T* x, T* y)
+template<class T, int BS, int MINB, int VD>
+void launch_slices_v(Context& c, const Matrix& m, const T* x, T* y)
 {
     static int per_sm = 0;
     if (per_sm == 0) {
-        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_slices<T, BS>, 256, 0));
+        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_slices<T, BS, MINB, VD>, 256, 0));
         per_sm = std::max(per_sm, 1);
     }
     const RowSlices& sl = m.slices;
     const unsigned grid = static_cast<unsigned>(
         std::max(1, std::min((sl.slices + 7) / 8, c.sm_count * per_sm)));
-    k_spmv_slices<T, BS><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
-                                                     sl.cols.as<int>(), sl.vals.as<T>(), x, y, sl.slices,
-                                                     static_cast<int>(m.owned));
+    k_spmv_slices<T, BS, MINB, VD><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
+                                                               sl.cols.as<int>(), sl.vals.as<T>(), x, y, sl.slices,
+                                                               static_cast<int>(m.owned));
+}
+
+// Resident CTAs per SM asked of the compiler for each element type and block
+// size (measured on the 2M-vertex mesh, 20-30 launches each: FP64 bs 3 at 5
+// CTAs 94.9 us against 107.7-147.1 us for 4 (no cap), 6 and the two-step
+// value prefetch; FP64 bs 4 spills under a cap (143.7 us uncapped, 184.1 at
+// 5); FP32 bs 3 and 4 at 6 CTAs 61.4 and 78.0 us against 66.3 and 79.1 at 5).
+template<class T, int BS>
+constexpr int slice_ctas() { return sizeof(T) == 4 ? 6 : (BS == 4 ? 1 : 5); }
+
+template<class T, int BS>
+void launch_slices(Context& c, const Matrix& m, const T* x, T* y)
+{
+    launch_slices_v<T, BS, slice_ctas<T, BS>(), 1>(c, m, x, y);
 }
 
 // First diagonal entry of every row (block_csr.hpp:217-236).
