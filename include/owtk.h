@@ -540,10 +540,13 @@ owtk_status owtk_learned_set_adam_state(owtk_learned* net, const float* first_mo
 /* out = M(in), FP64 vectors of the matrix layout. */
 owtk_status owtk_learned_apply(owtk_learned* net, owtk_vector* in, owtk_vector* out);
 /* Profiling: `repetitions` applications out = M(in), each stage bracketed by
- * CUDA events on the context's stream.  milliseconds[4] receives the mean
- * time of (0) the norms and the encoder, (1) one of the first three fused
- * message-passing layers (k_gnn_layer), (2) the last layer with the decoder
- * fused, (3) the whole application. */
+ * CUDA events on the context's stream.  milliseconds[5] receives the mean
+ * time of (0) the norms and the encoder (with the encoder folded into the
+ * first layer: the norms and the input records), (1) one fused
+ * message-passing layer (k_gnn_layer) before the last, (2) the last layer
+ * with the decoder fused, (3) the whole application, (4) the first layer
+ * with the encoder folded in (0 when the encoder runs on its own: training
+ * builds, block sizes above 4, OWTK_GNN_FUSED_FIRST=0). */
 owtk_status owtk_learned_stage_times(owtk_learned* net, owtk_vector* in, owtk_vector* out, uint32_t repetitions,
                                      double* milliseconds);
 /* Forward + backward of one training pair: the loss (weights below) and

@@ -618,6 +618,226 @@ __global__ void __launch_bounds__(kFwdThreads, DECODE ? OWTK_GNN_DEC_BLOCKS : 4)
     if (warp == 0) tmem_free(tmem, kCols);
 }
 
+// ---------------------------------------------------------------- fused first layer
+// Inference, block size <= 4: the encoder folded into the first layer.  Both
+// are linear up to the first ReLU, so with x_v = [r_v / rms(r), q_v / rms(q)]
+// (2 bs <= 8 nonzero inputs) and s_v = sum_u w_vu x_u,
+//   h0_v = x_v We^T,   Y1_v = [h0_v | sum_u w_vu h0_u] Wl1^T
+//        = x_v (Wl1_h We)^T + s_v (Wl1_m We)^T,   h1_v = h0_v + relu(Y1_v).
+// k_gnn_first_weights folds the weights into one BF16 operand B1 (N = 128,
+// K = 16): rows 0-63 [Wl1_h We | Wl1_m We] (Y1), rows 64-127 [We | 0] (h0).
+// The layer then gathers the neighbours' 32-byte input records (FP32
+// [r_u, q_u, 0...], unnormalised: the norms scale the sums afterwards)
+// instead of their 128-byte feature rows, and one M=128, N=128, K=16 MMA of
+// the tile's [x | s] rows gives Y1 and h0 together in TMEM.
+constexpr int kFirstThreads = 128;   // a thread per tile row (its TMEM lane)
+constexpr int kFirstCols = 128;      // TMEM columns: Y1 (0-63), h0 (64-127)
+// B1 and two A/out tiles (alternate tiles, so a tile's store drains while
+// the next is built), 16 KB each after up to 1 KB of alignment; the request
+// also keeps at most four CTAs on an SM: 4 x 128 TMEM columns fill its 512.
+constexpr int kFirstSmem = 1024 + 3 * kTile * 128;
+static_assert(5 * kFirstSmem > 228 * 1024, "first layer: at most 4 CTAs per SM");
+
+// rec[v] = [r_v (BS values rounded to FP32), q_v (BS), 0...] as 8 floats: a
+// thread per vertex, two 16-byte stores.
+template<class T, int BS>
+__global__ void __launch_bounds__(256) k_gnn_records(long long n, const T* __restrict__ r,
+                                                     const float* __restrict__ q, float4* __restrict__ rec)
+{
+    const long long v = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    float x[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) x[f] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < BS; ++c) {
+        x[c] = static_cast<float>(r[v * BS + c]);
+        x[BS + c] = q[v * BS + c];
+    }
+    rec[2 * v] = make_float4(x[0], x[1], x[2], x[3]);
+    rec[2 * v + 1] = make_float4(x[4], x[5], x[6], x[7]);
+}
+
+template<class T>
+void launch_records(unsigned grid, cudaStream_t st, long long n, int bs, const T* r, const float* q, float4* rec)
+{
+    switch (bs) {
+    case 1: k_gnn_records<T, 1><<<grid, 256, 0, st>>>(n, r, q, rec); break;
+    case 2: k_gnn_records<T, 2><<<grid, 256, 0, st>>>(n, r, q, rec); break;
+    case 3: k_gnn_records<T, 3><<<grid, 256, 0, st>>>(n, r, q, rec); break;
+    default: k_gnn_records<T, 4><<<grid, 256, 0, st>>>(n, r, q, rec); break;
+    }
+}
+
+// B1 (128 rows of 16 BF16, K-major) from the FP32 master weights; each sum
+// in FP32 over k in ascending order.
+__global__ void k_gnn_first_weights(const float* __restrict__ we, const float* __restrict__ wl1, bf16* __restrict__ b1)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;    // over 128 * 16
+    if (i >= 2 * kH * 16) return;
+    const int row = i >> 4, j = i & 15;
+    float v = 0.0f;
+    if (row < kH) {
+        const int f = j & 7, half = j >> 3;   // half 0: Wl1_h We, half 1: Wl1_m We
+        for (int k = 0; k < kH; ++k) v = fmaf(wl1[row * 2 * kH + half * kH + k], we[k * kF + f], v);
+    } else if (j < 8) {
+        v = we[(row - kH) * kF + j];
+    }
+    b1[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void __launch_bounds__(kFirstThreads, 4)
+    k_gnn_first_layer(GraphArgs g, const __grid_constant__ CUtensorMap tmap_out, const float4* __restrict__ rec,
+                      const double* norms, const bf16* __restrict__ b1, unsigned* status)
+{
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) std::uint64_t bar_storage[1];
+    __shared__ std::uint32_t tmem_base_s;
+    const std::uint32_t raw = smem_u32(smem_raw), base = align1024(raw);
+    unsigned char* tiles = smem_raw + (base - raw);   // B1, then A0 and A1 (rows [x | s], then output rows)
+    const std::uint32_t b = base;
+    const std::uint32_t bar = smem_u32(&bar_storage[0]);
+    const int warp = threadIdx.x >> 5, r = threadIdx.x;
+    const int ntiles = (g.n + kTile - 1) / kTile;
+
+    // B1: two 16-byte chunks per row into the swizzled block.
+    for (int i = threadIdx.x; i < 2 * kH * 2; i += kFirstThreads)
+        *reinterpret_cast<uint4*>(tiles + sw128(i >> 1, i & 1)) = reinterpret_cast<const uint4*>(b1)[i];
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async_smem();
+    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base_s), kFirstCols);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const std::uint32_t tmem = tmem_base_s;
+    constexpr std::uint32_t idesc = umma_idesc_bf16(kTile, 2 * kH);
+    const double root = sqrt(static_cast<double>(g.n) * g.bs), nr = norms[0], nq = norms[2];
+    const float inv_r = nr > 0.0 ? static_cast<float>(root / nr) : 0.0f;
+    const float inv_q = nq > 0.0 ? static_cast<float>(root / nq) : 0.0f;
+    const int bs = g.bs;
+    const auto fma_record = [](float w, const float4& lo, const float4& hi, float (&s)[8]) {
+        s[0] = fmaf(w, lo.x, s[0]);
+        s[1] = fmaf(w, lo.y, s[1]);
+        s[2] = fmaf(w, lo.z, s[2]);
+        s[3] = fmaf(w, lo.w, s[3]);
+        s[4] = fmaf(w, hi.x, s[4]);
+        s[5] = fmaf(w, hi.y, s[5]);
+        s[6] = fmaf(w, hi.z, s[6]);
+        s[7] = fmaf(w, hi.w, s[7]);
+    };
+    // A row's 8 slots (columns, BF16 weights) and its own record, loaded one
+    // tile ahead of their use.
+    int4 c0 = make_int4(-1, -1, -1, -1), c1 = c0;
+    uint4 wv = make_uint4(0, 0, 0, 0);
+    float4 own0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), own1 = own0;
+    const auto load_row = [&](int t) {
+        const int v = t * kTile + r;
+        if (t < ntiles && v < g.n) {
+            c0 = __ldg(reinterpret_cast<const int4*>(g.ell_col) + 2ll * v);
+            c1 = __ldg(reinterpret_cast<const int4*>(g.ell_col) + 2ll * v + 1);
+            wv = __ldg(reinterpret_cast<const uint4*>(g.ell_w) + v);
+            own0 = __ldg(rec + 2ll * v);
+            own1 = __ldg(rec + 2ll * v + 1);
+        }
+    };
+    load_row(blockIdx.x);
+    std::uint32_t phase = 0;
+    bool ok = true;
+    int buf = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, buf ^= 1) {
+        const int row0 = t * kTile, v = row0 + r;
+        const std::uint32_t a = base + static_cast<std::uint32_t>(1 + buf) * kTile * 128;
+        unsigned char* tile = tiles + (1 + buf) * kTile * 128;
+        float x[8], s[8];
+#pragma unroll
+        for (int f = 0; f < 8; ++f) x[f] = s[f] = 0.0f;
+        if (v < g.n) {
+            // All eight neighbour records before the sums (slot order,
+            // padding slots skipped), then the next tile's row data.
+            const int col[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+            const std::uint32_t wp[4] = {wv.x, wv.y, wv.z, wv.w};
+            const float own[8] = {own0.x, own0.y, own0.z, own0.w, own1.x, own1.y, own1.z, own1.w};
+            float4 lo[8], hi[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                lo[j] = hi[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (col[j] >= 0) {
+                    lo[j] = __ldg(rec + 2ll * col[j]);
+                    hi[j] = __ldg(rec + 2ll * col[j] + 1);
+                }
+            }
+            load_row(t + static_cast<int>(gridDim.x));
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (col[j] >= 0)
+                    fma_record(__uint_as_float((j & 1 ? wp[j >> 1] >> 16 : wp[j >> 1] & 0xffffu) << 16), lo[j], hi[j],
+                               s);
+            if (g.tile_ovf[t]) {   // more than 8 neighbours: the rest in CSR order
+                const int e1 = g.nb_ptr[v + 1];
+                for (int e = g.nb_ptr[v] + kEll; e < e1; ++e) {
+                    const int u = g.nb_col[e];
+                    fma_record(bf16_round(g.nb_w[e]), __ldg(rec + 2ll * u), __ldg(rec + 2ll * u + 1), s);
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < 8; ++f) {
+                const float sc = f < bs ? inv_r : (f < 2 * bs ? inv_q : 0.0f);
+                x[f] = own[f] * sc;
+                s[f] *= sc;
+            }
+        } else {
+            load_row(t + static_cast<int>(gridDim.x));
+        }
+        *reinterpret_cast<uint4*>(tile + sw128(r, 0)) = f32_to_bf16x8(x);
+        *reinterpret_cast<uint4*>(tile + sw128(r, 1)) = f32_to_bf16x8(s);
+        fence_proxy_async_smem();
+        tmem_fence_before_sync();
+        __syncthreads();
+        // ---- [Y1 | h0] = [x | s] B1^T
+        if (threadIdx.x == 0) {
+            tmem_fence_after_sync();
+            umma_bf16(tmem, umma_desc_sw128(a), umma_desc_sw128(b), idesc, false);
+            umma_commit(bar);
+        }
+        ok = wait_phase(bar, phase);
+        phase ^= 1;
+        tmem_fence_after_sync();
+        if (!__syncthreads_and(ok)) break;
+        // ---- epilogue: h1 = h0 + relu(Y1) over the tile's row r (TMEM lane r)
+        const std::uint32_t trow = tmem + (static_cast<std::uint32_t>(32 * warp) << 16);
+#pragma unroll
+        for (int c16 = 0; c16 < 4; ++c16) {
+            float y[16], h[16];
+            tmem_ld16(trow + 16 * c16, y);
+            tmem_ld16(trow + kH + 16 * c16, h);
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                float o[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) o[i] = h[8 * half + i] + fmaxf(y[8 * half + i], 0.0f);
+                *reinterpret_cast<uint4*>(tile + sw128(r, 2 * c16 + half)) = f32_to_bf16x8(o);
+            }
+        }
+        fence_proxy_async_smem();
+        tmem_fence_before_sync();
+        __syncthreads();
+        // Store this tile; the other buffer, written next, is free once the
+        // store before this one has read it.
+        if (threadIdx.x == 0) {
+            tma_store_2d(&tmap_out, a, 0, row0);
+            bulk_wait_read_all_but_one();
+        }
+        __syncthreads();
+    }
+    if (!ok && threadIdx.x == 0) atomicOr(status, kErrTimeout);
+    if (threadIdx.x == 0) bulk_wait_all();
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, kFirstCols);
+}
+
 // ---------------------------------------------------------------- TMA-fed layer
 // The same layer, warp-specialised.  A producer warp streams, per 16-row
 // sub-tile, the neighbours' feature rows with TMA gathers (tile::gather4, box
@@ -1332,6 +1552,10 @@ struct Gnn {
     DeviceBuffer ha, hb;                                                       // inference ping-pong
     DeviceBuffer norm_r, norm_e, out32, dz, dh, dm, dy, partials, loss_partials, ticket, loss;
     DeviceBuffer qbuf;   // q = r / d (FP32); norm_r holds |r|, |q| at [0], [2]
+    // Inference with the encoder folded into the first layer (bs <= 4): the
+    // per-vertex input records and the folded first-layer operand B1.
+    bool fused_first = false;
+    DeviceBuffer rec, b1;
     // Gather plan of the TMA-fed layer (per 16-row sub-tile: neighbour rows in
     // quads, per row {slot or -1, degree, edge offset, 1}) and the tensor maps
     // of every feature buffer (gather: box 64 x 1; tile: box 64 x 128, swizzled).
@@ -1385,6 +1609,12 @@ void gnn_pack(Gnn& G)
         G.params.as<float>() + Gnn::kOffWl, G.wl16.as<gnn::bf16>(), G.wlt16.as<gnn::bf16>());
     OWTK_CUDA(cudaGetLastError());
     G.ctx->launched();
+    if (G.fused_first) {
+        gnn::k_gnn_first_weights<<<G.blocks(2 * gnn::kH * 16), 256, 0, G.ctx->stream>>>(
+            G.params.as<float>() + Gnn::kOffWe, G.params.as<float>() + Gnn::kOffWl, G.b1.as<gnn::bf16>());
+        OWTK_CUDA(cudaGetLastError());
+        G.ctx->launched();
+    }
 }
 
 void gnn_set_attrs()
@@ -1395,6 +1625,8 @@ void gnn_set_attrs()
                                    gnn::kLayerSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer<false, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kLayerSmemDec));
+    OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_first_layer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   gnn::kFirstSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    gnn::kBwdSmem));
     OWTK_CUDA(cudaFuncSetAttribute(gnn::k_gnn_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1463,14 +1695,31 @@ void gnn_forward(Gnn& G, const T* r, O* out)
     };
     mark(0);
     kern::prepare_norms<T>(c, static_cast<std::size_t>(nb), r, G.dinv.as<float>(), G.qbuf.as<float>(), norms);
-    gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
-    gnn::launch_encode<T>(std::min(G.blocks(G.n), static_cast<unsigned>(c.sm_count * 8)), c.stream, g, r,
-                          G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
-    OWTK_CUDA(cudaGetLastError());
-    c.launched();
-    mark(1);
-    const gnn::bf16* hin = h0;
-    for (int l = 0; l < gnn::kLayers; ++l) {
+    const bool fused = !TRAIN && G.fused_first;
+    const gnn::bf16* hin = nullptr;
+    if (fused) {
+        // Input records, then the encoder and the first layer in one kernel
+        // (output in hb, the buffer the second layer reads).
+        gnn::launch_records<T>(G.blocks(G.n), c.stream, G.n, G.bs, r, G.qbuf.as<float>(), G.rec.as<float4>());
+        OWTK_CUDA(cudaGetLastError());
+        c.launched();
+        mark(1);
+        gnn::k_gnn_first_layer<<<G.layer_grid(4), gnn::kFirstThreads, gnn::kFirstSmem, c.stream>>>(
+            g, G.tmap_b, G.rec.as<float4>(), norms, G.b1.as<gnn::bf16>(), c.status.as<unsigned>());
+        OWTK_CUDA(cudaGetLastError());
+        c.launched();
+        mark(2);
+        hin = G.hb.as<gnn::bf16>();
+    } else {
+        gnn::bf16* h0 = TRAIN ? G.h[0].as<gnn::bf16>() : G.ha.as<gnn::bf16>();
+        gnn::launch_encode<T>(std::min(G.blocks(G.n), static_cast<unsigned>(c.sm_count * 8)), c.stream, g, r,
+                              G.qbuf.as<float>(), norms, G.params.as<float>() + Gnn::kOffWe, h0);
+        OWTK_CUDA(cudaGetLastError());
+        c.launched();
+        mark(1);
+        hin = h0;
+    }
+    for (int l = fused ? 1 : 0; l < gnn::kLayers; ++l) {
         gnn::bf16* hout = TRAIN ? G.h[l + 1].as<gnn::bf16>() : (l % 2 == 0 ? G.hb : G.ha).as<gnn::bf16>();
         if (G.tma) {
             const CUtensorMap& gm = TRAIN ? G.gmap_h[l] : (l % 2 == 0 ? G.gmap_a : G.gmap_b);
@@ -1888,6 +2137,14 @@ owtk_status owtk_learned_create(owtk_matrix* m, uint64_t seed, owtk_learned** ou
         const char* tma_env = std::getenv("OWTK_GNN_TMA");
         G->tma = tma_env && tma_env[0] == '1';
         G->qbuf.allocate(static_cast<std::size_t>(G->n) * G->bs * sizeof(float) + 16);
+        // The encoder folded into the first layer (inference, bs <= 4) unless
+        // OWTK_GNN_FUSED_FIRST=0 or the TMA-gather layer is selected.
+        const char* fused_env = std::getenv("OWTK_GNN_FUSED_FIRST");
+        G->fused_first = G->bs <= 4 && !G->tma && !(fused_env && fused_env[0] == '0');
+        if (G->fused_first) {
+            G->rec.allocate(static_cast<std::size_t>(G->n) * 8 * sizeof(float) + 16);
+            G->b1.allocate(2 * owtk::gnn::kH * 16 * 2 + 16);
+        }
         owtk::gnn_set_attrs();
         owtk::gnn_pack(*G);
         owtk::gnn_bind_matrix(*G, *m);
@@ -1985,11 +2242,13 @@ owtk_status owtk_learned_stage_times(owtk_learned* net, owtk_vector* in, owtk_ve
         const double r = static_cast<double>(repetitions);
         double layers = 0.0, total = 0.0;
         for (int k = 0; k < kMarks - 1; ++k) total += acc[k];
-        for (int l = 0; l < owtk::gnn::kLayers - 1; ++l) layers += acc[1 + l];
+        const int first_plain = net->fused_first ? 1 : 0;   // layers before the last without the encoder
+        for (int l = first_plain; l < owtk::gnn::kLayers - 1; ++l) layers += acc[1 + l];
         milliseconds[0] = acc[0] / r;
-        milliseconds[1] = layers / r / (owtk::gnn::kLayers - 1);
+        milliseconds[1] = layers / r / (owtk::gnn::kLayers - 1 - first_plain);
         milliseconds[2] = acc[kMarks - 2] / r;
         milliseconds[3] = total / r;
+        milliseconds[4] = net->fused_first ? acc[1] / r : 0.0;
     });
 }
 

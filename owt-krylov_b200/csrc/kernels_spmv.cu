@@ -737,9 +737,11 @@ void launch_slices_v(Context& c, const Matrix& m, const T* x, T* y)
 // size (measured on the 2M-vertex mesh, 20-30 launches each: FP64 bs 3 at 5
 // CTAs 94.9 us against 107.7-147.1 us for 4 (no cap), 6 and the two-step
 // value prefetch; FP64 bs 4 spills under a cap (143.7 us uncapped, 184.1 at
-// 5); FP32 bs 3 and 4 at 6 CTAs 61.4 and 78.0 us against 66.3 and 79.1 at 5).
+// 5); FP64 bs 1 took 54.1 us at 5 CTAs (48 registers) against 43.7 us for an
+// earlier 32-register form, so it asks for 6 (40 registers; 8 spills); FP32
+// bs 3 and 4 at 6 CTAs 61.4 and 78.0 us against 66.3 and 79.1 at 5).
 template<class T, int BS>
-constexpr int slice_ctas() { return sizeof(T) == 4 ? 6 : (BS == 4 ? 1 : 5); }
+constexpr int slice_ctas() { return sizeof(T) == 4 ? 6 : (BS == 1 ? 6 : (BS == 4 ? 1 : 5)); }
 
 template<class T, int BS>
 void launch_slices(Context& c, const Matrix& m, const T* x, T* y)

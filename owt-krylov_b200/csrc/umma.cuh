@@ -157,6 +157,13 @@ __device__ __forceinline__ void bulk_wait_read()
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// Wait until at most the latest committed bulk store may still be reading
+// shared memory.
+__device__ __forceinline__ void bulk_wait_read_all_but_one()
+{
+    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+
 // Wait until every committed bulk store has completed.
 __device__ __forceinline__ void bulk_wait_all()
 {

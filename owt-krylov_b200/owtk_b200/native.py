@@ -779,9 +779,10 @@ class Learned:
 
     def stage_times(self, x: Vector, y: Vector, repetitions: int = 10) -> dict:
         """Mean milliseconds per stage of y = M(x) (CUDA events on the stream)."""
-        ms = (c_double * 4)()
+        ms = (c_double * 5)()
         check(lib().owtk_learned_stage_times(self.h, x.h, y.h, repetitions, ms))
-        return {"norms_encoder": ms[0], "layer": ms[1], "last_layer_decoder": ms[2], "application": ms[3]}
+        return {"norms_encoder": ms[0], "layer": ms[1], "last_layer_decoder": ms[2], "application": ms[3],
+                "encoder_first_layer": ms[4]}
 
     def loss_grad(self, r: Vector, e: Vector, want_grads: bool = False):
         loss = c_double()
