@@ -69,6 +69,9 @@ def parse(argv=None):
                    help="learned: the headline (8M anisotropic, learned FGMRES vs plain FP64 ILU(0)-GMRES); "
                         "plain: FP64 GMRES(30)+ILU(0) on the 2M disk mesh; mixed / batching: the other forms")
     p.add_argument("--systems", type=int, default=256, help="batching: number of systems")
+    p.add_argument("--jacobi-correction", default="1,0.7",
+                   help="learned: STEPS[,OMEGA] damped Jacobi corrections after each accepted network step "
+                        "(0: the network alone)")
     p.add_argument("--weights", default=WEIGHTS, help="learned: checkpoint of the trained network")
     a = p.parse_args(argv)
     if a.vertices is None:
@@ -204,12 +207,21 @@ def build_system(form: str, n_vertices: int, seed: int, rcm=None):
     return s, time.time() - t
 
 
-def workload_config(form: str, s, world: int) -> dict:
+def correction_of(args) -> tuple:
+    """--jacobi-correction STEPS[,OMEGA]: damped Jacobi corrections after
+    each accepted network step of the learned preconditioner."""
+    parts = str(getattr(args, "jacobi_correction", "0")).split(",")
+    return int(parts[0]), float(parts[1]) if len(parts) > 1 else 1.0
+
+
+def workload_config(form: str, s, world: int, correction: tuple = (0, 1.0)) -> dict:
     """The `config` both arms print for one workload (same keys and values)."""
     if form == "learned":
+        steps, omega = correction
+        net = "learned network" + (f" + {steps} damped jacobi correction(s) (omega {omega:g})" if steps else "")
         return {"workload": WORKLOADS["learned"], "vertices": s.owned, "entries": s.nnz, "block_size": s.bs,
                 "mesh": "poisson-disk unit square, delaunay, anisotropic w=1+1e4(e.d)^2, skew U(-0.3,0.3)",
-                "solver": "ours: fgmres(30) + learned network (ilu(0) fallback), fp64 outer; "
+                "solver": f"ours: fgmres(30) + {net} (ilu(0) fallback), fp64 outer; "
                           "reference: gmres(30) + ilu(0) fp64",
                 "rtol": 1e-8, "ordering": "rcm", "parallelism": f"replicas{world}",
                 "l2": "inputs larger than L2 (matrix 1.3 GB, Krylov basis 11.5 GB)"}
@@ -318,7 +330,7 @@ def run_reference(args):
         "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": len(timed),
         "warmup": len(warm), "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(form, s, world),
+        "config": workload_config(form, s, world, correction_of(args)),
         "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
                          "sample": f"{len(timed)} full reference GMRES(30)+ILU(0) solves of the "
@@ -423,6 +435,7 @@ def run_learned(args):
     net = native.Learned(m, seed=1)
     ck = checkpoint.load_network(args.weights, net, with_optimizer=False)
     pcl = native.LearnedPreconditioner(net, ilu)
+    pcl.set_correction(*correction_of(args))
     ctx.synchronize()
     setup_s = time.time() - t
     opts = native.default_options(restart=30, relative_tolerance=1e-8)
@@ -503,7 +516,7 @@ def run_learned(args):
             "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+bf16", "data": "synthetic",
-            "config": workload_config("learned", s, world),
+            "config": workload_config("learned", s, world, correction_of(args)),
             "e2e": {"value": e2e_ms / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * n * bs * 8,
                     "d2h_bytes_per_step": n * bs * 8,
                     "x0": "one pinned zero buffer per step, zeroed before the timed region",

@@ -564,6 +564,12 @@ owtk_status owtk_learned_set_loss_weights(owtk_learned* net, double error_weight
  * handles are borrowed. */
 owtk_status owtk_pc_create_learned(owtk_learned* net, owtk_preconditioner* fallback, owtk_preconditioner** out);
 owtk_status owtk_pc_learned_counts(owtk_preconditioner* p, uint64_t* applications, uint64_t* fallbacks);
+/* No reference counterpart (the learned form is new).  After each accepted
+ * network step z = M(v), `steps` (0..8, default 0) damped Jacobi corrections
+ * z += omega D^-1 (v - A z), 0 < omega < 2, with D^-1 the FP32 reciprocal
+ * diagonal; each costs one element-wise pass and one SpMV, and the solver
+ * reuses the last product A z as its next operator application. */
+owtk_status owtk_pc_learned_set_correction(owtk_preconditioner* p, uint32_t steps, double omega);
 
 #ifdef __cplusplus
 }

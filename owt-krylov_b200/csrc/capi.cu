@@ -895,6 +895,7 @@ owtk_status owtk_dense_bsr_create(owtk_context* ctx, owtk_dtype dtype, size_t ow
         const std::size_t bytes = m->entries * bs * bs * dsize(dtype);
         m->values.allocate(bytes + 16);
         OWTK_CUDA(cudaMemcpyAsync(m->values.ptr, values, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        kern::slices_fill(*ctx, *m);
         ctx->sync();
         *out = m.release();
     });

@@ -1901,6 +1901,20 @@ namespace owtk {
 
 // z = M(v); judged by ||v - A z|| against ||v||, the fallback steps in when
 // the network does not reduce the residual.
+namespace gnn {
+// One damped Jacobi correction of the network's output: z += omega D^-1 (v - A z),
+// each operation rounded as written (no contraction).
+__global__ void __launch_bounds__(256) k_jacobi_correct(long long count, const double* __restrict__ v,
+                                                        const double* __restrict__ az,
+                                                        const float* __restrict__ dinv, double omega,
+                                                        double* __restrict__ z)
+{
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count)
+        z[i] = __dadd_rn(z[i], __dmul_rn(omega, __dmul_rn(static_cast<double>(dinv[i]), __dsub_rn(v[i], az[i]))));
+}
+}  // namespace gnn
+
 bool learned_apply(Preconditioner& p, Vector& in, Vector& out, double* product)
 {
     Gnn& G = *p.net;
@@ -1915,7 +1929,8 @@ bool learned_apply(Preconditioner& p, Vector& in, Vector& out, double* product)
     }
     gnn_forward<double, double, false>(G, x, y);
     ++p.learned_applications;
-    if (p.fallback == nullptr) return false;
+    const int corrections = p.learned_correction_steps;
+    if (p.fallback == nullptr && corrections == 0) return false;
     // The check's product A z is the solver's next operator application: it
     // lands in `product` when the caller asks for it.
     double* w = product;
@@ -1924,6 +1939,21 @@ bool learned_apply(Preconditioner& p, Vector& in, Vector& out, double* product)
         w = p.check_work.as<double>();
     }
     kern::spmv<double>(c, *G.matrix, y, w);
+    const auto correct = [&] {
+        // After an accepted step: the corrections, each followed by the
+        // product of the corrected z (the solver's next operator application).
+        for (int k = 0; k < corrections; ++k) {
+            gnn::k_jacobi_correct<<<G.blocks(static_cast<long long>(n)), 256, 0, c.stream>>>(
+                static_cast<long long>(n), x, w, G.dinv.as<float>(), p.learned_correction_omega, y);
+            OWTK_CUDA(cudaGetLastError());
+            c.launched();
+            kern::spmv<double>(c, *G.matrix, y, w);
+        }
+    };
+    if (p.fallback == nullptr) {
+        correct();
+        return product != nullptr;
+    }
     constexpr int kSlot = kScalarSlots - 4;
     kern::residual_norms(c, n, x, w, c.dev_scalar_copy.as<double>() + kSlot, c.dev_scalars + kSlot);
     c.sync();
@@ -1941,6 +1971,7 @@ bool learned_apply(Preconditioner& p, Vector& in, Vector& out, double* product)
         apply_preconditioner(p.fallback, src, out);
         return false;
     }
+    correct();
     return product != nullptr;
 }
 
@@ -2342,6 +2373,16 @@ owtk_status owtk_pc_create_learned(owtk_learned* net, owtk_preconditioner* fallb
         p->net = net;
         p->fallback = fallback;
         *out = p.release();
+    });
+}
+
+owtk_status owtk_pc_learned_set_correction(owtk_preconditioner* p, uint32_t steps, double omega)
+{
+    return owtk::guarded([&] {
+        owtk::require(p != nullptr && p->kind == OWTK_PC_LEARNED, "not a learned preconditioner");
+        owtk::require(steps <= 8 && omega > 0.0 && omega < 2.0, "correction steps must be <= 8, omega in (0, 2)");
+        p->learned_correction_steps = static_cast<int>(steps);
+        p->learned_correction_omega = omega;
     });
 }
 

@@ -686,15 +686,88 @@ __global__ void __launch_bounds__(256, MINB) k_spmv_slices(const int* __restrict
     }
 }
 
+// Dense-block BSR (DenseBlockCsrMatrix, bs <= 4) on the same row-slice
+// layout with BS * BS value runs per step ([block row][block column][lane]):
+// per entry and block row the contribution sums B[br][bc] x[bc] from +0 over
+// bc, then adds to the row's sum — the reference's sequence
+// (dense_block_csr.hpp:173-205), as k_spmv_tiles evaluates it.  Columns two
+// steps ahead, values and x one step ahead.
+template<class T, int BS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_spmv_slices_dense(const int* __restrict__ base,
+                                                                 const unsigned short* __restrict__ lanes,
+                                                                 const int* __restrict__ scols,
+                                                                 const T* __restrict__ svals, const T* __restrict__ x,
+                                                                 T* __restrict__ y, int slices, int owned)
+{
+    constexpr int P = BS * BS;
+    __shared__ T out[8][32 * BS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nw = static_cast<int>(gridDim.x) * 8;
+    for (int s = static_cast<int>(blockIdx.x) * 8 + wib; s < slices; s += nw) {
+        const unsigned meta = lanes[static_cast<long long>(s) * 32 + lane];
+        const int len = static_cast<int>(meta >> 8), pos = static_cast<int>(meta & 255u);
+        const int steps = __shfl_sync(0xffffffffu, len, 0);
+        T acc[BS];
+#pragma unroll
+        for (int c = 0; c < BS; ++c) acc[c] = T(0);
+        const auto count = [&](int k) { return __popc(__ballot_sync(0xffffffffu, len > k)); };
+        const auto load_vx = [&](int k, int o, int n, int col, T (&vv)[P], T (&xx)[BS]) {
+            if (len > k) {
+                const T* vp = svals + static_cast<long long>(o) * P + lane;
+                const T* xp = x + static_cast<long long>(col) * BS;
+#pragma unroll
+                for (int q = 0; q < P; ++q) vv[q] = __ldcs(vp + q * n);
+#pragma unroll
+                for (int c = 0; c < BS; ++c) xx[c] = __ldg(xp + c);
+            }
+        };
+        const auto load_col = [&](int k, int o) { return len > k ? __ldcs(scols + o + lane) : 0; };
+        int o0 = base[s], n0 = count(0);
+        int o1 = o0 + n0, n1 = count(1);
+        T v[P], xv[BS];
+        load_vx(0, o0, n0, load_col(0, o0), v, xv);
+        int col1 = load_col(1, o1);
+        for (int k = 0; k < steps; ++k) {
+            T vn[P], xn[BS];
+            load_vx(k + 1, o1, n1, col1, vn, xn);
+            const int o2 = o1 + n1, n2 = count(k + 2);
+            col1 = load_col(k + 2, o2);
+            if (len > k) {
+#pragma unroll
+                for (int br = 0; br < BS; ++br) {
+                    T part = T(0);
+#pragma unroll
+                    for (int bc = 0; bc < BS; ++bc) part = add_rn(part, mul_rn(v[br * BS + bc], xv[bc]));
+                    acc[br] = add_rn(acc[br], part);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < P; ++q) v[q] = vn[q];
+#pragma unroll
+            for (int c = 0; c < BS; ++c) xv[c] = xn[c];
+            o1 = o2;
+            n1 = n2;
+        }
+        if (pos < 32)
+#pragma unroll
+            for (int c = 0; c < BS; ++c) out[wib][pos * BS + c] = acc[c];
+        __syncwarp();
+        const int rows = min(32, owned - 32 * s);
+        T* ys = y + static_cast<long long>(s) * 32 * BS;
+        for (int i = lane; i < rows * BS; i += 32) ys[i] = out[wib][i];
+        __syncwarp();
+    }
+}
+
 // Fill the row-slice copy from the CSR arrays: a warp per slice walks the
-// same steps as k_spmv_slices and writes each entry where that kernel reads
-// it.
+// same steps as the row-slice kernels and writes each entry's `per` values
+// (bs, or bs * bs for dense blocks) where they read them.
 template<class T>
 __global__ void __launch_bounds__(256) k_slices_fill(const int* __restrict__ base,
                                                      const unsigned short* __restrict__ lanes,
                                                      const int* __restrict__ rowptr, const int* __restrict__ cols,
                                                      const T* __restrict__ vals, int* __restrict__ scols,
-                                                     T* __restrict__ svals, int slices, int bs)
+                                                     T* __restrict__ svals, int slices, int per)
 {
     const int lane = threadIdx.x & 31;
     const int s = static_cast<int>(blockIdx.x) * 8 + static_cast<int>(threadIdx.x >> 5);
@@ -709,9 +782,9 @@ __global__ void __launch_bounds__(256) k_slices_fill(const int* __restrict__ bas
         if (len > k) {
             const int e = e0 + k;
             scols[off + lane] = cols[e];
-            for (int c = 0; c < bs; ++c)
-                svals[static_cast<long long>(off) * bs + static_cast<long long>(c) * n + lane] =
-                    vals[static_cast<long long>(e) * bs + c];
+            for (int c = 0; c < per; ++c)
+                svals[static_cast<long long>(off) * per + static_cast<long long>(c) * n + lane] =
+                    vals[static_cast<long long>(e) * per + c];
         }
         off += n;
     }
@@ -747,6 +820,32 @@ template<class T, int BS>
 void launch_slices(Context& c, const Matrix& m, const T* x, T* y)
 {
     launch_slices_v<T, BS, slice_ctas<T, BS>(), 1>(c, m, x, y);
+}
+
+template<class T, int BS, int kMinBlocks>
+void launch_slices_dense_v(Context& c, const Matrix& m, const T* x, T* y)
+{
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        OWTK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_slices_dense<T, BS, kMinBlocks>, 256,
+                                                                0));
+        per_sm = std::max(per_sm, 1);
+    }
+    const RowSlices& sl = m.slices;
+    const unsigned grid = static_cast<unsigned>(std::max(1, std::min((sl.slices + 7) / 8, c.sm_count * per_sm)));
+    k_spmv_slices_dense<T, BS, kMinBlocks><<<grid, 256, 0, c.stream>>>(
+        sl.base.as<int>(), sl.lanes.as<unsigned short>(), sl.cols.as<int>(), sl.vals.as<T>(), x, y, sl.slices,
+        static_cast<int>(m.owned));
+}
+
+// Dense blocks at 3 resident CTAs per SM (2M-vertex mesh, 3x3 blocks: FP64
+// 198.2 us against 234.0 us uncapped (92 registers) and 199.8 us at 4; FP32
+// 114 us at 1, 3 and 4 alike); FP64 4x4 blocks at 2 (128 registers, 48
+// bytes spilled; at 3 the 16 values per step spill 332 bytes).
+template<class T, int BS>
+void launch_slices_dense(Context& c, const Matrix& m, const T* x, T* y)
+{
+    launch_slices_dense_v<T, BS, (sizeof(T) == 8 && BS == 4) ? 2 : 3>(c, m, x, y);
 }
 
 // First diagonal entry of every row (block_csr.hpp:217-236).
@@ -828,12 +927,21 @@ static bool slices_enabled()
 template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
 {
     if (m.plan.tiles == 0) return;
-    if (m.kind == 0 && m.slices.filled && slices_enabled()) {
-        switch (m.bs) {
-        case 1: launch_slices<T, 1>(c, m, x, y); break;
-        case 2: launch_slices<T, 2>(c, m, x, y); break;
-        case 3: launch_slices<T, 3>(c, m, x, y); break;
-        default: launch_slices<T, 4>(c, m, x, y); break;
+    if ((m.kind == 0 || m.kind == 2) && m.slices.filled && slices_enabled()) {
+        if (m.kind == 0) {
+            switch (m.bs) {
+            case 1: launch_slices<T, 1>(c, m, x, y); break;
+            case 2: launch_slices<T, 2>(c, m, x, y); break;
+            case 3: launch_slices<T, 3>(c, m, x, y); break;
+            default: launch_slices<T, 4>(c, m, x, y); break;
+            }
+        } else {
+            switch (m.bs) {
+            case 1: launch_slices_dense<T, 1>(c, m, x, y); break;
+            case 2: launch_slices_dense<T, 2>(c, m, x, y); break;
+            case 3: launch_slices_dense<T, 3>(c, m, x, y); break;
+            default: launch_slices_dense<T, 4>(c, m, x, y); break;
+            }
         }
         OWTK_CUDA(cudaGetLastError());
         c.launched();
@@ -841,8 +949,8 @@ template<class T> void spmv(Context& c, const Matrix& m, const T* x, T* y)
         if (count > 0) {
             const long long total = static_cast<long long>(count) * static_cast<long long>(m.bs);
             k_spmv_rows<T><<<static_cast<unsigned>((total + 255) / 256), 256, 0, c.stream>>>(
-                0, static_cast<int>(m.bs), m.slices.long_rows.as<int>(), count, m.rowptr.as<int>(), m.cols.as<int>(),
-                static_cast<const T*>(m.values.ptr), nullptr, x, y);
+                m.kind, static_cast<int>(m.bs), m.slices.long_rows.as<int>(), count, m.rowptr.as<int>(),
+                m.cols.as<int>(), static_cast<const T*>(m.values.ptr), nullptr, x, y);
             OWTK_CUDA(cudaGetLastError());
             c.launched();
         }
@@ -901,16 +1009,15 @@ void slices_fill(Context& c, Matrix& m)
     RowSlices& sl = m.slices;
     if (sl.slices == 0) return;
     const unsigned grid = static_cast<unsigned>((sl.slices + 7) / 8);
+    const int per = static_cast<int>(m.kind == 2 ? m.bs * m.bs : m.bs);
     if (m.dtype == OWTK_F64)
         k_slices_fill<double><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
                                                           m.rowptr.as<int>(), m.cols.as<int>(), m.values.as<double>(),
-                                                          sl.cols.as<int>(), sl.vals.as<double>(), sl.slices,
-                                                          static_cast<int>(m.bs));
+                                                          sl.cols.as<int>(), sl.vals.as<double>(), sl.slices, per);
     else
         k_slices_fill<float><<<grid, 256, 0, c.stream>>>(sl.base.as<int>(), sl.lanes.as<unsigned short>(),
                                                          m.rowptr.as<int>(), m.cols.as<int>(), m.values.as<float>(),
-                                                         sl.cols.as<int>(), sl.vals.as<float>(), sl.slices,
-                                                         static_cast<int>(m.bs));
+                                                         sl.cols.as<int>(), sl.vals.as<float>(), sl.slices, per);
     OWTK_CUDA(cudaGetLastError());
     c.launched();
     sl.filled = true;
@@ -990,7 +1097,8 @@ void build_tile_plan(Matrix& m)
     build_row_slices(m);
 }
 
-// Row-slice layout of a component-diagonal BSR with bs <= 4: per slice of 32
+// Row-slice layout of a component-diagonal or dense-block BSR with bs <= 4
+// (FP64 or FP32): per slice of 32
 // rows the lanes in order of decreasing row length (ties by row), the first
 // packed entry of each slice, and the long rows; the arrays it fills are
 // allocated here and written by kern::slices_fill.
@@ -998,7 +1106,8 @@ void build_row_slices(Matrix& m)
 {
     RowSlices& sl = m.slices;
     sl = RowSlices{};
-    if (m.kind != 0 || m.bs > 4 || m.owned == 0 || (m.dtype != OWTK_F64 && m.dtype != OWTK_F32)) return;
+    if ((m.kind != 0 && m.kind != 2) || m.bs > 4 || m.owned == 0 || (m.dtype != OWTK_F64 && m.dtype != OWTK_F32))
+        return;
     const int owned = static_cast<int>(m.owned);
     sl.slices = (owned + 31) / 32;
     std::vector<std::uint16_t> lanes(static_cast<std::size_t>(sl.slices) * 32, 255);
@@ -1028,7 +1137,8 @@ void build_row_slices(Matrix& m)
     sl.base = upload(m.ctx->stream, base);
     sl.lanes = upload(m.ctx->stream, lanes);
     sl.cols.allocate(packed * 4 + 16);
-    sl.vals.allocate(packed * m.bs * (m.dtype == OWTK_F64 ? 8 : 4) + 16);
+    const std::size_t per = m.kind == 2 ? m.bs * m.bs : m.bs;
+    sl.vals.allocate(packed * per * (m.dtype == OWTK_F64 ? 8 : 4) + 16);
     sl.long_count = static_cast<int>(long_rows.size());
     if (!long_rows.empty()) sl.long_rows = upload(m.ctx->stream, long_rows);
 }

@@ -129,12 +129,13 @@ struct TilePlan {
     int tile_values = 0;       // stage capacity used to build the plan
 };
 
-// Row-slice copy of a component-diagonal BSR (bs <= 4), read by its SpMV.
-// Slices of 32 consecutive rows, one warp each; a slice's lanes take its rows
-// longest first.  Step k of a slice holds entry k of the n_k rows longer than
-// k: their columns [lane] and values [component][lane], packed with no
-// padding (step k + 1 starts n_k entries later).  Rows longer than
-// kSliceMaxRow have length 0 in their slice and are listed in long_rows.
+// Row-slice copy of a component-diagonal or dense-block BSR (bs <= 4), read
+// by its SpMV.  Slices of 32 consecutive rows, one warp each; a slice's lanes
+// take its rows longest first.  Step k of a slice holds entry k of the n_k
+// rows longer than k: their columns [lane] and values [value of the entry]
+// [lane] (bs values, or bs * bs for dense blocks), packed with no padding
+// (step k + 1 starts n_k entries later).  Rows longer than kSliceMaxRow have
+// length 0 in their slice and are listed in long_rows.
 constexpr int kSliceMaxRow = 48;
 struct RowSlices {
     int slices = 0;
@@ -288,6 +289,10 @@ struct Preconditioner {
     struct Gnn* net = nullptr;
     Preconditioner* fallback = nullptr;
     std::uint64_t learned_applications = 0, learned_fallbacks = 0;
+    // Damped Jacobi corrections after each accepted network step
+    // (owtk_pc_learned_set_correction): z += omega D^-1 (v - A z).
+    int learned_correction_steps = 0;
+    double learned_correction_omega = 1.0;
     DeviceBuffer check_work, alias_copy;
     // OWTK_PC_CALLBACK: an application function applied on host copies.
     owtk_host_apply_fn host_apply = nullptr;

@@ -189,6 +189,7 @@ def lib():
             "owtk_learned_set_loss_weights": (c_int, [vp, c_double, c_double]),
             "owtk_pc_create_learned": (c_int, [vp, vp, POINTER(vp)]),
             "owtk_pc_learned_counts": (c_int, [vp, u64p, u64p]),
+            "owtk_pc_learned_set_correction": (c_int, [vp, ctypes.c_uint32, c_double]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -826,6 +827,11 @@ class LearnedPreconditioner(Preconditioner):
         a, f = c_uint64(), c_uint64()
         check(lib().owtk_pc_learned_counts(self.h, ctypes.byref(a), ctypes.byref(f)))
         return a.value, f.value
+
+    def set_correction(self, steps: int, omega: float = 1.0):
+        """Damped Jacobi corrections z += omega D^-1 (v - A z) after each
+        accepted network step."""
+        check(lib().owtk_pc_learned_set_correction(self.h, steps, omega))
 
 
 # ---------------------------------------------------------------- batching

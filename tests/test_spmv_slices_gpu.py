@@ -86,3 +86,46 @@ def test_slices_repeated_applies_identical(native, ctx, restatement):
     for _ in range(3):
         m.apply(xv, y)
         assert_bitwise(y.download(), want, "row-slice spmv, repeated")
+
+
+def float32_dense_sequence(n, bs, rowptr, cols, vals, x):
+    """The dense-block loop in float32: per entry and block row the
+    contribution from +0 over the block columns, then added to the row sum."""
+    v = vals.astype(np.float32).reshape(-1, bs, bs)
+    xs = x.astype(np.float32).reshape(-1, bs)
+    y = np.zeros((n, bs), np.float32)
+    lens = np.diff(rowptr)
+    for k in range(int(lens.max(initial=0))):
+        rows = np.nonzero(lens > k)[0]
+        e = rowptr[rows] + k
+        part = np.zeros((rows.size, bs), np.float32)
+        for bc in range(bs):
+            part = (part + (v[e, :, bc] * xs[cols[e], bc][:, None]).astype(np.float32)).astype(np.float32)
+        y[rows] = (y[rows] + part).astype(np.float32)
+    return y.reshape(-1)
+
+
+@pytest.mark.parametrize("n,ghosts,bs", [(1000, 5, 3), (417, 0, 2), (655, 3, 4), (300, 0, 1)])
+def test_dense_slices_bitwise_mixed_rows(native, ctx, restatement, n, ghosts, bs):
+    """Dense bs x bs blocks on the row-slice copy: empty, ordinary and long
+    rows, a partial last slice, ghost columns, value updates, FP32."""
+    rowptr, cols, _, x = mixed_rows(n, ghosts, bs, seed=3 * n + bs)
+    vals = np.random.default_rng(n).uniform(-1.0, 1.0, size=cols.size * bs * bs)
+    m = native.Matrix(ctx, "dense", n, ghosts, bs, rowptr, cols, vals)
+    xv = native.Vector(ctx, n, ghosts, bs).upload(x)
+    y = native.Vector(ctx, n, ghosts, bs).upload(np.full((n + ghosts) * bs, 4.0))
+    m.apply(xv, y)
+    out = y.download()
+    assert_bitwise(out[: n * bs], restatement.dense_spmv(n, bs, rowptr, cols, vals, x), "dense row-slice spmv")
+    assert (out[n * bs:] == 4.0).all(), "SpMV wrote ghost entries"
+    vals2 = 0.5 * vals[::-1].copy()
+    m.update_values(vals2)
+    m.apply(xv, y)
+    assert_bitwise(y.download()[: n * bs], restatement.dense_spmv(n, bs, rowptr, cols, vals2, x),
+                   "dense row-slice spmv after update_values")
+    m32 = native.Matrix(ctx, "dense", n, ghosts, bs, rowptr, cols, vals, dtype=np.float32)
+    x32 = native.Vector(ctx, n, ghosts, bs, dtype=np.float32).upload(x)
+    y32 = native.Vector(ctx, n, ghosts, bs, dtype=np.float32)
+    m32.apply(x32, y32)
+    assert_bitwise(y32.download()[: n * bs], float32_dense_sequence(n, bs, rowptr, cols, vals, x),
+                   "FP32 dense row-slice spmv")
